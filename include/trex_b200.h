@@ -1,0 +1,172 @@
+/*
+ * trex_b200 -- B200 (sm_100a) automaton-simulation engine, C ABI.
+ *
+ * Two groups of entry points live in libtrex_b200.so:
+ *
+ *  1. Drop-in replacements for the reference's ctypes C ABI. Names, argument
+ *     order and meaning follow the reference exactly; each declaration cites
+ *     the reference definition it replaces (paths inside the reference
+ *     project). As in the reference, every pointer is caller-owned HOST
+ *     memory, the library owns the device buffers, copies inputs in and
+ *     results out, and keeps one engine per family (init replaces it).
+ *     Return codes: 0 ok, -1 not initialised, -2 unsupported shape; this
+ *     library adds the negative codes below and never exits the process.
+ *
+ *  2. trex_* handle entry points (no reference counterpart): many resident
+ *     automata, device pointers, 64-bit offsets, explicit streams, the
+ *     per-position scan, Boolean and probabilistic NFAs.
+ *
+ * Strings are passed CSR-style: a byte buffer plus offsets[n+1].
+ */
+#ifndef TREX_B200_H
+#define TREX_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- return codes ---------------------------------------------------------- */
+#define TREX_OK 0
+#define TREX_ERR_NOT_INIT (-1)    /* reference: engine not initialised        */
+#define TREX_ERR_SHAPE (-2)       /* reference: unsupported shape / device    */
+#define TREX_ERR_CUDA (-3)        /* a CUDA call failed; see trex_last_error  */
+#define TREX_ERR_CAPACITY (-4)    /* batch larger than the init-time maximum  */
+#define TREX_ERR_ARG (-5)         /* invalid argument (null, negative, bad CSR)*/
+#define TREX_ERR_DEVICE (-6)      /* a kernel reported an error or a timeout  */
+#define TREX_ERR_OOM (-7)         /* device allocation failed                  */
+
+/* Message of the last error raised on the calling thread ("" if none). */
+const char *trex_last_error(void);
+/* Library version string. */
+const char *trex_version(void);
+
+/* Launch profiler: after trex_profile_begin(n), the main kernel of each of the
+ * next n runs is bracketed by CUDA events on its stream. trex_profile_end
+ * stops recording, waits for the events and writes up to `capacity`
+ * per-launch durations (ms) plus the number recorded. */
+int trex_profile_begin(int max_launches);
+int trex_profile_end(float *ms_out, int capacity, int *count);
+
+/* ========================================================================== *
+ * 1. Reference C ABI                                                          *
+ * ========================================================================== */
+
+/* ---- monoid batch engine (reference cuda/monoid_batch.cu:594-673) ---------- */
+/* Replaces monoid_batch_engine_device_check (monoid_batch.cu:601-609):
+ * 0 = a device is present, -1 = no device, -2 = compute capability < 7. */
+int monoid_batch_engine_device_check(void);
+/* Replaces monoid_batch_engine_init (monoid_batch.cu:611-628). The monoid is
+ * walked as an automaton over M elements: curr = char_compose[curr*sigma_ext +
+ * raw_char_map[byte]], result = accept[curr]. M <= 255. */
+int monoid_batch_engine_init(int M, int sigma_ext, int identity,
+                             const uint8_t *char_compose, const uint8_t *raw_char_map,
+                             const uint8_t *accept, const uint8_t *monoid_compose,
+                             int max_total_chars, int max_batch);
+/* Replaces monoid_batch_engine_set_kgram (monoid_batch.cu:630-638). The fused
+ * [M*256] table is validated against char_compose; the k-gram table is kept
+ * for API compatibility. */
+int monoid_batch_engine_set_kgram(const uint8_t *fused_compose, const uint8_t *kgram_compose,
+                                  int kgram_k, int sigma_k, int sigma);
+/* Replaces monoid_batch_engine_destroy (monoid_batch.cu:640-645). */
+void monoid_batch_engine_destroy(void);
+/* Replaces monoid_batch_engine_dispatch (monoid_batch.cu:647-658):
+ * results[B] = 0/1, kernel_ms / total_ms from CUDA events. */
+int monoid_batch_engine_dispatch(const uint8_t *raw_concat, const int *offsets, int *results,
+                                 int B, int total_chars, float *kernel_ms, float *total_ms);
+/* Replaces monoid_batch_engine_dispatch_prefix (monoid_batch.cu:660-671): same
+ * results; long strings are split across the GPU (segment maps). */
+int monoid_batch_engine_dispatch_prefix(const uint8_t *raw_concat, const int *offsets,
+                                        int *results, int B, int total_chars,
+                                        float *kernel_ms, float *total_ms);
+
+/* ---- prefix compose engine (reference cuda/prefix_compose.cu:418-472) ------ */
+/* Replaces prefix_engine_device_check (prefix_compose.cu:425-433). */
+int prefix_engine_device_check(void);
+/* Replaces prefix_engine_init (prefix_compose.cu:435-449): tmap[256*N] with
+ * tmap[byte*N + s] = next state, accept[N], start state; N <= 16 in the
+ * reference, N <= 256 here. K is accepted and ignored, as in the reference. */
+int prefix_engine_init(const uint8_t *tmap, const uint8_t *accept, int start_state, int N,
+                       int K, int max_total_chars, int max_batch);
+/* Replaces prefix_engine_dispatch (prefix_compose.cu:451-462). */
+int prefix_engine_dispatch(const uint8_t *raw_concat, const int *offsets, int *results,
+                           int B, int total_chars, float *kernel_ms, float *total_ms);
+/* Replaces prefix_engine_destroy (prefix_compose.cu:464-469). */
+void prefix_engine_destroy(void);
+
+/* ---- monoid scan engine (reference cuda/monoid_scan.cu:457-515) ------------ */
+/* Replaces monoid_engine_init (monoid_scan.cu:468-478): compose[M*M] uint16 with
+ * compose[c_new*M + acc_old], accept[M]. */
+int monoid_engine_init(int monoid_size, int identity_idx, const uint16_t *compose_table,
+                       const uint8_t *accept_table, int max_total_chars, int max_batch);
+/* Replaces monoid_engine_destroy (monoid_scan.cu:480-485). */
+void monoid_engine_destroy(void);
+/* Replaces monoid_engine_dispatch_batch (monoid_scan.cu:492-503): chars are
+ * monoid element indices (uint16), one per input character. */
+int monoid_engine_dispatch_batch(const uint16_t *chars, const int *offsets, int *results,
+                                 int B, int total_chars, float *kernel_ms, float *total_ms);
+/* Replaces monoid_engine_device_check (monoid_scan.cu:505-513). */
+int monoid_engine_device_check(void);
+
+/* ---- NFA engine (reference cuda/nfa_tc_evolution.cu:936-1015) -------------- */
+/* Replaces nfa_tc_engine_init (nfa_tc_evolution.cu:941-952): T[sigma*n*n]
+ * float with T[c][dst][src] > 0.5 meaning an edge, accept[n], start[n].
+ * The reference requires sigma == 2 and n == 64; here n <= 64, sigma <= 255. */
+int nfa_tc_engine_init(const float *T_matrices, const float *accept_mask,
+                       const float *start_vec, int n, int sigma, int max_B, int max_L);
+/* Replaces nfa_tc_engine_dispatch (nfa_tc_evolution.cu:954-1010): results[B]
+ * = accept flag; bytes >= sigma are skipped (the C engine's convention). */
+int nfa_tc_engine_dispatch(const uint8_t *raw_concat, const int *offsets, int *results,
+                           int B, int total_chars, float *kernel_ms, float *total_ms);
+/* Replaces nfa_tc_engine_destroy (nfa_tc_evolution.cu:1012-1014). */
+void nfa_tc_engine_destroy(void);
+
+/* ========================================================================== *
+ * 2. Handle API (device pointers, 64-bit offsets, explicit stream)            *
+ * ========================================================================== */
+
+typedef struct trex_dfa_set trex_dfa_set;
+
+/* Upload n_dfas byte DFAs (n_dfas <= 64). DFA d has n_states[d] (1..256)
+ * states, start state starts[d], transition table tmaps + sum_{e<d} 256*N_e
+ * (entry [byte*N + s] = next state) and accept flags accepts + sum_{e<d} N_e. */
+int trex_dfa_set_create(int n_dfas, const int32_t *n_states, const int32_t *starts,
+                        const uint8_t *tmaps, const uint8_t *accepts, trex_dfa_set **out);
+void trex_dfa_set_destroy(trex_dfa_set *set);
+
+/* Device scratch (bytes) needed by trex_dfa_batch_run for a batch. */
+int64_t trex_dfa_batch_scratch_bytes(int64_t n_strings, int64_t total_bytes, int32_t seg_len);
+
+/* Final state / accept flag of every string. All pointers are DEVICE
+ * pointers: data[total_bytes], offsets[n+1] (int64, non-decreasing),
+ * dfa_id[n] (NULL = automaton 0), outputs (each may be NULL):
+ * final_state[n], accept[n] (uint8 0/1), accept_i32[n] (int 0/1).
+ * scratch: at least trex_dfa_batch_scratch_bytes bytes, or NULL to use a
+ * buffer owned by the set. seg_len: characters per work item (0 = default;
+ * longer strings are split and their segment maps composed). stream: a
+ * cudaStream_t (NULL = legacy default stream). */
+int trex_dfa_batch_run(trex_dfa_set *set, const uint8_t *data, const int64_t *offsets,
+                       const int32_t *dfa_id, int64_t n_strings, int64_t total_bytes,
+                       uint8_t *final_state, uint8_t *accept, int32_t *accept_i32,
+                       void *scratch, int64_t scratch_bytes, int32_t seg_len, void *stream);
+
+/* Error word of the last trex_dfa_batch_run that used `scratch` (NULL = the
+ * set's own scratch): 0 = fine, bit 0 = malformed offsets, bit 1 = automaton
+ * id out of range (the affected strings were skipped). Synchronises. */
+int trex_dfa_batch_error(trex_dfa_set *set, void *scratch, int32_t *err_out);
+
+/* The same batch from HOST buffers (64-bit offsets): copies the inputs in,
+ * runs, copies the requested outputs (each may be NULL) back and reports
+ * kernel_ms (device work) and total_ms (copies + device work). Device staging
+ * buffers are owned by the set and grow on demand. */
+int trex_dfa_batch_host(trex_dfa_set *set, const uint8_t *h_data, const int64_t *h_offsets,
+                        const int32_t *h_dfa_id, int64_t n_strings, int64_t total_bytes,
+                        uint8_t *h_final_state, uint8_t *h_accept, int32_t *h_accept_i32,
+                        int32_t seg_len, float *kernel_ms, float *total_ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TREX_B200_H */

@@ -1,0 +1,133 @@
+"""Handle-based engines over the trex_* C ABI.
+
+``DFASet`` keeps up to 64 byte DFAs resident on the GPU and runs ragged
+batches from device tensors (``run``) or host arrays (``run_host``). PyTorch
+is used only to hold device memory and streams; all compute goes through
+libtrex_b200.so.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from .workloads import ByteDFA
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _dptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def _stream_handle(stream):
+    if stream is None:
+        torch = _torch()
+        return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+def profile_begin(max_launches: int) -> None:
+    """Bracket the main kernel of the next ``max_launches`` runs with CUDA events."""
+    _lib.check(_lib.load().trex_profile_begin(max_launches), "trex_profile_begin")
+
+
+def profile_end(capacity: int = 100000) -> list:
+    """Stop recording; per-launch main-kernel durations in ms (synchronises)."""
+    buf = np.zeros(capacity, dtype=np.float32)
+    cnt = ctypes.c_int(0)
+    _lib.check(_lib.load().trex_profile_end(_lib.ptr(buf, ctypes.c_float), capacity,
+                                            ctypes.byref(cnt)), "trex_profile_end")
+    return buf[:min(cnt.value, capacity)].tolist()
+
+
+class DFASet:
+    """Resident set of byte DFAs (N <= 256 each, at most 64)."""
+
+    def __init__(self, dfas: Sequence[ByteDFA]):
+        self.lib = _lib.load()
+        self.dfas = list(dfas)
+        n = len(self.dfas)
+        ns = np.array([d.n_states for d in self.dfas], dtype=np.int32)
+        st = np.array([d.start for d in self.dfas], dtype=np.int32)
+        tm = np.ascontiguousarray(np.concatenate([d.tmap for d in self.dfas]).astype(np.uint8))
+        ac = np.ascontiguousarray(np.concatenate([d.accept for d in self.dfas]).astype(np.uint8))
+        h = ctypes.c_void_p()
+        rc = self.lib.trex_dfa_set_create(n, _lib.ptr(ns, ctypes.c_int32), _lib.ptr(st, ctypes.c_int32),
+                                          _lib.ptr(tm, ctypes.c_uint8), _lib.ptr(ac, ctypes.c_uint8),
+                                          ctypes.byref(h))
+        _lib.check(rc, "trex_dfa_set_create")
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.trex_dfa_set_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def scratch_bytes(n_strings: int, total_bytes: int, seg_len: int = 0) -> int:
+        return int(_lib.load().trex_dfa_batch_scratch_bytes(n_strings, total_bytes, seg_len))
+
+    def run(self, data, offsets, dfa_id=None, *, final_state=None, accept=None, accept_i32=None,
+            scratch=None, seg_len: int = 0, stream=None, want=("final_state", "accept")):
+        """Device run. data: uint8 CUDA tensor; offsets: int64 CUDA tensor [n+1];
+        dfa_id: optional int32 CUDA tensor [n]. Missing outputs listed in
+        ``want`` are allocated. Returns (final_state, accept, accept_i32)."""
+        torch = _torch()
+        n = offsets.numel() - 1
+        dev = offsets.device
+        if final_state is None and "final_state" in want:
+            final_state = torch.empty(n, dtype=torch.uint8, device=dev)
+        if accept is None and "accept" in want:
+            accept = torch.empty(n, dtype=torch.uint8, device=dev)
+        if accept_i32 is None and "accept_i32" in want:
+            accept_i32 = torch.empty(n, dtype=torch.int32, device=dev)
+        sc_bytes = scratch.numel() if scratch is not None else 0
+        rc = self.lib.trex_dfa_batch_run(
+            self._h, _dptr(data), _dptr(offsets), _dptr(dfa_id), n, data.numel(),
+            _dptr(final_state), _dptr(accept), _dptr(accept_i32), _dptr(scratch), sc_bytes,
+            seg_len, _stream_handle(stream))
+        _lib.check(rc, "trex_dfa_batch_run")
+        return final_state, accept, accept_i32
+
+    def last_error_word(self, scratch=None) -> int:
+        v = ctypes.c_int32(0)
+        rc = self.lib.trex_dfa_batch_error(self._h, _dptr(scratch), ctypes.byref(v))
+        _lib.check(rc, "trex_dfa_batch_error")
+        return v.value
+
+    def run_host(self, data: np.ndarray, offsets: np.ndarray, dfa_id: Optional[np.ndarray] = None,
+                 seg_len: int = 0, final_state=None, accept=None):
+        """Host-buffer run (copies in and out). Returns (final_state, accept,
+        kernel_ms, total_ms). Passing pinned numpy views makes the copies
+        asynchronous DMA."""
+        data = np.ascontiguousarray(data, dtype=np.uint8)
+        offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+        n = len(offsets) - 1
+        ids = None if dfa_id is None else np.ascontiguousarray(dfa_id, dtype=np.int32)
+        fs = final_state if final_state is not None else np.zeros(n, dtype=np.uint8)
+        ac = accept if accept is not None else np.zeros(n, dtype=np.uint8)
+        km, tm = ctypes.c_float(0), ctypes.c_float(0)
+        rc = self.lib.trex_dfa_batch_host(
+            self._h, _lib.ptr(data if data.size else np.zeros(1, np.uint8), ctypes.c_uint8),
+            _lib.ptr(offsets, ctypes.c_int64), _lib.ptr(ids, ctypes.c_int32), n, data.size,
+            _lib.ptr(fs, ctypes.c_uint8), _lib.ptr(ac, ctypes.c_uint8), None, seg_len,
+            ctypes.byref(km), ctypes.byref(tm))
+        _lib.check(rc, "trex_dfa_batch_host")
+        return fs, ac, km.value, tm.value
