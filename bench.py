@@ -51,6 +51,8 @@ def parse_args():
     ap.add_argument("--workload", choices=["ragged", "plain"], default="ragged")
     ap.add_argument("--strings", type=int, default=None, help="override the number of strings")
     ap.add_argument("--seg-len", type=int, default=0)
+    ap.add_argument("--dfa-sizes", type=str, default=None,
+                    help="comma list of DFA state counts replacing the default 5x8,5x12,6x16")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
@@ -75,12 +77,15 @@ def workload_spec(kind: str, n_override=None):
                 n_strings=n, kind=kind)
 
 
-def make_automata(kind: str, seed: int):
+def make_automata(kind: str, seed: int, sizes_override=None):
     from trex_b200.workloads import ACGT, random_dfa
     rng = np.random.default_rng(seed)
     if kind == "plain":
         return [random_dfa(16, ACGT, rng)]
     sizes = (8,) * 5 + (12,) * 5 + (16,) * 6
+    if sizes_override:
+        base = [int(x) for x in sizes_override.split(",")]
+        sizes = [base[i % len(base)] for i in range(16)]
     return [random_dfa(n, np.arange(256), rng) for n in sizes]
 
 
@@ -257,7 +262,7 @@ def reference_arm(args, rank):
     if rank != 0:
         return
     spec = workload_spec(args.workload, args.strings)
-    dfas = make_automata(args.workload, args.seed)
+    dfas = make_automata(args.workload, args.seed, args.dfa_sizes)
     lens, off, ids, is_sub = make_lengths(args.workload, spec["n_strings"], args.seed)
     from oracle import oracle as orc
     orc.build()
@@ -311,7 +316,7 @@ def trex_arm(args, rank, world, local_rank):
         import torch.distributed as dist
     spec = workload_spec(args.workload, args.strings)
     seed = args.seed + 7919 * rank
-    dfas = make_automata(args.workload, args.seed)
+    dfas = make_automata(args.workload, args.seed, args.dfa_sizes)
     lens, off, ids, is_sub = make_lengths(args.workload, spec["n_strings"], seed)
     data = make_device_bytes(torch, lens, is_sub, seed, dev)
     d_off = torch.from_numpy(off).to(dev)

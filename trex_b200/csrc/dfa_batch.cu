@@ -4,50 +4,50 @@
 // Semantics (reference src/simulation.py:274-297 precompute_tmap and
 // cuda/prefix_compose.cu:217-258 prefix_fused_kernel): every string walks
 //     s = tmap[byte * N + s]
-// from the DFA's start state; outputs are the final state and accept[s].
+// from its DFA's start state; outputs are the final state and accept[s].
 //
 // Design
-//  * Planning (3 small kernels): every string is cut into work items of at
-//    most seg_len bytes; items are bucketed by DFA so one CTA serves one DFA
-//    at a time. Item k of a string covers bytes [k*seg_len, (k+1)*seg_len).
+//  * Planning kernels cut every string into work items of at most seg_len
+//    bytes, bucket them by DFA (one CTA serves one DFA at a time) and, inside
+//    a DFA, order them by length class, longest first, so queues drain on
+//    short items. Queue slots are reserved per tile of strings with one
+//    global atomic per (DFA, class).
+//  * Speculative entry states: an item other than the first of its string
+//    does not know its entry state. It starts kWarmBytes earlier, inside the
+//    previous item, from state 0; for a synchronising DFA (random DFAs merge
+//    two chains with probability ~1/N per byte) the chain has then reached
+//    the true entry state. The item records that guess next to its end
+//    state; the last item of the string to finish composes the string
+//    (start -> end of item 0 -> ...), and wherever the true state differs
+//    from an item's guess it re-walks that item exactly. Results are exact
+//    for every DFA; only non-synchronising DFAs pay for re-walks.
 //  * Main kernel: one persistent 1024-thread CTA per SM. The CTA expands the
-//    current DFA's 4 KiB byte map into a per-lane replicated table in shared
-//    memory so that the 32 lanes of a warp always hit 32 different banks:
-//      N <= 8 : byte address = c<<8 | (s>>2)<<7 | lane<<2 | (s&3)   (64 KiB)
-//               the stored byte IS the next address minus c<<8, so one step
-//               is PRMT (merge state byte with input byte c) + LDS.U8;
-//      N <= 16: byte address = c<<9 | (s>>2)<<7 | lane<<2 | (s&3)   (128 KiB)
-//               the stored byte is (s&3) | (s>>2)<<6 and one step is
-//               PRMT + LOP3 + IADD3 + LDS.U8;
-//      N <= 256: the plain 256*N table (bank conflicts, no string splitting).
-//  * Each thread walks one item. The first item of a string starts from the
-//    DFA start state. Later items compute the item's state map: all N start
-//    states walk together until they coincide (random DFAs synchronise within
-//    a few dozen bytes), then a single chain finishes the item. A per-string
-//    counter lets the last item to finish compose the maps in order
-//    (no spin-waits).
-//  * Input is streamed with 16-byte non-coherent loads (L2 256-byte
-//    prefetch), one load ahead of the dependent chain.
+//    current DFA's byte map into a per-lane replicated shared-memory table
+//    (dfa_walk.cuh) so table lookups never conflict on banks. Each lane owns
+//    one item and the warp advances in lock step over 32-byte windows; edge
+//    windows apply bytes under a per-lane mask. Each lane holds the record of
+//    its next item (fetched one iteration ahead with a warp-aggregated atomic)
+//    and the next input window (across item boundaries), so refills do not
+//    stall the warp. No spin-waits anywhere.
 #include <algorithm>
 #include <cstring>
 #include <new>
 #include <vector>
 
-#include "trex_internal.cuh"
+#include "dfa_walk.cuh"
 
 namespace trex {
 
-struct DfaDesc {
-    int32_t n_states;
-    int32_t start;
-    int64_t tmap_off;
-    int64_t accept_off;
-};
-
 struct WorkItem {
+    int64_t p0;          // first byte walked (warm-up bytes included)
+    int64_t end;         // one past the last byte of the item
     uint32_t str;
-    uint32_t seg;
+    uint32_t segn;       // item index (low 16 bits) | items of the string (high 16 bits)
+    uint32_t map_base;   // first result slot of the string (strings with > 1 item)
+    uint32_t entry;      // start state (bits 0-7) | warm-up bytes (bits 8-15)
 };
+constexpr int64_t kMaxItemsPerString = 65535;
+constexpr int kWarmBytes = 128;
 
 // Error bits reported through the device error word.
 enum : uint32_t {
@@ -57,37 +57,64 @@ enum : uint32_t {
 
 constexpr int kRaggedThreads = 1024;
 constexpr int kPlanThreads = 256;
-constexpr int kDefaultSegLen = 8192;
+constexpr int kDefaultSegLen = 2048;
+constexpr int kLenClasses = 8;
 
 // ---- scratch layout -----------------------------------------------------------
 struct ScratchLayout {
-    size_t q_count, q_base, q_head, q_cursor, q_bytes, err, items, maps, done, total;
+    size_t cls_count, cls_cursor, q_base, q_count, q_head, q_bytes, err, map_cursor, items, maps,
+        done, total;
     int64_t max_items;
 };
 
+static int32_t effective_seg_len(int32_t seg_len) {
+    if (seg_len <= 0) seg_len = kDefaultSegLen;
+    return seg_len < 64 ? 64 : seg_len;
+}
+
 static ScratchLayout scratch_layout(int64_t n_strings, int64_t total_bytes, int32_t seg_len) {
     ScratchLayout L{};
-    if (seg_len <= 0) seg_len = kDefaultSegLen;
+    seg_len = effective_seg_len(seg_len);
     L.max_items = n_strings + total_bytes / seg_len + 1;
     size_t o = 0;
     auto take = [&](size_t bytes) { size_t at = o; o = (o + bytes + 255) & ~size_t(255); return at; };
-    L.q_count = take(kMaxDfasPerSet * 4);
+    L.cls_count = take(kMaxDfasPerSet * kLenClasses * 4);
+    L.cls_cursor = take(kMaxDfasPerSet * kLenClasses * 4);
     L.q_base = take(kMaxDfasPerSet * 4);
+    L.q_count = take(kMaxDfasPerSet * 4);
     L.q_head = take(kMaxDfasPerSet * 4);
-    L.q_cursor = take(kMaxDfasPerSet * 4);
     L.q_bytes = take(kMaxDfasPerSet * 8);
     L.err = take(4);
+    L.map_cursor = take(4);
     L.items = take((size_t)L.max_items * sizeof(WorkItem));
-    L.maps = take((size_t)L.max_items * sizeof(uint64_t));
+    L.maps = take((size_t)L.max_items * sizeof(uint32_t));
     L.done = take((size_t)std::max<int64_t>(n_strings, 1) * 4);
     L.total = o;
     return L;
 }
 
 // ---- planning kernels -------------------------------------------------------------
-__device__ __forceinline__ uint32_t n_items_of(int64_t len, int n_states, int32_t seg_len) {
-    if (len <= 0 || n_states > kSmallDfaStates) return 1;
-    return (uint32_t)((len + seg_len - 1) / seg_len);
+// Items of one string: its bytes are cut into pieces of seg bytes (seg grows
+// for strings that would need more than kMaxItemsPerString pieces); strings of
+// automata with more than 16 states are never cut.
+__device__ __forceinline__ uint32_t n_items_of(int64_t len, int n_states, int32_t seg_len,
+                                               int64_t *seg_out) {
+    if (len <= 0 || n_states > kSmallDfaStates) {
+        *seg_out = len;
+        return 1;
+    }
+    int64_t seg = seg_len;
+    if ((len + seg - 1) / seg > kMaxItemsPerString)
+        seg = (len + kMaxItemsPerString - 1) / kMaxItemsPerString;
+    *seg_out = seg;
+    return (uint32_t)((len + seg - 1) / seg);
+}
+
+// Length class: 0 for >= 4096 bytes, then one class per halving, 7 for < 64.
+__device__ __forceinline__ int len_class(int64_t len) {
+    int lg = len > 0 ? 63 - __clzll(len) : 0;
+    int c = 12 - lg;
+    return c < 0 ? 0 : (c > kLenClasses - 1 ? kLenClasses - 1 : c);
 }
 
 // Returns the DFA index of string i, or -1 (and raises an error bit) when the
@@ -111,200 +138,121 @@ __device__ __forceinline__ int checked_dfa(const int64_t *offsets, const int32_t
 
 __global__ void plan_count_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n,
                                   int64_t total_bytes, const DfaDesc *desc, int n_dfas,
-                                  int32_t seg_len, uint32_t *q_count,
+                                  int32_t seg_len, uint32_t *cls_count,
                                   unsigned long long *q_bytes, uint32_t *err) {
-    __shared__ uint32_t cnt[kMaxDfasPerSet];
+    __shared__ uint32_t cnt[kMaxDfasPerSet * kLenClasses];
     __shared__ unsigned long long byt[kMaxDfasPerSet];
-    for (int t = threadIdx.x; t < n_dfas; t += blockDim.x) { cnt[t] = 0; byt[t] = 0; }
+    for (int t = threadIdx.x; t < n_dfas * kLenClasses; t += blockDim.x) cnt[t] = 0;
+    for (int t = threadIdx.x; t < n_dfas; t += blockDim.x) byt[t] = 0;
     __syncthreads();
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
         int64_t len;
         int d = checked_dfa(offsets, dfa_id, i, n_dfas, total_bytes, err, &len);
         if (d < 0) continue;
-        atomicAdd(&cnt[d], n_items_of(len, desc[d].n_states, seg_len));
+        int64_t seg;
+        uint32_t k = n_items_of(len, desc[d].n_states, seg_len, &seg);
+        if (k > 1) atomicAdd(&cnt[d * kLenClasses + len_class(seg)], k - 1);
+        atomicAdd(&cnt[d * kLenClasses + len_class(len - (int64_t)(k - 1) * seg)], 1u);
         atomicAdd(&byt[d], (unsigned long long)len + 64ull);
     }
     __syncthreads();
-    for (int t = threadIdx.x; t < n_dfas; t += blockDim.x) {
-        if (cnt[t]) atomicAdd(&q_count[t], cnt[t]);
+    for (int t = threadIdx.x; t < n_dfas * kLenClasses; t += blockDim.x)
+        if (cnt[t]) atomicAdd(&cls_count[t], cnt[t]);
+    for (int t = threadIdx.x; t < n_dfas; t += blockDim.x)
         if (byt[t]) atomicAdd(&q_bytes[t], byt[t]);
-    }
 }
 
-__global__ void plan_scan_kernel(const uint32_t *q_count, uint32_t *q_base, uint32_t *q_cursor,
-                                 int n_dfas) {
+__global__ void plan_scan_kernel(const uint32_t *cls_count, uint32_t *cls_cursor, uint32_t *q_base,
+                                 uint32_t *q_count, int n_dfas) {
     if (threadIdx.x == 0) {
         uint32_t run = 0;
         for (int d = 0; d < n_dfas; ++d) {
             q_base[d] = run;
-            q_cursor[d] = run;
-            run += q_count[d];
+            for (int c = 0; c < kLenClasses; ++c) {
+                cls_cursor[d * kLenClasses + c] = run;
+                run += cls_count[d * kLenClasses + c];
+            }
+            q_count[d] = run - q_base[d];
         }
     }
 }
 
-__global__ void plan_fill_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n,
-                                 int64_t total_bytes, const DfaDesc *desc, int n_dfas,
-                                 int32_t seg_len, uint32_t *q_cursor, WorkItem *items,
-                                 uint32_t *done, uint32_t *err) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        done[i] = 0;
-        int64_t len;
-        int d = checked_dfa(offsets, dfa_id, i, n_dfas, total_bytes, err, &len);
-        if (d < 0) continue;
-        uint32_t k = n_items_of(len, desc[d].n_states, seg_len);
-        uint32_t pos = atomicAdd(&q_cursor[d], k);
-        for (uint32_t j = 0; j < k; ++j) items[pos + j] = WorkItem{(uint32_t)i, j};
-    }
-}
-
-// ---- replicated-table walkers ------------------------------------------------------
-// LAYOUT 8: N <= 8, LAYOUT 16: N <= 16, LAYOUT 0: plain table (N <= 256).
-template <int LAYOUT> struct Walker;
-
-template <> struct Walker<8> {
-    static constexpr int kChains = 8;
-    uint32_t lane;
-    __device__ uint32_t enc(uint32_t s) const { return (s & 3u) | (lane << 2) | ((s >> 2) << 7); }
-    __device__ static uint32_t dec(uint32_t e) { return (e & 3u) | ((e >> 7) << 2); }
-    template <int I>
-    __device__ __forceinline__ uint32_t step(const uint8_t *tbl, uint32_t e, uint32_t x) const {
-        uint32_t a = __byte_perm(e, x, 0x1100 | ((4 + I) << 4));
-        return tbl[a];
-    }
-};
-
-template <> struct Walker<16> {
-    static constexpr int kChains = 16;
-    uint32_t lane;
-    __device__ uint32_t enc(uint32_t s) const { return (s & 3u) | ((s >> 2) << 6); }
-    __device__ static uint32_t dec(uint32_t e) { return (e & 3u) | ((e >> 6) << 2); }
-    template <int I>
-    __device__ __forceinline__ uint32_t step(const uint8_t *tbl, uint32_t e, uint32_t x) const {
-        uint32_t t = __byte_perm(e, x, 0x1100 | ((4 + I) << 4));
-        uint32_t a = t + (t & 0xFFC0u) + (lane << 2);
-        return tbl[a];
-    }
-};
-
-template <> struct Walker<0> {
-    static constexpr int kChains = 0;
-    uint32_t n;
-    __device__ uint32_t enc(uint32_t s) const { return s; }
-    __device__ static uint32_t dec(uint32_t e) { return e; }
-    template <int I>
-    __device__ __forceinline__ uint32_t step(const uint8_t *tbl, uint32_t e, uint32_t x) const {
-        uint32_t c = (x >> (8 * I)) & 0xFFu;
-        return tbl[c * n + e];
-    }
-};
-
-template <class W>
-__device__ __forceinline__ uint32_t step_word(const W &w, const uint8_t *tbl, uint32_t e,
-                                              uint32_t x) {
-    e = w.template step<0>(tbl, e, x);
-    e = w.template step<1>(tbl, e, x);
-    e = w.template step<2>(tbl, e, x);
-    e = w.template step<3>(tbl, e, x);
-    return e;
-}
-
-template <class W>
-__device__ __forceinline__ uint32_t step16(const W &w, const uint8_t *tbl, uint32_t e, uint4 v) {
-    e = step_word(w, tbl, e, v.x);
-    e = step_word(w, tbl, e, v.y);
-    e = step_word(w, tbl, e, v.z);
-    e = step_word(w, tbl, e, v.w);
-    return e;
-}
-
-// Walks bytes [p, end) from encoded state e.
-template <class W>
-__device__ uint32_t walk_chain(const W &w, const uint8_t *tbl, const uint8_t *__restrict__ data,
-                               int64_t p, int64_t end, uint32_t e) {
-    while (p < end && (p & 15)) {
-        e = w.template step<0>(tbl, e, (uint32_t)__ldg(data + p));
-        ++p;
-    }
-    if (end - p >= 32) {
-        uint4 a = ld_stream16(data + p);
-        uint4 b = ld_stream16(data + p + 16);
-        p += 32;
-        while (end - p >= 32) {
-            uint4 na = ld_stream16(data + p);
-            uint4 nb = ld_stream16(data + p + 16);
-            e = step16(w, tbl, e, a);
-            e = step16(w, tbl, e, b);
-            a = na;
-            b = nb;
-            p += 32;
+// Writes the work items. Strings are handled in tiles of kPlanThreads; the
+// queue positions of a tile are reserved with one global atomic per
+// (DFA, length class) and ranks come from shared-memory atomics.
+__global__ void __launch_bounds__(kPlanThreads)
+plan_fill_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n, int64_t total_bytes,
+                 const DfaDesc *desc, int n_dfas, int32_t seg_len, uint32_t *cls_cursor,
+                 uint32_t *map_cursor, WorkItem *items, uint32_t *done, uint32_t *err) {
+    __shared__ uint32_t s_cnt[kMaxDfasPerSet * kLenClasses];
+    __shared__ uint32_t s_base[kMaxDfasPerSet * kLenClasses];
+    __shared__ uint32_t s_map, s_map_base;
+    const int n_slots = n_dfas * kLenClasses;
+    for (int t = threadIdx.x; t < n_slots; t += blockDim.x) s_cnt[t] = 0;
+    if (threadIdx.x == 0) s_map = 0;
+    __syncthreads();
+    for (int64_t tile = blockIdx.x; tile * kPlanThreads < n; tile += gridDim.x) {
+        const int64_t i = tile * kPlanThreads + threadIdx.x;
+        int d = -1;
+        int64_t len = 0, seg = 0;
+        uint32_t k = 0, cf = 0, cl = 0, r_full = 0, r_last = 0, r_map = 0;
+        if (i < n) {
+            done[i] = 0;
+            d = checked_dfa(offsets, dfa_id, i, n_dfas, total_bytes, err, &len);
         }
-        e = step16(w, tbl, e, a);
-        e = step16(w, tbl, e, b);
-    }
-    if (end - p >= 16) {
-        uint4 a = ld_stream16(data + p);
-        e = step16(w, tbl, e, a);
-        p += 16;
-    }
-    while (p < end) {
-        e = w.template step<0>(tbl, e, (uint32_t)__ldg(data + p));
-        ++p;
-    }
-    return e;
-}
-
-// State map of bytes [p, end) for states 0..n-1 packed as nibbles.
-template <class W>
-__device__ uint64_t walk_map(const W &w, const uint8_t *tbl, const uint8_t *__restrict__ data,
-                             int64_t p, int64_t end, int n) {
-    constexpr int C = W::kChains;
-    uint32_t e[C];
-#pragma unroll
-    for (int j = 0; j < C; ++j) e[j] = w.enc(j < n ? (uint32_t)j : 0u);
-    bool same = false;
-    while (p < end) {
-        int64_t stop = p + 8 < end ? p + 8 : end;
-        for (; p < stop; ++p) {
-            uint32_t c = __ldg(data + p);
-#pragma unroll
-            for (int j = 0; j < C; ++j) e[j] = w.template step<0>(tbl, e[j], c);
+        if (d >= 0) {
+            k = n_items_of(len, desc[d].n_states, seg_len, &seg);
+            cf = d * kLenClasses + len_class(seg);
+            cl = d * kLenClasses + len_class(len - (int64_t)(k - 1) * seg);
+            if (k > 1) {
+                r_full = atomicAdd(&s_cnt[cf], k - 1);
+                r_map = atomicAdd(&s_map, k);
+            }
+            r_last = atomicAdd(&s_cnt[cl], 1u);
         }
-        same = true;
-#pragma unroll
-        for (int j = 1; j < C; ++j) same &= (e[j] == e[0]);
-        if (same) break;
+        __syncthreads();
+        for (int t = threadIdx.x; t < n_slots; t += blockDim.x)
+            if (s_cnt[t]) s_base[t] = atomicAdd(&cls_cursor[t], s_cnt[t]);
+        if (threadIdx.x == 0 && s_map) s_map_base = atomicAdd(map_cursor, s_map);
+        __syncthreads();
+        if (d >= 0) {
+            const int64_t s0 = offsets[i];
+            const uint32_t mb = k > 1 ? s_map_base + r_map : 0u;
+            const uint32_t warm = (uint32_t)(seg < kWarmBytes ? seg : (int64_t)kWarmBytes);
+            for (uint32_t j = 0; j < k; ++j) {
+                const uint32_t pos = (j + 1 == k) ? s_base[cl] + r_last : s_base[cf] + r_full + j;
+                const int64_t b0 = s0 + (int64_t)j * seg;
+                const int64_t b1 = (j + 1 == k) ? s0 + len : b0 + seg;
+                items[pos] = (j == 0)
+                    ? WorkItem{b0, b1, (uint32_t)i, j | (k << 16), mb, (uint32_t)desc[d].start}
+                    : WorkItem{b0 - warm, b1, (uint32_t)i, j | (k << 16), mb, warm << 8};
+            }
+        }
+        __syncthreads();
+        for (int t = threadIdx.x; t < n_slots; t += blockDim.x) s_cnt[t] = 0;
+        if (threadIdx.x == 0) s_map = 0;
+        __syncthreads();
     }
-    uint64_t m = 0;
-    if (same) {
-        uint32_t e0 = walk_chain(w, tbl, data, p, end, e[0]);
-        uint64_t s = W::dec(e0);
-        m = s * 0x1111111111111111ull;
-    } else {
-#pragma unroll
-        for (int j = 0; j < C; ++j) m |= (uint64_t)W::dec(e[j]) << (4 * j);
-    }
-    return m;
 }
 
+// ---- main kernel -------------------------------------------------------------------------
 struct RaggedParams {
     const uint8_t *data;
+    int64_t total_bytes;
     const int64_t *offsets;
-    int64_t n_strings;
     const uint8_t *tmaps;
     const uint8_t *accepts;
     const DfaDesc *desc;
     int n_dfas;
+    int32_t seg_len;
     const WorkItem *items;
     const uint32_t *q_base;
     const uint32_t *q_count;
     uint32_t *q_head;
     const unsigned long long *q_bytes;
-    uint64_t *maps;
+    uint32_t *maps;
     uint32_t *done;
-    int32_t seg_len;
     uint8_t *final_state;
     uint8_t *accept;
     int32_t *accept_i32;
@@ -318,75 +266,162 @@ __device__ __forceinline__ void write_result(const RaggedParams &P, uint32_t str
     if (P.accept_i32) P.accept_i32[str] = a ? 1 : 0;
 }
 
+// Records (guessed entry state, end state) of one item of a split string; the
+// last item of the string to finish composes the string in order and
+// re-walks every item whose guess was wrong.
 template <class W>
-__device__ void process_item(const RaggedParams &P, const W &w, const uint8_t *tbl, WorkItem it,
-                             uint32_t item_idx, const DfaDesc &D) {
-    int64_t s0 = P.offsets[it.str], s1 = P.offsets[it.str + 1];
-    uint32_t nseg = n_items_of(s1 - s0, D.n_states, P.seg_len);
-    int64_t b0 = (nseg == 1) ? s0 : s0 + (int64_t)it.seg * P.seg_len;
-    int64_t b1 = (nseg == 1) ? s1 : min(s1, b0 + (int64_t)P.seg_len);
-    uint64_t map;
-    if (it.seg == 0) {
-        uint32_t e = walk_chain(w, tbl, P.data, b0, b1, w.enc((uint32_t)D.start));
-        uint32_t fs = W::dec(e);
-        if (nseg == 1) {
-            write_result(P, it.str, fs, D.accept_off);
-            return;
-        }
-        map = (uint64_t)fs * 0x1111111111111111ull;
-    } else {
-        if constexpr (W::kChains > 0) map = walk_map(w, tbl, P.data, b0, b1, D.n_states);
-        else map = 0;  // unreachable: large automata are never split
-    }
-    P.maps[item_idx] = map;
+__device__ __forceinline__ void publish_item(const RaggedParams &P, const W &w, uint32_t str,
+                                          uint32_t segn, uint32_t mb, uint32_t guess,
+                                          uint32_t fin, const DfaDesc &D) {
+    const uint32_t seg = segn & 0xffffu, nseg = segn >> 16;
+    P.maps[mb + seg] = guess | (fin << 8);
     __threadfence();
-    uint32_t prev = atomicAdd(&P.done[it.str], 1u);
-    if (prev == nseg - 1) {
-        __threadfence();
-        uint32_t base = item_idx - it.seg;
-        uint32_t s = (uint32_t)D.start;
-        for (uint32_t k = 0; k < nseg; ++k) {
-            uint64_t m = ld_relaxed_u64(P.maps + base + k);
-            s = (uint32_t)(m >> (4 * s)) & 15u;
+    uint32_t prev = atomicAdd(&P.done[str], 1u);
+    if (prev != nseg - 1) return;
+    __threadfence();
+    const int64_t s0 = P.offsets[str], len = P.offsets[str + 1] - s0;
+    int64_t seg_bytes;
+    n_items_of(len, D.n_states, P.seg_len, &seg_bytes);
+    uint32_t s = (uint32_t)D.start;
+    for (uint32_t k = 0; k < nseg; ++k) {
+        const uint32_t v = ld_acquire_u32(P.maps + mb + k);
+        if (k == 0 || (v & 0xffu) == s) {
+            s = (v >> 8) & 0xffu;
+        } else {
+            // the chain had not synchronised: walk this item from the true state
+            const int64_t b0 = s0 + (int64_t)k * seg_bytes;
+            const int64_t b1 = (k + 1 == nseg) ? s0 + len : b0 + seg_bytes;
+            uint32_t e = w.enc(s);
+            for (int64_t q = b0; q < b1; ++q) e = w.template step<0>(e, (uint32_t)__ldg(P.data + q));
+            s = W::dec(e);
         }
-        write_result(P, it.str, s, D.accept_off);
     }
+    write_result(P, str, s, D.accept_off);
 }
 
-// Fills the shared-memory table of DFA d for the layout its size selects.
-__device__ void build_table(const RaggedParams &P, const DfaDesc &D, uint8_t *tbl) {
-    const uint8_t *src = P.tmaps + D.tmap_off;
-    const int N = D.n_states;
-    uint32_t *w32 = reinterpret_cast<uint32_t *>(tbl);
-    if (N <= 8) {
-        for (int w = threadIdx.x; w < kRepTableBytes8 / 4; w += blockDim.x) {
-            uint32_t c = w >> 6, q = (w >> 5) & 1u, ln = w & 31u, word = 0;
-#pragma unroll
-            for (int b = 0; b < 4; ++b) {
-                uint32_t s = q * 4 + b;
-                uint32_t t = s < (uint32_t)N ? src[c * N + s] : s;
-                word |= ((t & 3u) | (ln << 2) | ((t >> 2) << 7)) << (8 * b);
+// Drains queue d with this warp. All lanes of the warp call it together.
+template <class W>
+__device__ void drain_queue(const RaggedParams &P, const W &w, const DfaDesc &D, uint32_t base,
+                            uint32_t count, uint32_t *head) {
+    const uint32_t FULL = 0xffffffffu;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t mis = (uint32_t)((uintptr_t)P.data & 31u);
+    // current item: bytes [p, end) are still to be walked; during the warm-up
+    // end marks the item's first own byte and `rest` its remaining length.
+    int64_t p = 0, end = 0;
+    uint32_t e = 0, c_str = 0, c_segn = 0, c_mb = 0, guess = 0, rest = 0;
+    // flags: bit 0 item live, bits 1-2 next slot (0 empty, 1 index requested,
+    // 2 record loaded), bit 3 queue exhausted for this lane, bit 4 warm-up
+    uint32_t fl = 0;
+    WorkItem nx{0, 0, 0, 0, 0, 0};
+    uint32_t req_mask = 0, pending = 0;
+    // lookahead window (data index of its first byte, 32-aligned in memory)
+    int64_t la_w = INT64_MIN;   // no window can start here
+    uint4 la_a = make_uint4(0, 0, 0, 0), la_b = la_a;
+    while (true) {
+        // A. resolve last iteration's request: item index -> record load
+        if (req_mask) {
+            const uint32_t b = __shfl_sync(FULL, pending, __ffs(req_mask) - 1);
+            if (req_mask & (1u << lane)) {
+                const uint32_t idx = b + (uint32_t)__popc(req_mask & ((1u << lane) - 1u));
+                if (idx < count) {
+                    nx = P.items[base + idx];
+                    fl = (fl & ~6u) | 4u;
+                } else {
+                    fl = (fl & ~6u) | 8u;
+                }
             }
-            w32[w] = word;
+            req_mask = 0;
         }
-    } else if (N <= 16) {
-        for (int w = threadIdx.x; w < kRepTableBytes16 / 4; w += blockDim.x) {
-            uint32_t c = w >> 7, q = (w >> 5) & 3u, word = 0;
-#pragma unroll
-            for (int b = 0; b < 4; ++b) {
-                uint32_t s = q * 4 + b;
-                uint32_t t = s < (uint32_t)N ? src[c * N + s] : s;
-                word |= ((t & 3u) | ((t >> 2) << 6)) << (8 * b);
+        // B. lanes at the end of their bytes: warm-up done -> own bytes; item
+        //    done -> publish it and take the next record
+        if (p >= end) {
+            if (fl & 16u) {
+                guess = W::dec(e);
+                end = p + rest;
+                fl &= ~16u;
+            } else {
+                if (fl & 1u) {
+                    if ((c_segn >> 16) == 1) write_result(P, c_str, W::dec(e), D.accept_off);
+                    else publish_item(P, w, c_str, c_segn, c_mb, guess, W::dec(e), D);
+                    fl &= ~1u;
+                }
+                p = end = 0;
+                if (fl & 4u) {
+                    fl &= ~6u;
+                    const uint32_t warm = (nx.entry >> 8) & 0xffu;
+                    if (nx.p0 + warm < nx.end) {
+                        c_str = nx.str;
+                        c_segn = nx.segn;
+                        c_mb = nx.map_base;
+                        p = nx.p0;
+                        e = w.enc(nx.entry & 0xffu);
+                        guess = nx.entry & 0xffu;
+                        if (warm) {
+                            end = p + warm;
+                            rest = (uint32_t)(nx.end - end);
+                            fl |= 17u;
+                        } else {
+                            end = nx.end;
+                            fl |= 1u;
+                        }
+                    } else {
+                        // empty string: its final state is the start state
+                        write_result(P, nx.str, nx.entry & 0xffu, D.accept_off);
+                    }
+                }
             }
-            w32[w] = word;
         }
-    } else {
-        for (int i = threadIdx.x; i < 256 * N; i += blockDim.x) tbl[i] = src[i];
+        // C. request the next item for lanes with an empty slot
+        const uint32_t need = __ballot_sync(FULL, (fl & 14u) == 0u);
+        if (need) {
+            if ((int)lane == __ffs(need) - 1) pending = atomicAdd(head, (uint32_t)__popc(need));
+            if (need & (1u << lane)) fl |= 2u;
+            req_mask = need;
+        }
+        if (__all_sync(FULL, (fl & 7u) == 0u && (fl & 8u))) break;
+        // D. one 32-byte window per lane, the following one loaded ahead
+        uint4 a = make_uint4(0, 0, 0, 0), b = a;
+        uint32_t m = 0;
+        if (p < end) {
+            const int64_t wst = ((p + mis) & ~(int64_t)31) - mis;
+            if (la_w == wst) {
+                a = la_a;
+                b = la_b;
+            } else {
+                load_window(P.data + wst, P.data, P.data + P.total_bytes, a, b);
+            }
+            const int h0 = (int)min(end - wst, (int64_t)32);
+            m = bit_range((int)(p - wst), h0);
+            const int64_t lim = (fl & 16u) ? end + rest : end;   // end of the item's bytes
+            if (wst + h0 < lim) {
+                if (h0 == 32) {
+                    load_window(P.data + wst + 32, P.data, P.data + P.total_bytes, la_a, la_b);
+                    la_w = wst + 32;
+                } else {
+                    // the warm-up ends inside this window: it is walked again
+                    la_a = a;
+                    la_b = b;
+                    la_w = wst;
+                }
+            } else if ((fl & 6u) == 4u) {
+                const int64_t nw = ((nx.p0 + mis) & ~(int64_t)31) - mis;
+                load_window(P.data + nw, P.data, P.data + P.total_bytes, la_a, la_b);
+                la_w = nw;
+            }
+            p = wst + h0;
+        }
+        if (__all_sync(FULL, m == FULL || m == 0u)) {
+            e = step16(w, e, a);
+            e = step16(w, e, b);
+        } else {
+            e = step16_masked(w, e, a, m);
+            e = step16_masked(w, e, b, m >> 16);
+        }
     }
 }
 
 __global__ void __launch_bounds__(kRaggedThreads, 1) dfa_ragged_kernel(RaggedParams P) {
-    extern __shared__ __align__(1024) uint8_t tbl[];
     __shared__ int s_dfa;
     if (threadIdx.x == 0) {
         // Home DFA: CTAs are spread over DFAs in proportion to their bytes.
@@ -413,24 +448,12 @@ __global__ void __launch_bounds__(kRaggedThreads, 1) dfa_ragged_kernel(RaggedPar
         const int d = s_dfa;
         if (d < 0) break;
         const DfaDesc D = P.desc[d];
-        build_table(P, D, tbl);
+        build_table(P.tmaps + D.tmap_off, D.n_states);
         __syncthreads();
         const uint32_t base = P.q_base[d], count = P.q_count[d];
-        while (true) {
-            uint32_t idx = atomicAdd(&P.q_head[d], 1u);
-            if (idx >= count) break;
-            WorkItem it = P.items[base + idx];
-            if (D.n_states <= 8) {
-                Walker<8> w{lane};
-                process_item(P, w, tbl, it, base + idx, D);
-            } else if (D.n_states <= 16) {
-                Walker<16> w{lane};
-                process_item(P, w, tbl, it, base + idx, D);
-            } else {
-                Walker<0> w{(uint32_t)D.n_states};
-                process_item(P, w, tbl, it, base + idx, D);
-            }
-        }
+        if (D.n_states <= 8) drain_queue(P, Walker<8>{lane}, D, base, count, &P.q_head[d]);
+        else if (D.n_states <= 16) drain_queue(P, Walker<16>{lane}, D, base, count, &P.q_head[d]);
+        else drain_queue(P, Walker<0>{(uint32_t)D.n_states}, D, base, count, &P.q_head[d]);
         __syncthreads();
         if (threadIdx.x == 0) {
             int best = -1;
@@ -446,8 +469,6 @@ __global__ void __launch_bounds__(kRaggedThreads, 1) dfa_ragged_kernel(RaggedPar
         __syncthreads();
     }
 }
-
-// ---- host side --------------------------------------------------------------------------
 
 }  // namespace trex
 
@@ -484,8 +505,7 @@ int dfa_set_run(trex_dfa_set *set, const uint8_t *data, const int64_t *offsets,
     if (n < 0 || total_bytes < 0 || (n > 0 && !offsets) || (total_bytes > 0 && !data))
         return TREX_ERR_ARG;
     if (n >= (int64_t)0x7fffffff) return TREX_ERR_CAPACITY;
-    if (seg_len <= 0) seg_len = kDefaultSegLen;
-    if (seg_len < 64) seg_len = 64;
+    seg_len = effective_seg_len(seg_len);
     if (n == 0) return TREX_OK;
     ScratchLayout L = scratch_layout(n, total_bytes, seg_len);
     if (L.max_items >= (int64_t)0xffffffffLL) return TREX_ERR_CAPACITY;
@@ -506,39 +526,43 @@ int dfa_set_run(trex_dfa_set *set, const uint8_t *data, const int64_t *offsets,
     } else if ((size_t)scratch_bytes < L.total) {
         return TREX_ERR_ARG;
     }
+    uint32_t *cls_count = reinterpret_cast<uint32_t *>(sc + L.cls_count);
+    uint32_t *cls_cursor = reinterpret_cast<uint32_t *>(sc + L.cls_cursor);
     uint32_t *q_count = reinterpret_cast<uint32_t *>(sc + L.q_count);
     uint32_t *q_base = reinterpret_cast<uint32_t *>(sc + L.q_base);
     uint32_t *q_head = reinterpret_cast<uint32_t *>(sc + L.q_head);
-    uint32_t *q_cursor = reinterpret_cast<uint32_t *>(sc + L.q_cursor);
     auto *q_bytes = reinterpret_cast<unsigned long long *>(sc + L.q_bytes);
     uint32_t *err = reinterpret_cast<uint32_t *>(sc + L.err);
+    uint32_t *map_cursor = reinterpret_cast<uint32_t *>(sc + L.map_cursor);
     WorkItem *items = reinterpret_cast<WorkItem *>(sc + L.items);
-    uint64_t *maps = reinterpret_cast<uint64_t *>(sc + L.maps);
+    uint32_t *maps = reinterpret_cast<uint32_t *>(sc + L.maps);
     uint32_t *done = reinterpret_cast<uint32_t *>(sc + L.done);
 
-    // Counters, bases, heads, cursors, byte counts and the error word are
-    // contiguous at the front of the scratch buffer.
+    // Counters, bases, heads, cursors, byte counts, the error word and the
+    // map cursor are contiguous at the front of the scratch buffer.
     TREX_CUDA(cudaMemsetAsync(sc, 0, L.items, stream));
     int plan_grid = (int)std::min<int64_t>((n + kPlanThreads - 1) / kPlanThreads,
                                            (int64_t)set->n_sms * 8);
     plan_count_kernel<<<plan_grid, kPlanThreads, 0, stream>>>(
-        offsets, dfa_id, n, total_bytes, set->d_desc, set->n_dfas, seg_len, q_count, q_bytes, err);
+        offsets, dfa_id, n, total_bytes, set->d_desc, set->n_dfas, seg_len, cls_count, q_bytes,
+        err);
     TREX_CHECK_LAUNCH();
-    plan_scan_kernel<<<1, 32, 0, stream>>>(q_count, q_base, q_cursor, set->n_dfas);
+    plan_scan_kernel<<<1, 32, 0, stream>>>(cls_count, cls_cursor, q_base, q_count, set->n_dfas);
     TREX_CHECK_LAUNCH();
     plan_fill_kernel<<<plan_grid, kPlanThreads, 0, stream>>>(
-        offsets, dfa_id, n, total_bytes, set->d_desc, set->n_dfas, seg_len, q_cursor, items, done,
-        err);
+        offsets, dfa_id, n, total_bytes, set->d_desc, set->n_dfas, seg_len, cls_cursor,
+        map_cursor, items, done, err);
     TREX_CHECK_LAUNCH();
 
     RaggedParams P;
     P.data = data;
+    P.total_bytes = total_bytes;
     P.offsets = offsets;
-    P.n_strings = n;
     P.tmaps = set->d_tmaps;
     P.accepts = set->d_accepts;
     P.desc = set->d_desc;
     P.n_dfas = set->n_dfas;
+    P.seg_len = seg_len;
     P.items = items;
     P.q_base = q_base;
     P.q_count = q_count;
@@ -546,7 +570,6 @@ int dfa_set_run(trex_dfa_set *set, const uint8_t *data, const int64_t *offsets,
     P.q_bytes = q_bytes;
     P.maps = maps;
     P.done = done;
-    P.seg_len = seg_len;
     P.final_state = final_state;
     P.accept = accept;
     P.accept_i32 = accept_i32;
