@@ -299,24 +299,35 @@ __device__ __forceinline__ void publish_item(const RaggedParams &P, const W &w, 
     write_result(P, str, s, D.accept_off);
 }
 
+// Per-lane fields of the current item that are only touched when an item
+// starts or ends live in shared memory after the table (struct of arrays,
+// indexed by thread), which keeps the walking loop's registers free.
+constexpr int kColdOff = kRepTableBytes16;
+constexpr int kColdFields = 5;   // str, segn, map_base, guess, rest
+constexpr int kColdBytes = kColdFields * kRaggedThreads * 4;
+__device__ __forceinline__ uint32_t *cold(int field) {
+    return reinterpret_cast<uint32_t *>(g_dfa_tbl + kColdOff) + field * kRaggedThreads + threadIdx.x;
+}
+enum { kCStr = 0, kCSegn = 1, kCMb = 2, kCGuess = 3, kCRest = 4 };
+
 // Drains queue d with this warp. All lanes of the warp call it together.
 template <class W>
 __device__ void drain_queue(const RaggedParams &P, const W &w, const DfaDesc &D, uint32_t base,
                             uint32_t count, uint32_t *head) {
     const uint32_t FULL = 0xffffffffu;
     const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t mis = (uint32_t)((uintptr_t)P.data & 31u);
-    // current item: bytes [p, end) are still to be walked; during the warm-up
-    // end marks the item's first own byte and `rest` its remaining length.
-    int64_t p = 0, end = 0;
-    uint32_t e = 0, c_str = 0, c_segn = 0, c_mb = 0, guess = 0, rest = 0;
+    const uint8_t *const lo_ok = P.data, *const hi_ok = P.data + P.total_bytes;
+    // Walking state: the current 32-byte window starts at wp (32-aligned in
+    // memory); bytes [lo, lo + left) of the phase (warm-up or the item's own
+    // bytes) are still to be walked from there.
+    const uint8_t *wp = P.data;
+    uint32_t lo = 0, left = 0, e = 0;
     // flags: bit 0 item live, bits 1-2 next slot (0 empty, 1 index requested,
-    // 2 record loaded), bit 3 queue exhausted for this lane, bit 4 warm-up
+    // 2 record loaded), bit 3 queue exhausted for this lane, bit 4 warm-up,
+    // bit 5 lookahead (la) holds the next window to walk
     uint32_t fl = 0;
     WorkItem nx{0, 0, 0, 0, 0, 0};
     uint32_t req_mask = 0, pending = 0;
-    // lookahead window (data index of its first byte, 32-aligned in memory)
-    int64_t la_w = INT64_MIN;   // no window can start here
     uint4 la_a = make_uint4(0, 0, 0, 0), la_b = la_a;
     while (true) {
         // A. resolve last iteration's request: item index -> record load
@@ -333,42 +344,50 @@ __device__ void drain_queue(const RaggedParams &P, const W &w, const DfaDesc &D,
             }
             req_mask = 0;
         }
-        // B. lanes at the end of their bytes: warm-up done -> own bytes; item
-        //    done -> publish it and take the next record
-        if (p >= end) {
+        // B. end of a phase: warm-up -> the item's own bytes; item -> publish
+        //    it and start the next record
+        if (left == 0) {
             if (fl & 16u) {
-                guess = W::dec(e);
-                end = p + rest;
+                *cold(kCGuess) = W::dec(e);
+                left = *cold(kCRest);
                 fl &= ~16u;
             } else {
                 if (fl & 1u) {
-                    if ((c_segn >> 16) == 1) write_result(P, c_str, W::dec(e), D.accept_off);
-                    else publish_item(P, w, c_str, c_segn, c_mb, guess, W::dec(e), D);
+                    const uint32_t segn = *cold(kCSegn);
+                    if ((segn >> 16) == 1)
+                        write_result(P, *cold(kCStr), W::dec(e), D.accept_off);
+                    else
+                        publish_item(P, w, *cold(kCStr), segn, *cold(kCMb), *cold(kCGuess),
+                                     W::dec(e), D);
                     fl &= ~1u;
                 }
-                p = end = 0;
                 if (fl & 4u) {
                     fl &= ~6u;
                     const uint32_t warm = (nx.entry >> 8) & 0xffu;
                     if (nx.p0 + warm < nx.end) {
-                        c_str = nx.str;
-                        c_segn = nx.segn;
-                        c_mb = nx.map_base;
-                        p = nx.p0;
+                        const uint8_t *q = P.data + nx.p0;
+                        wp = reinterpret_cast<const uint8_t *>((uintptr_t)q & ~(uintptr_t)31);
+                        lo = (uint32_t)(q - wp);
+                        *cold(kCStr) = nx.str;
+                        *cold(kCSegn) = nx.segn;
+                        *cold(kCMb) = nx.map_base;
+                        *cold(kCGuess) = nx.entry & 0xffu;
                         e = w.enc(nx.entry & 0xffu);
-                        guess = nx.entry & 0xffu;
                         if (warm) {
-                            end = p + warm;
-                            rest = (uint32_t)(nx.end - end);
+                            left = warm;
+                            *cold(kCRest) = (uint32_t)(nx.end - nx.p0 - warm);
                             fl |= 17u;
                         } else {
-                            end = nx.end;
+                            left = (uint32_t)(nx.end - nx.p0);
                             fl |= 1u;
                         }
                     } else {
                         // empty string: its final state is the start state
                         write_result(P, nx.str, nx.entry & 0xffu, D.accept_off);
+                        fl &= ~32u;
                     }
+                } else {
+                    fl &= ~32u;
                 }
             }
         }
@@ -379,37 +398,44 @@ __device__ void drain_queue(const RaggedParams &P, const W &w, const DfaDesc &D,
             if (need & (1u << lane)) fl |= 2u;
             req_mask = need;
         }
-        if (__all_sync(FULL, (fl & 7u) == 0u && (fl & 8u))) break;
-        // D. one 32-byte window per lane, the following one loaded ahead
+        if (__all_sync(FULL, (fl & 15u) == 8u)) break;
+        // D. walk one window; load the next one ahead
         uint4 a = make_uint4(0, 0, 0, 0), b = a;
         uint32_t m = 0;
-        if (p < end) {
-            const int64_t wst = ((p + mis) & ~(int64_t)31) - mis;
-            if (la_w == wst) {
+        if (left) {
+            if (fl & 32u) {
                 a = la_a;
                 b = la_b;
             } else {
-                load_window(P.data + wst, P.data, P.data + P.total_bytes, a, b);
+                load_window(wp, lo_ok, hi_ok, a, b);
             }
-            const int h0 = (int)min(end - wst, (int64_t)32);
-            m = bit_range((int)(p - wst), h0);
-            const int64_t lim = (fl & 16u) ? end + rest : end;   // end of the item's bytes
-            if (wst + h0 < lim) {
-                if (h0 == 32) {
-                    load_window(P.data + wst + 32, P.data, P.data + P.total_bytes, la_a, la_b);
-                    la_w = wst + 32;
-                } else {
-                    // the warm-up ends inside this window: it is walked again
+            const uint32_t h = min(32u, lo + left);
+            m = bit_range((int)lo, (int)h);
+            left -= h - lo;
+            fl |= 32u;
+            if (left) {
+                wp += 32;
+                lo = 0;
+                load_window(wp, lo_ok, hi_ok, la_a, la_b);
+            } else if (fl & 16u) {
+                // warm-up ends here; the item's own bytes follow
+                if (h < 32u) {
+                    lo = h;
                     la_a = a;
                     la_b = b;
-                    la_w = wst;
+                } else {
+                    wp += 32;
+                    lo = 0;
+                    load_window(wp, lo_ok, hi_ok, la_a, la_b);
                 }
             } else if ((fl & 6u) == 4u) {
-                const int64_t nw = ((nx.p0 + mis) & ~(int64_t)31) - mis;
-                load_window(P.data + nw, P.data, P.data + P.total_bytes, la_a, la_b);
-                la_w = nw;
+                // item ends here: fetch the first window of the next record
+                const uint8_t *q = reinterpret_cast<const uint8_t *>(
+                    (uintptr_t)(P.data + nx.p0) & ~(uintptr_t)31);
+                load_window(q, lo_ok, hi_ok, la_a, la_b);
+            } else {
+                fl &= ~32u;
             }
-            p = wst + h0;
         }
         if (__all_sync(FULL, m == FULL || m == 0u)) {
             e = step16(w, e, a);
@@ -628,13 +654,8 @@ int trex_dfa_set_create(int n_dfas, const int32_t *n_states, const int32_t *star
         trex::set_last_error_msg("trex_dfa_set_create: no CUDA device");
         return TREX_ERR_SHAPE;
     }
-    set->smem_bytes = 0;
-    for (int d = 0; d < n_dfas; ++d) {
-        int N = set->n_states[d];
-        size_t need = N <= 8 ? trex::kRepTableBytes8
-                    : N <= 16 ? trex::kRepTableBytes16 : (size_t)256 * N;
-        set->smem_bytes = std::max(set->smem_bytes, need);
-    }
+    // table region (sized for the largest layout) + per-lane cold state
+    set->smem_bytes = (size_t)trex::kColdOff + trex::kColdBytes;
     auto fail = [&](cudaError_t e, const char *what) {
         trex::set_last_error(what, e);
         cudaFree(set->d_tmaps);
@@ -659,7 +680,7 @@ int trex_dfa_set_create(int n_dfas, const int32_t *n_states, const int32_t *star
     // table any set can need (128 KiB).
     if ((e = cudaFuncSetAttribute(trex::dfa_ragged_kernel,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  trex::kRepTableBytes16)) != cudaSuccess)
+                                  trex::kColdOff + trex::kColdBytes)) != cudaSuccess)
         return fail(e, "cudaFuncSetAttribute");
     *out = set;
     return TREX_OK;

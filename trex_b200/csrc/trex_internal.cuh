@@ -42,6 +42,10 @@ __device__ __forceinline__ uint4 ld_stream16(const void *p) {
     return v;
 }
 
+__device__ __forceinline__ void prefetch_l2(const void *p) {
+    asm volatile("prefetch.global.L2 [%0];" :: "l"(p));
+}
+
 __device__ __forceinline__ void st_stream16(void *p, uint4 v) {
     asm volatile("st.global.L1::no_allocate.v4.u32 [%0], {%1,%2,%3,%4};"
                  :: "l"(p), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w) : "memory");
