@@ -1,29 +1,31 @@
-"""Benchmark: ragged DFA batch on B200 (one JSON line on stdout, rank 0).
+"""Benchmark: automaton simulation on B200 (one JSON line on stdout, rank 0).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl trex|reference]
-                    [--workload ragged|plain] [--strings S]
+                    [--workload ragged|plain|scan] [--strings S]
 
-Workload (default, the benchmark's headline case): 16 random DFAs (5 x 8,
-5 x 12, 6 x 16 states) over all 256 byte values, 1M strings with log-normal
-lengths (median 2048, sigma 1.18, clipped to [16, 65536], ~4.1 GB), 10% of
-the strings over the 4-byte sub-alphabet "ACGT", string i on DFA i mod 16.
-Inputs are generated on the device from a seed (synthetic; the reference
-ships no dataset). One step = one ragged launch over the whole batch.
+Workloads (synthetic, seeded; the reference ships no dataset):
+  ragged (default, the headline case): 16 random DFAs (5 x 8, 5 x 12, 6 x 16
+      states) over all 256 byte values, 1M strings with log-normal lengths
+      (median 2048, sigma 1.18, clipped to [16, 65536], ~4.1 GB), 10% of the
+      strings over the 4-byte sub-alphabet "ACGT", string i on DFA i mod 16.
+      One step = one ragged launch over the whole batch.
+  plain: one random 16-state DFA over the bytes "ACGT", 4096 x 1024 bytes.
+  scan: one random 16-state DFA over 256 bytes, 8 strings x 256 MiB; one step
+      writes the state of every position (2 bytes moved per character).
 
 Multi-GPU: one process per GPU (torchrun); every rank runs its own seeded
-batch (weak scaling, no data-path collective); timings are the max over
-ranks (NCCL all-reduce of one float).
+batch (weak scaling, no data-path collective); times are the max over ranks
+(an NCCL all-reduce of one float).
 
---impl reference times the reference's CPU algorithm (the C oracle,
-oracle/oracle.c, a restatement of DFA.simulate over the byte map) on the
-host cores over a bounded sample of the same workload.
+--impl reference times the reference's CPU algorithm for the path (the C
+oracle, oracle/oracle.c: DFA.simulate over the byte map / the per-position
+walk) with OpenMP on the host cores, on a bounded sample of the same workload.
 """
 
 from __future__ import annotations
 
 import argparse
 import json
-import math
 import os
 import re
 import statistics
@@ -48,9 +50,9 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["trex", "reference"], default="trex")
-    ap.add_argument("--workload", choices=["ragged", "plain"], default="ragged")
+    ap.add_argument("--workload", choices=["ragged", "plain", "scan"], default="ragged")
     ap.add_argument("--strings", type=int, default=None, help="override the number of strings")
-    ap.add_argument("--seg-len", type=int, default=0)
+    ap.add_argument("--seg-len", type=int, default=0, help="bytes per work item / scan tile (0 = default)")
     ap.add_argument("--dfa-sizes", type=str, default=None,
                     help="comma list of DFA state counts replacing the default 5x8,5x12,6x16")
     ap.add_argument("--seed", type=int, default=2024)
@@ -62,57 +64,31 @@ def parse_args():
 
 
 # ---------------------------------------------------------------------------------
-# workload
+# workloads
 # ---------------------------------------------------------------------------------
 
-def workload_spec(kind: str, n_override=None):
-    if kind == "plain":
-        n = n_override or 4096
-        return dict(workload="plain DFA: N=16 random DFA over bytes ACGT, 4096 strings x 1024 bytes",
-                    n_strings=n, kind=kind)
-    n = n_override or 1_000_000
-    return dict(workload=("ragged DFA batch: 16 random DFAs (5x8, 5x12, 6x16 states) over 256 byte "
-                          "symbols; 1M strings, log-normal lengths median 2048 sigma 1.18 clipped "
-                          "[16, 65536]; 10% of strings over 'ACGT'; string i on DFA i mod 16"),
-                n_strings=n, kind=kind)
-
-
-def make_automata(kind: str, seed: int, sizes_override=None):
-    from trex_b200.workloads import ACGT, random_dfa
-    rng = np.random.default_rng(seed)
-    if kind == "plain":
-        return [random_dfa(16, ACGT, rng)]
-    sizes = (8,) * 5 + (12,) * 5 + (16,) * 6
-    if sizes_override:
-        base = [int(x) for x in sizes_override.split(",")]
-        sizes = [base[i % len(base)] for i in range(16)]
-    return [random_dfa(n, np.arange(256), rng) for n in sizes]
-
-
-def make_lengths(kind: str, n: int, seed: int):
+def lognormal_offsets(n: int, seed: int):
     from trex_b200.workloads import lognormal_lengths
     rng = np.random.default_rng(seed + 1)
-    if kind == "plain":
-        lens = np.full(n, 1024, dtype=np.int64)
-        is_sub = np.ones(n, dtype=bool)
-    else:
-        lens = lognormal_lengths(n, rng)
-        is_sub = np.zeros(n, dtype=bool)
-        is_sub[rng.choice(n, size=int(round(0.10 * n)), replace=False)] = True
-    off = np.zeros(n + 1, dtype=np.int64)
+    lens = lognormal_lengths(n, rng)
+    is_sub = np.zeros(n, dtype=bool)
+    is_sub[rng.choice(n, size=int(round(0.10 * n)), replace=False)] = True
+    return lens, is_sub
+
+
+def offsets_of(lens):
+    off = np.zeros(len(lens) + 1, dtype=np.int64)
     np.cumsum(lens, out=off[1:])
-    n_dfas = 1 if kind == "plain" else 16
-    ids = (np.arange(n) % n_dfas).astype(np.int32)
-    return lens, off, ids, is_sub
+    return off
 
 
-def make_device_bytes(torch, lens, is_sub, seed, device):
+def device_bytes(torch, lens, is_sub, seed, device):
     """Uniform random bytes; strings flagged is_sub are re-drawn over ACGT."""
     total = int(lens.sum())
     g = torch.Generator(device=device)
     g.manual_seed(seed + 2)
     data = torch.randint(0, 256, (max(total, 1),), dtype=torch.uint8, device=device, generator=g)
-    if is_sub.any():
+    if is_sub is not None and is_sub.any():
         acgt = torch.tensor(list(SUB_ALPHABET), dtype=torch.uint8, device=device)
         flag = torch.repeat_interleave(torch.from_numpy(is_sub).to(device),
                                        torch.from_numpy(lens).to(device))
@@ -122,18 +98,178 @@ def make_device_bytes(torch, lens, is_sub, seed, device):
     return data[:total]
 
 
-def make_host_bytes(lens, is_sub, seed):
+def host_bytes(lens, is_sub, seed):
     rng = np.random.default_rng(seed + 3)
     total = int(lens.sum())
     data = rng.integers(0, 256, size=total, dtype=np.uint8)
-    if is_sub.any():
-        off = np.zeros(len(lens) + 1, dtype=np.int64)
-        np.cumsum(lens, out=off[1:])
+    if is_sub is not None and is_sub.any():
+        off = offsets_of(lens)
         acgt = np.frombuffer(SUB_ALPHABET, dtype=np.uint8)
         for i in np.flatnonzero(is_sub):
             a, b = off[i], off[i + 1]
             data[a:b] = acgt[data[a:b] & 3]
     return data
+
+
+class DFAWorkload:
+    """ragged / plain / scan: byte DFAs over CSR strings."""
+
+    def __init__(self, args):
+        from trex_b200.workloads import ACGT, random_dfa
+        self.kind = args.workload
+        self.args = args
+        rng = np.random.default_rng(args.seed)
+        if self.kind == "plain":
+            self.n = args.strings or 4096
+            self.dfas = [random_dfa(16, ACGT, rng)]
+            self.lens = np.full(self.n, 1024, dtype=np.int64)
+            self.is_sub = np.ones(self.n, dtype=bool)
+            self.ids = np.zeros(self.n, dtype=np.int32)
+            self.workload = "plain DFA: N=16 random DFA over bytes ACGT, 4096 strings x 1024 bytes"
+        elif self.kind == "scan":
+            self.n = args.strings or 8
+            self.dfas = [random_dfa(16, np.arange(256), rng)]
+            self.lens = np.full(self.n, 1 << 28, dtype=np.int64)
+            self.is_sub = None
+            self.ids = np.zeros(self.n, dtype=np.int32)
+            self.workload = ("long-string scan: N=16 random DFA over 256 bytes, 8 strings x 256 MiB, "
+                             "state of every position written")
+        else:
+            self.n = args.strings or 1_000_000
+            sizes = (8,) * 5 + (12,) * 5 + (16,) * 6
+            if args.dfa_sizes:
+                base = [int(x) for x in args.dfa_sizes.split(",")]
+                sizes = [base[i % len(base)] for i in range(16)]
+            self.dfas = [random_dfa(n, np.arange(256), rng) for n in sizes]
+            self.lens, self.is_sub = None, None
+            self.ids = (np.arange(self.n) % 16).astype(np.int32)
+            self.workload = ("ragged DFA batch: 16 random DFAs (5x8, 5x12, 6x16 states) over 256 byte "
+                             "symbols; 1M strings, log-normal lengths median 2048 sigma 1.18 clipped "
+                             "[16, 65536]; 10% of strings over 'ACGT'; string i on DFA i mod 16")
+
+    def lengths(self, seed):
+        if self.lens is None:
+            return lognormal_offsets(self.n, seed)
+        return self.lens, self.is_sub
+
+    # ---- GPU side
+    def setup(self, torch, dev, seed):
+        from trex_b200.engine import DFASet
+        self.torch = torch
+        lens, is_sub = self.lengths(seed)
+        self.off = offsets_of(lens)
+        self.total = int(self.off[-1])
+        self.data = device_bytes(torch, lens, is_sub, seed, dev)
+        self.d_off = torch.from_numpy(self.off).to(dev)
+        self.d_ids = torch.from_numpy(self.ids).to(dev)
+        self.set = DFASet(self.dfas)
+        n = self.n
+        if self.kind == "scan":
+            self.scratch = torch.empty(DFASet.scan_scratch_bytes(n, self.total, self.args.seg_len),
+                                       dtype=torch.uint8, device=dev)
+            self.states = torch.empty(self.total, dtype=torch.uint8, device=dev)
+        else:
+            self.scratch = torch.empty(DFASet.scratch_bytes(n, self.total, self.args.seg_len),
+                                       dtype=torch.uint8, device=dev)
+        self.fs = torch.empty(n, dtype=torch.uint8, device=dev)
+        self.ac = torch.empty(n, dtype=torch.uint8, device=dev)
+
+    def step(self, stream):
+        if self.kind == "scan":
+            self.set.scan(self.data, self.d_off, 0, states=self.states, final_state=self.fs,
+                          accept=self.ac, scratch=self.scratch, tile_len=self.args.seg_len,
+                          stream=stream)
+        else:
+            self.set.run(self.data, self.d_off, self.d_ids, final_state=self.fs, accept=self.ac,
+                         scratch=self.scratch, seg_len=self.args.seg_len, stream=stream)
+
+    def error_word(self):
+        if self.kind == "scan":
+            return self.set.scan_error_word(self.scratch, self.n, self.total, self.args.seg_len)
+        return self.set.last_error_word(self.scratch)
+
+    @property
+    def chars(self):
+        return self.total
+
+    @property
+    def kernel(self):
+        return "dfa_scan_kernel" if self.kind == "scan" else "dfa_ragged_kernel"
+
+    @property
+    def alg_bytes(self):
+        # 1 B/char in (+1 B/char out for the scan) + 16 B per string
+        # (64-bit offset, automaton id, state, accept)
+        per_char = 2 if self.kind == "scan" else 1
+        return per_char * self.total + 16 * self.n
+
+    @property
+    def launches_per_step(self):
+        return 3 if self.kind == "scan" else 4
+
+    def config(self):
+        return {"workload": self.workload, "n_strings": self.n, "total_bytes_per_gpu": self.total,
+                "seg_len": self.args.seg_len or (8192 if self.kind == "scan" else 2048),
+                "l2": "inputs larger than L2 (126 MB), no flush" if self.total > 126e6 else
+                      "inputs smaller than L2: L2 flushed by a 256 MB write between steps"}
+
+    # ---- end to end (host buffers through the C ABI host entry point)
+    def e2e(self, torch, steps, dist, dev):
+        if self.kind == "scan":
+            return None
+        h_data = torch.empty(self.total, dtype=torch.uint8, pin_memory=True)
+        h_data.copy_(self.data)
+        h_off = torch.from_numpy(self.off).pin_memory()
+        h_ids = torch.from_numpy(self.ids).pin_memory()
+        h_fs = torch.empty(self.n, dtype=torch.uint8).pin_memory()
+        h_ac = torch.empty(self.n, dtype=torch.uint8).pin_memory()
+        hd, ho, hi, hf, ha = (h_data.numpy(), h_off.numpy(), h_ids.numpy(), h_fs.numpy(),
+                              h_ac.numpy())
+        self.set.run_host(hd, ho, hi, self.args.seg_len, hf, ha)   # warm the staging buffers
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            self.set.run_host(hd, ho, hi, self.args.seg_len, hf, ha)
+        dt = time.perf_counter() - t0
+        if dist:
+            t = torch.tensor([dt], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            dt = float(t.item())
+        if not (np.array_equal(hf, self.fs.cpu().numpy()) and np.array_equal(ha, self.ac.cpu().numpy())):
+            raise RuntimeError("host-buffer run disagrees with the device run")
+        self.host_data = hd
+        return dt, int(self.total + self.off.nbytes + self.ids.nbytes), int(2 * self.n + 4)
+
+    # ---- CPU (oracle) sample
+    def cpu_run(self, orc, data, k):
+        d = self.dfas
+        if self.kind == "scan":
+            orc.dfa_positions(d[0].tmap, d[0].n_states, d[0].start, data, self.off_cpu[:k + 1])
+        else:
+            orc.dfa_walk([x.tmap for x in d], [x.n_states for x in d], [x.start for x in d],
+                         [x.accept for x in d], data, self.off_cpu[:k + 1], self.ids[:k])
+
+    def cpu_sample(self, seed, seconds, threads):
+        """(k strings, their bytes, host data) sized to ~seconds of oracle work."""
+        from oracle import oracle as orc
+        lens, is_sub = self.lengths(seed)
+        if self.kind == "scan":
+            # per-position walk on a prefix of each string
+            per = max(1 << 16, int(seconds * 4e8 / max(1, len(lens))))
+            lens = np.minimum(lens, per)
+        self.off_cpu = offsets_of(lens)
+        rate_guess = 3e8 * threads
+        k0 = max(1, int(np.searchsorted(self.off_cpu, 0.05 * rate_guess, side="right")) - 1)
+        k0 = min(k0, len(lens))
+        data0 = host_bytes(lens[:k0], None if is_sub is None else is_sub[:k0], seed)
+        t0 = time.perf_counter()
+        self.cpu_run(orc, data0, k0)
+        rate = self.off_cpu[k0] / max(time.perf_counter() - t0, 1e-6)
+        k = max(1, min(len(lens), int(np.searchsorted(self.off_cpu, seconds * rate, side="right")) - 1))
+        data = host_bytes(lens[:k], None if is_sub is None else is_sub[:k], seed)
+        return k, int(self.off_cpu[k]), data
 
 
 # ---------------------------------------------------------------------------------
@@ -204,10 +340,6 @@ def gpu_index_for(local_rank: int) -> str:
     return str(local_rank)
 
 
-# ---------------------------------------------------------------------------------
-# helpers
-# ---------------------------------------------------------------------------------
-
 def measured_peaks():
     p = REPO / "MEASURED_PEAKS.json"
     if p.exists():
@@ -226,78 +358,46 @@ def committed_traffic(kernel: str, workload: str):
     return None
 
 
-def cpu_sample(off, seconds_budget, rate_guess_bps):
-    """Number of leading strings whose bytes take about `seconds_budget` at
-    `rate_guess_bps`."""
-    target = seconds_budget * rate_guess_bps
-    k = int(np.searchsorted(off, target, side="right")) - 1
-    return max(1, min(k, len(off) - 1))
-
-
-def run_cpu_baseline(dfas, data_host, off, ids, budget_s):
-    from oracle import oracle as orc
-    orc.build()
-    threads = orc.threads()
-    # calibrate on ~0.05 s of work, then run the bounded sample
-    k0 = cpu_sample(off, 0.05, 3e8 * threads)
-    t0 = time.perf_counter()
-    orc.dfa_walk([d.tmap for d in dfas], [d.n_states for d in dfas], [d.start for d in dfas],
-                 [d.accept for d in dfas], data_host[:off[k0]], off[:k0 + 1], ids[:k0])
-    rate = off[k0] / max(time.perf_counter() - t0, 1e-6)
-    k = cpu_sample(off, budget_s, rate)
-    t0 = time.perf_counter()
-    orc.dfa_walk([d.tmap for d in dfas], [d.n_states for d in dfas], [d.start for d in dfas],
-                 [d.accept for d in dfas], data_host[:off[k]], off[:k + 1], ids[:k])
-    dt = time.perf_counter() - t0
-    chars = int(off[k])
-    return {"value": chars / dt / 1e9, "unit": "Gchar/s", "cores": threads, "kind": "port",
-            "sample": f"first {k} strings ({chars} bytes) of the same workload, OpenMP over {threads} threads"}
-
-
 # ---------------------------------------------------------------------------------
 # arms
 # ---------------------------------------------------------------------------------
 
+def base_line(args, wl, value, ms_per_step, steps, warmup, world):
+    return {
+        "metric": METRIC, "value": value, "unit": "Gchar/s", "n_gpus": world, "steps": steps,
+        "warmup": warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic (seeded, generated on the device)",
+    }
+
+
 def reference_arm(args, rank):
     if rank != 0:
         return
-    spec = workload_spec(args.workload, args.strings)
-    dfas = make_automata(args.workload, args.seed, args.dfa_sizes)
-    lens, off, ids, is_sub = make_lengths(args.workload, spec["n_strings"], args.seed)
     from oracle import oracle as orc
     orc.build()
     threads = orc.threads()
-    # per-step sample sized so warmup + steps fit the CPU budget
+    wl = DFAWorkload(args)
     n_runs = max(1, args.steps + args.warmup)
-    # host bytes for a generous prefix only
-    calib_k = cpu_sample(off, 0.02, 3e8 * threads)
-    sample_data = make_host_bytes(lens[:calib_k], is_sub[:calib_k], args.seed)
-    t0 = time.perf_counter()
-    orc.dfa_walk([d.tmap for d in dfas], [d.n_states for d in dfas], [0] * len(dfas),
-                 [d.accept for d in dfas], sample_data, off[:calib_k + 1], ids[:calib_k])
-    rate = off[calib_k] / max(time.perf_counter() - t0, 1e-6)
-    per_step_s = max(0.05, min(2.0, (max(args.cpu_seconds, 30.0)) / n_runs))
-    k = cpu_sample(off, per_step_s, rate)
-    data = make_host_bytes(lens[:k], is_sub[:k], args.seed)
+    per_step = max(0.02, min(2.0, max(args.cpu_seconds, 30.0) / n_runs))
+    k, chars, data = wl.cpu_sample(args.seed, per_step, threads)
     times = []
     for step in range(n_runs):
         t0 = time.perf_counter()
-        orc.dfa_walk([d.tmap for d in dfas], [d.n_states for d in dfas], [0] * len(dfas),
-                     [d.accept for d in dfas], data, off[:k + 1], ids[:k])
+        wl.cpu_run(orc, data, k)
         dt = time.perf_counter() - t0
         if step >= args.warmup:
             times.append(dt)
-    chars = int(off[k])
     tot = sum(times)
     value = chars * len(times) / tot / 1e9
     sample = (f"first {k} strings ({chars} bytes) of the workload per step, C oracle "
-              f"(restatement of DFA.simulate over the byte map) with OpenMP over {threads} threads")
+              f"(restatement of the reference's walk) with OpenMP over {threads} threads")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "Gchar/s",
         "n_gpus": args.gpus, "steps": len(times), "warmup": args.warmup,
         "ms_per_step": tot / len(times) * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded, same generator as the trex arm)",
-        "config": {**{k_: v for k_, v in spec.items() if k_ != "kind"}, "parallelism": "cpu"},
+        "config": {"workload": wl.workload, "n_strings": wl.n, "parallelism": "cpu"},
         "cpu_baseline": {"value": value, "unit": "Gchar/s", "cores": threads, "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": "Gchar/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -308,36 +408,25 @@ def reference_arm(args, rank):
 
 def trex_arm(args, rank, world, local_rank):
     import torch
-    from trex_b200.engine import DFASet, profile_begin, profile_end
+    from trex_b200.engine import profile_begin, profile_end
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
     dist = None
     if world > 1:
         import torch.distributed as dist
-    spec = workload_spec(args.workload, args.strings)
     seed = args.seed + 7919 * rank
-    dfas = make_automata(args.workload, args.seed, args.dfa_sizes)
-    lens, off, ids, is_sub = make_lengths(args.workload, spec["n_strings"], seed)
-    data = make_device_bytes(torch, lens, is_sub, seed, dev)
-    d_off = torch.from_numpy(off).to(dev)
-    d_ids = torch.from_numpy(ids).to(dev)
-    n = spec["n_strings"]
-    total = int(off[-1])
-    s = DFASet(dfas)
-    scratch = torch.empty(DFASet.scratch_bytes(n, total, args.seg_len), dtype=torch.uint8, device=dev)
-    fs = torch.empty(n, dtype=torch.uint8, device=dev)
-    ac = torch.empty(n, dtype=torch.uint8, device=dev)
+    wl = DFAWorkload(args)
+    wl.setup(torch, dev, seed)
     stream = torch.cuda.current_stream(dev)
-
-    def step():
-        s.run(data, d_off, d_ids, final_state=fs, accept=ac, scratch=scratch, seg_len=args.seg_len,
-              stream=stream)
-
-    for _ in range(max(3, args.warmup)):
-        step()
+    flush = None
+    if wl.chars < 126e6:
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    warm = max(3, args.warmup)
+    for _ in range(warm):
+        wl.step(stream)
     torch.cuda.synchronize()
-    if s.last_error_word(scratch) != 0:
-        raise RuntimeError("device reported malformed input")
+    if wl.error_word() != 0:
+        raise RuntimeError("device reported malformed input or a look-back timeout")
     clocks = ClockSampler(gpu_index_for(local_rank))
     clocks.start()
     time.sleep(0.3)
@@ -349,87 +438,63 @@ def trex_arm(args, rank, world, local_rank):
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     for _ in range(args.steps):
-        step()
+        if flush is not None:
+            flush.fill_(1)
+        wl.step(stream)
     ev1.record(stream)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     kern_ms = profile_end(args.steps)
     clock_info = clocks.stop()
+    if wl.error_word() != 0:
+        raise RuntimeError("device reported an error during the timed steps")
     ms = ev0.elapsed_time(ev1)
-    t_max = ms
     if dist:
         t = torch.tensor([ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
-    ms_per_step = t_max / args.steps
-    chars_all = total * world
+        ms = float(t.item())
+    ms_per_step = ms / args.steps
+    chars_all = wl.chars * world
     value = chars_all / (ms_per_step * 1e-3) / 1e9
 
-    # roofline of the dominant kernel (dfa_ragged_kernel)
     peak, peak_kind = measured_peaks()
-    alg_bytes = total + 16 * n
     kmean = sum(kern_ms) / max(1, len(kern_ms))
-    achieved = alg_bytes / (kmean * 1e-3) / 1e9
-    traffic = committed_traffic("dfa_ragged_kernel", args.workload)
+    achieved = wl.alg_bytes / (kmean * 1e-3) / 1e9
+    traffic = committed_traffic(wl.kernel, args.workload)
 
-    # end to end through the host-buffer C ABI entry point (pinned buffers)
     e2e = None
-    if rank == 0 or world > 1:
-        h_data = torch.empty(total, dtype=torch.uint8, pin_memory=True)
-        h_data.copy_(data)
-        h_off = torch.from_numpy(off).pin_memory()
-        h_ids = torch.from_numpy(ids).pin_memory()
-        h_fs = torch.empty(n, dtype=torch.uint8).pin_memory()
-        h_ac = torch.empty(n, dtype=torch.uint8).pin_memory()
-        hd, ho, hi, hf, ha = (h_data.numpy(), h_off.numpy(), h_ids.numpy(), h_fs.numpy(), h_ac.numpy())
-        s.run_host(hd, ho, hi, args.seg_len, hf, ha)  # warm the staging buffers
-        torch.cuda.synchronize()
-        if dist:
-            dist.barrier()
-        t0 = time.perf_counter()
-        for _ in range(args.e2e_steps):
-            s.run_host(hd, ho, hi, args.seg_len, hf, ha)
-        dt = time.perf_counter() - t0
-        if dist:
-            t = torch.tensor([dt], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            dt = float(t.item())
-        if not (np.array_equal(hf, fs.cpu().numpy()) and np.array_equal(ha, ac.cpu().numpy())):
-            raise RuntimeError("host-buffer run disagrees with the device run")
+    res = wl.e2e(torch, args.e2e_steps, dist, dev)
+    if res is not None:
+        dt, h2d, d2h = res
         e2e = {"value": chars_all * args.e2e_steps / dt / 1e9, "unit": "Gchar/s",
-               "h2d_bytes_per_step": int(total + off.nbytes + ids.nbytes),
-               "d2h_bytes_per_step": int(2 * n + 4)}
-        cpu_data = hd
-    else:
-        cpu_data = None
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = run_cpu_baseline(dfas, cpu_data, off, ids, args.cpu_seconds)
+        from oracle import oracle as orc
+        orc.build()
+        threads = orc.threads()
+        k, chars, data = wl.cpu_sample(seed, args.cpu_seconds, threads)
+        t0 = time.perf_counter()
+        wl.cpu_run(orc, data, k)
+        dt = time.perf_counter() - t0
+        cpu = {"value": chars / dt / 1e9, "unit": "Gchar/s", "cores": threads, "kind": "port",
+               "sample": f"first {k} strings ({chars} bytes) of the same workload, OpenMP over {threads} threads"}
 
     if rank == 0:
-        line = {
-            "metric": METRIC, "value": value, "unit": "Gchar/s", "n_gpus": world,
-            "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms_per_step,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
-            "data": "synthetic (seeded, generated on the device)",
-            "config": {**{k: v for k, v in spec.items() if k != "kind"},
-                       "total_bytes_per_gpu": total, "seg_len": args.seg_len or 8192,
-                       "l2": "inputs (>= 4 GB) larger than L2, no flush",
-                       "parallelism": f"dp{world} (independent shards, no collective)"},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "dfa_ragged_kernel", "kernel_ms_mean": kmean,
-                         "algorithmic_bytes_per_launch": alg_bytes,
-                         "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})"},
-            "e2e": e2e,
-            "cpu_baseline": cpu,
-            "gpu_launches": 4 * args.steps,
-            "clocks": clock_info,
-        }
+        line = base_line(args, wl, value, ms_per_step, args.steps, warm, world)
+        line["config"] = {**wl.config(), "parallelism": f"dp{world} (independent shards, no collective)"}
+        line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                            "frac": achieved / peak, "traffic": traffic, "kernel": wl.kernel,
+                            "kernel_ms_mean": kmean, "algorithmic_bytes_per_launch": wl.alg_bytes,
+                            "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})"}
+        line["e2e"] = e2e
+        line["cpu_baseline"] = cpu
+        line["gpu_launches"] = wl.launches_per_step * args.steps
+        line["clocks"] = clock_info
         print(json.dumps(line), flush=True)
-    s.close()
+    wl.set.close()
 
 
 def main():

@@ -165,6 +165,24 @@ int trex_dfa_batch_host(trex_dfa_set *set, const uint8_t *h_data, const int64_t 
                         uint8_t *h_final_state, uint8_t *h_accept, int32_t *h_accept_i32,
                         int32_t seg_len, float *kernel_ms, float *total_ms);
 
+/* Per-position states (the reference's prefix products,
+ * src/simulation.py:142-153, evaluated on the start state): states[p] = the
+ * state after byte p of its string, for every byte of the batch (DEVICE
+ * buffers; states has total_bytes bytes and the same layout as data). Also
+ * final_state[n] / accept[n] (each may be NULL). Automaton dfa_index of the
+ * set must have at most 16 states. Long strings are split into tiles of
+ * tile_len bytes (0 = default) scanned in one pass with a decoupled
+ * look-back. scratch: trex_dfa_scan_scratch_bytes bytes (required). */
+int64_t trex_dfa_scan_scratch_bytes(int64_t n_strings, int64_t total_bytes, int32_t tile_len);
+int trex_dfa_scan_run(trex_dfa_set *set, int dfa_index, const uint8_t *data,
+                      const int64_t *offsets, int64_t n_strings, int64_t total_bytes,
+                      uint8_t *states, uint8_t *final_state, uint8_t *accept, void *scratch,
+                      int64_t scratch_bytes, int32_t tile_len, void *stream);
+/* Error word of the last scan that used `scratch` (same sizes as the run):
+ * bit 0 malformed offsets, bit 2 a look-back wait ran out. Synchronises. */
+int trex_dfa_scan_error(void *scratch, int64_t n_strings, int64_t total_bytes, int32_t tile_len,
+                        int32_t *err_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -62,6 +62,12 @@ SIGNATURES = {
                                           c_vp, c_vp, c_vp, c_vp, ctypes.c_int64, ctypes.c_int32,
                                           c_vp]),
     "trex_dfa_batch_error": (ctypes.c_int, [c_vp, c_vp, c_i32p]),
+    "trex_dfa_scan_scratch_bytes": (ctypes.c_int64, [ctypes.c_int64, ctypes.c_int64, ctypes.c_int32]),
+    "trex_dfa_scan_run": (ctypes.c_int, [c_vp, ctypes.c_int, c_vp, c_vp, ctypes.c_int64,
+                                         ctypes.c_int64, c_vp, c_vp, c_vp, c_vp, ctypes.c_int64,
+                                         ctypes.c_int32, c_vp]),
+    "trex_dfa_scan_error": (ctypes.c_int, [c_vp, ctypes.c_int64, ctypes.c_int64, ctypes.c_int32,
+                                           c_i32p]),
     "trex_dfa_batch_host": (ctypes.c_int, [c_vp, c_u8p, c_i64p, c_i32p, ctypes.c_int64,
                                            ctypes.c_int64, c_u8p, c_u8p, c_i32p, ctypes.c_int32,
                                            c_f32p, c_f32p]),

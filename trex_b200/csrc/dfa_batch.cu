@@ -773,6 +773,24 @@ int trex_dfa_batch_host(trex_dfa_set *set, const uint8_t *h_data, const int64_t 
     return TREX_OK;
 }
 
+}  // extern "C"
+
+namespace trex {
+int dfa_set_table(const trex_dfa_set *set, int index, int *n_states, int *start,
+                  const uint8_t **tmap, const uint8_t **accept, int *n_sms) {
+    if (!set) return TREX_ERR_NOT_INIT;
+    if (index < 0 || index >= set->n_dfas) return TREX_ERR_ARG;
+    *n_states = set->n_states[index];
+    *start = set->starts[index];
+    *tmap = set->d_tmaps + set->tmap_off[index];
+    *accept = set->d_accepts + set->accept_off[index];
+    *n_sms = set->n_sms;
+    return TREX_OK;
+}
+}  // namespace trex
+
+extern "C" {
+
 int trex_dfa_batch_error(trex_dfa_set *set, void *scratch, int32_t *err_out) {
     // Error word of the last trex_dfa_batch_run that used `scratch` (NULL =
     // the set's own scratch); synchronises with the device.

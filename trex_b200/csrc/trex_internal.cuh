@@ -42,6 +42,14 @@ __device__ __forceinline__ uint4 ld_stream16(const void *p) {
     return v;
 }
 
+// Streaming 32-byte load (two halves returned as uint4).
+__device__ __forceinline__ void ld_stream32(const void *p, uint4 &lo, uint4 &hi) {
+    asm volatile("ld.global.nc.L1::no_allocate.L2::256B.v8.u32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(lo.x), "=r"(lo.y), "=r"(lo.z), "=r"(lo.w),
+                   "=r"(hi.x), "=r"(hi.y), "=r"(hi.z), "=r"(hi.w)
+                 : "l"(p));
+}
+
 __device__ __forceinline__ void prefetch_l2(const void *p) {
     asm volatile("prefetch.global.L2 [%0];" :: "l"(p));
 }

@@ -106,6 +106,41 @@ class DFASet:
         _lib.check(rc, "trex_dfa_batch_run")
         return final_state, accept, accept_i32
 
+    @staticmethod
+    def scan_scratch_bytes(n_strings: int, total_bytes: int, tile_len: int = 0) -> int:
+        return int(_lib.load().trex_dfa_scan_scratch_bytes(n_strings, total_bytes, tile_len))
+
+    def scan(self, data, offsets, dfa_index: int = 0, *, states=None, final_state=None,
+             accept=None, scratch=None, tile_len: int = 0, stream=None):
+        """Per-position states of every string (device tensors). Returns
+        (states[total_bytes], final_state[n], accept[n], scratch)."""
+        torch = _torch()
+        n = offsets.numel() - 1
+        dev = offsets.device
+        total = data.numel()
+        if states is None:
+            states = torch.empty(max(total, 1), dtype=torch.uint8, device=dev)
+        if final_state is None:
+            final_state = torch.empty(max(n, 1), dtype=torch.uint8, device=dev)
+        if accept is None:
+            accept = torch.empty(max(n, 1), dtype=torch.uint8, device=dev)
+        need = self.scan_scratch_bytes(n, total, tile_len)
+        if scratch is None or scratch.numel() < need:
+            scratch = torch.empty(need, dtype=torch.uint8, device=dev)
+        rc = self.lib.trex_dfa_scan_run(self._h, dfa_index, _dptr(data), _dptr(offsets), n, total,
+                                        _dptr(states), _dptr(final_state), _dptr(accept),
+                                        _dptr(scratch), scratch.numel(), tile_len,
+                                        _stream_handle(stream))
+        _lib.check(rc, "trex_dfa_scan_run")
+        return states[:total], final_state[:n], accept[:n], scratch
+
+    def scan_error_word(self, scratch, n_strings: int, total_bytes: int, tile_len: int = 0) -> int:
+        v = ctypes.c_int32(0)
+        rc = self.lib.trex_dfa_scan_error(_dptr(scratch), n_strings, total_bytes, tile_len,
+                                          ctypes.byref(v))
+        _lib.check(rc, "trex_dfa_scan_error")
+        return v.value
+
     def last_error_word(self, scratch=None) -> int:
         v = ctypes.c_int32(0)
         rc = self.lib.trex_dfa_batch_error(self._h, _dptr(scratch), ctypes.byref(v))
