@@ -12,6 +12,8 @@ Workloads (synthetic, seeded; the reference ships no dataset):
   plain: one random 16-state DFA over the bytes "ACGT", 4096 x 1024 bytes.
   scan: one random 16-state DFA over 256 bytes, 8 strings x 256 MiB; one step
       writes the state of every position (2 bytes moved per character).
+  nfa: random 64-state Boolean NFA over 20 symbols (bytes 0..19), per-symbol
+      edge density 0.05, 256K strings x 4096 symbols, bit-parallel kernel.
 
 Multi-GPU: one process per GPU (torchrun); every rank runs its own seeded
 batch (weak scaling, no data-path collective); times are the max over ranks
@@ -50,7 +52,7 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["trex", "reference"], default="trex")
-    ap.add_argument("--workload", choices=["ragged", "plain", "scan"], default="ragged")
+    ap.add_argument("--workload", choices=["ragged", "plain", "scan", "nfa"], default="ragged")
     ap.add_argument("--strings", type=int, default=None, help="override the number of strings")
     ap.add_argument("--seg-len", type=int, default=0, help="bytes per work item / scan tile (0 = default)")
     ap.add_argument("--dfa-sizes", type=str, default=None,
@@ -272,6 +274,108 @@ class DFAWorkload:
         return k, int(self.off_cpu[k]), data
 
 
+class NFAWorkload:
+    """Boolean NFA, 64 states, 20 symbols (bit-parallel kernel)."""
+
+    kind = "nfa"
+    kernel = "nfa_bitpar_kernel"
+    launches_per_step = 1
+
+    def __init__(self, args):
+        from trex_b200.workloads import random_bool_nfa
+        self.args = args
+        rng = np.random.default_rng(args.seed)
+        self.T, self.start, self.acc = random_bool_nfa(rng, n_states=64, sigma=20, density=0.05)
+        self.n = args.strings or 262144
+        self.L = 4096
+        self.off = np.arange(self.n + 1, dtype=np.int64) * self.L
+        self.workload = ("Boolean NFA: random 64-state NFA over 20 symbols (bytes 0..19), edge density "
+                         "0.05, 256K strings x 4096 symbols")
+
+    def setup(self, torch, dev, seed):
+        from trex_b200.engine import NFA
+        self.torch = torch
+        self.total = self.n * self.L
+        self.off = np.arange(self.n + 1, dtype=np.int64) * self.L
+        g = torch.Generator(device=dev)
+        g.manual_seed(seed + 2)
+        self.data = torch.randint(0, 20, (self.total,), dtype=torch.uint8, device=dev, generator=g)
+        self.d_off = torch.from_numpy(self.off).to(dev)
+        self.nfa = NFA(self.T, self.start, self.acc, unknown_rejects=True)
+        self.fm = torch.empty(self.n, dtype=torch.int64, device=dev)
+        self.ac = torch.empty(self.n, dtype=torch.uint8, device=dev)
+        self.set = self.nfa
+
+    def step(self, stream):
+        self.nfa.run(self.data, self.d_off, final_mask=self.fm, accept=self.ac, stream=stream)
+
+    def error_word(self):
+        return self.nfa.error_word()
+
+    @property
+    def chars(self):
+        return self.total
+
+    @property
+    def alg_bytes(self):
+        return self.total + 17 * self.n
+
+    def config(self):
+        return {"workload": self.workload, "n_strings": self.n, "total_bytes_per_gpu": self.total,
+                "useful_ops_per_char": 2 * 64 * 64, "kernel_bound": "integer ALU / shared-memory lookups",
+                "l2": "inputs larger than L2 (126 MB), no flush"}
+
+    def e2e(self, torch, steps, dist, dev):
+        import ctypes
+        from trex_b200 import _lib
+        L = _lib.load()
+        Tf = np.ascontiguousarray(self.T.astype(np.float32))
+        st = np.ascontiguousarray(self.start.astype(np.float32))
+        ac = np.ascontiguousarray(self.acc.astype(np.float32))
+        f32 = ctypes.c_float
+        _lib.check(L.nfa_tc_engine_init(_lib.ptr(Tf, f32), _lib.ptr(ac, f32), _lib.ptr(st, f32), 64,
+                                        20, self.n, self.L), "nfa_tc_engine_init")
+        h_data = torch.empty(self.total, dtype=torch.uint8, pin_memory=True)
+        h_data.copy_(self.data)
+        h_off = torch.from_numpy(self.off.astype(np.int32)).pin_memory()
+        h_res = torch.empty(self.n, dtype=torch.int32).pin_memory()
+        hd, ho, hr = h_data.numpy(), h_off.numpy(), h_res.numpy()
+        km, tm = ctypes.c_float(), ctypes.c_float()
+        args = (_lib.ptr(hd, ctypes.c_uint8), _lib.ptr(ho, ctypes.c_int), _lib.ptr(hr, ctypes.c_int),
+                self.n, self.total, ctypes.byref(km), ctypes.byref(tm))
+        _lib.check(L.nfa_tc_engine_dispatch(*args), "nfa_tc_engine_dispatch")
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            _lib.check(L.nfa_tc_engine_dispatch(*args), "nfa_tc_engine_dispatch")
+        dt = time.perf_counter() - t0
+        if dist:
+            t = torch.tensor([dt], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            dt = float(t.item())
+        L.nfa_tc_engine_destroy()
+        if not np.array_equal(hr.astype(np.uint8), self.ac.cpu().numpy()):
+            raise RuntimeError("host-buffer run disagrees with the device run")
+        self.host_data = hd
+        return dt, int(self.total + ho.nbytes), int(hr.nbytes)
+
+    def cpu_run(self, orc, data, k):
+        orc.nfa_bool(self.T, self.start, self.acc, data, self.off[:k + 1], unknown_rejects=True)
+
+    def cpu_sample(self, seed, seconds, threads):
+        from oracle import oracle as orc
+        rng = np.random.default_rng(seed + 3)
+        k0 = max(1, min(self.n, threads * 4))
+        data0 = rng.integers(0, 20, size=k0 * self.L, dtype=np.uint8)
+        t0 = time.perf_counter()
+        self.cpu_run(orc, data0, k0)
+        rate = k0 * self.L / max(time.perf_counter() - t0, 1e-6)
+        k = max(1, min(self.n, int(seconds * rate / self.L)))
+        data = rng.integers(0, 20, size=k * self.L, dtype=np.uint8)
+        return k, k * self.L, data
+
+
 # ---------------------------------------------------------------------------------
 # clocks
 # ---------------------------------------------------------------------------------
@@ -362,6 +466,10 @@ def committed_traffic(kernel: str, workload: str):
 # arms
 # ---------------------------------------------------------------------------------
 
+def make_workload(args):
+    return NFAWorkload(args) if args.workload == "nfa" else DFAWorkload(args)
+
+
 def base_line(args, wl, value, ms_per_step, steps, warmup, world):
     return {
         "metric": METRIC, "value": value, "unit": "Gchar/s", "n_gpus": world, "steps": steps,
@@ -377,7 +485,7 @@ def reference_arm(args, rank):
     from oracle import oracle as orc
     orc.build()
     threads = orc.threads()
-    wl = DFAWorkload(args)
+    wl = make_workload(args)
     n_runs = max(1, args.steps + args.warmup)
     per_step = max(0.02, min(2.0, max(args.cpu_seconds, 30.0) / n_runs))
     k, chars, data = wl.cpu_sample(args.seed, per_step, threads)
@@ -415,7 +523,7 @@ def trex_arm(args, rank, world, local_rank):
     if world > 1:
         import torch.distributed as dist
     seed = args.seed + 7919 * rank
-    wl = DFAWorkload(args)
+    wl = make_workload(args)
     wl.setup(torch, dev, seed)
     stream = torch.cuda.current_stream(dev)
     flush = None

@@ -183,6 +183,22 @@ int trex_dfa_scan_run(trex_dfa_set *set, int dfa_index, const uint8_t *data,
 int trex_dfa_scan_error(void *scratch, int64_t n_strings, int64_t total_bytes, int32_t tile_len,
                         int32_t *err_out);
 
+/* ---- Boolean NFA (<= 64 states), bit-parallel --------------------------- */
+typedef struct trex_nfa trex_nfa;
+/* cols[c*64 + j] = destination mask of source state j on symbol c (epsilon
+ * closure folded in), c < sigma <= 255. Bytes >= sigma are skipped
+ * (unknown_rejects = 0, the reference C engine) or make the string reject
+ * with an empty final mask (unknown_rejects = 1, Python simulate_nfa). */
+int trex_nfa_create(int n_states, int sigma, const uint64_t *cols, uint64_t start_mask,
+                    uint64_t accept_mask, int unknown_rejects, trex_nfa **out);
+void trex_nfa_destroy(trex_nfa *nfa);
+/* DEVICE buffers; final_mask[n] (uint64), accept[n], accept_i32[n] may each be NULL. */
+int trex_nfa_run(trex_nfa *nfa, const uint8_t *data, const int64_t *offsets, int64_t n_strings,
+                 int64_t total_bytes, uint64_t *final_mask, uint8_t *accept, int32_t *accept_i32,
+                 void *stream);
+/* Error word of the last run (bit 0: malformed offsets). Synchronises. */
+int trex_nfa_error(trex_nfa *nfa, int32_t *err_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -53,6 +53,17 @@ SIGNATURES = {
     "monoid_engine_dispatch_batch": (ctypes.c_int, [c_u16p, c_intp, c_intp, ctypes.c_int, ctypes.c_int,
                                                     c_f32p, c_f32p]),
     "monoid_engine_device_check": (ctypes.c_int, []),
+    "nfa_tc_engine_init": (ctypes.c_int, [c_f32p, c_f32p, c_f32p, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_int, ctypes.c_int]),
+    "nfa_tc_engine_dispatch": (ctypes.c_int, [c_u8p, c_intp, c_intp, ctypes.c_int, ctypes.c_int,
+                                              c_f32p, c_f32p]),
+    "nfa_tc_engine_destroy": (None, []),
+    "trex_nfa_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, c_u64p, ctypes.c_uint64,
+                                       ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(c_vp)]),
+    "trex_nfa_destroy": (None, [c_vp]),
+    "trex_nfa_run": (ctypes.c_int, [c_vp, c_vp, c_vp, ctypes.c_int64, ctypes.c_int64, c_vp, c_vp,
+                                    c_vp, c_vp]),
+    "trex_nfa_error": (ctypes.c_int, [c_vp, c_i32p]),
     # handle API
     "trex_dfa_set_create": (ctypes.c_int, [ctypes.c_int, c_i32p, c_i32p, c_u8p, c_u8p,
                                            ctypes.POINTER(c_vp)]),

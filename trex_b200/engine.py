@@ -166,3 +166,68 @@ class DFASet:
             ctypes.byref(km), ctypes.byref(tm))
         _lib.check(rc, "trex_dfa_batch_host")
         return fs, ac, km.value, tm.value
+
+
+def nfa_columns(T) -> np.ndarray:
+    """Dense Boolean T[sigma, N, N] (row = destination, column = source),
+    N <= 64 -> uint64 cols[sigma * 64] with cols[c*64 + src] = destination mask."""
+    T = np.asarray(T) != 0
+    sigma, N, _ = T.shape
+    cols = np.zeros((sigma, 64), dtype=np.uint64)
+    w = np.left_shift(np.uint64(1), np.arange(N, dtype=np.uint64))
+    for c in range(sigma):
+        cols[c, :N] = np.bitwise_or.reduce(np.where(T[c], w[:, None], np.uint64(0)), axis=0)
+    return np.ascontiguousarray(cols.reshape(-1))
+
+
+def mask_of(vec) -> int:
+    m = 0
+    for b in np.flatnonzero(np.asarray(vec)).tolist():
+        m |= 1 << b
+    return m
+
+
+class NFA:
+    """Resident Boolean NFA with at most 64 states (bit-parallel kernel)."""
+
+    def __init__(self, T, start_vec, accept_vec, unknown_rejects: bool = True):
+        self.lib = _lib.load()
+        T = np.asarray(T)
+        self.sigma, self.n_states, _ = T.shape
+        cols = nfa_columns(T)
+        h = ctypes.c_void_p()
+        rc = self.lib.trex_nfa_create(self.n_states, self.sigma, _lib.ptr(cols, ctypes.c_uint64),
+                                      mask_of(start_vec), mask_of(accept_vec),
+                                      1 if unknown_rejects else 0, ctypes.byref(h))
+        _lib.check(rc, "trex_nfa_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.trex_nfa_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, data, offsets, *, final_mask=None, accept=None, stream=None):
+        """Device run: returns (final_mask int64 tensor [n] (bit pattern of the
+        uint64 mask), accept uint8 tensor [n])."""
+        torch = _torch()
+        n = offsets.numel() - 1
+        if final_mask is None:
+            final_mask = torch.empty(max(n, 1), dtype=torch.int64, device=offsets.device)
+        if accept is None:
+            accept = torch.empty(max(n, 1), dtype=torch.uint8, device=offsets.device)
+        rc = self.lib.trex_nfa_run(self._h, _dptr(data), _dptr(offsets), n, data.numel(),
+                                   _dptr(final_mask), _dptr(accept), None, _stream_handle(stream))
+        _lib.check(rc, "trex_nfa_run")
+        return final_mask[:n], accept[:n]
+
+    def error_word(self) -> int:
+        v = ctypes.c_int32(0)
+        _lib.check(self.lib.trex_nfa_error(self._h, ctypes.byref(v)), "trex_nfa_error")
+        return v.value
