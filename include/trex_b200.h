@@ -156,6 +156,29 @@ int trex_dfa_batch_run(trex_dfa_set *set, const uint8_t *data, const int64_t *of
  * id out of range (the affected strings were skipped). Synchronises. */
 int trex_dfa_batch_error(trex_dfa_set *set, void *scratch, int32_t *err_out);
 
+/* The same device-pointer batch without any allocation (no counterpart in the
+ * reference). Some callers cannot allocate device memory while they run: a
+ * process whose device memory belongs to another allocator (a framework's
+ * caching allocator, a memory pool with a fixed budget), a real-time serving
+ * loop that must not enter the driver's allocator (cudaMalloc / cudaFree can
+ * synchronise the device). This entry point takes no scratch argument: its
+ * scratch is a
+ * file-scope device array of 8 MiB (every GPU that loads the library holds it
+ * until the process exits), so a batch whose trex_dfa_batch_scratch_bytes is
+ * above 8 MiB is refused with TREX_ERR_CAPACITY (about 200K strings at the
+ * default segment length). The caller still passes inputs and outputs. The
+ * first call on each device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * Every call on a device shares the one array and it keeps the last call's
+ * contents (the counters it needs zeroed are cleared at the start of each
+ * call), so calls whose work overlaps on the GPU -- different streams, or
+ * other host threads -- race: serialise them. Strings with malformed offsets
+ * are skipped (their outputs are not written). */
+int trex_dfa_batch_run_static(trex_dfa_set *set, const uint8_t *data, const int64_t *offsets,
+                              const int32_t *dfa_id, int64_t n_strings, int64_t total_bytes,
+                              uint8_t *final_state, uint8_t *accept, int32_t *accept_i32,
+                              int32_t seg_len, void *stream);
+
 /* The same batch from HOST buffers (64-bit offsets): copies the inputs in,
  * runs, copies the requested outputs (each may be NULL) back and reports
  * kernel_ms (device work) and total_ms (copies + device work). Device staging

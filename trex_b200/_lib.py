@@ -73,6 +73,9 @@ SIGNATURES = {
                                           c_vp, c_vp, c_vp, c_vp, ctypes.c_int64, ctypes.c_int32,
                                           c_vp]),
     "trex_dfa_batch_error": (ctypes.c_int, [c_vp, c_vp, c_i32p]),
+    "trex_dfa_batch_run_static": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, ctypes.c_int64,
+                                                 ctypes.c_int64, c_vp, c_vp, c_vp, ctypes.c_int32,
+                                                 c_vp]),
     "trex_dfa_scan_scratch_bytes": (ctypes.c_int64, [ctypes.c_int64, ctypes.c_int64, ctypes.c_int32]),
     "trex_dfa_scan_run": (ctypes.c_int, [c_vp, ctypes.c_int, c_vp, c_vp, ctypes.c_int64,
                                          ctypes.c_int64, c_vp, c_vp, c_vp, c_vp, ctypes.c_int64,

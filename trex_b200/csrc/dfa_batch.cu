@@ -31,6 +31,7 @@
 //    stall the warp. No spin-waits anywhere.
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -819,3 +820,70 @@ int trex_dfa_batch_run(trex_dfa_set *set, const uint8_t *data, const int64_t *of
 }
 
 }  // extern "C"
+
+// ---- batch with statically allocated scratch ------------------------------------------------
+// For callers that cannot allocate device memory while they run -- a process
+// whose memory is owned by another allocator, a real-time loop that must not
+// call into the driver's allocator (cudaMalloc / cudaFree can synchronise the
+// device) -- the scratch of trex_dfa_batch_run_static lives in this
+// file-scope device array instead of a cudaMalloc'd buffer. Every GPU that
+// loads the library holds the array until the process exits. All calls on a
+// device share it, so calls whose work overlaps on the GPU race.
+namespace trex {
+
+constexpr int64_t kStaticScratchBytes = 8ll << 20;   // 8 MiB per GPU
+constexpr int kMaxStaticDevices = 64;
+
+static __device__ __align__(256) uint8_t g_static_scratch[kStaticScratchBytes];
+
+// Device address of g_static_scratch on each device, looked up once per device
+// (in host code the symbol name is only a stand-in, not a device address).
+static void *g_static_scratch_ptr[kMaxStaticDevices] = {};
+static std::mutex g_static_scratch_mu;
+
+static int static_scratch_address(void **out) {
+    int dev = 0;
+    TREX_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxStaticDevices) {
+        set_last_error_msg("trex_dfa_batch_run_static: device ordinal out of range");
+        return TREX_ERR_SHAPE;
+    }
+    std::lock_guard<std::mutex> lock(g_static_scratch_mu);
+    if (!g_static_scratch_ptr[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+        if (e != cudaSuccess || !p) {
+            set_last_error("trex_dfa_batch_run_static: cudaGetSymbolAddress", e);
+            return TREX_ERR_CUDA;
+        }
+        g_static_scratch_ptr[dev] = p;
+    }
+    *out = g_static_scratch_ptr[dev];
+    return TREX_OK;
+}
+
+}  // namespace trex
+
+extern "C" int trex_dfa_batch_run_static(trex_dfa_set *set, const uint8_t *data,
+                                         const int64_t *offsets, const int32_t *dfa_id,
+                                         int64_t n_strings, int64_t total_bytes,
+                                         uint8_t *final_state, uint8_t *accept,
+                                         int32_t *accept_i32, int32_t seg_len, void *stream) {
+    if (!set) return TREX_ERR_NOT_INIT;
+    if (n_strings < 0 || total_bytes < 0) return TREX_ERR_ARG;
+    const int64_t need = (int64_t)trex::scratch_layout(n_strings, total_bytes, seg_len).total;
+    if (need > trex::kStaticScratchBytes) {
+        trex::set_last_error_msg(
+            "trex_dfa_batch_run_static: batch needs more than the 8 MiB static scratch; "
+            "use trex_dfa_batch_run with a caller-provided scratch buffer");
+        return TREX_ERR_CAPACITY;
+    }
+    void *scratch = nullptr;
+    const int rc = trex::static_scratch_address(&scratch);
+    if (rc) return rc;
+    // dfa_set_run clears the counters at the front of the scratch before use
+    // and writes every item / map slot before reading it.
+    return trex::dfa_set_run(set, data, offsets, dfa_id, n_strings, total_bytes, final_state,
+                             accept, accept_i32, scratch, trex::kStaticScratchBytes, seg_len,
+                             static_cast<cudaStream_t>(stream), nullptr);
+}
