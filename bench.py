@@ -127,15 +127,15 @@ class DFAWorkload:
             self.lens = np.full(self.n, 1024, dtype=np.int64)
             self.is_sub = np.ones(self.n, dtype=bool)
             self.ids = np.zeros(self.n, dtype=np.int32)
-            self.workload = "plain DFA: N=16 random DFA over bytes ACGT, 4096 strings x 1024 bytes"
+            self.workload = f"plain DFA: N=16 random DFA over bytes ACGT, {self.n} strings x 1024 bytes"
         elif self.kind == "scan":
             self.n = args.strings or 8
             self.dfas = [random_dfa(16, np.arange(256), rng)]
             self.lens = np.full(self.n, 1 << 28, dtype=np.int64)
             self.is_sub = None
             self.ids = np.zeros(self.n, dtype=np.int32)
-            self.workload = ("long-string scan: N=16 random DFA over 256 bytes, 8 strings x 256 MiB, "
-                             "state of every position written")
+            self.workload = (f"long-string scan: N=16 random DFA over 256 bytes, {self.n} strings x "
+                             "256 MiB, state of every position written")
         else:
             self.n = args.strings or 1_000_000
             sizes = (8,) * 5 + (12,) * 5 + (16,) * 6
@@ -145,9 +145,10 @@ class DFAWorkload:
             self.dfas = [random_dfa(n, np.arange(256), rng) for n in sizes]
             self.lens, self.is_sub = None, None
             self.ids = (np.arange(self.n) % 16).astype(np.int32)
-            self.workload = ("ragged DFA batch: 16 random DFAs (5x8, 5x12, 6x16 states) over 256 byte "
-                             "symbols; 1M strings, log-normal lengths median 2048 sigma 1.18 clipped "
-                             "[16, 65536]; 10% of strings over 'ACGT'; string i on DFA i mod 16")
+            shape = ", ".join(f"{sizes.count(v)}x{v}" for v in sorted(set(sizes)))
+            self.workload = (f"ragged DFA batch: 16 random DFAs ({shape} states) over 256 byte "
+                             f"symbols; {self.n} strings, log-normal lengths median 2048 sigma 1.18 "
+                             "clipped [16, 65536]; 10% of strings over 'ACGT'; string i on DFA i mod 16")
 
     def lengths(self, seed):
         if self.lens is None:
@@ -290,7 +291,7 @@ class NFAWorkload:
         self.L = 4096
         self.off = np.arange(self.n + 1, dtype=np.int64) * self.L
         self.workload = ("Boolean NFA: random 64-state NFA over 20 symbols (bytes 0..19), edge density "
-                         "0.05, 256K strings x 4096 symbols")
+                         f"0.05, {self.n} strings x 4096 symbols")
 
     def setup(self, torch, dev, seed):
         from trex_b200.engine import NFA
