@@ -222,6 +222,31 @@ int trex_nfa_run(trex_nfa *nfa, const uint8_t *data, const int64_t *offsets, int
 /* Error word of the last run (bit 0: malformed offsets). Synchronises. */
 int trex_nfa_error(trex_nfa *nfa, int32_t *err_out);
 
+/* ---- probabilistic NFA (<= 64 states): s' = T[c] s ----------------------
+ * Replaces the reference's nfa_prob_v5_tc_kernel / nfa_prob_v6_cuda_kernel
+ * (cuda/nfa_tc_evolution.cu:456-610), which are reachable only from its test
+ * main and return dot(s_L, accept) > 0.5; this form returns the natural
+ * log-likelihood log(dot(s_L, accept)) in FP64 as well as that flag.
+ * T[c][dst][src] (row-major, sigma x n x n), start[n], accept[n]. Bytes
+ * >= sigma are skipped (the reference kernels leave the state unchanged). */
+typedef struct trex_pnfa trex_pnfa;
+enum { TREX_PNFA_BF16 = 0, TREX_PNFA_FP16 = 1, TREX_PNFA_FP32 = 2 };
+int trex_pnfa_create(int n_states, int sigma, const float *T, const float *start,
+                     const float *accept, trex_pnfa **out);
+void trex_pnfa_destroy(trex_pnfa *pnfa);
+/* mode TREX_PNFA_BF16 / TREX_PNFA_FP16: tensor-core products (tcgen05) with
+ * 16-bit operands and FP32 accumulation, sigma <= 28 (else TREX_ERR_SHAPE);
+ * TREX_PNFA_FP32: FP32 on CUDA cores, any sigma. Every step renormalises the
+ * state by a power of two kept as an integer exponent. DEVICE buffers;
+ * loglik[n] (-inf when the likelihood is 0), accept[n], accept_i32[n]
+ * (dot > 0.5) may each be NULL. One run at a time per handle. */
+int trex_pnfa_run(trex_pnfa *pnfa, int mode, const uint8_t *data, const int64_t *offsets,
+                  int64_t n_strings, int64_t total_bytes, double *loglik, uint8_t *accept,
+                  int32_t *accept_i32, void *stream);
+/* Error word of the last run: bit 0 malformed offsets (those strings get no
+ * result), bit 2 an internal wait ran out. Synchronises. */
+int trex_pnfa_error(trex_pnfa *pnfa, int32_t *err_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,153 @@
+"""Family (d) on the GPU: probabilistic NFA log-likelihoods vs the FP64 oracle.
+
+The oracle (oracle/oracle.c oracle_pnfa_fp64) restates s' = T[c] s of the
+reference's nfa_prob_v5_tc_kernel (cuda/nfa_tc_evolution.cu:506-559) in FP64
+with exact power-of-two scaling. Parity for the log-likelihood is unpinned by
+the reference (it has no CPU path and reports only dot > 0.5).
+
+Tolerances. The 16-bit forms round T and the state to the operand type once
+per step, so a string of k symbols can be off by about k unit roundoffs in
+log-likelihood when k is small; over long strings the errors average out and
+the relative error is what is bounded:
+  any string:            |LL - LL_fp64| <= max(rtol * |LL_fp64|, u * (k + 1))
+  strings of 2048 symbols (the benchmark shape): |LL - LL_fp64| <= 1e-4 * |LL_fp64|
+with rtol = 1e-5 / 1e-4 / 1e-4 and u = 1e-7 / 2^-8 / 2^-11 for fp32 / bf16 /
+fp16 (u is twice the operand type's unit roundoff).
+"""
+
+import numpy as np
+import pytest
+
+from trex_b200.workloads import random_prob_nfa
+
+pytestmark = pytest.mark.gpu
+
+RTOL = {"fp32": 1e-5, "bf16": 1e-4, "fp16": 1e-4}
+U = {"fp32": 1e-7, "bf16": 2.0 ** -8, "fp16": 2.0 ** -11}
+
+
+def _run(torch, T, start, acc, data, off, mode):
+    from trex_b200.engine import PNFA
+    m = PNFA(T, start, acc)
+    d = torch.from_numpy(np.ascontiguousarray(data if data.size else np.zeros(16, np.uint8))).cuda()
+    ll, ac = m.run(d, torch.from_numpy(off.astype(np.int64)).cuda(), mode)
+    torch.cuda.synchronize()
+    err = m.error_word()
+    m.close()
+    return ll.cpu().numpy(), ac.cpu().numpy(), err
+
+
+def _symbols(data, off, sigma):
+    valid = np.concatenate([[0], np.cumsum(data < sigma)])
+    return valid[off[1:]] - valid[off[:-1]]
+
+
+def _check(ll, ac, ref, mode, k, rtol=None):
+    both_inf = np.isneginf(ll) & np.isneginf(ref)
+    d = np.abs(ll - ref)
+    d[both_inf] = 0.0
+    assert np.all(np.isfinite(d)), f"{mode}: non-finite result where the oracle has {ref[~np.isfinite(d)][:4]}"
+    if rtol is not None:   # long strings: the relative bound alone
+        tol = np.maximum(rtol * np.abs(ref), 1e-12)
+    else:
+        tol = np.maximum(RTOL[mode] * np.abs(ref), U[mode] * (k + 1))
+    worst = np.argmax(d / tol)
+    assert np.all(d <= tol), (f"{mode}: |dLL| {d[worst]:.3g} > tol {tol[worst]:.3g} at LL {ref[worst]:.4g} "
+                              f"({k[worst]} symbols)")
+    # accept flag = dot > 0.5 = LL > log 0.5, where the margin exceeds the tolerance
+    clear = np.abs(ref - np.log(0.5)) > 4 * tol
+    assert np.array_equal(ac[clear].astype(bool), (ref > np.log(0.5))[clear])
+
+
+@pytest.mark.parametrize("mode", ["fp32", "bf16", "fp16"])
+def test_pnfa_ragged_matches_fp64(cuda, oracle, mode):
+    rng = np.random.default_rng(7)
+    T, start, acc = random_prob_nfa(rng, 64, 20)
+    lens = rng.integers(0, 700, size=3000)
+    lens[:6] = [0, 1, 2, 15, 16, 17]
+    off = np.zeros(len(lens) + 1, dtype=np.int64)
+    np.cumsum(lens, out=off[1:])
+    data = rng.integers(0, 20, size=int(off[-1]), dtype=np.uint8)
+    ll, ac, err = _run(cuda, T, start, acc, data, off, mode)
+    ref = oracle.pnfa_fp64(T, start, acc, data, off)
+    assert err == 0
+    _check(ll, ac, ref, mode, _symbols(data, off, 20))
+
+
+@pytest.mark.parametrize("mode", ["fp32", "bf16", "fp16"])
+def test_pnfa_small_automaton_skips_unknown_bytes(cuda, oracle, mode):
+    # 5 states, 7 symbols (odd: the last symbol pair is half empty), bytes >= 7 skipped
+    rng = np.random.default_rng(11)
+    T, start, acc = random_prob_nfa(rng, 5, 7, keep=0.6)
+    start = rng.random(5)
+    acc = (rng.random(5) < 0.5).astype(np.float64)
+    acc[0] = 1.0
+    lens = rng.integers(0, 300, size=900)
+    off = np.zeros(len(lens) + 1, dtype=np.int64)
+    np.cumsum(lens, out=off[1:])
+    data = rng.integers(0, 10, size=int(off[-1]), dtype=np.uint8)
+    data[off[7]:off[8]] = 200   # a string with no valid symbol: the start vector's likelihood
+    ll, ac, err = _run(cuda, T, start, acc, data, off, mode)
+    ref = oracle.pnfa_fp64(T, start, acc, data, off)
+    assert err == 0
+    _check(ll, ac, ref, mode, _symbols(data, off, 7))
+
+
+@pytest.mark.parametrize("mode", ["bf16", "fp16"])
+def test_pnfa_many_strings_multiple_waves(cuda, oracle, mode):
+    # more strings than slots: slots take new strings at block boundaries
+    rng = np.random.default_rng(5)
+    T, start, acc = random_prob_nfa(rng, 64, 20)
+    n = 160_000
+    lens = rng.integers(1, 40, size=n)
+    off = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(lens, out=off[1:])
+    data = rng.integers(0, 20, size=int(off[-1]), dtype=np.uint8)
+    ll, ac, err = _run(cuda, T, start, acc, data, off, mode)
+    ref = oracle.pnfa_fp64(T, start, acc, data, off)
+    assert err == 0
+    _check(ll, ac, ref, mode, _symbols(data, off, 20))
+
+
+def test_pnfa_long_uniform_strings_error(cuda, oracle):
+    # the benchmark shape (length 2048), on a subset of strings
+    rng = np.random.default_rng(3)
+    T, start, acc = random_prob_nfa(rng, 64, 20)
+    n, L = 4096, 2048
+    off = np.arange(n + 1, dtype=np.int64) * L
+    data = rng.integers(0, 20, size=n * L, dtype=np.uint8)
+    ref = oracle.pnfa_fp64(T, start, acc, data, off)
+    for mode in ("bf16", "fp16", "fp32"):
+        ll, ac, err = _run(cuda, T, start, acc, data, off, mode)
+        assert err == 0
+        _check(ll, ac, ref, mode, _symbols(data, off, 20), rtol=RTOL[mode])
+
+
+def test_pnfa_reference_stochastic_matrices(cuda, oracle):
+    # the reference test's construction (nfa_tc_evolution.cu:1320-1345): sigma = 2,
+    # T[dst][src] positive and normalised over dst for every src; start e0, accept ~1/4
+    rng = np.random.default_rng(77)
+    T = rng.integers(1, 101, size=(2, 64, 64)).astype(np.float64)
+    T /= T.sum(axis=1, keepdims=True)
+    start = np.zeros(64)
+    start[0] = 1.0
+    acc = (rng.integers(0, 4, size=64) == 0).astype(np.float64)
+    lens = rng.integers(1, 300, size=500)
+    off = np.zeros(len(lens) + 1, dtype=np.int64)
+    np.cumsum(lens, out=off[1:])
+    data = rng.integers(0, 2, size=int(off[-1]), dtype=np.uint8)
+    ref = oracle.pnfa_fp64(T, start, acc, data, off)
+    for mode in ("fp32", "bf16", "fp16"):
+        ll, ac, err = _run(cuda, T, start, acc, data, off, mode)
+        assert err == 0
+        _check(ll, ac, ref, mode, _symbols(data, off, 2))
+
+
+def test_pnfa_malformed_offsets_flagged(cuda):
+    rng = np.random.default_rng(1)
+    T, start, acc = random_prob_nfa(rng, 64, 20)
+    off = np.array([0, 10, 5, 20], dtype=np.int64)   # string 1 ends before it starts
+    data = rng.integers(0, 20, size=20, dtype=np.uint8)
+    for mode in ("fp32", "bf16"):
+        _, _, err = _run(cuda, T, start, acc, data, off, mode)
+        assert err & 1

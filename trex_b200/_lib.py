@@ -64,6 +64,12 @@ SIGNATURES = {
     "trex_nfa_run": (ctypes.c_int, [c_vp, c_vp, c_vp, ctypes.c_int64, ctypes.c_int64, c_vp, c_vp,
                                     c_vp, c_vp]),
     "trex_nfa_error": (ctypes.c_int, [c_vp, c_i32p]),
+    "trex_pnfa_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, c_f32p, c_f32p, c_f32p,
+                                        ctypes.POINTER(c_vp)]),
+    "trex_pnfa_destroy": (None, [c_vp]),
+    "trex_pnfa_run": (ctypes.c_int, [c_vp, ctypes.c_int, c_vp, c_vp, ctypes.c_int64, ctypes.c_int64,
+                                     c_vp, c_vp, c_vp, c_vp]),
+    "trex_pnfa_error": (ctypes.c_int, [c_vp, c_i32p]),
     # handle API
     "trex_dfa_set_create": (ctypes.c_int, [ctypes.c_int, c_i32p, c_i32p, c_u8p, c_u8p,
                                            ctypes.POINTER(c_vp)]),

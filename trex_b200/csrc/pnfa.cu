@@ -1,0 +1,1187 @@
+// Family (d): probabilistic NFA (weighted automaton, HMM forward pass) with up
+// to 64 states.
+//
+// Semantics (reference cuda/nfa_tc_evolution.cu:456-561 nfa_prob_v5_tc_kernel,
+// :572-610 nfa_prob_v6_cuda_kernel): T[c] is a real 64 x 64 matrix in the
+// T[dst][src] convention; the state starts at the start vector and symbol c
+// maps it to s' = T[c] s; a string's result is dot(s_L, accept). The
+// reference returns only dot > 0.5; this engine returns the natural
+// log-likelihood log(dot) in FP64 and that flag. Bytes >= sigma are skipped
+// (the reference kernels leave the state unchanged for them).
+//
+// Range: every step renormalises s by an exact power of two 2^-f and adds the
+// integer f to the string's exponent E, so log-likelihood = log(dot) + E ln 2.
+//
+// Plain form (FP32, CUDA cores): a warp per string, lane l owns states l and
+// l + 32, T[c] rows read through L1; f = the frexp exponent of the step's
+// max |s'|, the rule of the FP64 oracle.
+//
+// Tensor form (tcgen05, BF16 or FP16 operands, FP32 accumulation in TMEM).
+// One persistent CTA per SM holds up to 2 x 256 strings ("slots") in two
+// sub-batches that alternate, so the tensor core works on one while the other
+// is in its epilogue. Orientation: D[dst][string] = T[c][dst][:] . S[:][string]
+// -- the 64 states are the MMA's M rows (TMEM lanes) and the strings its N
+// columns, because strings of one step carry different symbols and only the
+// N side can be regrouped cheaply. Symbols are paired (2p, 2p+1): the A
+// operand of pair p is [T[2p]; T[2p+1]] (M = 128), resident in TMEM for the
+// whole kernel (32 columns a pair: 64 16-bit K values per lane), so the shared
+// memory traffic of an MMA is only its B columns. Each step, the strings of a
+// sub-batch are grouped by pair in the B buffer (even symbol first), and one
+// MMA chain (K = 64 as 4 x K16) per group of <= 64 strings writes a 64-column
+// region of a TMEM ring. Rows 0-63 of the result are valid for the even-symbol
+// strings, rows 64-127 for the odd ones (half the MMA work is discarded: the
+// price of keeping A in TMEM and B small).
+//
+// Warp roles (256 threads): warps 0-3 epilogue (warp q reads TMEM lanes
+// 32q..32q+31), warp 4 scheduler, warp 5 MMA issuer (and TMEM owner), warps
+// 6-7 loader.
+//  * loader: gives each slot its next string from a global atomic queue and
+//    copies the next 16 valid symbols of every slot into a shared block
+//    (strings change slots only at 16-step block boundaries).
+//  * scheduler: per step and sub-batch, sorts the slots of the next step by
+//    symbol pair (counting sort with shared atomics), writes the chunk list,
+//    writes the start vector into the rows of strings that begin, and for
+//    the current step writes one record per column: destination row in the
+//    next B buffer and the scale 2^-f, f from the bound max|s_t| * R_c with
+//    R_c = max row sum of |T[c]| (so max|s_t+1| < 1) and max|s_t| measured by
+//    the previous epilogue. When a string ends it turns the two partial dot
+//    products left by the epilogue into the FP64 log-likelihood.
+//  * MMA: per chunk waits for a free ring region, issues 4 tcgen05.mma
+//    (A from TMEM, B from shared memory, no swizzle) and commits to the
+//    region's mbarrier.
+//  * epilogue: tcgen05.ld of the region, scale, round to 16 bits and store
+//    each state into the string's row of the next B buffer; warp max (redux)
+//    of the column for the next step's scale; for a string's last symbol the
+//    accept-weighted sum instead.
+// B buffers (shared memory, K-major, no swizzle): row r, state k at
+// (k/8)*LBO + r*16 + (k%8)*2 with LBO = rows*16 and rows = 1 (mod 8), so the
+// 32 lanes of an epilogue store hit 32 different banks and an MMA may start
+// at any row.
+// Every wait is bounded; a wait that runs out sets the error word (bit 2) and
+// an abort flag that every role polls, the MMA warp drains its commits and
+// the TMEM is freed before the kernel returns.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "trex_internal.cuh"
+
+namespace trex {
+
+constexpr int kPnStates = 64;
+constexpr int kPnBlk = 16;             // steps per symbol block
+constexpr int kPnThreads = 256;
+constexpr int kPnMaxPSub = 256;        // slots per sub-batch (8 per scheduler lane)
+constexpr int kPnMaxChunks = 32;
+constexpr int kPnRegionCols = 64;
+constexpr int kPnMaxSigmaTc = 28;      // 14 pairs: 448 TMEM columns + one ring region
+constexpr int kPnMiscBytes = 1280;
+constexpr uint32_t kPnSmemCap = 232448;
+constexpr uint32_t kPnFinish = 0x80000000u;
+constexpr int32_t kPnTerminate = -1;
+constexpr uint32_t kPnErrOffsets = 1u, kPnErrTimeout = 4u;
+constexpr uint32_t kPnSpinLimit = 1u << 25;
+
+// slot flags (scheduler)
+constexpr uint8_t kSlotActive = 1, kSlotLast = 2, kSlotFresh = 4, kSlotFinPending = 8;
+// header flags (loader)
+constexpr uint8_t kHdrStart = 1, kHdrEnd = 2;
+
+struct PnHdr {
+    int32_t seq;
+    uint8_t count, flags;
+    uint16_t pad;
+};
+struct PnSlot {
+    int32_t seq, E;           // string in the slot and its exponent sum
+    int32_t fin_seq, fin_E;   // string whose last step's dot products are pending
+    int16_t row, finrow;
+    uint8_t c, flags, blkcnt, blkflags;
+};
+struct PnChunk {
+    uint16_t row0;
+    uint8_t ncols, split, pair, pad0, pad1, pad2;
+};
+
+struct PnLayout {
+    int p_sub, rows, npairs, nregions, ring_base;
+    uint32_t lbo;
+    uint32_t s_off, sym_off, hdr_off, rec_off, xmax_off, fin_off, chunk_off, slot_off, misc_off,
+        total;
+};
+
+__host__ __device__ inline uint32_t pn_align16(uint32_t x) { return (x + 15u) & ~15u; }
+
+static PnLayout pn_layout(int p_sub, int sigma) {
+    PnLayout L{};
+    L.p_sub = p_sub;
+    L.npairs = (sigma + 1) / 2;
+    L.ring_base = 32 * L.npairs;
+    L.nregions = std::min(6, (512 - L.ring_base) / kPnRegionCols);
+    int rows = p_sub + 16;
+    while (rows % 8 != 1) ++rows;
+    L.rows = rows;
+    L.lbo = (uint32_t)rows * 16u;
+    uint32_t off = 0;
+    L.s_off = off;
+    off += 4u * 8u * L.lbo;
+    L.sym_off = off;
+    off += 2u * kPnBlk * 2u * (uint32_t)p_sub;
+    L.hdr_off = pn_align16(off);
+    off = L.hdr_off + 2u * 2u * (uint32_t)p_sub * (uint32_t)sizeof(PnHdr);
+    L.rec_off = pn_align16(off);
+    off = L.rec_off + 2u * (uint32_t)rows * 16u;
+    L.xmax_off = off;
+    off += 2u * (uint32_t)rows * 8u;
+    L.fin_off = off;
+    off += 2u * (uint32_t)rows * 8u;
+    L.chunk_off = off;
+    off += 2u * 2u * kPnMaxChunks * (uint32_t)sizeof(PnChunk);
+    L.slot_off = pn_align16(off);
+    off = L.slot_off + 2u * (uint32_t)p_sub * (uint32_t)sizeof(PnSlot);
+    L.misc_off = pn_align16(off);
+    off = L.misc_off + kPnMiscBytes;
+    L.total = pn_align16(off);
+    return L;
+}
+
+// misc region offsets (bytes, relative to misc_off)
+constexpr uint32_t kMTmem = 0, kMAbort = 4, kMLoaded = 8, kMConsumed = 12, kMSched = 16,
+                   kMEpi = 24, kMEmpty = 32, kMLdSync = 56, kMFull = 64, kMNch = 128, kMBlkAct = 144,
+                   kMCnt = 160, kMPinfo = 416, kMRsym = 672, kMStart = 800, kMAcc = 928;
+
+struct PnParams {
+    const uint8_t *data;
+    int64_t total_bytes;
+    const int64_t *offsets;
+    int64_t n;
+    const uint32_t *tpack;     // [npairs][128][32] 16-bit pairs
+    const float *rsym;         // [sigma] growth bound per symbol
+    const uint4 *start_img;    // [8] start vector, 16-bit, one B row
+    const float *acc;          // [64] accept weights
+    float start_max;
+    double ll_empty;
+    int sigma;
+    double *loglik;
+    uint8_t *accept;
+    int32_t *accept_i32;
+    unsigned long long *queue;
+    uint32_t *err;
+    PnLayout L;
+};
+
+// ---- small device helpers -------------------------------------------------------------------
+__device__ __forceinline__ uint32_t pn_smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void pn_tc_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void pn_tc_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void pn_fence_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ bool pn_mbar_test(uint32_t addr, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}"
+        : "=r"(done) : "r"(addr), "r"(parity) : "memory");
+    return done != 0;
+}
+
+// Lane 0 spins until *ctr >= target (wrap-safe); bounded; broadcast to the warp.
+__device__ __forceinline__ bool pn_wait_ge(const volatile uint32_t *ctr, uint32_t target,
+                                           volatile uint32_t *abort_flag, uint32_t *err) {
+    int ok = 1;
+    if ((threadIdx.x & 31) == 0) {
+        uint32_t it = 0;
+        while ((int32_t)(*ctr - target) < 0) {
+            if (*abort_flag) { ok = 0; break; }
+            if (++it > kPnSpinLimit) {
+                atomicOr(err, kPnErrTimeout);
+                *abort_flag = 1u;
+                ok = 0;
+                break;
+            }
+            if (it > 32) __nanosleep(40);
+        }
+        __threadfence_block();
+    }
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    __syncwarp();
+    return ok != 0;
+}
+
+__device__ __forceinline__ bool pn_wait_mbar(uint32_t addr, uint32_t parity,
+                                             volatile uint32_t *abort_flag, uint32_t *err) {
+    int ok = 1;
+    if ((threadIdx.x & 31) == 0) {
+        uint32_t it = 0;
+        while (!pn_mbar_test(addr, parity)) {
+            if (*abort_flag) { ok = 0; break; }
+            if (++it > kPnSpinLimit) {
+                atomicOr(err, kPnErrTimeout);
+                *abort_flag = 1u;
+                ok = 0;
+                break;
+            }
+            if (it > 32) __nanosleep(40);
+        }
+    }
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    __syncwarp();
+    return ok != 0;
+}
+
+__device__ __forceinline__ void pn_write_result(double *loglik, uint8_t *accept, int32_t *accept_i32,
+                                                int64_t seq, double ll) {
+    if (loglik) loglik[seq] = ll;
+    const int a = ll > -0.69314718055994530942;   // dot > 0.5
+    if (accept) accept[seq] = (uint8_t)a;
+    if (accept_i32) accept_i32[seq] = a;
+}
+
+// exponent f with x < 2^f for a finite positive float x (x >= 2^-126); 0 for x == 0
+__device__ __forceinline__ int pn_ceil_exp(float x) {
+    const uint32_t e = (__float_as_uint(x) >> 23) & 0xFFu;
+    if (e == 0) return 0;
+    return (int)e - 126;
+}
+__device__ __forceinline__ float pn_pow2(int f) {   // 2^f, |f| <= 126
+    return __uint_as_float((uint32_t)(127 + f) << 23);
+}
+
+template <bool FP16>
+__device__ __forceinline__ uint16_t pn_to16(float v) {
+    if constexpr (FP16) return __half_as_ushort(__float2half_rn(v));
+    else return __bfloat16_as_ushort(__float2bfloat16_rn(v));
+}
+
+__device__ __forceinline__ void pn_tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,"
+        "%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+          "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr) : "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void pn_tmem_st32(uint32_t taddr, const uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+        "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};"
+        :: "r"(taddr), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]),
+           "r"(r[7]), "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]),
+           "r"(r[14]), "r"(r[15]), "r"(r[16]), "r"(r[17]), "r"(r[18]), "r"(r[19]), "r"(r[20]),
+           "r"(r[21]), "r"(r[22]), "r"(r[23]), "r"(r[24]), "r"(r[25]), "r"(r[26]), "r"(r[27]),
+           "r"(r[28]), "r"(r[29]), "r"(r[30]), "r"(r[31])
+        : "memory");
+}
+
+// ---- roles ------------------------------------------------------------------------------------
+struct PnShared {
+    uint8_t *base;
+    PnLayout L;
+    __device__ uint8_t *misc() const { return base + L.misc_off; }
+    __device__ volatile uint32_t *u32(uint32_t off) const {
+        return reinterpret_cast<volatile uint32_t *>(misc() + off);
+    }
+    __device__ uint32_t sbuf(int b, int par) const {   // byte offset of a B buffer
+        return L.s_off + (uint32_t)(b * 2 + par) * 8u * L.lbo;
+    }
+    __device__ uint8_t *sym(int buf) const { return base + L.sym_off + buf * kPnBlk * 2 * L.p_sub; }
+    __device__ PnHdr *hdr(int buf) const {
+        return reinterpret_cast<PnHdr *>(base + L.hdr_off) + buf * 2 * L.p_sub;
+    }
+    __device__ uint4 *rec(int b) const { return reinterpret_cast<uint4 *>(base + L.rec_off) + b * L.rows; }
+    __device__ float2 *xmax(int b) const {
+        return reinterpret_cast<float2 *>(base + L.xmax_off) + b * L.rows;
+    }
+    __device__ float2 *fin(int b) const { return reinterpret_cast<float2 *>(base + L.fin_off) + b * L.rows; }
+    __device__ PnChunk *chunks(int b, int par) const {
+        return reinterpret_cast<PnChunk *>(base + L.chunk_off) + (b * 2 + par) * kPnMaxChunks;
+    }
+    __device__ PnSlot *slots() const { return reinterpret_cast<PnSlot *>(base + L.slot_off); }
+    __device__ volatile int32_t *nch(int b, int par) const {
+        return reinterpret_cast<volatile int32_t *>(misc() + kMNch) + b * 2 + par;
+    }
+    __device__ int32_t *cnt(int b) const {   // [16 pairs][2 parities]
+        return reinterpret_cast<int32_t *>(misc() + kMCnt) + b * 32;
+    }
+    __device__ int32_t *pinfo(int b) const {   // [16 pairs][base, neven]
+        return reinterpret_cast<int32_t *>(misc() + kMPinfo) + b * 32;
+    }
+    __device__ uint32_t full_addr(int r) const { return pn_smem_u32(misc() + kMFull + 8 * r); }
+};
+
+// Loader: warps 6-7. Fills symbol block blk into buffer blk & 1.
+__device__ void pn_loader(const PnParams &P, const PnShared &S, volatile uint32_t *abort_flag) {
+    const int lane = threadIdx.x & 31;
+    const int lw = (threadIdx.x >> 5) - 6;
+    const int ll = lw * 32 + lane;
+    const int PC = 2 * S.L.p_sub;
+    const uint32_t sig4 = (uint32_t)P.sigma * 0x01010101u;
+    int32_t seq[8];
+    int64_t pos[8], end[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) { seq[i] = -1; pos[i] = 0; end[i] = 0; }
+    for (int blk = 0;; ++blk) {
+        if (blk >= 2 && !pn_wait_ge(S.u32(kMConsumed), (uint32_t)(blk - 1), abort_flag, P.err)) break;
+        const int buf = blk & 1;
+        uint8_t *sym = S.sym(buf);
+        PnHdr *hd = S.hdr(buf);
+        int nact = 0;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int j = ll + 64 * i;
+            if (j >= PC) continue;
+            uint8_t flags = 0;
+            if (seq[i] < 0 || pos[i] >= end[i]) {
+                seq[i] = -1;
+                for (;;) {
+                    const unsigned long long idx = atomicAdd(P.queue, 1ull);
+                    if (idx >= (unsigned long long)P.n) break;
+                    int64_t p0 = P.offsets[idx], p1 = P.offsets[idx + 1];
+                    if (p0 < 0 || p1 < p0 || p1 > P.total_bytes) {
+                        atomicOr(P.err, kPnErrOffsets);
+                        continue;
+                    }
+                    while (p0 < p1 && P.data[p0] >= (uint8_t)P.sigma) ++p0;
+                    if (p0 == p1) {
+                        pn_write_result(P.loglik, P.accept, P.accept_i32, (int64_t)idx, P.ll_empty);
+                        continue;
+                    }
+                    seq[i] = (int32_t)idx;
+                    pos[i] = p0;
+                    end[i] = p1;
+                    flags = kHdrStart;
+                    break;
+                }
+            }
+            int count = 0;
+            if (seq[i] >= 0) {
+                int64_t p = pos[i];
+                const int64_t e = end[i];
+                bool fast = false;
+                // 20-byte window of aligned words; only when it lies inside [data, data + e)
+                const uintptr_t ap = reinterpret_cast<uintptr_t>(P.data + p);
+                const uintptr_t aw = ap & ~(uintptr_t)3;
+                if (e - p >= 20 && aw >= reinterpret_cast<uintptr_t>(P.data)) {
+                    const uint32_t *wp = reinterpret_cast<const uint32_t *>(aw);
+                    uint32_t w[5];
+#pragma unroll
+                    for (int k = 0; k < 5; ++k) w[k] = __ldg(wp + k);
+                    const uint32_t sh = (uint32_t)(ap & 3) * 8u;
+                    uint32_t wd[4];
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) wd[k] = __funnelshift_r(w[k], w[k + 1], sh);
+                    uint32_t bad = 0;
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) bad |= __vcmpgeu4(wd[k], sig4);
+                    if (bad == 0) {
+                        fast = true;
+#pragma unroll
+                        for (int s = 0; s < 16; ++s)
+                            sym[s * PC + j] = (uint8_t)(wd[s >> 2] >> (8 * (s & 3)));
+                        count = 16;
+                        p += 16;
+                    }
+                }
+                if (!fast) {
+                    while (count < 16 && p < e) {
+                        const uint8_t b = P.data[p++];
+                        if (b < (uint8_t)P.sigma) sym[(count++) * PC + j] = b;
+                    }
+                }
+                while (p < e && P.data[p] >= (uint8_t)P.sigma) ++p;
+                pos[i] = p;
+                if (p == e) flags |= kHdrEnd;
+            }
+            PnHdr h;
+            h.seq = seq[i];
+            h.count = (uint8_t)count;
+            h.flags = count > 0 ? flags : 0;
+            h.pad = 0;
+            hd[j] = h;
+            nact += count > 0;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) nact += __shfl_xor_sync(0xffffffffu, nact, o);
+        if (lane == 0) {
+            reinterpret_cast<volatile int32_t *>(S.misc() + kMBlkAct)[buf * 2 + lw] = nact;
+            __threadfence_block();
+            atomicAdd(const_cast<uint32_t *>(S.u32(kMLdSync)), 1u);
+        }
+        __syncwarp();
+        // both loader warps have written their block (bounded wait, no barrier)
+        if (!pn_wait_ge(S.u32(kMLdSync), 2u * (uint32_t)(blk + 1), abort_flag, P.err)) break;
+        const volatile int32_t *ba = reinterpret_cast<const volatile int32_t *>(S.misc() + kMBlkAct);
+        const int total_act = ba[buf * 2] + ba[buf * 2 + 1];
+        if (ll == 0) {
+            __threadfence_block();
+            *S.u32(kMLoaded) = (uint32_t)(blk + 1);
+        }
+        if (total_act == 0 || *abort_flag) break;
+    }
+}
+
+// Scheduler: warp 4.
+template <bool FP16>
+__device__ void pn_scheduler(const PnParams &P, const PnShared &S, volatile uint32_t *abort_flag) {
+    const int lane = threadIdx.x & 31;
+    const PnLayout &L = S.L;
+    const int PS = L.p_sub, PC = 2 * PS, SL = PS / 32;
+    const float *rsym = reinterpret_cast<const float *>(S.misc() + kMRsym);
+    const uint4 *simg = reinterpret_cast<const uint4 *>(S.misc() + kMStart);
+    PnSlot *slots = S.slots();
+    for (int j = lane; j < PC; j += 32) {
+        PnSlot z;
+        z.seq = -1; z.E = 0; z.fin_seq = -1; z.fin_E = 0; z.row = 0; z.finrow = 0; z.c = 0;
+        z.flags = 0; z.blkcnt = 0; z.blkflags = 0;
+        slots[j] = z;
+    }
+    for (int k = lane; k < 64; k += 32) S.cnt(0)[k] = 0;
+    __syncwarp();
+    int done = 0;            // bit b: sub-batch b finished
+    int term_step[2] = {-2, -2};
+    bool final_blk = false;
+    for (int t = -1;; ++t) {
+        const int s1 = t + 1;
+        const int in = s1 % kPnBlk;
+        const int buf = (s1 / kPnBlk) & 1;
+        if (in == 0 && done != 3) {
+            const int blk = s1 / kPnBlk;
+            if (lane == 0) {
+                __threadfence_block();
+                *S.u32(kMConsumed) = (uint32_t)blk;
+            }
+            if (!pn_wait_ge(S.u32(kMLoaded), (uint32_t)(blk + 1), abort_flag, P.err)) break;
+            const volatile int32_t *ba = reinterpret_cast<const volatile int32_t *>(S.misc() + kMBlkAct);
+            final_blk = (ba[buf * 2] + ba[buf * 2 + 1]) == 0;
+        }
+        for (int b = 0; b < 2; ++b) {
+            if (done & (1 << b)) continue;
+            if (t >= 1 && !pn_wait_ge(S.u32(kMEpi + 4 * b), 4u * (uint32_t)t, abort_flag, P.err)) {
+                done = 3;
+                break;
+            }
+            const bool terminal = (term_step[b] == t);   // only emissions left
+            float2 *fin = S.fin(b);
+            float2 *xm = S.xmax(b);
+            uint4 *rec = S.rec(b);
+            int32_t *cnt = S.cnt(b);
+            int32_t *pinfo = S.pinfo(b);
+            const uint8_t *sym = S.sym(buf);
+            const PnHdr *hd = S.hdr(buf);
+            // (1) strings that ended at step t-1; (2) next-step activity and ranks
+            int rank[8], c1v[8], newseq[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                rank[i] = -1; c1v[i] = -1; newseq[i] = -1;
+                if (i >= SL) continue;
+                const int j = b * PS + lane + 32 * i;
+                PnSlot sl = slots[j];
+                if (sl.flags & kSlotFinPending) {
+                    const float2 f = fin[sl.finrow];
+                    const double dot = (double)f.x + (double)f.y;
+                    const double ll = dot > 0.0 ? log(dot) + (double)sl.fin_E * 0.69314718055994530942
+                                                : -INFINITY;
+                    pn_write_result(P.loglik, P.accept, P.accept_i32, sl.fin_seq, ll);
+                    sl.flags &= (uint8_t)~kSlotFinPending;
+                }
+                if (!terminal) {
+                    if (in == 0) {
+                        const PnHdr h = hd[j];
+                        sl.blkcnt = h.count;
+                        sl.blkflags = h.flags;
+                        if (h.flags & kHdrStart) newseq[i] = h.seq;   // applied after rec(t)
+                    }
+                    if (in < sl.blkcnt) {
+                        const int c1 = sym[in * PC + j];
+                        c1v[i] = c1;
+                        rank[i] = atomicAdd(&cnt[(c1 >> 1) * 2 + (c1 & 1)], 1);
+                    }
+                }
+                slots[j] = sl;
+            }
+            if (terminal) {
+                done |= 1 << b;
+                __syncwarp();
+                if (lane == 0) {
+                    __threadfence_block();
+                    *S.u32(kMSched + 4 * b) = (uint32_t)(t + 2);
+                }
+                continue;
+            }
+            __syncwarp();
+            // pair bases and the chunk list of step t+1
+            const int par1 = s1 & 1;
+            PnChunk *ch = S.chunks(b, par1);
+            {
+                int ne = 0, no = 0;
+                if (lane < L.npairs) {
+                    ne = cnt[lane * 2];
+                    no = cnt[lane * 2 + 1];
+                    cnt[lane * 2] = 0;
+                    cnt[lane * 2 + 1] = 0;
+                }
+                const int np = ne + no;
+                const int nc = (np + kPnRegionCols - 1) / kPnRegionCols;
+                int incl = np, cincl = nc;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int a = __shfl_up_sync(0xffffffffu, incl, o);
+                    const int c = __shfl_up_sync(0xffffffffu, cincl, o);
+                    if (lane >= o) { incl += a; cincl += c; }
+                }
+                const int base = incl - np, cbase = cincl - nc;
+                if (lane < L.npairs) {
+                    pinfo[lane * 2] = base;
+                    pinfo[lane * 2 + 1] = ne;
+                    for (int k = 0; k < nc; ++k) {
+                        PnChunk d;
+                        d.row0 = (uint16_t)(base + k * kPnRegionCols);
+                        const int cols = min(kPnRegionCols, np - k * kPnRegionCols);
+                        d.ncols = (uint8_t)cols;
+                        d.split = (uint8_t)min(max(ne - k * kPnRegionCols, 0), cols);
+                        d.pair = (uint8_t)lane;
+                        d.pad0 = d.pad1 = d.pad2 = 0;
+                        ch[cbase + k] = d;
+                    }
+                }
+                const int total_chunks = __shfl_sync(0xffffffffu, cincl, 31);
+                if (lane == 0) {
+                    const bool term = final_blk && in == 0;
+                    *S.nch(b, par1) = term ? kPnTerminate : total_chunks;
+                    if (term) term_step[b] = t + 1;
+                }
+                term_step[b] = __shfl_sync(0xffffffffu, term_step[b], 0);
+            }
+            __syncwarp();
+            // (3) records of step t, (4) start rows of step t+1, slot state
+            const uint32_t snext = S.sbuf(b, par1);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                if (i >= SL) continue;
+                const int j = b * PS + lane + 32 * i;
+                PnSlot sl = slots[j];
+                int row1 = -1;
+                if (c1v[i] >= 0) {
+                    const int p = c1v[i] >> 1;
+                    row1 = pinfo[p * 2] + ((c1v[i] & 1) ? pinfo[p * 2 + 1] : 0) + rank[i];
+                }
+                if (t >= 0 && (sl.flags & kSlotActive)) {
+                    float m;
+                    if (sl.flags & kSlotFresh) {
+                        m = P.start_max;
+                    } else {
+                        const float2 x = xm[sl.row];
+                        m = fmaxf(x.x, x.y);
+                    }
+                    const float bound = m * rsym[sl.c];
+                    int f = pn_ceil_exp(bound);
+                    f = min(max(f, -125), 125);
+                    sl.E += f;
+                    uint4 r;
+                    r.z = __float_as_uint(pn_pow2(-f));
+                    r.w = 0;
+                    if (sl.flags & kSlotLast) {
+                        r.x = 0;
+                        r.y = kPnFinish;
+                        sl.flags |= kSlotFinPending;
+                        sl.finrow = sl.row;
+                        sl.fin_seq = sl.seq;
+                        sl.fin_E = sl.E;
+                    } else {
+                        // a continuing string is active at t+1 (the loader never leaves it empty)
+                        r.x = (uint32_t)max(row1, 0) * 16u;
+                        r.y = (uint32_t)max(row1, 0);
+                    }
+                    rec[sl.row] = r;
+                }
+                uint8_t nf = sl.flags & kSlotFinPending;
+                if (newseq[i] >= 0) {
+                    sl.seq = newseq[i];
+                    sl.E = 0;
+                }
+                if (row1 >= 0) {
+                    nf |= kSlotActive;
+                    if ((sl.blkflags & kHdrEnd) && in == sl.blkcnt - 1) nf |= kSlotLast;
+                    if (newseq[i] >= 0) {
+                        nf |= kSlotFresh;
+                        uint8_t *dst = S.base + snext + (uint32_t)row1 * 16u;
+#pragma unroll
+                        for (int c = 0; c < 8; ++c)
+                            *reinterpret_cast<uint4 *>(dst + c * L.lbo) = simg[c];
+                    }
+                    sl.row = (int16_t)row1;
+                    sl.c = (uint8_t)c1v[i];
+                }
+                sl.flags = nf;
+                slots[j] = sl;
+            }
+            pn_fence_async_smem();
+            __threadfence_block();
+            __syncwarp();
+            if (lane == 0) *S.u32(kMSched + 4 * b) = (uint32_t)(t + 2);
+        }
+        if (done == 3 || *abort_flag) break;
+    }
+}
+
+// MMA issuer: warp 5.
+template <bool FP16>
+__device__ void pn_mma(const PnParams &P, const PnShared &S, uint32_t tbase,
+                       volatile uint32_t *abort_flag) {
+    const int lane = threadIdx.x & 31;
+    const PnLayout &L = S.L;
+    const uint32_t fmt = FP16 ? 0u : 1u;
+    const uint32_t smem_base = pn_smem_u32(S.base);
+    const uint32_t desc_hi = (128u >> 4) | (1u << 14);   // SBO = 128 B, descriptor version 1
+    uint32_t g = 0;
+    int done = 0;
+    bool aborted = false;
+    for (int t = 0; !aborted; ++t) {
+        for (int b = 0; b < 2 && !aborted; ++b) {
+            if (done & (1 << b)) continue;
+            if (!pn_wait_ge(S.u32(kMSched + 4 * b), (uint32_t)(t + 1), abort_flag, P.err)) { aborted = true; break; }
+            if (t > 0 && !pn_wait_ge(S.u32(kMEpi + 4 * b), 4u * (uint32_t)t, abort_flag, P.err)) { aborted = true; break; }
+            const int nch = *S.nch(b, t & 1);
+            if (nch == kPnTerminate) { done |= 1 << b; continue; }
+            const PnChunk *ch = S.chunks(b, t & 1);
+            const uint32_t sb = smem_base + S.sbuf(b, t & 1);
+            for (int k = 0; k < nch; ++k) {
+                const PnChunk d = ch[k];
+                const uint32_t r = g % (uint32_t)L.nregions, u = g / (uint32_t)L.nregions;
+                if (u > 0 && !pn_wait_ge(S.u32(kMEmpty + 4 * r), 4u * u, abort_flag, P.err)) { aborted = true; break; }
+                pn_tc_after();
+                if (lane == 0) {
+                    const uint32_t n16 = ((uint32_t)d.ncols + 15u) & ~15u;
+                    const uint32_t idesc = (1u << 4) | (fmt << 7) | (fmt << 10) | ((n16 >> 3) << 17) |
+                                           ((128u >> 4) << 24);
+                    const uint32_t td = tbase + (uint32_t)L.ring_base + r * kPnRegionCols;
+#pragma unroll
+                    for (int kk = 0; kk < 4; ++kk) {
+                        const uint32_t saddr = sb + (uint32_t)d.row0 * 16u + (uint32_t)kk * 2u * L.lbo;
+                        const uint64_t desc = (uint64_t)(((saddr >> 4) & 0x3FFFu) | ((L.lbo >> 4) << 16)) |
+                                              ((uint64_t)desc_hi << 32);
+                        const uint32_t ta = tbase + 32u * d.pair + 8u * kk;
+                        const uint32_t acc = kk > 0;
+                        asm volatile(
+                            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                            "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}"
+                            :: "r"(td), "r"(ta), "l"(desc), "r"(idesc), "r"(acc) : "memory");
+                    }
+                    asm volatile(
+                        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                        :: "r"(S.full_addr((int)r)) : "memory");
+                }
+                __syncwarp();
+                ++g;
+            }
+        }
+        if (done == 3) break;
+    }
+    // Drain: every committed chain must have finished before the TMEM is freed.
+    const uint32_t nr = (uint32_t)L.nregions;
+    for (uint32_t r = 0; r < nr && r < g; ++r) {
+        const uint32_t uses = (g - r + nr - 1) / nr;   // commits made to region r
+        if (lane == 0) {                               // completion of the last one
+            uint32_t it = 0;
+            while (!pn_mbar_test(S.full_addr((int)r), (uses - 1) & 1u)) {
+                if (++it > kPnSpinLimit) { atomicOr(P.err, kPnErrTimeout); break; }
+                if (it > 32) __nanosleep(40);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Epilogue: warps 0-3.
+template <bool FP16>
+__device__ void pn_epilogue(const PnParams &P, const PnShared &S, uint32_t tbase,
+                            volatile uint32_t *abort_flag) {
+    const int lane = threadIdx.x & 31;
+    const int q = threadIdx.x >> 5;                 // TMEM lane quadrant
+    const PnLayout &L = S.L;
+    const int s = 32 * (q & 1) + lane;              // state index within its symbol
+    const uint32_t toff = (uint32_t)(s >> 3) * L.lbo + (uint32_t)(s & 7) * 2u;
+    const float accw = reinterpret_cast<const float *>(S.misc() + kMAcc)[s];
+    const bool even = q < 2;
+    uint32_t g = 0;
+    int done = 0;
+    bool aborted = false;
+    for (int t = 0; !aborted; ++t) {
+        for (int b = 0; b < 2 && !aborted; ++b) {
+            if (done & (1 << b)) continue;
+            if (!pn_wait_ge(S.u32(kMSched + 4 * b), (uint32_t)(t + 2), abort_flag, P.err)) { aborted = true; break; }
+            const int nch = *S.nch(b, t & 1);
+            if (nch == kPnTerminate) { done |= 1 << b; continue; }
+            const PnChunk *ch = S.chunks(b, t & 1);
+            const uint4 *rec = S.rec(b);
+            float2 *xm = S.xmax(b);
+            float2 *fin = S.fin(b);
+            uint8_t *snext = S.base + S.sbuf(b, (t + 1) & 1);
+            for (int k = 0; k < nch; ++k) {
+                const PnChunk d = ch[k];
+                const uint32_t r = g % (uint32_t)L.nregions, u = g / (uint32_t)L.nregions;
+                if (!pn_wait_mbar(S.full_addr((int)r), u & 1u, abort_flag, P.err)) { aborted = true; break; }
+                pn_tc_after();
+                const int c_lo = even ? 0 : d.split;
+                const int c_hi = even ? d.split : d.ncols;
+                const uint32_t tcol = tbase + ((uint32_t)(32 * q) << 16) + (uint32_t)L.ring_base +
+                                      r * kPnRegionCols;
+                for (int c = c_lo & ~15; c < c_hi; c += 16) {
+                    uint32_t v[16];
+                    pn_tmem_ld16(tcol + (uint32_t)c, v);
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) {
+                        const int col = c + i;
+                        if (col < c_lo || col >= c_hi) continue;
+                        const int row = d.row0 + col;
+                        const uint4 rc = rec[row];
+                        const float x = __uint_as_float(v[i]) * __uint_as_float(rc.z);
+                        if (rc.y & kPnFinish) {
+                            float p = x * accw;
+#pragma unroll
+                            for (int o = 16; o > 0; o >>= 1) p += __shfl_xor_sync(0xffffffffu, p, o);
+                            if (lane == 0) {
+                                if (q & 1) fin[row].y = p;
+                                else fin[row].x = p;
+                            }
+                        } else {
+                            *reinterpret_cast<uint16_t *>(snext + rc.x + toff) = pn_to16<FP16>(x);
+                            uint32_t mx;
+                            asm volatile("redux.sync.max.u32 %0, %1, 0xffffffff;"
+                                         : "=r"(mx) : "r"(__float_as_uint(x) & 0x7FFFFFFFu));
+                            if (lane == 0) {
+                                const int dr = (int)(rc.y & 0xFFFFu);
+                                if (q & 1) xm[dr].y = __uint_as_float(mx);
+                                else xm[dr].x = __uint_as_float(mx);
+                            }
+                        }
+                    }
+                }
+                pn_tc_before();
+                __syncwarp();
+                if (lane == 0) atomicAdd(const_cast<uint32_t *>(S.u32(kMEmpty + 4 * r)), 1u);
+                ++g;
+            }
+            if (aborted) break;
+            pn_fence_async_smem();
+            __threadfence_block();
+            __syncwarp();
+            if (lane == 0) atomicAdd(const_cast<uint32_t *>(S.u32(kMEpi + 4 * b)), 1u);
+        }
+        if (done == 3) break;
+    }
+}
+
+template <bool FP16>
+__global__ void __launch_bounds__(kPnThreads, 1) pnfa_tc_kernel(PnParams P) {
+    extern __shared__ __align__(1024) uint8_t pn_smem[];
+    PnShared S{pn_smem, P.L};
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint8_t *misc = S.misc();
+    for (int i = threadIdx.x; i < kPnMiscBytes / 4; i += blockDim.x)
+        reinterpret_cast<uint32_t *>(misc)[i] = 0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int r = 0; r < P.L.nregions; ++r)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(S.full_addr(r)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (threadIdx.x < P.sigma) reinterpret_cast<float *>(misc + kMRsym)[threadIdx.x] = P.rsym[threadIdx.x];
+    if (threadIdx.x < 8) reinterpret_cast<uint4 *>(misc + kMStart)[threadIdx.x] = P.start_img[threadIdx.x];
+    if (threadIdx.x < 64) reinterpret_cast<float *>(misc + kMAcc)[threadIdx.x] = P.acc[threadIdx.x];
+    if (warp == 5) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(pn_smem_u32(misc + kMTmem)), "r"(512));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    pn_tc_before();
+    __syncthreads();
+    pn_tc_after();
+    const uint32_t tbase = *reinterpret_cast<volatile uint32_t *>(misc + kMTmem);
+    // A operands: pair p -> TMEM columns [32p, 32p + 32), lane = row of [T[2p]; T[2p+1]]
+    if (warp < 4) {
+        for (int p = 0; p < P.L.npairs; ++p) {
+            const uint32_t *src = P.tpack + ((size_t)p * 128 + 32 * warp + lane) * 32;
+            uint32_t r[32];
+#pragma unroll
+            for (int k = 0; k < 32; ++k) r[k] = __ldg(src + k);
+            pn_tmem_st32(tbase + ((uint32_t)(32 * warp) << 16) + 32u * p, r);
+        }
+        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+    }
+    pn_tc_before();
+    __syncthreads();
+    pn_tc_after();
+    volatile uint32_t *abort_flag = S.u32(kMAbort);
+    if (warp < 4) pn_epilogue<FP16>(P, S, tbase, abort_flag);
+    else if (warp == 4) pn_scheduler<FP16>(P, S, abort_flag);
+    else if (warp == 5) pn_mma<FP16>(P, S, tbase, abort_flag);
+    else pn_loader(P, S, abort_flag);
+    pn_tc_before();
+    __syncthreads();
+    pn_tc_after();
+    if (warp == 5) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tbase), "r"(512));
+}
+
+// ---- plain FP32 form -------------------------------------------------------------------------
+struct PnPlainParams {
+    const uint8_t *data;
+    int64_t total_bytes;
+    const int64_t *offsets;
+    int64_t n;
+    const float *T;         // [sigma][64][64]
+    const float *start;     // [64]
+    const float *acc;       // [64]
+    int sigma;
+    double ll_empty;
+    double *loglik;
+    uint8_t *accept;
+    int32_t *accept_i32;
+    unsigned long long *queue;
+    uint32_t *err;
+};
+
+constexpr int kPnPlainWarps = 8;
+
+__global__ void __launch_bounds__(kPnPlainWarps * 32) pnfa_plain_kernel(PnPlainParams P) {
+    __shared__ __align__(16) float sv[kPnPlainWarps][64];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    float *v = sv[w];
+    for (;;) {
+        unsigned long long idx = 0;
+        if (lane == 0) idx = atomicAdd(P.queue, 1ull);
+        idx = __shfl_sync(0xffffffffu, idx, 0);
+        if (idx >= (unsigned long long)P.n) break;
+        const int64_t p0 = P.offsets[idx], p1 = P.offsets[idx + 1];
+        if (p0 < 0 || p1 < p0 || p1 > P.total_bytes) {
+            if (lane == 0) atomicOr(P.err, kPnErrOffsets);
+            continue;
+        }
+        float s0 = P.start[lane], s1 = P.start[lane + 32];
+        int64_t E = 0;
+        for (int64_t base = p0; base < p1; base += 32) {
+            const int64_t pl = base + lane;
+            const uint32_t mybyte = pl < p1 ? P.data[pl] : 255u;
+            const int nb = (int)min((int64_t)32, p1 - base);
+            for (int k = 0; k < nb; ++k) {
+                const uint32_t c = __shfl_sync(0xffffffffu, mybyte, k);
+                if (c >= (uint32_t)P.sigma) continue;
+                v[lane] = s0;
+                v[lane + 32] = s1;
+                __syncwarp();
+                const float4 *r0 = reinterpret_cast<const float4 *>(P.T + ((size_t)c * 64 + lane) * 64);
+                const float4 *r1 = reinterpret_cast<const float4 *>(P.T + ((size_t)c * 64 + lane + 32) * 64);
+                const float4 *vv = reinterpret_cast<const float4 *>(v);
+                float a0 = 0.f, a1 = 0.f;
+#pragma unroll
+                for (int q = 0; q < 16; ++q) {
+                    const float4 x = vv[q];
+                    const float4 t0 = __ldg(r0 + q), t1 = __ldg(r1 + q);
+                    a0 = fmaf(t0.x, x.x, a0); a0 = fmaf(t0.y, x.y, a0);
+                    a0 = fmaf(t0.z, x.z, a0); a0 = fmaf(t0.w, x.w, a0);
+                    a1 = fmaf(t1.x, x.x, a1); a1 = fmaf(t1.y, x.y, a1);
+                    a1 = fmaf(t1.z, x.z, a1); a1 = fmaf(t1.w, x.w, a1);
+                }
+                __syncwarp();
+                float m = fmaxf(fabsf(a0), fabsf(a1));
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+                if (m > 0.f) {
+                    // frexp exponent of m: m = mant * 2^e, mant in [0.5, 1)
+                    uint32_t bits = __float_as_uint(m);
+                    int pre = 0;
+                    if (((bits >> 23) & 0xFFu) == 0) {   // subnormal: lift by 2^64 first
+                        m *= 18446744073709551616.0f;
+                        bits = __float_as_uint(m);
+                        pre = 64;
+                    }
+                    const int e = (int)((bits >> 23) & 0xFFu) - 126 - pre;
+                    // scale by 2^-e in (at most) two exact steps
+                    const int e1 = max(min(e, 126), -126);
+                    const float sc1 = pn_pow2(-e1);
+                    s0 = a0 * sc1;
+                    s1 = a1 * sc1;
+                    if (e != e1) {
+                        const float sc2 = pn_pow2(-(e - e1));
+                        s0 *= sc2;
+                        s1 *= sc2;
+                    }
+                    E += e;
+                } else {
+                    s0 = 0.f;
+                    s1 = 0.f;
+                }
+            }
+        }
+        float d = s0 * P.acc[lane] + s1 * P.acc[lane + 32];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+        if (lane == 0) {
+            const double ll = d > 0.f ? log((double)d) + (double)E * 0.69314718055994530942 : -INFINITY;
+            pn_write_result(P.loglik, P.accept, P.accept_i32, (int64_t)idx, ll);
+        }
+    }
+}
+
+}  // namespace trex
+
+// ---- handle -----------------------------------------------------------------------------------
+struct trex_pnfa {
+    int n_states = 0, sigma = 0, npairs = 0, n_sms = 0;
+    double ll_empty = 0.0;
+    float start_max16[2] = {0.f, 0.f};   // [bf16, fp16]
+    float *d_T32 = nullptr, *d_start32 = nullptr, *d_acc = nullptr;
+    uint32_t *d_tpack[2] = {nullptr, nullptr};
+    float *d_rsym[2] = {nullptr, nullptr};
+    uint4 *d_simg[2] = {nullptr, nullptr};
+    uint8_t *d_misc = nullptr;   // [0,8) queue, [8,12) error word
+};
+
+namespace trex {
+
+static uint16_t pn_host16(float x, bool fp16) {
+    if (fp16) {
+        const __half h = __float2half_rn(x);
+        return __half_as_ushort(h);
+    }
+    const __nv_bfloat16 b = __float2bfloat16_rn(x);
+    return __bfloat16_as_ushort(b);
+}
+static float pn_host16_to_f(uint16_t v, bool fp16) {
+    if (fp16) return __half2float(__ushort_as_half(v));
+    return __bfloat162float(__ushort_as_bfloat16(v));
+}
+
+static void pn_free(trex_pnfa *h) {
+    cudaFree(h->d_T32);
+    cudaFree(h->d_start32);
+    cudaFree(h->d_acc);
+    for (int k = 0; k < 2; ++k) {
+        cudaFree(h->d_tpack[k]);
+        cudaFree(h->d_rsym[k]);
+        cudaFree(h->d_simg[k]);
+    }
+    cudaFree(h->d_misc);
+}
+
+static int pn_choose(const trex_pnfa *h, int64_t n, int *grid, int *p_sub) {
+    int pmax = 0;
+    for (int p = 32; p <= kPnMaxPSub; p += 32)
+        if (pn_layout(p, h->sigma).total <= kPnSmemCap) pmax = p;
+    if (pmax == 0) return TREX_ERR_SHAPE;
+    const int64_t sms = h->n_sms;
+    if (n <= sms * 64) {
+        *grid = (int)std::max<int64_t>(1, (n + 63) / 64);
+        *p_sub = 32;
+    } else {
+        *grid = (int)sms;
+        int64_t need = (n + 2 * sms - 1) / (2 * sms);
+        need = (need + 31) / 32 * 32;
+        *p_sub = (int)std::min<int64_t>(need, pmax);
+    }
+    return TREX_OK;
+}
+
+}  // namespace trex
+
+extern "C" {
+
+int trex_pnfa_create(int n_states, int sigma, const float *T, const float *start, const float *accept,
+                     trex_pnfa **out) {
+    using namespace trex;
+    if (!out) return TREX_ERR_ARG;
+    *out = nullptr;
+    if (n_states < 1 || n_states > kPnStates || sigma < 1 || sigma > 255 || !T || !start || !accept)
+        return TREX_ERR_ARG;
+    trex_pnfa *h = new (std::nothrow) trex_pnfa();
+    if (!h) return TREX_ERR_OOM;
+    h->n_states = n_states;
+    h->sigma = sigma;
+    h->npairs = (sigma + 1) / 2;
+    h->n_sms = sm_count();
+    if (h->n_sms <= 0) {
+        delete h;
+        set_last_error_msg("trex_pnfa_create: no CUDA device");
+        return TREX_ERR_SHAPE;
+    }
+    const int N = n_states;
+    // padded FP32 copies (states >= n_states are zero: they never gain mass)
+    std::vector<float> T32((size_t)sigma * 64 * 64, 0.f), s32(64, 0.f), a32(64, 0.f);
+    for (int c = 0; c < sigma; ++c)
+        for (int d = 0; d < N; ++d)
+            for (int q = 0; q < N; ++q) T32[((size_t)c * 64 + d) * 64 + q] = T[((size_t)c * N + d) * N + q];
+    double dot = 0.0;
+    for (int i = 0; i < N; ++i) {
+        s32[i] = start[i];
+        a32[i] = accept[i];
+        dot += (double)start[i] * (double)accept[i];
+    }
+    h->ll_empty = dot > 0.0 ? std::log(dot) : -INFINITY;
+    std::vector<uint32_t> tp[2];
+    std::vector<float> rs[2];
+    std::vector<uint4> simg[2];
+    for (int k = 0; k < 2; ++k) {
+        const bool fp16 = k == 1;
+        tp[k].assign((size_t)h->npairs * 128 * 32, 0u);
+        rs[k].assign(sigma, 0.f);
+        for (int c = 0; c < sigma; ++c) {
+            const int p = c >> 1, half_ = c & 1;
+            double rmax = 0.0;
+            for (int d = 0; d < 64; ++d) {
+                double rsum = 0.0;
+                for (int q = 0; q < 64; ++q) {
+                    const uint16_t v = pn_host16(T32[((size_t)c * 64 + d) * 64 + q], fp16);
+                    rsum += std::fabs((double)pn_host16_to_f(v, fp16));
+                    uint32_t &w = tp[k][((size_t)p * 128 + half_ * 64 + d) * 32 + (q >> 1)];
+                    w |= (uint32_t)v << (16 * (q & 1));
+                }
+                rmax = std::max(rmax, rsum);
+            }
+            // a little above the largest row sum: bounds max|T s| / max|s| through FP32 rounding
+            rs[k][c] = (float)(rmax * (1.0 + 1.0 / 64));
+        }
+        simg[k].assign(8, make_uint4(0, 0, 0, 0));
+        float smax = 0.f;
+        for (int i = 0; i < 64; ++i) {
+            const uint16_t v = pn_host16(s32[i], fp16);
+            smax = std::max(smax, std::fabs(pn_host16_to_f(v, fp16)));
+            uint32_t *w = reinterpret_cast<uint32_t *>(&simg[k][i >> 3]);
+            w[(i & 7) >> 1] |= (uint32_t)v << (16 * (i & 1));
+        }
+        h->start_max16[k] = smax;
+    }
+    cudaError_t e = cudaSuccess;
+    auto up = [&](void **dst, const void *src, size_t bytes) {
+        if (e != cudaSuccess) return;
+        if ((e = cudaMalloc(dst, std::max<size_t>(bytes, 16))) != cudaSuccess) return;
+        if (bytes) e = cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice);
+    };
+    up((void **)&h->d_T32, T32.data(), T32.size() * 4);
+    up((void **)&h->d_start32, s32.data(), 256);
+    up((void **)&h->d_acc, a32.data(), 256);
+    for (int k = 0; k < 2; ++k) {
+        up((void **)&h->d_tpack[k], tp[k].data(), tp[k].size() * 4);
+        up((void **)&h->d_rsym[k], rs[k].data(), rs[k].size() * 4);
+        up((void **)&h->d_simg[k], simg[k].data(), 8 * sizeof(uint4));
+    }
+    if (e == cudaSuccess) e = cudaMalloc(&h->d_misc, 16);
+    if (e == cudaSuccess) e = cudaMemset(h->d_misc, 0, 16);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(pnfa_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kPnSmemCap);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(pnfa_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kPnSmemCap);
+    if (e != cudaSuccess) {
+        set_last_error("trex_pnfa_create", e);
+        pn_free(h);
+        delete h;
+        return e == cudaErrorMemoryAllocation ? TREX_ERR_OOM : TREX_ERR_CUDA;
+    }
+    *out = h;
+    return TREX_OK;
+}
+
+void trex_pnfa_destroy(trex_pnfa *h) {
+    if (!h) return;
+    trex::pn_free(h);
+    delete h;
+}
+
+int trex_pnfa_run(trex_pnfa *h, int mode, const uint8_t *data, const int64_t *offsets,
+                  int64_t n_strings, int64_t total_bytes, double *loglik, uint8_t *accept,
+                  int32_t *accept_i32, void *stream) {
+    using namespace trex;
+    if (!h) return TREX_ERR_NOT_INIT;
+    if (n_strings < 0 || total_bytes < 0 || n_strings >= (int64_t)1 << 31) return TREX_ERR_ARG;
+    if (mode < TREX_PNFA_BF16 || mode > TREX_PNFA_FP32) return TREX_ERR_ARG;
+    if (n_strings == 0) return TREX_OK;
+    if (!offsets || (total_bytes > 0 && !data)) return TREX_ERR_ARG;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    unsigned long long *queue = reinterpret_cast<unsigned long long *>(h->d_misc);
+    uint32_t *err = reinterpret_cast<uint32_t *>(h->d_misc + 8);
+    TREX_CUDA(cudaMemsetAsync(h->d_misc, 0, 16, st));
+    if (mode == TREX_PNFA_FP32) {
+        PnPlainParams Q;
+        Q.data = data;
+        Q.total_bytes = total_bytes;
+        Q.offsets = offsets;
+        Q.n = n_strings;
+        Q.T = h->d_T32;
+        Q.start = h->d_start32;
+        Q.acc = h->d_acc;
+        Q.sigma = h->sigma;
+        Q.ll_empty = h->ll_empty;
+        Q.loglik = loglik;
+        Q.accept = accept;
+        Q.accept_i32 = accept_i32;
+        Q.queue = queue;
+        Q.err = err;
+        const int64_t warps = std::min<int64_t>(n_strings, (int64_t)h->n_sms * 64);
+        const int grid = (int)std::max<int64_t>(1, (warps + kPnPlainWarps - 1) / kPnPlainWarps);
+        profile_kernel_begin(st);
+        pnfa_plain_kernel<<<grid, kPnPlainWarps * 32, 0, st>>>(Q);
+        profile_kernel_end(st);
+        TREX_CHECK_LAUNCH();
+        return TREX_OK;
+    }
+    if (h->sigma > kPnMaxSigmaTc) {
+        set_last_error_msg("trex_pnfa_run: the tensor-core form takes at most 28 symbols");
+        return TREX_ERR_SHAPE;
+    }
+    int grid = 0, p_sub = 0;
+    int rc = pn_choose(h, n_strings, &grid, &p_sub);
+    if (rc) return rc;
+    const int k = mode == TREX_PNFA_FP16 ? 1 : 0;
+    PnParams P;
+    P.data = data;
+    P.total_bytes = total_bytes;
+    P.offsets = offsets;
+    P.n = n_strings;
+    P.tpack = h->d_tpack[k];
+    P.rsym = h->d_rsym[k];
+    P.start_img = h->d_simg[k];
+    P.acc = h->d_acc;
+    P.start_max = h->start_max16[k];
+    P.ll_empty = h->ll_empty;
+    P.sigma = h->sigma;
+    P.loglik = loglik;
+    P.accept = accept;
+    P.accept_i32 = accept_i32;
+    P.queue = queue;
+    P.err = err;
+    P.L = pn_layout(p_sub, h->sigma);
+    // one CTA per SM: it owns all 512 TMEM columns
+    const uint32_t smem = std::max<uint32_t>(P.L.total, 120u * 1024u);
+    profile_kernel_begin(st);
+    if (k) pnfa_tc_kernel<true><<<grid, kPnThreads, smem, st>>>(P);
+    else pnfa_tc_kernel<false><<<grid, kPnThreads, smem, st>>>(P);
+    profile_kernel_end(st);
+    TREX_CHECK_LAUNCH();
+    return TREX_OK;
+}
+
+int trex_pnfa_error(trex_pnfa *h, int32_t *err_out) {
+    if (!h || !err_out) return TREX_ERR_ARG;
+    uint32_t v = 0;
+    TREX_CUDA(cudaMemcpy(&v, h->d_misc + 8, 4, cudaMemcpyDeviceToHost));
+    *err_out = (int32_t)v;
+    return TREX_OK;
+}
+
+}  // extern "C"

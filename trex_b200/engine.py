@@ -231,3 +231,65 @@ class NFA:
         v = ctypes.c_int32(0)
         _lib.check(self.lib.trex_nfa_error(self._h, ctypes.byref(v)), "trex_nfa_error")
         return v.value
+
+
+PNFA_MODES = {"bf16": 0, "fp16": 1, "fp32": 2}
+
+
+class PNFA:
+    """Resident probabilistic NFA (at most 64 states): s' = T[c] s per symbol,
+    result log(dot(s_L, accept)) in FP64 (reference
+    cuda/nfa_tc_evolution.cu:456-610 computes only dot > 0.5).
+
+    Modes: "bf16" / "fp16" run the tcgen05 tensor-core kernel (16-bit
+    operands, FP32 accumulation, sigma <= 28); "fp32" the CUDA-core kernel.
+    """
+
+    def __init__(self, T, start_vec, accept_vec):
+        self.lib = _lib.load()
+        T = np.ascontiguousarray(np.asarray(T, dtype=np.float32))
+        if T.ndim != 3 or T.shape[1] != T.shape[2]:
+            raise ValueError("T must have shape (sigma, n, n)")
+        self.sigma, self.n_states, _ = T.shape
+        start = np.ascontiguousarray(np.asarray(start_vec, dtype=np.float32).reshape(-1))
+        acc = np.ascontiguousarray(np.asarray(accept_vec, dtype=np.float32).reshape(-1))
+        if start.size != self.n_states or acc.size != self.n_states:
+            raise ValueError("start and accept vectors must have n entries")
+        h = ctypes.c_void_p()
+        rc = self.lib.trex_pnfa_create(self.n_states, self.sigma, _lib.ptr(T, ctypes.c_float),
+                                       _lib.ptr(start, ctypes.c_float), _lib.ptr(acc, ctypes.c_float),
+                                       ctypes.byref(h))
+        _lib.check(rc, "trex_pnfa_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.trex_pnfa_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, data, offsets, mode: str = "bf16", *, loglik=None, accept=None, stream=None):
+        """Device run: returns (loglik float64 tensor [n], accept uint8 tensor [n])."""
+        torch = _torch()
+        if mode not in PNFA_MODES:
+            raise ValueError(f"mode must be one of {sorted(PNFA_MODES)}")
+        n = offsets.numel() - 1
+        if loglik is None:
+            loglik = torch.empty(max(n, 1), dtype=torch.float64, device=offsets.device)
+        if accept is None:
+            accept = torch.empty(max(n, 1), dtype=torch.uint8, device=offsets.device)
+        rc = self.lib.trex_pnfa_run(self._h, PNFA_MODES[mode], _dptr(data), _dptr(offsets), n,
+                                    data.numel(), _dptr(loglik), _dptr(accept), None,
+                                    _stream_handle(stream))
+        _lib.check(rc, "trex_pnfa_run")
+        return loglik[:n], accept[:n]
+
+    def error_word(self) -> int:
+        v = ctypes.c_int32(0)
+        _lib.check(self.lib.trex_pnfa_error(self._h, ctypes.byref(v)), "trex_pnfa_error")
+        return v.value
