@@ -14,6 +14,10 @@ Workloads (synthetic, seeded; the reference ships no dataset):
       writes the state of every position (2 bytes moved per character).
   nfa: random 64-state Boolean NFA over 20 symbols (bytes 0..19), per-symbol
       edge density 0.05, 256K strings x 4096 symbols, bit-parallel kernel.
+  pnfa: probabilistic 64-state NFA over 20 symbols (rows Dirichlet(0.5) x 0.9,
+      ~30% kept), 64K strings x 2048 symbols, tcgen05 kernel with BF16 (or
+      --pnfa-mode fp16 / fp32) operands; also reports the log-likelihood error
+      against the FP64 oracle on 256 strings.
 
 Multi-GPU: one process per GPU (torchrun); every rank runs its own seeded
 batch (weak scaling, no data-path collective); times are the max over ranks
@@ -52,7 +56,9 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["trex", "reference"], default="trex")
-    ap.add_argument("--workload", choices=["ragged", "plain", "scan", "nfa"], default="ragged")
+    ap.add_argument("--workload", choices=["ragged", "plain", "scan", "nfa", "pnfa"], default="ragged")
+    ap.add_argument("--pnfa-mode", choices=["bf16", "fp16", "fp32"], default="bf16",
+                    help="operand type of the probabilistic NFA workload")
     ap.add_argument("--strings", type=int, default=None, help="override the number of strings")
     ap.add_argument("--seg-len", type=int, default=0, help="bytes per work item / scan tile (0 = default)")
     ap.add_argument("--dfa-sizes", type=str, default=None,
@@ -115,6 +121,8 @@ def host_bytes(lens, is_sub, seed):
 
 class DFAWorkload:
     """ragged / plain / scan: byte DFAs over CSR strings."""
+
+    dtype = ref_dtype = "u8"
 
     def __init__(self, args):
         from trex_b200.workloads import ACGT, random_dfa
@@ -281,6 +289,7 @@ class NFAWorkload:
     kind = "nfa"
     kernel = "nfa_bitpar_kernel"
     launches_per_step = 1
+    dtype = ref_dtype = "u64"
 
     def __init__(self, args):
         from trex_b200.workloads import random_bool_nfa
@@ -377,6 +386,122 @@ class NFAWorkload:
         return k, k * self.L, data
 
 
+class PNFAWorkload:
+    """Probabilistic NFA, 64 states, 20 symbols (tcgen05 kernel, or the FP32 kernel)."""
+
+    kind = "pnfa"
+    launches_per_step = 1
+    bound = "tensor"
+    ref_dtype = "f64"
+
+    def __init__(self, args):
+        from trex_b200.workloads import random_prob_nfa
+        self.args = args
+        self.mode = args.pnfa_mode
+        rng = np.random.default_rng(args.seed)
+        self.T, self.start, self.acc = random_prob_nfa(rng, 64, 20)
+        self.n = args.strings or 65536
+        self.L = 2048
+        self.off = np.arange(self.n + 1, dtype=np.int64) * self.L
+        self.kernel = "pnfa_plain_kernel" if self.mode == "fp32" else "pnfa_tc_kernel"
+        self.dtype = {"bf16": "bf16", "fp16": "f16", "fp32": "f32"}[self.mode]
+        self.workload = ("probabilistic NFA: 64 states, 20 symbols (bytes 0..19), rows of T[c] "
+                         "Dirichlet(0.5) x 0.9 with ~30% kept, start e0, accept all states; "
+                         f"{self.n} strings x 2048 symbols; {self.mode} operands"
+                         + ("" if self.mode == "fp32" else ", FP32 accumulation (tcgen05)"))
+
+    def setup(self, torch, dev, seed):
+        from trex_b200.engine import PNFA
+        self.torch = torch
+        self.total = self.n * self.L
+        g = torch.Generator(device=dev)
+        g.manual_seed(seed + 4)
+        self.data = torch.randint(0, 20, (self.total,), dtype=torch.uint8, device=dev, generator=g)
+        self.d_off = torch.from_numpy(self.off).to(dev)
+        self.pnfa = PNFA(self.T, self.start, self.acc)
+        self.ll = torch.empty(self.n, dtype=torch.float64, device=dev)
+        self.ac = torch.empty(self.n, dtype=torch.uint8, device=dev)
+        self.set = self.pnfa
+
+    def step(self, stream):
+        self.pnfa.run(self.data, self.d_off, self.mode, loglik=self.ll, accept=self.ac, stream=stream)
+
+    def error_word(self):
+        return self.pnfa.error_word()
+
+    @property
+    def chars(self):
+        return self.total
+
+    @property
+    def alg_bytes(self):
+        return self.total + 17 * self.n
+
+    @property
+    def alg_flops(self):
+        return 2.0 * 64 * 64 * self.total
+
+    def config(self):
+        return {"workload": self.workload, "n_strings": self.n, "total_bytes_per_gpu": self.total,
+                "useful_flops_per_char": 2 * 64 * 64, "mode": self.mode,
+                "l2": "inputs (134 MB) larger than L2 (126 MB), no flush"}
+
+    def llerr(self, orc, k=256):
+        """Max relative log-likelihood error vs the FP64 oracle on the first k strings."""
+        data = self.data[:k * self.L].cpu().numpy()
+        ref = orc.pnfa_fp64(self.T, self.start, self.acc, data, self.off[:k + 1])
+        got = self.ll[:k].cpu().numpy()
+        return float(np.max(np.abs(got - ref) / np.maximum(1.0, np.abs(ref))))
+
+    def e2e(self, torch, steps, dist, dev):
+        # the public API with host buffers: pinned H2D of the step's bytes and offsets,
+        # the run, D2H of the log-likelihoods, every step
+        h_data = torch.empty(self.total, dtype=torch.uint8, pin_memory=True)
+        h_data.copy_(self.data)
+        h_off = torch.from_numpy(self.off).pin_memory()
+        h_ll = torch.empty(self.n, dtype=torch.float64).pin_memory()
+        d_data = torch.empty_like(self.data)
+        d_off = torch.empty_like(self.d_off)
+        d_ll = torch.empty_like(self.ll)
+
+        def one():
+            d_data.copy_(h_data, non_blocking=True)
+            d_off.copy_(h_off, non_blocking=True)
+            self.pnfa.run(d_data, d_off, self.mode, loglik=d_ll)
+            h_ll.copy_(d_ll, non_blocking=True)
+            torch.cuda.current_stream().synchronize()
+
+        one()
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            one()
+        dt = time.perf_counter() - t0
+        if dist:
+            t = torch.tensor([dt], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            dt = float(t.item())
+        if not np.array_equal(h_ll.numpy(), self.ll.cpu().numpy()):
+            raise RuntimeError("host-buffer run disagrees with the device run")
+        return dt, int(self.total + self.off.nbytes), int(h_ll.numpy().nbytes)
+
+    def cpu_run(self, orc, data, k):
+        orc.pnfa_fp64(self.T, self.start, self.acc, data, self.off[:k + 1])
+
+    def cpu_sample(self, seed, seconds, threads):
+        rng = np.random.default_rng(seed + 5)
+        from oracle import oracle as orc
+        k0 = max(1, min(self.n, threads * 2))
+        data0 = rng.integers(0, 20, size=k0 * self.L, dtype=np.uint8)
+        t0 = time.perf_counter()
+        self.cpu_run(orc, data0, k0)
+        rate = k0 * self.L / max(time.perf_counter() - t0, 1e-6)
+        k = max(1, min(self.n, int(seconds * rate / self.L)))
+        data = rng.integers(0, 20, size=k * self.L, dtype=np.uint8)
+        return k, k * self.L, data
+
+
 # ---------------------------------------------------------------------------------
 # clocks
 # ---------------------------------------------------------------------------------
@@ -453,6 +578,14 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def measured_tensor_peak():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d.get("bf16_tflops_sustained", d["bf16_tflops"])), "measured"
+    return 1400.0, "fallback"
+
+
 def committed_traffic(kernel: str, workload: str):
     """DRAM bytes per launch recorded from an ncu capture in profiles/."""
     for f in sorted((REPO / "profiles").glob("*.md")):
@@ -468,14 +601,18 @@ def committed_traffic(kernel: str, workload: str):
 # ---------------------------------------------------------------------------------
 
 def make_workload(args):
-    return NFAWorkload(args) if args.workload == "nfa" else DFAWorkload(args)
+    if args.workload == "nfa":
+        return NFAWorkload(args)
+    if args.workload == "pnfa":
+        return PNFAWorkload(args)
+    return DFAWorkload(args)
 
 
 def base_line(args, wl, value, ms_per_step, steps, warmup, world):
     return {
         "metric": METRIC, "value": value, "unit": "Gchar/s", "n_gpus": world, "steps": steps,
         "warmup": warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u8",
+        "vs_baseline": None, "dtype": wl.dtype,
         "data": "synthetic (seeded, generated on the device)",
     }
 
@@ -505,7 +642,8 @@ def reference_arm(args, rank):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "Gchar/s",
         "n_gpus": args.gpus, "steps": len(times), "warmup": args.warmup,
         "ms_per_step": tot / len(times) * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded, same generator as the trex arm)",
+        "vs_baseline": None, "dtype": wl.ref_dtype,
+        "data": "synthetic (seeded, same generator as the trex arm)",
         "config": {"workload": wl.workload, "n_strings": wl.n, "parallelism": "cpu"},
         "cpu_baseline": {"value": value, "unit": "Gchar/s", "cores": threads, "kind": "port",
                          "sample": sample},
@@ -567,10 +705,23 @@ def trex_arm(args, rank, world, local_rank):
     chars_all = wl.chars * world
     value = chars_all / (ms_per_step * 1e-3) / 1e9
 
-    peak, peak_kind = measured_peaks()
     kmean = sum(kern_ms) / max(1, len(kern_ms))
-    achieved = wl.alg_bytes / (kmean * 1e-3) / 1e9
     traffic = committed_traffic(wl.kernel, args.workload)
+    if getattr(wl, "bound", "hbm") == "tensor":
+        peak, peak_kind = measured_tensor_peak()
+        achieved = wl.alg_flops / (kmean * 1e-3) / 1e12
+        roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak, "traffic": traffic, "kernel": wl.kernel,
+                "kernel_ms_mean": kmean, "algorithmic_flops_per_launch": wl.alg_flops,
+                "peak_source": f"MEASURED_PEAKS.json bf16_tflops_sustained ({peak_kind}); "
+                               "useful flops 2*64*64 per symbol (the pair layout issues 2x)"}
+    else:
+        peak, peak_kind = measured_peaks()
+        achieved = wl.alg_bytes / (kmean * 1e-3) / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "kernel": wl.kernel,
+                "kernel_ms_mean": kmean, "algorithmic_bytes_per_launch": wl.alg_bytes,
+                "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})"}
 
     e2e = None
     res = wl.e2e(torch, args.e2e_steps, dist, dev)
@@ -594,10 +745,11 @@ def trex_arm(args, rank, world, local_rank):
     if rank == 0:
         line = base_line(args, wl, value, ms_per_step, args.steps, warm, world)
         line["config"] = {**wl.config(), "parallelism": f"dp{world} (independent shards, no collective)"}
-        line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                            "frac": achieved / peak, "traffic": traffic, "kernel": wl.kernel,
-                            "kernel_ms_mean": kmean, "algorithmic_bytes_per_launch": wl.alg_bytes,
-                            "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})"}
+        line["roofline"] = roof
+        if hasattr(wl, "llerr"):
+            from oracle import oracle as orc
+            orc.build()
+            line["loglik_max_rel_err_vs_fp64"] = wl.llerr(orc)
         line["e2e"] = e2e
         line["cpu_baseline"] = cpu
         line["gpu_launches"] = wl.launches_per_step * args.steps

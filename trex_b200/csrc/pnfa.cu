@@ -32,34 +32,36 @@
 // strings, rows 64-127 for the odd ones (half the MMA work is discarded: the
 // price of keeping A in TMEM and B small).
 //
-// Warp roles (256 threads): warps 0-3 epilogue (warp q reads TMEM lanes
-// 32q..32q+31), warp 4 scheduler, warp 5 MMA issuer (and TMEM owner), warps
-// 6-7 loader.
-//  * loader: gives each slot its next string from a global atomic queue and
-//    copies the next 16 valid symbols of every slot into a shared block
-//    (strings change slots only at 16-step block boundaries).
-//  * scheduler: per step and sub-batch, sorts the slots of the next step by
-//    symbol pair (counting sort with shared atomics), writes the chunk list,
-//    writes the start vector into the rows of strings that begin, and for
-//    the current step writes one record per column: destination row in the
-//    next B buffer and the scale 2^-f, f from the bound max|s_t| * R_c with
-//    R_c = max row sum of |T[c]| (so max|s_t+1| < 1) and max|s_t| measured by
-//    the previous epilogue. When a string ends it turns the two partial dot
-//    products left by the epilogue into the FP64 log-likelihood.
-//  * MMA: per chunk waits for a free ring region, issues 4 tcgen05.mma
-//    (A from TMEM, B from shared memory, no swizzle) and commits to the
-//    region's mbarrier.
-//  * epilogue: tcgen05.ld of the region, scale, round to 16 bits and store
-//    each state into the string's row of the next B buffer; warp max (redux)
-//    of the column for the next step's scale; for a string's last symbol the
-//    accept-weighted sum instead.
-// B buffers (shared memory, K-major, no swizzle): row r, state k at
-// (k/8)*LBO + r*16 + (k%8)*2 with LBO = rows*16 and rows = 1 (mod 8), so the
-// 32 lanes of an epilogue store hit 32 different banks and an MMA may start
-// at any row.
-// Every wait is bounded; a wait that runs out sets the error word (bit 2) and
-// an abort flag that every role polls, the MMA warp drains its commits and
-// the TMEM is freed before the kernel returns.
+// Warp roles (480 threads):
+//  * warps 0-7, epilogue, two sets of four taking alternate chunks (warp q of a
+//    set reads TMEM lanes 32q..32q+31 with 16x256b loads, four states of four
+//    columns a thread): it scales each string's states by the record's 2^-f,
+//    rounds them to 16 bits, stores them in pairs in the string's row of the
+//    next B buffer and records max|s_t+1| (a butterfly max); on a string's
+//    last symbol it writes the accept-weighted sum instead.
+//  * warp 8, MMA: per chunk waits for a free ring region, issues 4
+//    tcgen05.mma (A from TMEM, B from shared memory, no swizzle) and commits
+//    to the region's mbarrier.
+//  * warps 9-12, planner: per step and sub-batch, sorts the slots of the step
+//    by symbol pair (counting sort with shared atomics), writes the chunk list
+//    and the start vector into the rows of strings that begin; for the
+//    previous step it writes one record per row: the string's row in the next
+//    B buffer and the scale 2^-f, f = the exponent of max|s| * R_c (R_c = max
+//    row sum of |T[c]|, so max|s'| < 1; max|s| left by the epilogue), adding f
+//    to the string's exponent sum; and it turns finished strings' dot
+//    products and exponents into the FP64 log-likelihood.
+//  * warps 13-14, loader: gives each slot its next string from a global
+//    atomic queue and copies the next 16 valid symbols of every slot into a
+//    shared block (strings change slots only at 16-step block boundaries).
+// Hand-offs are mbarriers (one per sub-batch and step parity, so no waiter is
+// ever two phases behind); the planner warps meet at a named barrier and only
+// their leader waits on mbarriers. B buffers (shared memory, K-major, no
+// swizzle): row r, state k at (k/8)*LBO + r*16 + (k%8)*2 with LBO = rows*16 and
+// rows = 1 (mod 8), so the 32 lanes of an epilogue store hit 32 different banks
+// and an MMA may start at any row.
+// Every wait is bounded; one that runs out sets the error word (bit 2) and an
+// abort flag that every role polls; the MMA warp drains its commits and the
+// TMEM is freed before the kernel returns.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -75,19 +77,24 @@ namespace trex {
 
 constexpr int kPnStates = 64;
 constexpr int kPnBlk = 16;             // steps per symbol block
-constexpr int kPnThreads = 256;
-constexpr int kPnMaxPSub = 256;        // slots per sub-batch (8 per scheduler lane)
+constexpr int kPnEpiWarps = 8, kPnMmaWarp = 8, kPnPlanWarp0 = 9, kPnPlanWarps = 4,
+              kPnLoadWarp0 = 13, kPnLoadWarps = 2;
+constexpr int kPnThreads = 32 * (kPnLoadWarp0 + kPnLoadWarps);
+constexpr int kPnPlanThreads = 32 * kPnPlanWarps;
+constexpr int kPnMaxPSub = 256;        // slots per sub-batch (2 per planner thread)
 constexpr int kPnMaxChunks = 32;
-constexpr int kPnRegionCols = 64;
+constexpr int kPnRegionCols = 32;
+constexpr int kPnMaxRegions = 6;
 constexpr int kPnMaxSigmaTc = 28;      // 14 pairs: 448 TMEM columns + one ring region
-constexpr int kPnMiscBytes = 1280;
+constexpr int kPnMiscBytes = 2048;
 constexpr uint32_t kPnSmemCap = 232448;
-constexpr uint32_t kPnFinish = 0x80000000u;
 constexpr int32_t kPnTerminate = -1;
 constexpr uint32_t kPnErrOffsets = 1u, kPnErrTimeout = 4u;
-constexpr uint32_t kPnSpinLimit = 1u << 25;
+constexpr long long kPnWaitCycles = 4000000000ll;   // about 2 s
 
-// slot flags (scheduler)
+// record of a row (one string at one step), written by the planner
+constexpr uint32_t kRecFinish = 1u << 31;
+// slot flags (planner)
 constexpr uint8_t kSlotActive = 1, kSlotLast = 2, kSlotFresh = 4, kSlotFinPending = 8;
 // header flags (loader)
 constexpr uint8_t kHdrStart = 1, kHdrEnd = 2;
@@ -98,10 +105,13 @@ struct PnHdr {
     uint16_t pad;
 };
 struct PnSlot {
-    int32_t seq, E;           // string in the slot and its exponent sum
-    int32_t fin_seq, fin_E;   // string whose last step's dot products are pending
-    int16_t row, finrow;
-    uint8_t c, flags, blkcnt, blkflags;
+    int32_t seq;          // string in the slot
+    int32_t E;            // its exponent sum
+    int32_t fin_seq;      // string whose last step's results are pending
+    int32_t fin_step;     // that last step
+    int32_t fin_E;        // and its final exponent sum
+    int16_t row;          // row at the current (last planned) step
+    uint8_t c, flags, blkcnt, blkflags, pad0, pad1;
 };
 struct PnChunk {
     uint16_t row0;
@@ -111,8 +121,8 @@ struct PnChunk {
 struct PnLayout {
     int p_sub, rows, npairs, nregions, ring_base;
     uint32_t lbo;
-    uint32_t s_off, sym_off, hdr_off, rec_off, xmax_off, fin_off, chunk_off, slot_off, misc_off,
-        total;
+    uint32_t s_off, sym_off, hdr_off, rec_off, xmax_off, fin_off, chunk_off, slot_off,
+        misc_off, total;
 };
 
 __host__ __device__ inline uint32_t pn_align16(uint32_t x) { return (x + 15u) & ~15u; }
@@ -122,38 +132,53 @@ static PnLayout pn_layout(int p_sub, int sigma) {
     L.p_sub = p_sub;
     L.npairs = (sigma + 1) / 2;
     L.ring_base = 32 * L.npairs;
-    L.nregions = std::min(6, (512 - L.ring_base) / kPnRegionCols);
+    L.nregions = std::min(kPnMaxRegions, (512 - L.ring_base) / kPnRegionCols);
     int rows = p_sub + 16;
     while (rows % 8 != 1) ++rows;
     L.rows = rows;
     L.lbo = (uint32_t)rows * 16u;
+    const uint32_t ps = (uint32_t)p_sub, nr = (uint32_t)rows;
     uint32_t off = 0;
-    L.s_off = off;
+    L.s_off = off;                    // [b][parity] B buffers, 8 * lbo bytes each
     off += 4u * 8u * L.lbo;
-    L.sym_off = off;
-    off += 2u * kPnBlk * 2u * (uint32_t)p_sub;
-    L.hdr_off = pn_align16(off);
-    off = L.hdr_off + 2u * 2u * (uint32_t)p_sub * (uint32_t)sizeof(PnHdr);
-    L.rec_off = pn_align16(off);
-    off = L.rec_off + 2u * (uint32_t)rows * 16u;
-    L.xmax_off = off;
-    off += 2u * (uint32_t)rows * 8u;
-    L.fin_off = off;
-    off += 2u * (uint32_t)rows * 8u;
-    L.chunk_off = off;
-    off += 2u * 2u * kPnMaxChunks * (uint32_t)sizeof(PnChunk);
-    L.slot_off = pn_align16(off);
-    off = L.slot_off + 2u * (uint32_t)p_sub * (uint32_t)sizeof(PnSlot);
+    L.sym_off = off;                  // [buf][16 steps][2 * p_sub] symbols
+    off += 2u * kPnBlk * 2u * ps;
+    L.hdr_off = pn_align16(off);      // [buf][2 * p_sub] headers
+    off = L.hdr_off + 2u * 2u * ps * (uint32_t)sizeof(PnHdr);
+    L.rec_off = pn_align16(off);      // [b][parity][rows] uint2 {destination, scale}
+    off = L.rec_off + 4u * nr * 8u;
+    L.xmax_off = pn_align16(off);     // [b][parity][rows] float2
+    off = L.xmax_off + 4u * nr * 8u;
+    L.fin_off = off;                  // [b][p_sub] float2
+    off += 2u * ps * 8u;
+    L.chunk_off = pn_align16(off);    // [b][parity][kPnMaxChunks]
+    off = L.chunk_off + 4u * kPnMaxChunks * (uint32_t)sizeof(PnChunk);
+    L.slot_off = pn_align16(off);     // [2 * p_sub]
+    off = L.slot_off + 2u * ps * (uint32_t)sizeof(PnSlot);
     L.misc_off = pn_align16(off);
     off = L.misc_off + kPnMiscBytes;
     L.total = pn_align16(off);
     return L;
 }
 
-// misc region offsets (bytes, relative to misc_off)
-constexpr uint32_t kMTmem = 0, kMAbort = 4, kMLoaded = 8, kMConsumed = 12, kMSched = 16,
-                   kMEpi = 24, kMEmpty = 32, kMLdSync = 56, kMFull = 64, kMNch = 128, kMBlkAct = 144,
-                   kMCnt = 160, kMPinfo = 416, kMRsym = 672, kMStart = 800, kMAcc = 928;
+// misc region (bytes, relative to misc_off)
+constexpr uint32_t kMTmem = 0, kMAbort = 4, kMPlanOk = 8, kMFinal = 12,
+                   kMNch = 16,        // int32 [b][parity]
+                   kMBlkAct = 32,     // int32 [buf][loader warp]
+                   kMBar = 64,        // mbarriers, 8 bytes each (see PnBar)
+                   kMCnt = 320,       // int32 [16 pairs][2 parities]
+                   kMPinfo = 448,     // int32 [16 pairs][base, neven]
+                   kMRsym = 576,      // float [32]
+                   kMStart = 704,     // uint4 [8]
+                   kMAcc = 832;       // float [64]
+// mbarrier indices
+constexpr int kBarPlan = 0,   // [b][parity]  1 arrival
+              kBarEpi = 4,    // [b][parity]  8 arrivals (all epilogue warps)
+              kBarFull = 8,   // [region]     tcgen05.commit
+              kBarEmpty = 14, // [region]     4 arrivals (the set that drained it)
+              kBarLoaded = 20,   // [buf]     2 arrivals
+              kBarConsumed = 22, // [buf]     1 arrival
+              kBarCount = 24;
 
 struct PnParams {
     const uint8_t *data;
@@ -196,44 +221,25 @@ __device__ __forceinline__ bool pn_mbar_test(uint32_t addr, uint32_t parity) {
         : "=r"(done) : "r"(addr), "r"(parity) : "memory");
     return done != 0;
 }
-
-// Lane 0 spins until *ctr >= target (wrap-safe); bounded; broadcast to the warp.
-__device__ __forceinline__ bool pn_wait_ge(const volatile uint32_t *ctr, uint32_t target,
-                                           volatile uint32_t *abort_flag, uint32_t *err) {
-    int ok = 1;
-    if ((threadIdx.x & 31) == 0) {
-        uint32_t it = 0;
-        while ((int32_t)(*ctr - target) < 0) {
-            if (*abort_flag) { ok = 0; break; }
-            if (++it > kPnSpinLimit) {
-                atomicOr(err, kPnErrTimeout);
-                *abort_flag = 1u;
-                ok = 0;
-                break;
-            }
-            if (it > 32) __nanosleep(40);
-        }
-        __threadfence_block();
-    }
-    ok = __shfl_sync(0xffffffffu, ok, 0);
-    __syncwarp();
-    return ok != 0;
+__device__ __forceinline__ void pn_mbar_arrive(uint32_t addr) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(addr) : "memory");
 }
 
-__device__ __forceinline__ bool pn_wait_mbar(uint32_t addr, uint32_t parity,
-                                             volatile uint32_t *abort_flag, uint32_t *err) {
+// Waits (lane 0 of the calling warp) for the completion of the phase with the
+// given parity; bounded; the result is broadcast to the warp.
+__device__ __forceinline__ bool pn_wait(uint32_t addr, uint32_t parity, volatile uint32_t *abort_flag,
+                                        uint32_t *err) {
     int ok = 1;
     if ((threadIdx.x & 31) == 0) {
-        uint32_t it = 0;
+        const long long t0 = clock64();
         while (!pn_mbar_test(addr, parity)) {
             if (*abort_flag) { ok = 0; break; }
-            if (++it > kPnSpinLimit) {
+            if (clock64() - t0 > kPnWaitCycles) {
                 atomicOr(err, kPnErrTimeout);
                 *abort_flag = 1u;
                 ok = 0;
                 break;
             }
-            if (it > 32) __nanosleep(40);
         }
     }
     ok = __shfl_sync(0xffffffffu, ok, 0);
@@ -276,6 +282,31 @@ __device__ __forceinline__ void pn_tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) 
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// 16 TMEM lanes x 16 columns: thread t gets lanes base + t/4 and base + t/4 + 8 for columns
+// 2(t%4), 2(t%4)+1 and 8 + 2(t%4), 9 + 2(t%4):
+// r = {(l, c), (l, c+1), (l+8, c), (l+8, c+1), (l, c+8), (l, c+9), (l+8, c+8), (l+8, c+9)}.
+__device__ __forceinline__ void pn_tmem_ld16x256(uint32_t taddr, uint32_t (&r)[8]) {
+    asm volatile("tcgen05.ld.sync.aligned.16x256b.x2.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                   "=r"(r[7])
+                 : "r"(taddr) : "memory");
+}
+__device__ __forceinline__ void pn_tmem_wait_ld() {
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// two values rounded to the operand type, packed low/high
+template <bool FP16>
+__device__ __forceinline__ uint32_t pn_pack2(float lo, float hi) {
+    if constexpr (FP16) {
+        const __half2 h = __floats2half2_rn(lo, hi);
+        return *reinterpret_cast<const uint32_t *>(&h);
+    } else {
+        const __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+        return *reinterpret_cast<const uint32_t *>(&h);
+    }
+}
+
 __device__ __forceinline__ void pn_tmem_st32(uint32_t taddr, const uint32_t (&r)[32]) {
     asm volatile(
         "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
@@ -288,7 +319,7 @@ __device__ __forceinline__ void pn_tmem_st32(uint32_t taddr, const uint32_t (&r)
         : "memory");
 }
 
-// ---- roles ------------------------------------------------------------------------------------
+// ---- shared-memory view -------------------------------------------------------------------------
 struct PnShared {
     uint8_t *base;
     PnLayout L;
@@ -296,6 +327,7 @@ struct PnShared {
     __device__ volatile uint32_t *u32(uint32_t off) const {
         return reinterpret_cast<volatile uint32_t *>(misc() + off);
     }
+    __device__ uint32_t bar(int i) const { return pn_smem_u32(misc() + kMBar + 8 * i); }
     __device__ uint32_t sbuf(int b, int par) const {   // byte offset of a B buffer
         return L.s_off + (uint32_t)(b * 2 + par) * 8u * L.lbo;
     }
@@ -303,11 +335,13 @@ struct PnShared {
     __device__ PnHdr *hdr(int buf) const {
         return reinterpret_cast<PnHdr *>(base + L.hdr_off) + buf * 2 * L.p_sub;
     }
-    __device__ uint4 *rec(int b) const { return reinterpret_cast<uint4 *>(base + L.rec_off) + b * L.rows; }
-    __device__ float2 *xmax(int b) const {
-        return reinterpret_cast<float2 *>(base + L.xmax_off) + b * L.rows;
+    __device__ uint2 *rec(int b, int par) const {
+        return reinterpret_cast<uint2 *>(base + L.rec_off) + (b * 2 + par) * L.rows;
     }
-    __device__ float2 *fin(int b) const { return reinterpret_cast<float2 *>(base + L.fin_off) + b * L.rows; }
+    __device__ float2 *xmax(int b, int par) const {
+        return reinterpret_cast<float2 *>(base + L.xmax_off) + (b * 2 + par) * L.rows;
+    }
+    __device__ float2 *fin(int b) const { return reinterpret_cast<float2 *>(base + L.fin_off) + b * L.p_sub; }
     __device__ PnChunk *chunks(int b, int par) const {
         return reinterpret_cast<PnChunk *>(base + L.chunk_off) + (b * 2 + par) * kPnMaxChunks;
     }
@@ -315,19 +349,14 @@ struct PnShared {
     __device__ volatile int32_t *nch(int b, int par) const {
         return reinterpret_cast<volatile int32_t *>(misc() + kMNch) + b * 2 + par;
     }
-    __device__ int32_t *cnt(int b) const {   // [16 pairs][2 parities]
-        return reinterpret_cast<int32_t *>(misc() + kMCnt) + b * 32;
-    }
-    __device__ int32_t *pinfo(int b) const {   // [16 pairs][base, neven]
-        return reinterpret_cast<int32_t *>(misc() + kMPinfo) + b * 32;
-    }
-    __device__ uint32_t full_addr(int r) const { return pn_smem_u32(misc() + kMFull + 8 * r); }
+    __device__ int32_t *cnt() const { return reinterpret_cast<int32_t *>(misc() + kMCnt); }
+    __device__ int32_t *pinfo() const { return reinterpret_cast<int32_t *>(misc() + kMPinfo); }
 };
 
-// Loader: warps 6-7. Fills symbol block blk into buffer blk & 1.
+// ---- loader: warps 13-14 -------------------------------------------------------------------------
 __device__ void pn_loader(const PnParams &P, const PnShared &S, volatile uint32_t *abort_flag) {
     const int lane = threadIdx.x & 31;
-    const int lw = (threadIdx.x >> 5) - 6;
+    const int lw = (threadIdx.x >> 5) - kPnLoadWarp0;
     const int ll = lw * 32 + lane;
     const int PC = 2 * S.L.p_sub;
     const uint32_t sig4 = (uint32_t)P.sigma * 0x01010101u;
@@ -336,8 +365,10 @@ __device__ void pn_loader(const PnParams &P, const PnShared &S, volatile uint32_
 #pragma unroll
     for (int i = 0; i < 8; ++i) { seq[i] = -1; pos[i] = 0; end[i] = 0; }
     for (int blk = 0;; ++blk) {
-        if (blk >= 2 && !pn_wait_ge(S.u32(kMConsumed), (uint32_t)(blk - 1), abort_flag, P.err)) break;
         const int buf = blk & 1;
+        if (blk >= 2 && !pn_wait(S.bar(kBarConsumed + buf), (uint32_t)((blk - 2) >> 1) & 1u,
+                                 abort_flag, P.err))
+            break;
         uint8_t *sym = S.sym(buf);
         PnHdr *hd = S.hdr(buf);
         int nact = 0;
@@ -419,115 +450,110 @@ __device__ void pn_loader(const PnParams &P, const PnShared &S, volatile uint32_
         for (int o = 16; o > 0; o >>= 1) nact += __shfl_xor_sync(0xffffffffu, nact, o);
         if (lane == 0) {
             reinterpret_cast<volatile int32_t *>(S.misc() + kMBlkAct)[buf * 2 + lw] = nact;
-            __threadfence_block();
-            atomicAdd(const_cast<uint32_t *>(S.u32(kMLdSync)), 1u);
+            pn_mbar_arrive(S.bar(kBarLoaded + buf));
         }
         __syncwarp();
-        // both loader warps have written their block (bounded wait, no barrier)
-        if (!pn_wait_ge(S.u32(kMLdSync), 2u * (uint32_t)(blk + 1), abort_flag, P.err)) break;
+        // both loader warps have written the block: its active count decides the end
+        if (!pn_wait(S.bar(kBarLoaded + buf), (uint32_t)(blk >> 1) & 1u, abort_flag, P.err)) break;
         const volatile int32_t *ba = reinterpret_cast<const volatile int32_t *>(S.misc() + kMBlkAct);
-        const int total_act = ba[buf * 2] + ba[buf * 2 + 1];
-        if (ll == 0) {
-            __threadfence_block();
-            *S.u32(kMLoaded) = (uint32_t)(blk + 1);
-        }
-        if (total_act == 0 || *abort_flag) break;
+        if (ba[buf * 2] + ba[buf * 2 + 1] == 0) break;
     }
 }
 
-// Scheduler: warp 4.
-template <bool FP16>
-__device__ void pn_scheduler(const PnParams &P, const PnShared &S, volatile uint32_t *abort_flag) {
-    const int lane = threadIdx.x & 31;
+// ---- planner: warps 9-12 ---------------------------------------------------------------------------
+// named barrier 1: the four planner warps only
+__device__ __forceinline__ void pn_plan_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+
+__device__ void pn_planner(const PnParams &P, const PnShared &S, volatile uint32_t *abort_flag) {
+    const int tid = threadIdx.x - 32 * kPnPlanWarp0;   // 0..127
+    const int lane = tid & 31;
+    const bool leader = tid == 0;
     const PnLayout &L = S.L;
-    const int PS = L.p_sub, PC = 2 * PS, SL = PS / 32;
-    const float *rsym = reinterpret_cast<const float *>(S.misc() + kMRsym);
+    const int PS = L.p_sub, PC = 2 * PS;
     const uint4 *simg = reinterpret_cast<const uint4 *>(S.misc() + kMStart);
     PnSlot *slots = S.slots();
-    for (int j = lane; j < PC; j += 32) {
+    int32_t *cnt = S.cnt();
+    int32_t *pinfo = S.pinfo();
+    volatile uint32_t *plan_ok = S.u32(kMPlanOk);
+    volatile uint32_t *final_flag = S.u32(kMFinal);
+    for (int j = tid; j < PC; j += kPnPlanThreads) {
         PnSlot z;
-        z.seq = -1; z.E = 0; z.fin_seq = -1; z.fin_E = 0; z.row = 0; z.finrow = 0; z.c = 0;
-        z.flags = 0; z.blkcnt = 0; z.blkflags = 0;
+        z.seq = -1; z.E = 0; z.fin_seq = -1; z.fin_step = -1; z.fin_E = 0; z.row = 0; z.c = 0; z.flags = 0;
+        z.blkcnt = 0; z.blkflags = 0; z.pad0 = z.pad1 = 0;
         slots[j] = z;
     }
-    for (int k = lane; k < 64; k += 32) S.cnt(0)[k] = 0;
-    __syncwarp();
-    int done = 0;            // bit b: sub-batch b finished
-    int term_step[2] = {-2, -2};
-    bool final_blk = false;
-    for (int t = -1;; ++t) {
-        const int s1 = t + 1;
-        const int in = s1 % kPnBlk;
-        const int buf = (s1 / kPnBlk) & 1;
-        if (in == 0 && done != 3) {
-            const int blk = s1 / kPnBlk;
-            if (lane == 0) {
-                __threadfence_block();
-                *S.u32(kMConsumed) = (uint32_t)blk;
-            }
-            if (!pn_wait_ge(S.u32(kMLoaded), (uint32_t)(blk + 1), abort_flag, P.err)) break;
-            const volatile int32_t *ba = reinterpret_cast<const volatile int32_t *>(S.misc() + kMBlkAct);
-            final_blk = (ba[buf * 2] + ba[buf * 2 + 1]) == 0;
-        }
+    for (int k = tid; k < 32; k += kPnPlanThreads) cnt[k] = 0;
+    pn_plan_sync();
+    int term_s = -1;   // step whose chunk list says "terminate"
+    for (int s = 0;; ++s) {
         for (int b = 0; b < 2; ++b) {
-            if (done & (1 << b)) continue;
-            if (t >= 1 && !pn_wait_ge(S.u32(kMEpi + 4 * b), 4u * (uint32_t)t, abort_flag, P.err)) {
-                done = 3;
-                break;
+            // --- the leader waits for the step's inputs; the others wait at the barrier
+            if (tid < 32) {
+                bool ok = true;
+                if (s >= 2)   // epilogue of step s-2: B buffer s&1, records s&1, dot products
+                    ok = pn_wait(S.bar(kBarEpi + b * 2 + (s & 1)), (uint32_t)((s - 2) >> 1) & 1u,
+                                 abort_flag, P.err);
+                if (ok && b == 0 && s % kPnBlk == 0 && term_s < 0) {
+                    const int blk = s / kPnBlk;
+                    if (leader && blk >= 1) pn_mbar_arrive(S.bar(kBarConsumed + ((blk - 1) & 1)));
+                    ok = pn_wait(S.bar(kBarLoaded + (blk & 1)), (uint32_t)(blk >> 1) & 1u, abort_flag,
+                                 P.err);
+                    if (ok && leader) {
+                        const volatile int32_t *ba =
+                            reinterpret_cast<const volatile int32_t *>(S.misc() + kMBlkAct);
+                        *final_flag = (ba[(blk & 1) * 2] + ba[(blk & 1) * 2 + 1]) == 0;
+                    }
+                }
+                if (leader) *plan_ok = ok ? 1u : 0u;
             }
-            const bool terminal = (term_step[b] == t);   // only emissions left
-            float2 *fin = S.fin(b);
-            float2 *xm = S.xmax(b);
-            uint4 *rec = S.rec(b);
-            int32_t *cnt = S.cnt(b);
-            int32_t *pinfo = S.pinfo(b);
+            pn_plan_sync();
+            if (!*plan_ok) return;
+            const bool done_now = term_s >= 0 && s > term_s;   // only emissions were left
+            const int in = s % kPnBlk;
+            const int buf = (s / kPnBlk) & 1;
             const uint8_t *sym = S.sym(buf);
             const PnHdr *hd = S.hdr(buf);
-            // (1) strings that ended at step t-1; (2) next-step activity and ranks
-            int rank[8], c1v[8], newseq[8];
+            const float2 *fin = S.fin(b);
+            // --- stage A: emissions of step s-2, headers, symbols and ranks of step s
+            int rank[2] = {-1, -1}, cs[2] = {-1, -1}, nseq[2] = {-1, -1};
 #pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                rank[i] = -1; c1v[i] = -1; newseq[i] = -1;
-                if (i >= SL) continue;
-                const int j = b * PS + lane + 32 * i;
+            for (int k = 0; k < 2; ++k) {
+                const int jl = tid + kPnPlanThreads * k;
+                if (jl >= PS) continue;
+                const int j = b * PS + jl;
                 PnSlot sl = slots[j];
-                if (sl.flags & kSlotFinPending) {
-                    const float2 f = fin[sl.finrow];
+                if ((sl.flags & kSlotFinPending) && sl.fin_step <= s - 2) {
+                    const float2 f = fin[jl];
                     const double dot = (double)f.x + (double)f.y;
                     const double ll = dot > 0.0 ? log(dot) + (double)sl.fin_E * 0.69314718055994530942
                                                 : -INFINITY;
                     pn_write_result(P.loglik, P.accept, P.accept_i32, sl.fin_seq, ll);
                     sl.flags &= (uint8_t)~kSlotFinPending;
                 }
-                if (!terminal) {
+                if (term_s < 0) {
                     if (in == 0) {
                         const PnHdr h = hd[j];
                         sl.blkcnt = h.count;
                         sl.blkflags = h.flags;
-                        if (h.flags & kHdrStart) newseq[i] = h.seq;   // applied after rec(t)
+                        if (h.flags & kHdrStart) nseq[k] = h.seq;
                     }
                     if (in < sl.blkcnt) {
-                        const int c1 = sym[in * PC + j];
-                        c1v[i] = c1;
-                        rank[i] = atomicAdd(&cnt[(c1 >> 1) * 2 + (c1 & 1)], 1);
+                        const int c = sym[in * PC + j];
+                        cs[k] = c;
+                        rank[k] = atomicAdd(&cnt[(c >> 1) * 2 + (c & 1)], 1);
                     }
                 }
                 slots[j] = sl;
             }
-            if (terminal) {
-                done |= 1 << b;
-                __syncwarp();
-                if (lane == 0) {
-                    __threadfence_block();
-                    *S.u32(kMSched + 4 * b) = (uint32_t)(t + 2);
-                }
+            if (done_now) {
+                if (b == 1) return;
                 continue;
             }
-            __syncwarp();
-            // pair bases and the chunk list of step t+1
-            const int par1 = s1 & 1;
-            PnChunk *ch = S.chunks(b, par1);
-            {
+            const bool terminal = term_s < 0 && in == 0 && *final_flag;
+            pn_plan_sync();
+            // --- stage B: pair bases and the chunk list of step s
+            const int par = s & 1;
+            if (tid < 32) {
                 int ne = 0, no = 0;
                 if (lane < L.npairs) {
                     ne = cnt[lane * 2];
@@ -548,6 +574,7 @@ __device__ void pn_scheduler(const PnParams &P, const PnShared &S, volatile uint
                 if (lane < L.npairs) {
                     pinfo[lane * 2] = base;
                     pinfo[lane * 2 + 1] = ne;
+                    PnChunk *ch = S.chunks(b, par);
                     for (int k = 0; k < nc; ++k) {
                         PnChunk d;
                         d.row0 = (uint16_t)(base + k * kPnRegionCols);
@@ -560,86 +587,80 @@ __device__ void pn_scheduler(const PnParams &P, const PnShared &S, volatile uint
                     }
                 }
                 const int total_chunks = __shfl_sync(0xffffffffu, cincl, 31);
-                if (lane == 0) {
-                    const bool term = final_blk && in == 0;
-                    *S.nch(b, par1) = term ? kPnTerminate : total_chunks;
-                    if (term) term_step[b] = t + 1;
-                }
-                term_step[b] = __shfl_sync(0xffffffffu, term_step[b], 0);
+                if (lane == 0) *S.nch(b, par) = terminal ? kPnTerminate : total_chunks;
             }
-            __syncwarp();
-            // (3) records of step t, (4) start rows of step t+1, slot state
-            const uint32_t snext = S.sbuf(b, par1);
+            pn_plan_sync();
+            // --- stage C: rows of step s, records of step s-1, start rows, slot state
+            uint2 *rec = S.rec(b, (s - 1) & 1);
+            const float2 *xm = S.xmax(b, (s - 1) & 1);
+            const float *rsym = reinterpret_cast<const float *>(S.misc() + kMRsym);
+            const uint32_t sb = S.sbuf(b, par);
 #pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                if (i >= SL) continue;
-                const int j = b * PS + lane + 32 * i;
+            for (int k = 0; k < 2; ++k) {
+                const int jl = tid + kPnPlanThreads * k;
+                if (jl >= PS) continue;
+                const int j = b * PS + jl;
                 PnSlot sl = slots[j];
                 int row1 = -1;
-                if (c1v[i] >= 0) {
-                    const int p = c1v[i] >> 1;
-                    row1 = pinfo[p * 2] + ((c1v[i] & 1) ? pinfo[p * 2 + 1] : 0) + rank[i];
+                if (cs[k] >= 0) {
+                    const int p = cs[k] >> 1;
+                    row1 = pinfo[p * 2] + ((cs[k] & 1) ? pinfo[p * 2 + 1] : 0) + rank[k];
                 }
-                if (t >= 0 && (sl.flags & kSlotActive)) {
+                if (s >= 1 && (sl.flags & kSlotActive)) {
+                    // scale of step s-1: max|s_(s-1)| (left by the epilogue of step s-2, or the
+                    // start vector's) times the symbol's growth bound, rounded up to 2^f
                     float m;
                     if (sl.flags & kSlotFresh) {
                         m = P.start_max;
+                        sl.E = 0;
                     } else {
                         const float2 x = xm[sl.row];
                         m = fmaxf(x.x, x.y);
                     }
-                    const float bound = m * rsym[sl.c];
-                    int f = pn_ceil_exp(bound);
+                    int f = pn_ceil_exp(m * rsym[sl.c]);
                     f = min(max(f, -125), 125);
                     sl.E += f;
-                    uint4 r;
-                    r.z = __float_as_uint(pn_pow2(-f));
-                    r.w = 0;
+                    uint2 r;
+                    r.y = __float_as_uint(pn_pow2(-f));
                     if (sl.flags & kSlotLast) {
-                        r.x = 0;
-                        r.y = kPnFinish;
+                        r.x = kRecFinish | (uint32_t)jl;
                         sl.flags |= kSlotFinPending;
-                        sl.finrow = sl.row;
                         sl.fin_seq = sl.seq;
+                        sl.fin_step = s - 1;
                         sl.fin_E = sl.E;
                     } else {
-                        // a continuing string is active at t+1 (the loader never leaves it empty)
+                        // a continuing string is active at step s (blocks never leave it empty)
                         r.x = (uint32_t)max(row1, 0) * 16u;
-                        r.y = (uint32_t)max(row1, 0);
                     }
                     rec[sl.row] = r;
                 }
                 uint8_t nf = sl.flags & kSlotFinPending;
-                if (newseq[i] >= 0) {
-                    sl.seq = newseq[i];
-                    sl.E = 0;
-                }
+                if (nseq[k] >= 0) sl.seq = nseq[k];
                 if (row1 >= 0) {
                     nf |= kSlotActive;
                     if ((sl.blkflags & kHdrEnd) && in == sl.blkcnt - 1) nf |= kSlotLast;
-                    if (newseq[i] >= 0) {
+                    if (nseq[k] >= 0) {
                         nf |= kSlotFresh;
-                        uint8_t *dst = S.base + snext + (uint32_t)row1 * 16u;
+                        uint8_t *dst = S.base + sb + (uint32_t)row1 * 16u;
 #pragma unroll
                         for (int c = 0; c < 8; ++c)
                             *reinterpret_cast<uint4 *>(dst + c * L.lbo) = simg[c];
                     }
                     sl.row = (int16_t)row1;
-                    sl.c = (uint8_t)c1v[i];
+                    sl.c = (uint8_t)cs[k];
                 }
                 sl.flags = nf;
                 slots[j] = sl;
             }
             pn_fence_async_smem();
-            __threadfence_block();
-            __syncwarp();
-            if (lane == 0) *S.u32(kMSched + 4 * b) = (uint32_t)(t + 2);
+            pn_plan_sync();
+            if (leader) pn_mbar_arrive(S.bar(kBarPlan + b * 2 + par));
+            if (terminal && b == 1) term_s = s;
         }
-        if (done == 3 || *abort_flag) break;
     }
 }
 
-// MMA issuer: warp 5.
+// ---- MMA issuer: warp 8 ----------------------------------------------------------------------------
 template <bool FP16>
 __device__ void pn_mma(const PnParams &P, const PnShared &S, uint32_t tbase,
                        volatile uint32_t *abort_flag) {
@@ -648,22 +669,33 @@ __device__ void pn_mma(const PnParams &P, const PnShared &S, uint32_t tbase,
     const uint32_t fmt = FP16 ? 0u : 1u;
     const uint32_t smem_base = pn_smem_u32(S.base);
     const uint32_t desc_hi = (128u >> 4) | (1u << 14);   // SBO = 128 B, descriptor version 1
+    const uint32_t nr = (uint32_t)L.nregions;
     uint32_t g = 0;
     int done = 0;
     bool aborted = false;
-    for (int t = 0; !aborted; ++t) {
+    for (int t = 0; !aborted && done != 3; ++t) {
         for (int b = 0; b < 2 && !aborted; ++b) {
             if (done & (1 << b)) continue;
-            if (!pn_wait_ge(S.u32(kMSched + 4 * b), (uint32_t)(t + 1), abort_flag, P.err)) { aborted = true; break; }
-            if (t > 0 && !pn_wait_ge(S.u32(kMEpi + 4 * b), 4u * (uint32_t)t, abort_flag, P.err)) { aborted = true; break; }
+            if (!pn_wait(S.bar(kBarPlan + b * 2 + (t & 1)), (uint32_t)(t >> 1) & 1u, abort_flag, P.err)) {
+                aborted = true;
+                break;
+            }
             const int nch = *S.nch(b, t & 1);
             if (nch == kPnTerminate) { done |= 1 << b; continue; }
+            if (t >= 1 && !pn_wait(S.bar(kBarEpi + b * 2 + ((t - 1) & 1)), (uint32_t)((t - 1) >> 1) & 1u,
+                                   abort_flag, P.err)) {
+                aborted = true;
+                break;
+            }
             const PnChunk *ch = S.chunks(b, t & 1);
             const uint32_t sb = smem_base + S.sbuf(b, t & 1);
             for (int k = 0; k < nch; ++k) {
                 const PnChunk d = ch[k];
-                const uint32_t r = g % (uint32_t)L.nregions, u = g / (uint32_t)L.nregions;
-                if (u > 0 && !pn_wait_ge(S.u32(kMEmpty + 4 * r), 4u * u, abort_flag, P.err)) { aborted = true; break; }
+                const uint32_t r = g % nr, u = g / nr;
+                if (u > 0 && !pn_wait(S.bar(kBarEmpty + (int)r), (u - 1) & 1u, abort_flag, P.err)) {
+                    aborted = true;
+                    break;
+                }
                 pn_tc_after();
                 if (lane == 0) {
                     const uint32_t n16 = ((uint32_t)d.ncols + 15u) & ~15u;
@@ -684,106 +716,156 @@ __device__ void pn_mma(const PnParams &P, const PnShared &S, uint32_t tbase,
                     }
                     asm volatile(
                         "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-                        :: "r"(S.full_addr((int)r)) : "memory");
+                        :: "r"(S.bar(kBarFull + (int)r)) : "memory");
                 }
                 __syncwarp();
                 ++g;
             }
         }
-        if (done == 3) break;
     }
     // Drain: every committed chain must have finished before the TMEM is freed.
-    const uint32_t nr = (uint32_t)L.nregions;
     for (uint32_t r = 0; r < nr && r < g; ++r) {
         const uint32_t uses = (g - r + nr - 1) / nr;   // commits made to region r
         if (lane == 0) {                               // completion of the last one
-            uint32_t it = 0;
-            while (!pn_mbar_test(S.full_addr((int)r), (uses - 1) & 1u)) {
-                if (++it > kPnSpinLimit) { atomicOr(P.err, kPnErrTimeout); break; }
-                if (it > 32) __nanosleep(40);
+            const long long t0 = clock64();
+            while (!pn_mbar_test(S.bar(kBarFull + (int)r), (uses - 1) & 1u)) {
+                if (clock64() - t0 > kPnWaitCycles) { atomicOr(P.err, kPnErrTimeout); break; }
             }
         }
         __syncwarp();
     }
 }
 
-// Epilogue: warps 0-3.
+// ---- epilogue: warps 0-7 ---------------------------------------------------------------------------
+// Two sets of four warps take alternate chunks. Warp q of a set reads TMEM lanes 32q..32q+31: the
+// even symbol's states 32(q&1).. for q < 2, the odd symbol's for q >= 2. The A rows are permuted
+// so that in each 16-lane half h the lanes j and j + 8 hold the adjacent states 2j and 2j + 1: a
+// 16x256b load then gives thread t (j = t/4) the states 32(q&1) + 16h + 2j, +1 of four columns,
+// which it scales, packs into one 32-bit store per pair, and reduces (max) with the seven other
+// threads holding the same columns.
 template <bool FP16>
 __device__ void pn_epilogue(const PnParams &P, const PnShared &S, uint32_t tbase,
                             volatile uint32_t *abort_flag) {
     const int lane = threadIdx.x & 31;
-    const int q = threadIdx.x >> 5;                 // TMEM lane quadrant
+    const int ew = threadIdx.x >> 5;
+    const int q = ew & 3;                           // TMEM lane quadrant
+    const uint32_t set = (uint32_t)(ew >> 2);       // chunk parity this warp drains
     const PnLayout &L = S.L;
-    const int s = 32 * (q & 1) + lane;              // state index within its symbol
-    const uint32_t toff = (uint32_t)(s >> 3) * L.lbo + (uint32_t)(s & 7) * 2u;
-    const float accw = reinterpret_cast<const float *>(S.misc() + kMAcc)[s];
+    const int j = lane >> 2, cp = lane & 3;
+    const int sg0 = 32 * (q & 1) + 2 * j, sg1 = sg0 + 16;   // first states of the two pairs
+    const uint32_t toff0 = (uint32_t)(sg0 >> 3) * L.lbo + (uint32_t)(sg0 & 7) * 2u;
+    const uint32_t toff1 = (uint32_t)(sg1 >> 3) * L.lbo + (uint32_t)(sg1 & 7) * 2u;
+    const float *accv = reinterpret_cast<const float *>(S.misc() + kMAcc);
+    const float a00 = accv[sg0], a01 = accv[sg0 + 1], a10 = accv[sg1], a11 = accv[sg1 + 1];
     const bool even = q < 2;
+    const uint32_t nr = (uint32_t)L.nregions;
     uint32_t g = 0;
     int done = 0;
     bool aborted = false;
-    for (int t = 0; !aborted; ++t) {
+    for (int t = 0; !aborted && done != 3; ++t) {
         for (int b = 0; b < 2 && !aborted; ++b) {
             if (done & (1 << b)) continue;
-            if (!pn_wait_ge(S.u32(kMSched + 4 * b), (uint32_t)(t + 2), abort_flag, P.err)) { aborted = true; break; }
+            if (t == 0 && !pn_wait(S.bar(kBarPlan + b * 2), 0u, abort_flag, P.err)) {
+                aborted = true;
+                break;
+            }
             const int nch = *S.nch(b, t & 1);
             if (nch == kPnTerminate) { done |= 1 << b; continue; }
+            // records of step t come with the plan of step t+1
+            if (!pn_wait(S.bar(kBarPlan + b * 2 + ((t + 1) & 1)), (uint32_t)((t + 1) >> 1) & 1u,
+                         abort_flag, P.err)) {
+                aborted = true;
+                break;
+            }
             const PnChunk *ch = S.chunks(b, t & 1);
-            const uint4 *rec = S.rec(b);
-            float2 *xm = S.xmax(b);
-            float2 *fin = S.fin(b);
+            const uint2 *rec = S.rec(b, t & 1);
+            float *xn = reinterpret_cast<float *>(S.xmax(b, (t + 1) & 1)) + (q & 1);
+            float *fin = reinterpret_cast<float *>(S.fin(b)) + (q & 1);
             uint8_t *snext = S.base + S.sbuf(b, (t + 1) & 1);
-            for (int k = 0; k < nch; ++k) {
+            for (int k = 0; k < nch; ++k, ++g) {
+                if ((g & 1u) != set) continue;
                 const PnChunk d = ch[k];
-                const uint32_t r = g % (uint32_t)L.nregions, u = g / (uint32_t)L.nregions;
-                if (!pn_wait_mbar(S.full_addr((int)r), u & 1u, abort_flag, P.err)) { aborted = true; break; }
+                const uint32_t r = g % nr, u = g / nr;
+                if (!pn_wait(S.bar(kBarFull + (int)r), u & 1u, abort_flag, P.err)) {
+                    aborted = true;
+                    break;
+                }
                 pn_tc_after();
                 const int c_lo = even ? 0 : d.split;
                 const int c_hi = even ? d.split : d.ncols;
                 const uint32_t tcol = tbase + ((uint32_t)(32 * q) << 16) + (uint32_t)L.ring_base +
                                       r * kPnRegionCols;
                 for (int c = c_lo & ~15; c < c_hi; c += 16) {
-                    uint32_t v[16];
-                    pn_tmem_ld16(tcol + (uint32_t)c, v);
+                    uint32_t v0[8], v1[8];
+                    pn_tmem_ld16x256(tcol + (uint32_t)c, v0);
+                    pn_tmem_ld16x256(tcol + (16u << 16) + (uint32_t)c, v1);
+                    // this thread's columns: c + {2cp, 2cp+1, 2cp+8, 2cp+9}
+                    uint2 rc[4];
+                    bool valid[4];
 #pragma unroll
-                    for (int i = 0; i < 16; ++i) {
-                        const int col = c + i;
-                        if (col < c_lo || col >= c_hi) continue;
-                        const int row = d.row0 + col;
-                        const uint4 rc = rec[row];
-                        const float x = __uint_as_float(v[i]) * __uint_as_float(rc.z);
-                        if (rc.y & kPnFinish) {
-                            float p = x * accw;
+                    for (int i = 0; i < 4; ++i) {
+                        const int col = c + (i >> 1) * 8 + 2 * cp + (i & 1);
+                        valid[i] = col >= c_lo && col < c_hi;
+                        rc[i] = rec[d.row0 + (valid[i] ? col : c_lo)];
+                    }
+                    pn_tmem_wait_ld();
+                    float x[4][4], m[4];
+                    bool any_fin = false;
 #pragma unroll
-                            for (int o = 16; o > 0; o >>= 1) p += __shfl_xor_sync(0xffffffffu, p, o);
-                            if (lane == 0) {
-                                if (q & 1) fin[row].y = p;
-                                else fin[row].x = p;
-                            }
-                        } else {
-                            *reinterpret_cast<uint16_t *>(snext + rc.x + toff) = pn_to16<FP16>(x);
-                            uint32_t mx;
-                            asm volatile("redux.sync.max.u32 %0, %1, 0xffffffff;"
-                                         : "=r"(mx) : "r"(__float_as_uint(x) & 0x7FFFFFFFu));
-                            if (lane == 0) {
-                                const int dr = (int)(rc.y & 0xFFFFu);
-                                if (q & 1) xm[dr].y = __uint_as_float(mx);
-                                else xm[dr].x = __uint_as_float(mx);
-                            }
+                    for (int i = 0; i < 4; ++i) {
+                        const int ri = (i >> 1) * 4 + (i & 1);
+                        const float sc = __uint_as_float(rc[i].y);
+                        x[i][0] = __uint_as_float(v0[ri]) * sc;       // state sg0
+                        x[i][1] = __uint_as_float(v0[ri + 2]) * sc;   // sg0 + 1
+                        x[i][2] = __uint_as_float(v1[ri]) * sc;       // sg1
+                        x[i][3] = __uint_as_float(v1[ri + 2]) * sc;   // sg1 + 1
+                        const bool fin_i = (rc[i].x & kRecFinish) != 0;
+                        const bool keep = valid[i] && !fin_i;
+                        any_fin |= valid[i] && fin_i;
+                        if (keep) {
+                            uint8_t *dst = snext + rc[i].x;
+                            *reinterpret_cast<uint32_t *>(dst + toff0) = pn_pack2<FP16>(x[i][0], x[i][1]);
+                            *reinterpret_cast<uint32_t *>(dst + toff1) = pn_pack2<FP16>(x[i][2], x[i][3]);
+                        }
+                        m[i] = keep ? fmaxf(fmaxf(fabsf(x[i][0]), fabsf(x[i][1])),
+                                            fmaxf(fabsf(x[i][2]), fabsf(x[i][3])))
+                                    : 0.f;
+                    }
+                    // column maxima over this warp's 32 states: the 8 threads with the same cp
+#pragma unroll
+                    for (int o = 4; o < 32; o <<= 1)
+#pragma unroll
+                        for (int i = 0; i < 4; ++i) m[i] = fmaxf(m[i], __shfl_xor_sync(0xffffffffu, m[i], o));
+                    if (j == 0) {
+#pragma unroll
+                        for (int i = 0; i < 4; ++i)
+                            if (valid[i] && !(rc[i].x & kRecFinish)) xn[(rc[i].x >> 4) * 2] = m[i];
+                    }
+                    if (__any_sync(0xffffffffu, any_fin)) {   // last symbols: accept-weighted sums
+                        float pz[4];
+#pragma unroll
+                        for (int i = 0; i < 4; ++i)
+                            pz[i] = x[i][0] * a00 + x[i][1] * a01 + x[i][2] * a10 + x[i][3] * a11;
+#pragma unroll
+                        for (int o = 4; o < 32; o <<= 1)
+#pragma unroll
+                            for (int i = 0; i < 4; ++i) pz[i] += __shfl_xor_sync(0xffffffffu, pz[i], o);
+                        if (j == 0) {
+#pragma unroll
+                            for (int i = 0; i < 4; ++i)
+                                if (valid[i] && (rc[i].x & kRecFinish)) fin[(rc[i].x & 511u) * 2] = pz[i];
                         }
                     }
                 }
                 pn_tc_before();
                 __syncwarp();
-                if (lane == 0) atomicAdd(const_cast<uint32_t *>(S.u32(kMEmpty + 4 * r)), 1u);
-                ++g;
+                if (lane == 0) pn_mbar_arrive(S.bar(kBarEmpty + (int)r));
             }
             if (aborted) break;
             pn_fence_async_smem();
-            __threadfence_block();
             __syncwarp();
-            if (lane == 0) atomicAdd(const_cast<uint32_t *>(S.u32(kMEpi + 4 * b)), 1u);
+            if (lane == 0) pn_mbar_arrive(S.bar(kBarEpi + b * 2 + (t & 1)));
         }
-        if (done == 3) break;
     }
 }
 
@@ -797,14 +879,22 @@ __global__ void __launch_bounds__(kPnThreads, 1) pnfa_tc_kernel(PnParams P) {
         reinterpret_cast<uint32_t *>(misc)[i] = 0;
     __syncthreads();
     if (threadIdx.x == 0) {
-        for (int r = 0; r < P.L.nregions; ++r)
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(S.full_addr(r)));
+        for (int i = 0; i < kBarCount; ++i) {
+            uint32_t count = 1;
+            if (i >= kBarEpi && i < kBarEpi + 4)
+                count = kPnEpiWarps;
+            else if (i >= kBarEmpty && i < kBarEmpty + kPnMaxRegions)
+                count = 4;
+            else if (i >= kBarLoaded && i < kBarLoaded + 2)
+                count = kPnLoadWarps;
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(S.bar(i)), "r"(count));
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (threadIdx.x < P.sigma) reinterpret_cast<float *>(misc + kMRsym)[threadIdx.x] = P.rsym[threadIdx.x];
     if (threadIdx.x < 8) reinterpret_cast<uint4 *>(misc + kMStart)[threadIdx.x] = P.start_img[threadIdx.x];
     if (threadIdx.x < 64) reinterpret_cast<float *>(misc + kMAcc)[threadIdx.x] = P.acc[threadIdx.x];
-    if (warp == 5) {
+    if (warp == kPnMmaWarp) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
                      :: "r"(pn_smem_u32(misc + kMTmem)), "r"(512));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
@@ -828,14 +918,15 @@ __global__ void __launch_bounds__(kPnThreads, 1) pnfa_tc_kernel(PnParams P) {
     __syncthreads();
     pn_tc_after();
     volatile uint32_t *abort_flag = S.u32(kMAbort);
-    if (warp < 4) pn_epilogue<FP16>(P, S, tbase, abort_flag);
-    else if (warp == 4) pn_scheduler<FP16>(P, S, abort_flag);
-    else if (warp == 5) pn_mma<FP16>(P, S, tbase, abort_flag);
+    if (warp < kPnEpiWarps) pn_epilogue<FP16>(P, S, tbase, abort_flag);
+    else if (warp == kPnMmaWarp) pn_mma<FP16>(P, S, tbase, abort_flag);
+    else if (warp < kPnLoadWarp0) pn_planner(P, S, abort_flag);
     else pn_loader(P, S, abort_flag);
     pn_tc_before();
     __syncthreads();
     pn_tc_after();
-    if (warp == 5) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tbase), "r"(512));
+    if (warp == kPnMmaWarp)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tbase), "r"(512));
 }
 
 // ---- plain FP32 form -------------------------------------------------------------------------
@@ -1042,12 +1133,16 @@ int trex_pnfa_create(int n_states, int sigma, const float *T, const float *start
         for (int c = 0; c < sigma; ++c) {
             const int p = c >> 1, half_ = c & 1;
             double rmax = 0.0;
-            for (int d = 0; d < 64; ++d) {
+            for (int rr = 0; rr < 64; ++rr) {
+                // A row rr holds destination state d: in each group of 16 rows, rows 0-7 are the
+                // even states and rows 8-15 the odd ones, so TMEM lanes j and j+8 of a 16-lane
+                // half carry the adjacent states 2j and 2j+1 (the epilogue's 16x256b loads)
+                const int d = (rr & ~15) | ((rr & 7) << 1) | ((rr >> 3) & 1);
                 double rsum = 0.0;
                 for (int q = 0; q < 64; ++q) {
                     const uint16_t v = pn_host16(T32[((size_t)c * 64 + d) * 64 + q], fp16);
                     rsum += std::fabs((double)pn_host16_to_f(v, fp16));
-                    uint32_t &w = tp[k][((size_t)p * 128 + half_ * 64 + d) * 32 + (q >> 1)];
+                    uint32_t &w = tp[k][((size_t)p * 128 + half_ * 64 + rr) * 32 + (q >> 1)];
                     w |= (uint32_t)v << (16 * (q & 1));
                 }
                 rmax = std::max(rmax, rsum);
