@@ -17,9 +17,14 @@
 // max |s'|, the rule of the FP64 oracle.
 //
 // Tensor form (tcgen05, BF16 or FP16 operands, FP32 accumulation in TMEM).
-// One persistent CTA per SM holds up to 2 x 256 strings ("slots") in two
-// sub-batches that alternate, so the tensor core works on one while the other
-// is in its epilogue. Orientation: D[dst][string] = T[c][dst][:] . S[:][string]
+// One persistent CTA per SM holds up to 512 strings ("slots") and advances
+// them all one symbol per step. A tcgen05.mma (M=128, K=16) costs about the
+// same time for any N up to 256 (measured: ~120-165 cycles whether N is 16 or
+// 192), so the kernel is bound by the number of MMA instructions per step:
+// every pair of symbols gets one MMA chain over all of the CTA's strings that
+// carry it (about 40 instructions a step), and chunks pipeline inside a step
+// (the MMA of one symbol pair runs while the epilogue drains the previous
+// one). Orientation: D[dst][string] = T[c][dst][:] . S[:][string]
 // -- the 64 states are the MMA's M rows (TMEM lanes) and the strings its N
 // columns, because strings of one step carry different symbols and only the
 // N side can be regrouped cheaply. Symbols are paired (2p, 2p+1): the A
@@ -81,9 +86,10 @@ constexpr int kPnEpiWarps = 8, kPnMmaWarp = 8, kPnPlanWarp0 = 9, kPnPlanWarps = 
               kPnLoadWarp0 = 13, kPnLoadWarps = 2;
 constexpr int kPnThreads = 32 * (kPnLoadWarp0 + kPnLoadWarps);
 constexpr int kPnPlanThreads = 32 * kPnPlanWarps;
-constexpr int kPnMaxPSub = 256;        // slots per sub-batch (2 per planner thread)
+constexpr int kPnMaxPSub = 512;        // slots per sub-batch
+constexpr int kPnSlotsPerPlanThread = kPnMaxPSub / kPnPlanThreads;
 constexpr int kPnMaxChunks = 32;
-constexpr int kPnRegionCols = 32;
+constexpr int kPnRegionCols = 64;
 constexpr int kPnMaxRegions = 6;
 constexpr int kPnMaxSigmaTc = 28;      // 14 pairs: 448 TMEM columns + one ring region
 constexpr int kPnMiscBytes = 2048;
@@ -92,10 +98,9 @@ constexpr int32_t kPnTerminate = -1;
 constexpr uint32_t kPnErrOffsets = 1u, kPnErrTimeout = 4u;
 constexpr long long kPnWaitCycles = 4000000000ll;   // about 2 s
 
-// record of a row (one string at one step), written by the planner
 constexpr uint32_t kRecFinish = 1u << 31;
 // slot flags (planner)
-constexpr uint8_t kSlotActive = 1, kSlotLast = 2, kSlotFresh = 4, kSlotFinPending = 8;
+constexpr uint8_t kSlotActive = 1, kSlotLast = 2, kSlotFresh = 4;
 // header flags (loader)
 constexpr uint8_t kHdrStart = 1, kHdrEnd = 2;
 
@@ -106,12 +111,9 @@ struct PnHdr {
 };
 struct PnSlot {
     int32_t seq;          // string in the slot
-    int32_t E;            // its exponent sum
-    int32_t fin_seq;      // string whose last step's results are pending
-    int32_t fin_step;     // that last step
-    int32_t fin_E;        // and its final exponent sum
-    int16_t row;          // row at the current (last planned) step
-    uint8_t c, flags, blkcnt, blkflags, pad0, pad1;
+    int32_t pend[2];      // string whose last step (of that parity) awaits its log-likelihood
+    int16_t row;          // row at the last planned step
+    uint8_t c, flags, blkcnt, blkflags;
 };
 struct PnChunk {
     uint16_t row0;
@@ -121,8 +123,8 @@ struct PnChunk {
 struct PnLayout {
     int p_sub, rows, npairs, nregions, ring_base;
     uint32_t lbo;
-    uint32_t s_off, sym_off, hdr_off, rec_off, xmax_off, fin_off, chunk_off, slot_off,
-        misc_off, total;
+    uint32_t s_off, sym_off, hdr_off, rec_off, xmax_off, fin_off, fine_off, e_off, chunk_off,
+        slot_off, misc_off, total;
 };
 
 __host__ __device__ inline uint32_t pn_align16(uint32_t x) { return (x + 15u) & ~15u; }
@@ -139,22 +141,26 @@ static PnLayout pn_layout(int p_sub, int sigma) {
     L.lbo = (uint32_t)rows * 16u;
     const uint32_t ps = (uint32_t)p_sub, nr = (uint32_t)rows;
     uint32_t off = 0;
-    L.s_off = off;                    // [b][parity] B buffers, 8 * lbo bytes each
-    off += 4u * 8u * L.lbo;
-    L.sym_off = off;                  // [buf][16 steps][2 * p_sub] symbols
-    off += 2u * kPnBlk * 2u * ps;
-    L.hdr_off = pn_align16(off);      // [buf][2 * p_sub] headers
-    off = L.hdr_off + 2u * 2u * ps * (uint32_t)sizeof(PnHdr);
-    L.rec_off = pn_align16(off);      // [b][parity][rows] uint2 {destination, scale}
+    L.s_off = off;                    // [step parity] B buffers, 8 * lbo bytes each
+    off += 2u * 8u * L.lbo;
+    L.sym_off = off;                  // [buf][16 steps][p_sub] symbols
+    off += 2u * kPnBlk * ps;
+    L.hdr_off = pn_align16(off);      // [buf][p_sub] headers
+    off = L.hdr_off + 2u * ps * (uint32_t)sizeof(PnHdr);
+    L.rec_off = pn_align16(off);      // [step & 3][rows] uint2 records
     off = L.rec_off + 4u * nr * 8u;
-    L.xmax_off = pn_align16(off);     // [b][parity][rows] float2
-    off = L.xmax_off + 4u * nr * 8u;
-    L.fin_off = off;                  // [b][p_sub] float2
+    L.xmax_off = pn_align16(off);     // [step parity][rows] float2: max|s| of each half
+    off = L.xmax_off + 2u * nr * 8u;
+    L.fin_off = off;                  // [step parity][p_sub] float2: accept-weighted halves
     off += 2u * ps * 8u;
-    L.chunk_off = pn_align16(off);    // [b][parity][kPnMaxChunks]
+    L.fine_off = off;                 // [step parity][p_sub] int32: final exponent sums
+    off += 2u * ps * 4u;
+    L.e_off = off;                    // [p_sub] int32: exponent sums
+    off += ps * 4u;
+    L.chunk_off = pn_align16(off);    // [step & 3][kPnMaxChunks]
     off = L.chunk_off + 4u * kPnMaxChunks * (uint32_t)sizeof(PnChunk);
-    L.slot_off = pn_align16(off);     // [2 * p_sub]
-    off = L.slot_off + 2u * ps * (uint32_t)sizeof(PnSlot);
+    L.slot_off = pn_align16(off);     // [p_sub]
+    off = L.slot_off + ps * (uint32_t)sizeof(PnSlot);
     L.misc_off = pn_align16(off);
     off = L.misc_off + kPnMiscBytes;
     L.total = pn_align16(off);
@@ -163,22 +169,26 @@ static PnLayout pn_layout(int p_sub, int sigma) {
 
 // misc region (bytes, relative to misc_off)
 constexpr uint32_t kMTmem = 0, kMAbort = 4, kMPlanOk = 8, kMFinal = 12,
-                   kMNch = 16,        // int32 [b][parity]
+                   kMNch = 16,        // int32 [step & 3]
                    kMBlkAct = 32,     // int32 [buf][loader warp]
-                   kMBar = 64,        // mbarriers, 8 bytes each (see PnBar)
+                   kMBar = 64,        // mbarriers, 8 bytes each
                    kMCnt = 320,       // int32 [16 pairs][2 parities]
                    kMPinfo = 448,     // int32 [16 pairs][base, neven]
                    kMRsym = 576,      // float [32]
                    kMStart = 704,     // uint4 [8]
                    kMAcc = 832;       // float [64]
 // mbarrier indices
-constexpr int kBarPlan = 0,   // [b][parity]  1 arrival
-              kBarEpi = 4,    // [b][parity]  8 arrivals (all epilogue warps)
-              kBarFull = 8,   // [region]     tcgen05.commit
-              kBarEmpty = 14, // [region]     4 arrivals (the set that drained it)
-              kBarLoaded = 20,   // [buf]     2 arrivals
-              kBarConsumed = 22, // [buf]     1 arrival
-              kBarCount = 24;
+constexpr int kBarPlan1 = 0,     // [step & 3]   layout, chunk list, records   1 arrival
+              kBarPlan2 = 4,     // [step & 1]   start rows                    1 arrival
+              kBarEpi = 6,       // [step & 3]   epilogue done                 8 arrivals
+              kBarFull = 10,     // [region]     tcgen05.commit
+              kBarEmpty = 16,    // [region]     4 arrivals (the set that drained it)
+              kBarLoaded = 22,   // [buf]        2 arrivals
+              kBarConsumed = 24, // [buf]        1 arrival
+              kBarCount = 26;
+// record of a row (one string at one step): x = destination row * 16 (or kRecFinish | slot),
+// y = slot | kRecFresh
+constexpr uint32_t kRecFresh = 1u << 31;
 
 struct PnParams {
     const uint8_t *data;
@@ -221,18 +231,29 @@ __device__ __forceinline__ bool pn_mbar_test(uint32_t addr, uint32_t parity) {
         : "=r"(done) : "r"(addr), "r"(parity) : "memory");
     return done != 0;
 }
+// non-suspending test: a spinning waiter sees the phase flip at once (try_wait may park the
+// thread for a few thousand cycles)
+__device__ __forceinline__ bool pn_mbar_poll(uint32_t addr, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}"
+        : "=r"(done) : "r"(addr), "r"(parity) : "memory");
+    return done != 0;
+}
 __device__ __forceinline__ void pn_mbar_arrive(uint32_t addr) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(addr) : "memory");
 }
 
 // Waits (lane 0 of the calling warp) for the completion of the phase with the
-// given parity; bounded; the result is broadcast to the warp.
+// given parity; bounded; the result is broadcast to the warp. Spins on the
+// non-suspending test: the hand-offs of this kernel are on its critical path.
 __device__ __forceinline__ bool pn_wait(uint32_t addr, uint32_t parity, volatile uint32_t *abort_flag,
                                         uint32_t *err) {
     int ok = 1;
     if ((threadIdx.x & 31) == 0) {
         const long long t0 = clock64();
-        while (!pn_mbar_test(addr, parity)) {
+        while (!pn_mbar_poll(addr, parity)) {
             if (*abort_flag) { ok = 0; break; }
             if (clock64() - t0 > kPnWaitCycles) {
                 atomicOr(err, kPnErrTimeout);
@@ -328,37 +349,44 @@ struct PnShared {
         return reinterpret_cast<volatile uint32_t *>(misc() + off);
     }
     __device__ uint32_t bar(int i) const { return pn_smem_u32(misc() + kMBar + 8 * i); }
-    __device__ uint32_t sbuf(int b, int par) const {   // byte offset of a B buffer
-        return L.s_off + (uint32_t)(b * 2 + par) * 8u * L.lbo;
-    }
-    __device__ uint8_t *sym(int buf) const { return base + L.sym_off + buf * kPnBlk * 2 * L.p_sub; }
+    __device__ uint32_t sbuf(int par) const { return L.s_off + (uint32_t)par * 8u * L.lbo; }
+    __device__ uint8_t *sym(int buf) const { return base + L.sym_off + buf * kPnBlk * L.p_sub; }
     __device__ PnHdr *hdr(int buf) const {
-        return reinterpret_cast<PnHdr *>(base + L.hdr_off) + buf * 2 * L.p_sub;
+        return reinterpret_cast<PnHdr *>(base + L.hdr_off) + buf * L.p_sub;
     }
-    __device__ uint2 *rec(int b, int par) const {
-        return reinterpret_cast<uint2 *>(base + L.rec_off) + (b * 2 + par) * L.rows;
+    __device__ uint2 *rec(int s) const {
+        return reinterpret_cast<uint2 *>(base + L.rec_off) + (s & 3) * L.rows;
     }
-    __device__ float2 *xmax(int b, int par) const {
-        return reinterpret_cast<float2 *>(base + L.xmax_off) + (b * 2 + par) * L.rows;
+    __device__ float2 *xmax(int s) const {
+        return reinterpret_cast<float2 *>(base + L.xmax_off) + (s & 1) * L.rows;
     }
-    __device__ float2 *fin(int b) const { return reinterpret_cast<float2 *>(base + L.fin_off) + b * L.p_sub; }
-    __device__ PnChunk *chunks(int b, int par) const {
-        return reinterpret_cast<PnChunk *>(base + L.chunk_off) + (b * 2 + par) * kPnMaxChunks;
+    __device__ float2 *fin(int s) const {
+        return reinterpret_cast<float2 *>(base + L.fin_off) + (s & 1) * L.p_sub;
+    }
+    __device__ int32_t *finE(int s) const {
+        return reinterpret_cast<int32_t *>(base + L.fine_off) + (s & 1) * L.p_sub;
+    }
+    __device__ int32_t *E() const { return reinterpret_cast<int32_t *>(base + L.e_off); }
+    __device__ PnChunk *chunks(int s) const {
+        return reinterpret_cast<PnChunk *>(base + L.chunk_off) + (s & 3) * kPnMaxChunks;
     }
     __device__ PnSlot *slots() const { return reinterpret_cast<PnSlot *>(base + L.slot_off); }
-    __device__ volatile int32_t *nch(int b, int par) const {
-        return reinterpret_cast<volatile int32_t *>(misc() + kMNch) + b * 2 + par;
+    __device__ volatile int32_t *nch(int s) const {
+        return reinterpret_cast<volatile int32_t *>(misc() + kMNch) + (s & 3);
     }
     __device__ int32_t *cnt() const { return reinterpret_cast<int32_t *>(misc() + kMCnt); }
     __device__ int32_t *pinfo() const { return reinterpret_cast<int32_t *>(misc() + kMPinfo); }
 };
+
+// phase parity of the k-th completion of a barrier that completes once every `period` steps
+__device__ __forceinline__ uint32_t pn_par(int step, int period) { return (uint32_t)(step / period) & 1u; }
 
 // ---- loader: warps 13-14 -------------------------------------------------------------------------
 __device__ void pn_loader(const PnParams &P, const PnShared &S, volatile uint32_t *abort_flag) {
     const int lane = threadIdx.x & 31;
     const int lw = (threadIdx.x >> 5) - kPnLoadWarp0;
     const int ll = lw * 32 + lane;
-    const int PC = 2 * S.L.p_sub;
+    const int PC = S.L.p_sub;
     const uint32_t sig4 = (uint32_t)P.sigma * 0x01010101u;
     int32_t seq[8];
     int64_t pos[8], end[8];
@@ -461,201 +489,204 @@ __device__ void pn_loader(const PnParams &P, const PnShared &S, volatile uint32_
 }
 
 // ---- planner: warps 9-12 ---------------------------------------------------------------------------
-// named barrier 1: the four planner warps only
+// named barrier 1: the four planner warps only; only warp 9 waits on mbarriers
 __device__ __forceinline__ void pn_plan_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
 
+// Per step s, in order:
+//  stage 1 (waits for the symbol block and for the epilogue of step s-4, the last user of the
+//          4-deep record and chunk rings): ranks of the slots by symbol pair, the chunk list of
+//          step s, the records of step s-1 (destination rows); signals kBarPlan1[s & 3].
+//  stage 2 (waits for the epilogue of step s-2): log-likelihoods of the strings that ended at
+//          step s-2, the start vector into the rows of strings that begin at step s (B buffer
+//          s & 1, last read by the MMA of step s-2); signals kBarPlan2[s & 1].
 __device__ void pn_planner(const PnParams &P, const PnShared &S, volatile uint32_t *abort_flag) {
     const int tid = threadIdx.x - 32 * kPnPlanWarp0;   // 0..127
     const int lane = tid & 31;
     const bool leader = tid == 0;
     const PnLayout &L = S.L;
-    const int PS = L.p_sub, PC = 2 * PS;
+    const int PS = L.p_sub;
     const uint4 *simg = reinterpret_cast<const uint4 *>(S.misc() + kMStart);
     PnSlot *slots = S.slots();
     int32_t *cnt = S.cnt();
     int32_t *pinfo = S.pinfo();
     volatile uint32_t *plan_ok = S.u32(kMPlanOk);
     volatile uint32_t *final_flag = S.u32(kMFinal);
-    for (int j = tid; j < PC; j += kPnPlanThreads) {
+    for (int j = tid; j < PS; j += kPnPlanThreads) {
         PnSlot z;
-        z.seq = -1; z.E = 0; z.fin_seq = -1; z.fin_step = -1; z.fin_E = 0; z.row = 0; z.c = 0; z.flags = 0;
-        z.blkcnt = 0; z.blkflags = 0; z.pad0 = z.pad1 = 0;
+        z.seq = -1; z.pend[0] = -1; z.pend[1] = -1; z.row = 0; z.c = 0; z.flags = 0;
+        z.blkcnt = 0; z.blkflags = 0;
         slots[j] = z;
     }
     for (int k = tid; k < 32; k += kPnPlanThreads) cnt[k] = 0;
     pn_plan_sync();
-    int term_s = -1;   // step whose chunk list says "terminate"
+    auto emit = [&](int s_done) {   // strings whose last step was s_done
+        const float2 *fin = S.fin(s_done);
+        const int32_t *finE = S.finE(s_done);
+        for (int j = tid; j < PS; j += kPnPlanThreads) {
+            const int32_t seq = slots[j].pend[s_done & 1];
+            if (seq < 0) continue;
+            const float2 f = fin[j];
+            const double dot = (double)f.x + (double)f.y;
+            const double ll = dot > 0.0 ? log(dot) + (double)finE[j] * 0.69314718055994530942 : -INFINITY;
+            pn_write_result(P.loglik, P.accept, P.accept_i32, seq, ll);
+            slots[j].pend[s_done & 1] = -1;
+        }
+    };
     for (int s = 0;; ++s) {
-        for (int b = 0; b < 2; ++b) {
-            // --- the leader waits for the step's inputs; the others wait at the barrier
-            if (tid < 32) {
-                bool ok = true;
-                if (s >= 2)   // epilogue of step s-2: B buffer s&1, records s&1, dot products
-                    ok = pn_wait(S.bar(kBarEpi + b * 2 + (s & 1)), (uint32_t)((s - 2) >> 1) & 1u,
-                                 abort_flag, P.err);
-                if (ok && b == 0 && s % kPnBlk == 0 && term_s < 0) {
-                    const int blk = s / kPnBlk;
-                    if (leader && blk >= 1) pn_mbar_arrive(S.bar(kBarConsumed + ((blk - 1) & 1)));
-                    ok = pn_wait(S.bar(kBarLoaded + (blk & 1)), (uint32_t)(blk >> 1) & 1u, abort_flag,
-                                 P.err);
-                    if (ok && leader) {
-                        const volatile int32_t *ba =
-                            reinterpret_cast<const volatile int32_t *>(S.misc() + kMBlkAct);
-                        *final_flag = (ba[(blk & 1) * 2] + ba[(blk & 1) * 2 + 1]) == 0;
-                    }
+        // ---------------- stage 1 ----------------
+        if (tid < 32) {
+            bool ok = true;
+            if (s >= 4)
+                ok = pn_wait(S.bar(kBarEpi + ((s - 4) & 3)), pn_par(s - 4, 4), abort_flag, P.err);
+            if (ok && s % kPnBlk == 0) {
+                const int blk = s / kPnBlk;
+                if (leader && blk >= 1) pn_mbar_arrive(S.bar(kBarConsumed + ((blk - 1) & 1)));
+                ok = pn_wait(S.bar(kBarLoaded + (blk & 1)), (uint32_t)(blk >> 1) & 1u, abort_flag, P.err);
+                if (ok && leader) {
+                    const volatile int32_t *ba =
+                        reinterpret_cast<const volatile int32_t *>(S.misc() + kMBlkAct);
+                    *final_flag = (ba[(blk & 1) * 2] + ba[(blk & 1) * 2 + 1]) == 0;
                 }
-                if (leader) *plan_ok = ok ? 1u : 0u;
             }
-            pn_plan_sync();
-            if (!*plan_ok) return;
-            const bool done_now = term_s >= 0 && s > term_s;   // only emissions were left
-            const int in = s % kPnBlk;
-            const int buf = (s / kPnBlk) & 1;
-            const uint8_t *sym = S.sym(buf);
-            const PnHdr *hd = S.hdr(buf);
-            const float2 *fin = S.fin(b);
-            // --- stage A: emissions of step s-2, headers, symbols and ranks of step s
-            int rank[2] = {-1, -1}, cs[2] = {-1, -1}, nseq[2] = {-1, -1};
+            if (leader) *plan_ok = ok ? 1u : 0u;
+        }
+        pn_plan_sync();
+        if (!*plan_ok) return;
+        const int in = s % kPnBlk;
+        const int buf = (s / kPnBlk) & 1;
+        const bool terminal = in == 0 && *final_flag;
+        const uint8_t *sym = S.sym(buf);
+        const PnHdr *hd = S.hdr(buf);
+        int rank[kPnSlotsPerPlanThread], cs[kPnSlotsPerPlanThread], nseq[kPnSlotsPerPlanThread];
 #pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                const int jl = tid + kPnPlanThreads * k;
-                if (jl >= PS) continue;
-                const int j = b * PS + jl;
-                PnSlot sl = slots[j];
-                if ((sl.flags & kSlotFinPending) && sl.fin_step <= s - 2) {
-                    const float2 f = fin[jl];
-                    const double dot = (double)f.x + (double)f.y;
-                    const double ll = dot > 0.0 ? log(dot) + (double)sl.fin_E * 0.69314718055994530942
-                                                : -INFINITY;
-                    pn_write_result(P.loglik, P.accept, P.accept_i32, sl.fin_seq, ll);
-                    sl.flags &= (uint8_t)~kSlotFinPending;
-                }
-                if (term_s < 0) {
-                    if (in == 0) {
-                        const PnHdr h = hd[j];
-                        sl.blkcnt = h.count;
-                        sl.blkflags = h.flags;
-                        if (h.flags & kHdrStart) nseq[k] = h.seq;
-                    }
-                    if (in < sl.blkcnt) {
-                        const int c = sym[in * PC + j];
-                        cs[k] = c;
-                        rank[k] = atomicAdd(&cnt[(c >> 1) * 2 + (c & 1)], 1);
-                    }
-                }
+        for (int k = 0; k < kPnSlotsPerPlanThread; ++k) {
+            rank[k] = -1;
+            cs[k] = -1;
+            nseq[k] = -1;
+            const int j = tid + kPnPlanThreads * k;
+            if (j >= PS || terminal) continue;
+            PnSlot sl = slots[j];
+            if (in == 0) {
+                const PnHdr h = hd[j];
+                sl.blkcnt = h.count;
+                sl.blkflags = h.flags;
+                if (h.flags & kHdrStart) nseq[k] = h.seq;
                 slots[j] = sl;
             }
-            if (done_now) {
-                if (b == 1) return;
-                continue;
+            if (in < sl.blkcnt) {
+                const int c = sym[in * PS + j];
+                cs[k] = c;
+                rank[k] = atomicAdd(&cnt[(c >> 1) * 2 + (c & 1)], 1);
             }
-            const bool terminal = term_s < 0 && in == 0 && *final_flag;
-            pn_plan_sync();
-            // --- stage B: pair bases and the chunk list of step s
-            const int par = s & 1;
-            if (tid < 32) {
-                int ne = 0, no = 0;
-                if (lane < L.npairs) {
-                    ne = cnt[lane * 2];
-                    no = cnt[lane * 2 + 1];
-                    cnt[lane * 2] = 0;
-                    cnt[lane * 2 + 1] = 0;
-                }
-                const int np = ne + no;
-                const int nc = (np + kPnRegionCols - 1) / kPnRegionCols;
-                int incl = np, cincl = nc;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const int a = __shfl_up_sync(0xffffffffu, incl, o);
-                    const int c = __shfl_up_sync(0xffffffffu, cincl, o);
-                    if (lane >= o) { incl += a; cincl += c; }
-                }
-                const int base = incl - np, cbase = cincl - nc;
-                if (lane < L.npairs) {
-                    pinfo[lane * 2] = base;
-                    pinfo[lane * 2 + 1] = ne;
-                    PnChunk *ch = S.chunks(b, par);
-                    for (int k = 0; k < nc; ++k) {
-                        PnChunk d;
-                        d.row0 = (uint16_t)(base + k * kPnRegionCols);
-                        const int cols = min(kPnRegionCols, np - k * kPnRegionCols);
-                        d.ncols = (uint8_t)cols;
-                        d.split = (uint8_t)min(max(ne - k * kPnRegionCols, 0), cols);
-                        d.pair = (uint8_t)lane;
-                        d.pad0 = d.pad1 = d.pad2 = 0;
-                        ch[cbase + k] = d;
-                    }
-                }
-                const int total_chunks = __shfl_sync(0xffffffffu, cincl, 31);
-                if (lane == 0) *S.nch(b, par) = terminal ? kPnTerminate : total_chunks;
+        }
+        pn_plan_sync();
+        if (tid < 32) {   // pair bases and the chunk list of step s
+            int ne = 0, no = 0;
+            if (lane < L.npairs) {
+                ne = cnt[lane * 2];
+                no = cnt[lane * 2 + 1];
+                cnt[lane * 2] = 0;
+                cnt[lane * 2 + 1] = 0;
             }
-            pn_plan_sync();
-            // --- stage C: rows of step s, records of step s-1, start rows, slot state
-            uint2 *rec = S.rec(b, (s - 1) & 1);
-            const float2 *xm = S.xmax(b, (s - 1) & 1);
-            const float *rsym = reinterpret_cast<const float *>(S.misc() + kMRsym);
-            const uint32_t sb = S.sbuf(b, par);
+            const int np = ne + no;
+            const int nc = (np + kPnRegionCols - 1) / kPnRegionCols;
+            int incl = np, cincl = nc;
 #pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                const int jl = tid + kPnPlanThreads * k;
-                if (jl >= PS) continue;
-                const int j = b * PS + jl;
-                PnSlot sl = slots[j];
-                int row1 = -1;
-                if (cs[k] >= 0) {
-                    const int p = cs[k] >> 1;
-                    row1 = pinfo[p * 2] + ((cs[k] & 1) ? pinfo[p * 2 + 1] : 0) + rank[k];
-                }
-                if (s >= 1 && (sl.flags & kSlotActive)) {
-                    // scale of step s-1: max|s_(s-1)| (left by the epilogue of step s-2, or the
-                    // start vector's) times the symbol's growth bound, rounded up to 2^f
-                    float m;
-                    if (sl.flags & kSlotFresh) {
-                        m = P.start_max;
-                        sl.E = 0;
-                    } else {
-                        const float2 x = xm[sl.row];
-                        m = fmaxf(x.x, x.y);
-                    }
-                    int f = pn_ceil_exp(m * rsym[sl.c]);
-                    f = min(max(f, -125), 125);
-                    sl.E += f;
-                    uint2 r;
-                    r.y = __float_as_uint(pn_pow2(-f));
-                    if (sl.flags & kSlotLast) {
-                        r.x = kRecFinish | (uint32_t)jl;
-                        sl.flags |= kSlotFinPending;
-                        sl.fin_seq = sl.seq;
-                        sl.fin_step = s - 1;
-                        sl.fin_E = sl.E;
-                    } else {
-                        // a continuing string is active at step s (blocks never leave it empty)
-                        r.x = (uint32_t)max(row1, 0) * 16u;
-                    }
-                    rec[sl.row] = r;
-                }
-                uint8_t nf = sl.flags & kSlotFinPending;
-                if (nseq[k] >= 0) sl.seq = nseq[k];
-                if (row1 >= 0) {
-                    nf |= kSlotActive;
-                    if ((sl.blkflags & kHdrEnd) && in == sl.blkcnt - 1) nf |= kSlotLast;
-                    if (nseq[k] >= 0) {
-                        nf |= kSlotFresh;
-                        uint8_t *dst = S.base + sb + (uint32_t)row1 * 16u;
-#pragma unroll
-                        for (int c = 0; c < 8; ++c)
-                            *reinterpret_cast<uint4 *>(dst + c * L.lbo) = simg[c];
-                    }
-                    sl.row = (int16_t)row1;
-                    sl.c = (uint8_t)cs[k];
-                }
-                sl.flags = nf;
-                slots[j] = sl;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int a = __shfl_up_sync(0xffffffffu, incl, o);
+                const int c = __shfl_up_sync(0xffffffffu, cincl, o);
+                if (lane >= o) { incl += a; cincl += c; }
             }
-            pn_fence_async_smem();
-            pn_plan_sync();
-            if (leader) pn_mbar_arrive(S.bar(kBarPlan + b * 2 + par));
-            if (terminal && b == 1) term_s = s;
+            const int base = incl - np, cbase = cincl - nc;
+            if (lane < L.npairs) {
+                pinfo[lane * 2] = base;
+                pinfo[lane * 2 + 1] = ne;
+                PnChunk *ch = S.chunks(s);
+                for (int k = 0; k < nc; ++k) {
+                    PnChunk d;
+                    d.row0 = (uint16_t)(base + k * kPnRegionCols);
+                    const int cols = min(kPnRegionCols, np - k * kPnRegionCols);
+                    d.ncols = (uint8_t)cols;
+                    d.split = (uint8_t)min(max(ne - k * kPnRegionCols, 0), cols);
+                    d.pair = (uint8_t)lane;
+                    d.pad0 = d.pad1 = d.pad2 = 0;
+                    ch[cbase + k] = d;
+                }
+            }
+            const int total_chunks = __shfl_sync(0xffffffffu, cincl, 31);
+            if (lane == 0) *S.nch(s) = terminal ? kPnTerminate : total_chunks;
+        }
+        pn_plan_sync();
+        uint2 *rec = S.rec(s - 1);
+#pragma unroll
+        for (int k = 0; k < kPnSlotsPerPlanThread; ++k) {
+            const int j = tid + kPnPlanThreads * k;
+            if (j >= PS) continue;
+            PnSlot sl = slots[j];
+            int row1 = -1;
+            if (cs[k] >= 0) {
+                const int p = cs[k] >> 1;
+                row1 = pinfo[p * 2] + ((cs[k] & 1) ? pinfo[p * 2 + 1] : 0) + rank[k];
+            }
+            if (s >= 1 && (sl.flags & kSlotActive)) {
+                uint2 r;
+                r.y = (uint32_t)j | ((sl.flags & kSlotFresh) ? kRecFresh : 0u);
+                if (sl.flags & kSlotLast) {
+                    r.x = kRecFinish | (uint32_t)j;
+                    sl.pend[(s - 1) & 1] = sl.seq;
+                } else {
+                    // a continuing string is active at step s (blocks never leave it empty)
+                    r.x = (uint32_t)max(row1, 0) * 16u;
+                }
+                rec[sl.row] = r;
+            }
+            uint8_t nf = 0;
+            if (nseq[k] >= 0) sl.seq = nseq[k];
+            if (row1 >= 0) {
+                nf |= kSlotActive;
+                if ((sl.blkflags & kHdrEnd) && in == sl.blkcnt - 1) nf |= kSlotLast;
+                if (nseq[k] >= 0) nf |= kSlotFresh;
+                sl.row = (int16_t)row1;
+                sl.c = (uint8_t)cs[k];
+            }
+            sl.flags = nf;
+            slots[j] = sl;
+        }
+        pn_plan_sync();
+        if (leader) pn_mbar_arrive(S.bar(kBarPlan1 + (s & 3)));
+        // ---------------- stage 2 ----------------
+        if (tid < 32) {
+            bool ok = true;
+            if (s >= 2) ok = pn_wait(S.bar(kBarEpi + ((s - 2) & 3)), pn_par(s - 2, 4), abort_flag, P.err);
+            if (leader) *plan_ok = ok ? 1u : 0u;
+        }
+        pn_plan_sync();
+        if (!*plan_ok) return;
+        if (s >= 2) emit(s - 2);
+        if (!terminal) {
+            const uint32_t sb = S.sbuf(s & 1);
+            for (int j = tid; j < PS; j += kPnPlanThreads) {
+                const PnSlot sl = slots[j];
+                if ((sl.flags & kSlotFresh) == 0) continue;
+                uint8_t *dst = S.base + sb + (uint32_t)sl.row * 16u;
+#pragma unroll
+                for (int c = 0; c < 8; ++c) *reinterpret_cast<uint4 *>(dst + c * L.lbo) = simg[c];
+            }
+        }
+        pn_fence_async_smem();
+        pn_plan_sync();
+        if (leader) pn_mbar_arrive(S.bar(kBarPlan2 + (s & 1)));
+        if (terminal) {   // the strings that ended at step s-1, then done
+            if (s >= 1) {
+                if (tid < 32) {
+                    const bool ok = pn_wait(S.bar(kBarEpi + ((s - 1) & 3)), pn_par(s - 1, 4), abort_flag,
+                                            P.err);
+                    if (leader) *plan_ok = ok ? 1u : 0u;
+                }
+                pn_plan_sync();
+                if (*plan_ok) emit(s - 1);
+            }
+            return;
         }
     }
 }
@@ -671,57 +702,47 @@ __device__ void pn_mma(const PnParams &P, const PnShared &S, uint32_t tbase,
     const uint32_t desc_hi = (128u >> 4) | (1u << 14);   // SBO = 128 B, descriptor version 1
     const uint32_t nr = (uint32_t)L.nregions;
     uint32_t g = 0;
-    int done = 0;
-    bool aborted = false;
-    for (int t = 0; !aborted && done != 3; ++t) {
-        for (int b = 0; b < 2 && !aborted; ++b) {
-            if (done & (1 << b)) continue;
-            if (!pn_wait(S.bar(kBarPlan + b * 2 + (t & 1)), (uint32_t)(t >> 1) & 1u, abort_flag, P.err)) {
+    for (int t = 0;; ++t) {
+        if (!pn_wait(S.bar(kBarPlan2 + (t & 1)), pn_par(t, 2), abort_flag, P.err)) break;
+        const int nch = *S.nch(t);
+        if (nch == kPnTerminate) break;
+        if (t >= 1 && !pn_wait(S.bar(kBarEpi + ((t - 1) & 3)), pn_par(t - 1, 4), abort_flag, P.err)) break;
+        const PnChunk *ch = S.chunks(t);
+        const uint32_t sb = smem_base + S.sbuf(t & 1);
+        bool aborted = false;
+        for (int k = 0; k < nch; ++k) {
+            const PnChunk d = ch[k];
+            const uint32_t r = g % nr, u = g / nr;
+            if (u > 0 && !pn_wait(S.bar(kBarEmpty + (int)r), (u - 1) & 1u, abort_flag, P.err)) {
                 aborted = true;
                 break;
             }
-            const int nch = *S.nch(b, t & 1);
-            if (nch == kPnTerminate) { done |= 1 << b; continue; }
-            if (t >= 1 && !pn_wait(S.bar(kBarEpi + b * 2 + ((t - 1) & 1)), (uint32_t)((t - 1) >> 1) & 1u,
-                                   abort_flag, P.err)) {
-                aborted = true;
-                break;
-            }
-            const PnChunk *ch = S.chunks(b, t & 1);
-            const uint32_t sb = smem_base + S.sbuf(b, t & 1);
-            for (int k = 0; k < nch; ++k) {
-                const PnChunk d = ch[k];
-                const uint32_t r = g % nr, u = g / nr;
-                if (u > 0 && !pn_wait(S.bar(kBarEmpty + (int)r), (u - 1) & 1u, abort_flag, P.err)) {
-                    aborted = true;
-                    break;
-                }
-                pn_tc_after();
-                if (lane == 0) {
-                    const uint32_t n16 = ((uint32_t)d.ncols + 15u) & ~15u;
-                    const uint32_t idesc = (1u << 4) | (fmt << 7) | (fmt << 10) | ((n16 >> 3) << 17) |
-                                           ((128u >> 4) << 24);
-                    const uint32_t td = tbase + (uint32_t)L.ring_base + r * kPnRegionCols;
+            pn_tc_after();
+            if (lane == 0) {
+                const uint32_t n16 = ((uint32_t)d.ncols + 15u) & ~15u;
+                const uint32_t idesc = (1u << 4) | (fmt << 7) | (fmt << 10) | ((n16 >> 3) << 17) |
+                                       ((128u >> 4) << 24);
+                const uint32_t td = tbase + (uint32_t)L.ring_base + r * kPnRegionCols;
 #pragma unroll
-                    for (int kk = 0; kk < 4; ++kk) {
-                        const uint32_t saddr = sb + (uint32_t)d.row0 * 16u + (uint32_t)kk * 2u * L.lbo;
-                        const uint64_t desc = (uint64_t)(((saddr >> 4) & 0x3FFFu) | ((L.lbo >> 4) << 16)) |
-                                              ((uint64_t)desc_hi << 32);
-                        const uint32_t ta = tbase + 32u * d.pair + 8u * kk;
-                        const uint32_t acc = kk > 0;
-                        asm volatile(
-                            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                            "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}"
-                            :: "r"(td), "r"(ta), "l"(desc), "r"(idesc), "r"(acc) : "memory");
-                    }
+                for (int kk = 0; kk < 4; ++kk) {
+                    const uint32_t saddr = sb + (uint32_t)d.row0 * 16u + (uint32_t)kk * 2u * L.lbo;
+                    const uint64_t desc = (uint64_t)(((saddr >> 4) & 0x3FFFu) | ((L.lbo >> 4) << 16)) |
+                                          ((uint64_t)desc_hi << 32);
+                    const uint32_t ta = tbase + 32u * d.pair + 8u * kk;
+                    const uint32_t acc = kk > 0;
                     asm volatile(
-                        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-                        :: "r"(S.bar(kBarFull + (int)r)) : "memory");
+                        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}"
+                        :: "r"(td), "r"(ta), "l"(desc), "r"(idesc), "r"(acc) : "memory");
                 }
-                __syncwarp();
-                ++g;
+                asm volatile(
+                    "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                    :: "r"(S.bar(kBarFull + (int)r)) : "memory");
             }
+            __syncwarp();
+            ++g;
         }
+        if (aborted) break;
     }
     // Drain: every committed chain must have finished before the TMEM is freed.
     for (uint32_t r = 0; r < nr && r < g; ++r) {
@@ -742,7 +763,9 @@ __device__ void pn_mma(const PnParams &P, const PnShared &S, uint32_t tbase,
 // so that in each 16-lane half h the lanes j and j + 8 hold the adjacent states 2j and 2j + 1: a
 // 16x256b load then gives thread t (j = t/4) the states 32(q&1) + 16h + 2j, +1 of four columns,
 // which it scales, packs into one 32-bit store per pair, and reduces (max) with the seven other
-// threads holding the same columns.
+// threads holding the same columns. The scale of a column, 2^-f with f the exponent of
+// max|s_t| * R_c (max|s_t| left by the previous step's epilogue), is computed by one lane per
+// column and shuffled to the others; warps q = 0, 2 keep the exponent sums.
 template <bool FP16>
 __device__ void pn_epilogue(const PnParams &P, const PnShared &S, uint32_t tbase,
                             volatile uint32_t *abort_flag) {
@@ -757,115 +780,139 @@ __device__ void pn_epilogue(const PnParams &P, const PnShared &S, uint32_t tbase
     const uint32_t toff1 = (uint32_t)(sg1 >> 3) * L.lbo + (uint32_t)(sg1 & 7) * 2u;
     const float *accv = reinterpret_cast<const float *>(S.misc() + kMAcc);
     const float a00 = accv[sg0], a01 = accv[sg0 + 1], a10 = accv[sg1], a11 = accv[sg1 + 1];
+    const float *rsym = reinterpret_cast<const float *>(S.misc() + kMRsym);
     const bool even = q < 2;
+    const bool owner = (q & 1) == 0;
+    int32_t *E = S.E();
     const uint32_t nr = (uint32_t)L.nregions;
     uint32_t g = 0;
-    int done = 0;
-    bool aborted = false;
-    for (int t = 0; !aborted && done != 3; ++t) {
-        for (int b = 0; b < 2 && !aborted; ++b) {
-            if (done & (1 << b)) continue;
-            if (t == 0 && !pn_wait(S.bar(kBarPlan + b * 2), 0u, abort_flag, P.err)) {
+    if (!pn_wait(S.bar(kBarPlan1), 0u, abort_flag, P.err)) return;
+    for (int t = 0;; ++t) {
+        const int nch = *S.nch(t);   // plan of step t: waited for in the previous iteration
+        if (nch == kPnTerminate) break;
+        // records of step t come with the plan of step t+1; the maxima of step t from both sets
+        if (!pn_wait(S.bar(kBarPlan1 + ((t + 1) & 3)), pn_par(t + 1, 4), abort_flag, P.err)) break;
+        if (t >= 1 && !pn_wait(S.bar(kBarEpi + ((t - 1) & 3)), pn_par(t - 1, 4), abort_flag, P.err)) break;
+        const PnChunk *ch = S.chunks(t);
+        const uint2 *rec = S.rec(t);
+        const float2 *xm = S.xmax(t);
+        float *xn = reinterpret_cast<float *>(S.xmax(t + 1)) + (q & 1);
+        float *fin = reinterpret_cast<float *>(S.fin(t)) + (q & 1);
+        int32_t *finE = S.finE(t);
+        uint8_t *snext = S.base + S.sbuf((t + 1) & 1);
+        bool aborted = false;
+        for (int k = 0; k < nch; ++k, ++g) {
+            if ((g & 1u) != set) continue;
+            const PnChunk d = ch[k];
+            const uint32_t r = g % nr, u = g / nr;
+            if (!pn_wait(S.bar(kBarFull + (int)r), u & 1u, abort_flag, P.err)) {
                 aborted = true;
                 break;
             }
-            const int nch = *S.nch(b, t & 1);
-            if (nch == kPnTerminate) { done |= 1 << b; continue; }
-            // records of step t come with the plan of step t+1
-            if (!pn_wait(S.bar(kBarPlan + b * 2 + ((t + 1) & 1)), (uint32_t)((t + 1) >> 1) & 1u,
-                         abort_flag, P.err)) {
-                aborted = true;
-                break;
-            }
-            const PnChunk *ch = S.chunks(b, t & 1);
-            const uint2 *rec = S.rec(b, t & 1);
-            float *xn = reinterpret_cast<float *>(S.xmax(b, (t + 1) & 1)) + (q & 1);
-            float *fin = reinterpret_cast<float *>(S.fin(b)) + (q & 1);
-            uint8_t *snext = S.base + S.sbuf(b, (t + 1) & 1);
-            for (int k = 0; k < nch; ++k, ++g) {
-                if ((g & 1u) != set) continue;
-                const PnChunk d = ch[k];
-                const uint32_t r = g % nr, u = g / nr;
-                if (!pn_wait(S.bar(kBarFull + (int)r), u & 1u, abort_flag, P.err)) {
-                    aborted = true;
-                    break;
-                }
-                pn_tc_after();
-                const int c_lo = even ? 0 : d.split;
-                const int c_hi = even ? d.split : d.ncols;
-                const uint32_t tcol = tbase + ((uint32_t)(32 * q) << 16) + (uint32_t)L.ring_base +
-                                      r * kPnRegionCols;
-                for (int c = c_lo & ~15; c < c_hi; c += 16) {
-                    uint32_t v0[8], v1[8];
-                    pn_tmem_ld16x256(tcol + (uint32_t)c, v0);
-                    pn_tmem_ld16x256(tcol + (16u << 16) + (uint32_t)c, v1);
-                    // this thread's columns: c + {2cp, 2cp+1, 2cp+8, 2cp+9}
-                    uint2 rc[4];
-                    bool valid[4];
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) {
-                        const int col = c + (i >> 1) * 8 + 2 * cp + (i & 1);
-                        valid[i] = col >= c_lo && col < c_hi;
-                        rc[i] = rec[d.row0 + (valid[i] ? col : c_lo)];
-                    }
-                    pn_tmem_wait_ld();
-                    float x[4][4], m[4];
-                    bool any_fin = false;
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) {
-                        const int ri = (i >> 1) * 4 + (i & 1);
-                        const float sc = __uint_as_float(rc[i].y);
-                        x[i][0] = __uint_as_float(v0[ri]) * sc;       // state sg0
-                        x[i][1] = __uint_as_float(v0[ri + 2]) * sc;   // sg0 + 1
-                        x[i][2] = __uint_as_float(v1[ri]) * sc;       // sg1
-                        x[i][3] = __uint_as_float(v1[ri + 2]) * sc;   // sg1 + 1
-                        const bool fin_i = (rc[i].x & kRecFinish) != 0;
-                        const bool keep = valid[i] && !fin_i;
-                        any_fin |= valid[i] && fin_i;
-                        if (keep) {
-                            uint8_t *dst = snext + rc[i].x;
-                            *reinterpret_cast<uint32_t *>(dst + toff0) = pn_pack2<FP16>(x[i][0], x[i][1]);
-                            *reinterpret_cast<uint32_t *>(dst + toff1) = pn_pack2<FP16>(x[i][2], x[i][3]);
+            pn_tc_after();
+            const int c_lo = even ? 0 : d.split;
+            const int c_hi = even ? d.split : d.ncols;
+            const float R = rsym[2 * d.pair + (even ? 0 : 1)];
+            const uint32_t tcol = tbase + ((uint32_t)(32 * q) << 16) + (uint32_t)L.ring_base +
+                                  r * kPnRegionCols;
+            for (int c = c_lo & ~15; c < c_hi; c += 16) {
+                uint32_t v0[8], v1[8];
+                pn_tmem_ld16x256(tcol + (uint32_t)c, v0);
+                pn_tmem_ld16x256(tcol + (16u << 16) + (uint32_t)c, v1);
+                // lane l < 16: the scale of column c + l (and the exponent sum of its string)
+                float scl = 1.f;
+                {
+                    const int col = c + lane;
+                    if (lane < 16 && col >= c_lo && col < c_hi) {
+                        const int row = d.row0 + col;
+                        const uint2 rcl = rec[row];
+                        const bool fresh = (rcl.y & kRecFresh) != 0;
+                        const int jl = (int)(rcl.y & 1023u);
+                        float m;
+                        if (fresh) {
+                            m = P.start_max;
+                        } else {
+                            const float2 x2 = xm[row];
+                            m = fmaxf(x2.x, x2.y);
                         }
-                        m[i] = keep ? fmaxf(fmaxf(fabsf(x[i][0]), fabsf(x[i][1])),
-                                            fmaxf(fabsf(x[i][2]), fabsf(x[i][3])))
-                                    : 0.f;
+                        int f = pn_ceil_exp(m * R);
+                        f = min(max(f, -125), 125);
+                        scl = pn_pow2(-f);
+                        if (owner) {
+                            const int e = (fresh ? 0 : E[jl]) + f;
+                            E[jl] = e;
+                            if (rcl.x & kRecFinish) finE[jl] = e;
+                        }
                     }
-                    // column maxima over this warp's 32 states: the 8 threads with the same cp
+                }
+                // this thread's columns: c + {2cp, 2cp+1, 2cp+8, 2cp+9}
+                uint2 rc[4];
+                bool valid[4];
+                float sc[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int co = (i >> 1) * 8 + 2 * cp + (i & 1);
+                    const int col = c + co;
+                    valid[i] = col >= c_lo && col < c_hi;
+                    rc[i] = rec[d.row0 + (valid[i] ? col : c_lo)];
+                    sc[i] = __shfl_sync(0xffffffffu, scl, co);
+                }
+                pn_tmem_wait_ld();
+                float x[4][4], m[4];
+                bool any_fin = false;
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int ri = (i >> 1) * 4 + (i & 1);
+                    x[i][0] = __uint_as_float(v0[ri]) * sc[i];       // state sg0
+                    x[i][1] = __uint_as_float(v0[ri + 2]) * sc[i];   // sg0 + 1
+                    x[i][2] = __uint_as_float(v1[ri]) * sc[i];       // sg1
+                    x[i][3] = __uint_as_float(v1[ri + 2]) * sc[i];   // sg1 + 1
+                    const bool fin_i = (rc[i].x & kRecFinish) != 0;
+                    const bool keep = valid[i] && !fin_i;
+                    any_fin |= valid[i] && fin_i;
+                    if (keep) {
+                        uint8_t *dst = snext + rc[i].x;
+                        *reinterpret_cast<uint32_t *>(dst + toff0) = pn_pack2<FP16>(x[i][0], x[i][1]);
+                        *reinterpret_cast<uint32_t *>(dst + toff1) = pn_pack2<FP16>(x[i][2], x[i][3]);
+                    }
+                    m[i] = keep ? fmaxf(fmaxf(fabsf(x[i][0]), fabsf(x[i][1])),
+                                        fmaxf(fabsf(x[i][2]), fabsf(x[i][3])))
+                                : 0.f;
+                }
+                // column maxima over this warp's 32 states: the 8 threads with the same cp
+#pragma unroll
+                for (int o = 4; o < 32; o <<= 1)
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) m[i] = fmaxf(m[i], __shfl_xor_sync(0xffffffffu, m[i], o));
+                if (j == 0) {
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+                        if (valid[i] && !(rc[i].x & kRecFinish)) xn[(rc[i].x >> 4) * 2] = m[i];
+                }
+                if (__any_sync(0xffffffffu, any_fin)) {   // last symbols: accept-weighted sums
+                    float pz[4];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+                        pz[i] = x[i][0] * a00 + x[i][1] * a01 + x[i][2] * a10 + x[i][3] * a11;
 #pragma unroll
                     for (int o = 4; o < 32; o <<= 1)
 #pragma unroll
-                        for (int i = 0; i < 4; ++i) m[i] = fmaxf(m[i], __shfl_xor_sync(0xffffffffu, m[i], o));
+                        for (int i = 0; i < 4; ++i) pz[i] += __shfl_xor_sync(0xffffffffu, pz[i], o);
                     if (j == 0) {
 #pragma unroll
                         for (int i = 0; i < 4; ++i)
-                            if (valid[i] && !(rc[i].x & kRecFinish)) xn[(rc[i].x >> 4) * 2] = m[i];
-                    }
-                    if (__any_sync(0xffffffffu, any_fin)) {   // last symbols: accept-weighted sums
-                        float pz[4];
-#pragma unroll
-                        for (int i = 0; i < 4; ++i)
-                            pz[i] = x[i][0] * a00 + x[i][1] * a01 + x[i][2] * a10 + x[i][3] * a11;
-#pragma unroll
-                        for (int o = 4; o < 32; o <<= 1)
-#pragma unroll
-                            for (int i = 0; i < 4; ++i) pz[i] += __shfl_xor_sync(0xffffffffu, pz[i], o);
-                        if (j == 0) {
-#pragma unroll
-                            for (int i = 0; i < 4; ++i)
-                                if (valid[i] && (rc[i].x & kRecFinish)) fin[(rc[i].x & 511u) * 2] = pz[i];
-                        }
+                            if (valid[i] && (rc[i].x & kRecFinish)) fin[(rc[i].x & 1023u) * 2] = pz[i];
                     }
                 }
-                pn_tc_before();
-                __syncwarp();
-                if (lane == 0) pn_mbar_arrive(S.bar(kBarEmpty + (int)r));
             }
-            if (aborted) break;
-            pn_fence_async_smem();
+            pn_tc_before();
             __syncwarp();
-            if (lane == 0) pn_mbar_arrive(S.bar(kBarEpi + b * 2 + (t & 1)));
+            if (lane == 0) pn_mbar_arrive(S.bar(kBarEmpty + (int)r));
         }
+        if (aborted) break;
+        pn_fence_async_smem();
+        __syncwarp();
+        if (lane == 0) pn_mbar_arrive(S.bar(kBarEpi + (t & 3)));
     }
 }
 
@@ -1078,10 +1125,10 @@ static int pn_choose(const trex_pnfa *h, int64_t n, int *grid, int *p_sub) {
     const int64_t sms = h->n_sms;
     if (n <= sms * 64) {
         *grid = (int)std::max<int64_t>(1, (n + 63) / 64);
-        *p_sub = 32;
+        *p_sub = 64;
     } else {
         *grid = (int)sms;
-        int64_t need = (n + 2 * sms - 1) / (2 * sms);
+        int64_t need = (n + sms - 1) / sms;
         need = (need + 31) / 32 * 32;
         *p_sub = (int)std::min<int64_t>(need, pmax);
     }
