@@ -1,0 +1,380 @@
+"""Serving: a continuous-batching request loop over resident automata.
+
+The reference serves nothing (it runs one static batch per call,
+cuda/monoid_batch.cu:498-588); this loop is the serving layer of the B200
+engine:
+
+* tables stay in HBM: one DFA set for all byte DFAs (up to 64, one ragged
+  launch carries any mix of them, a DFA id per string), a handle per Boolean
+  NFA and per probabilistic NFA;
+* admission by memory footprint: the HBM budget is split over two batch
+  slots; a request joins the forming batch while the slot's byte and request
+  capacities allow, and waits otherwise (a request larger than a slot is
+  refused at submit);
+* continuous batching: while one slot's batch runs on its stream, the loop
+  packs the requests that arrived meanwhile into the other slot and launches
+  it; a finished slot is drained (results handed to their requests) and
+  reused at once;
+* CUDA graphs: the DFA part of a batch (host-to-device copies, the planning
+  and ragged kernels, device-to-host copies) is captured once per slot and
+  size bucket (requests and bytes rounded up to powers of two, padded with
+  empty strings) and replayed;
+* per-request latency (submit to result) with p50/p99 and throughput.
+
+Results: DFA requests give (accept, final_state), NFA requests
+(accept, final_mask), probabilistic NFA requests (log_likelihood, accept).
+A request's result does not depend on what else is in its batch.
+"""
+
+from __future__ import annotations
+
+import collections
+import threading
+import time
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+KINDS = ("dfa", "nfa", "pnfa")
+
+
+@dataclass
+class Request:
+    rid: int
+    kind: str
+    engine: int
+    data: bytes
+    t_submit: float = 0.0
+    t_done: float = 0.0
+    result: object = None
+    error: Optional[str] = None
+    done: threading.Event = field(default_factory=threading.Event)
+
+    @property
+    def latency_ms(self) -> float:
+        return (self.t_done - self.t_submit) * 1e3
+
+
+def take_batch(queue: collections.deque, max_requests: int, max_bytes: int) -> list:
+    """FIFO admission: pop requests while the batch stays within both
+    capacities; the first request that does not fit stays at the head."""
+    batch, nbytes = [], 0
+    while queue and len(batch) < max_requests:
+        r = queue[0]
+        if nbytes + len(r.data) > max_bytes:
+            break
+        queue.popleft()
+        batch.append(r)
+        nbytes += len(r.data)
+    return batch
+
+
+def pack_batch(batch: Sequence[Request]):
+    """Order a batch as [DFA requests | NFA requests by engine | PNFA requests
+    by engine]. Returns (order, blob, dfa_offsets, dfa_ids, rest_offsets,
+    groups) where groups lists (kind, engine, first, count) over the non-DFA
+    part and both offset arrays are absolute into blob."""
+    dfa = [r for r in batch if r.kind == "dfa"]
+    rest = sorted((r for r in batch if r.kind != "dfa"), key=lambda r: (KINDS.index(r.kind), r.engine))
+    order = dfa + rest
+    lens = np.fromiter((len(r.data) for r in order), dtype=np.int64, count=len(order))
+    ends = np.cumsum(lens)
+    starts = ends - lens
+    blob = b"".join(r.data for r in order)
+    nd = len(dfa)
+    dfa_off = np.empty(nd + 1, dtype=np.int64)
+    dfa_off[0] = 0
+    dfa_off[1:] = ends[:nd]
+    dfa_ids = np.fromiter((r.engine for r in dfa), dtype=np.int32, count=nd)
+    rest_off = np.empty(len(rest) + 1, dtype=np.int64)
+    rest_off[0] = ends[nd - 1] if nd else 0
+    rest_off[1:] = ends[nd:]
+    groups = []
+    i = 0
+    while i < len(rest):
+        j = i
+        while j < len(rest) and rest[j].kind == rest[i].kind and rest[j].engine == rest[i].engine:
+            j += 1
+        groups.append((rest[i].kind, rest[i].engine, i, j - i))
+        i = j
+    return order, blob, dfa_off, dfa_ids, rest_off, groups
+
+
+def _bucket(x: int, lo: int) -> int:
+    b = lo
+    while b < x:
+        b <<= 1
+    return b
+
+
+class _Slot:
+    """Device and pinned host buffers of one in-flight batch."""
+
+    def __init__(self, torch, dev, max_requests: int, max_bytes: int, dfa_scratch: int):
+        u8, i32, i64, f64 = torch.uint8, torch.int32, torch.int64, torch.float64
+        R, B = max_requests, max_bytes
+        self.stream = torch.cuda.Stream(device=dev)
+        self.d_data = torch.zeros(B + 16, dtype=u8, device=dev)
+        self.d_doff = torch.zeros(R + 1, dtype=i64, device=dev)
+        self.d_ids = torch.zeros(max(R, 1), dtype=i32, device=dev)
+        self.d_roff = torch.zeros(R + 1, dtype=i64, device=dev)
+        self.d_fs = torch.zeros(max(R, 1), dtype=u8, device=dev)
+        self.d_ac = torch.zeros(max(R, 1), dtype=u8, device=dev)
+        self.d_ac2 = torch.zeros(max(R, 1), dtype=u8, device=dev)
+        self.d_mask = torch.zeros(max(R, 1), dtype=i64, device=dev)
+        self.d_ll = torch.zeros(max(R, 1), dtype=f64, device=dev)
+        self.d_scratch = torch.zeros(max(dfa_scratch, 16), dtype=u8, device=dev)
+        pin = dict(pin_memory=True)
+        self.h_data = torch.zeros(B + 16, dtype=u8, **pin)
+        self.h_doff = torch.zeros(R + 1, dtype=i64, **pin)
+        self.h_ids = torch.zeros(max(R, 1), dtype=i32, **pin)
+        self.h_roff = torch.zeros(R + 1, dtype=i64, **pin)
+        self.h_fs = torch.zeros(max(R, 1), dtype=u8, **pin)
+        self.h_ac = torch.zeros(max(R, 1), dtype=u8, **pin)
+        self.h_ac2 = torch.zeros(max(R, 1), dtype=u8, **pin)
+        self.h_mask = torch.zeros(max(R, 1), dtype=i64, **pin)
+        self.h_ll = torch.zeros(max(R, 1), dtype=f64, **pin)
+        self.event = torch.cuda.Event()
+        self.graphs = {}
+        self.batch = None
+        self.meta = None
+
+
+class Server:
+    """Continuous-batching server over resident automata (see the module docstring)."""
+
+    def __init__(self, dfas=(), nfas=(), pnfas=(), *, hbm_budget: int = 1 << 30,
+                 max_batch_requests: int = 1 << 14, pnfa_mode: str = "bf16", use_graphs: bool = True,
+                 device: int = 0):
+        import torch
+        from .engine import NFA, PNFA, DFASet
+        self.torch = torch
+        self.dev = torch.device("cuda", device)
+        torch.cuda.set_device(self.dev)
+        self.dfa_set = DFASet(list(dfas)) if len(dfas) else None
+        self.nfas = [NFA(T, s, a, unknown_rejects=True) for (T, s, a) in nfas]
+        self.pnfas = [PNFA(T, s, a) for (T, s, a) in pnfas]
+        self.pnfa_mode = pnfa_mode
+        self.use_graphs = use_graphs and self.dfa_set is not None
+        # admission: two slots share the budget; besides its bytes a request holds
+        # 8+4+8 B of offsets/ids and 1+1+1+8+8 B of outputs, plus the DFA scratch
+        per_req = 40
+        self.max_requests = max_batch_requests
+        slot_budget = hbm_budget // 2
+        self.max_bytes = max(1 << 16, slot_budget - per_req * max_batch_requests)
+        scratch = DFASet.scratch_bytes(max_batch_requests, self.max_bytes, 0)
+        while (scratch + self.max_bytes + per_req * max_batch_requests > slot_budget
+               and self.max_bytes > (1 << 16)):
+            self.max_bytes //= 2
+            scratch = DFASet.scratch_bytes(max_batch_requests, self.max_bytes, 0)
+        self.slots = [_Slot(torch, self.dev, max_batch_requests, self.max_bytes, scratch) for _ in range(2)]
+        if self.dfa_set is not None:   # first run outside any graph capture (one-time setup)
+            s0 = self.slots[0]
+            self.dfa_set.run(s0.d_data[:1], s0.d_doff[:2], s0.d_ids[:1], final_state=s0.d_fs,
+                             accept=s0.d_ac, scratch=s0.d_scratch, stream=s0.stream)
+            s0.stream.synchronize()
+        self._queue = collections.deque()
+        self._cv = threading.Condition()
+        self._next = 0
+        self._stop = False
+        self._completed: list = []
+        self._bytes_done = 0
+        self._batches = 0
+        self._t_first = None
+        self._t_last = None
+        self._error: Optional[BaseException] = None
+        self._thread = threading.Thread(target=self._loop, name="trex-serve", daemon=True)
+        self._thread.start()
+
+    # ---- client side ---------------------------------------------------------------------------
+    def submit(self, kind: str, engine: int, data: bytes) -> Request:
+        if kind not in KINDS:
+            raise ValueError(f"kind must be one of {KINDS}")
+        n_eng = {"dfa": len(self.dfa_set.dfas) if self.dfa_set else 0, "nfa": len(self.nfas),
+                 "pnfa": len(self.pnfas)}[kind]
+        if not 0 <= engine < n_eng:
+            raise ValueError(f"no {kind} automaton {engine}")
+        data = bytes(data)
+        if len(data) > self.max_bytes:
+            raise ValueError(f"request of {len(data)} bytes exceeds the slot capacity {self.max_bytes}")
+        with self._cv:
+            if self._error is not None:
+                raise RuntimeError("server loop failed") from self._error
+            r = Request(self._next, kind, engine, data, t_submit=time.perf_counter())
+            self._next += 1
+            self._queue.append(r)
+            self._cv.notify()
+        return r
+
+    def wait(self, reqs: Sequence[Request], timeout: float = 60.0) -> list:
+        end = time.perf_counter() + timeout
+        for r in reqs:
+            if not r.done.wait(max(0.0, end - time.perf_counter())):
+                raise TimeoutError(f"request {r.rid} not served in time")
+            if r.error:
+                raise RuntimeError(r.error)
+        return [r.result for r in reqs]
+
+    def stats(self) -> dict:
+        with self._cv:
+            lat = np.array([r.latency_ms for r in self._completed]) if self._completed else np.zeros(1)
+            span = (self._t_last - self._t_first) if self._t_first and self._t_last else 0.0
+            return {"requests": len(self._completed), "batches": self._batches,
+                    "bytes": self._bytes_done,
+                    "gchar_s": self._bytes_done / span / 1e9 if span > 0 else 0.0,
+                    "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                    "mean_ms": float(lat.mean())}
+
+    def reset_stats(self):
+        with self._cv:
+            self._completed = []
+            self._bytes_done = 0
+            self._batches = 0
+            self._t_first = self._t_last = None
+
+    def close(self):
+        with self._cv:
+            self._stop = True
+            self._cv.notify()
+        self._thread.join(timeout=30)
+        for s in self.slots:
+            s.graphs.clear()
+        if self.dfa_set is not None:
+            self.dfa_set.close()
+        for m in self.nfas + self.pnfas:
+            m.close()
+
+    # ---- loop ----------------------------------------------------------------------------------
+    def _loop(self):
+        torch = self.torch
+        torch.cuda.set_device(self.dev)
+        try:
+            while True:
+                for s in self.slots:
+                    if s.batch is not None and s.event.query():
+                        self._finish(s)
+                free = [s for s in self.slots if s.batch is None]
+                with self._cv:
+                    if self._stop and not self._queue and len(free) == len(self.slots):
+                        return
+                    batch = take_batch(self._queue, self.max_requests, self.max_bytes) if free else []
+                    if not batch and len(free) == len(self.slots) and not self._stop:
+                        self._cv.wait(timeout=0.05)
+                        continue
+                if batch:
+                    self._launch(free[0], batch)
+                else:
+                    time.sleep(20e-6)
+        except BaseException as e:   # hand the failure to every waiting request
+            with self._cv:
+                self._error = e
+                pending = list(self._queue) + [r for s in self.slots if s.batch for r in s.batch]
+                self._queue.clear()
+            for r in pending:
+                r.error = f"server loop failed: {e!r}"
+                r.done.set()
+
+    def _dfa_part(self, s: _Slot, nd: int, dfa_bytes: int):
+        torch = self.torch
+        if nd == 0:
+            return
+        if not self.use_graphs:
+            s.d_data[:dfa_bytes].copy_(s.h_data[:dfa_bytes], non_blocking=True)
+            s.d_doff[:nd + 1].copy_(s.h_doff[:nd + 1], non_blocking=True)
+            s.d_ids[:nd].copy_(s.h_ids[:nd], non_blocking=True)
+            self.dfa_set.run(s.d_data[:max(dfa_bytes, 1)], s.d_doff[:nd + 1], s.d_ids[:nd],
+                             final_state=s.d_fs, accept=s.d_ac, scratch=s.d_scratch, stream=s.stream)
+            s.h_fs[:nd].copy_(s.d_fs[:nd], non_blocking=True)
+            s.h_ac[:nd].copy_(s.d_ac[:nd], non_blocking=True)
+            return
+        nb = min(_bucket(nd, 64), self.max_requests)
+        bb = min(_bucket(max(dfa_bytes, 1), 1 << 16), self.max_bytes)
+        # padding: empty strings on automaton 0 after the last real one
+        s.h_doff[nd + 1:nb + 1] = int(s.h_doff[nd])
+        s.h_ids[nd:nb] = 0
+        key = (nb, bb)
+        g = s.graphs.get(key)
+        if g is None:
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=s.stream):
+                s.d_data[:bb].copy_(s.h_data[:bb], non_blocking=True)
+                s.d_doff[:nb + 1].copy_(s.h_doff[:nb + 1], non_blocking=True)
+                s.d_ids[:nb].copy_(s.h_ids[:nb], non_blocking=True)
+                self.dfa_set.run(s.d_data[:bb], s.d_doff[:nb + 1], s.d_ids[:nb], final_state=s.d_fs,
+                                 accept=s.d_ac, scratch=s.d_scratch,
+                                 stream=torch.cuda.current_stream())
+                s.h_fs[:nb].copy_(s.d_fs[:nb], non_blocking=True)
+                s.h_ac[:nb].copy_(s.d_ac[:nb], non_blocking=True)
+            s.graphs[key] = g
+        with torch.cuda.stream(s.stream):
+            g.replay()
+
+    def _launch(self, s: _Slot, batch: list):
+        torch = self.torch
+        order, blob, doff, ids, roff, groups = pack_batch(batch)
+        nd = len(doff) - 1
+        total = len(blob)
+        if total:
+            s.h_data[:total].copy_(torch.frombuffer(bytearray(blob), dtype=torch.uint8))
+        s.h_doff[:nd + 1].copy_(torch.from_numpy(doff))
+        if nd:
+            s.h_ids[:nd].copy_(torch.from_numpy(ids))
+        nr = len(roff) - 1
+        s.h_roff[:nr + 1].copy_(torch.from_numpy(roff))
+        dfa_bytes = int(doff[-1])
+        self._dfa_part(s, nd, dfa_bytes)
+        if nr:
+            # an NFA or PNFA handle keeps one work queue: its launches from the two slots
+            # must not overlap, so this slot's stream waits for the other slot's batch
+            for o in self.slots:
+                if o is not s and o.batch is not None:
+                    s.stream.wait_event(o.event)
+            with torch.cuda.stream(s.stream):
+                if total > dfa_bytes:
+                    s.d_data[dfa_bytes:total].copy_(s.h_data[dfa_bytes:total], non_blocking=True)
+                s.d_roff[:nr + 1].copy_(s.h_roff[:nr + 1], non_blocking=True)
+                for kind, eng, first, cnt in groups:
+                    off = s.d_roff[first:first + cnt + 1]
+                    data = s.d_data[:max(total, 1)]
+                    if kind == "nfa":
+                        self.nfas[eng].run(data, off, final_mask=s.d_mask[first:first + cnt],
+                                           accept=s.d_ac2[first:first + cnt], stream=s.stream)
+                    else:
+                        self.pnfas[eng].run(data, off, self.pnfa_mode, loglik=s.d_ll[first:first + cnt],
+                                            accept=s.d_ac2[first:first + cnt], stream=s.stream)
+                s.h_mask[:nr].copy_(s.d_mask[:nr], non_blocking=True)
+                s.h_ll[:nr].copy_(s.d_ll[:nr], non_blocking=True)
+                s.h_ac2[:nr].copy_(s.d_ac2[:nr], non_blocking=True)
+        s.event.record(s.stream)
+        s.batch = order
+        s.meta = (nd, nr, total)
+        with self._cv:
+            if self._t_first is None:
+                self._t_first = time.perf_counter()
+
+    def _finish(self, s: _Slot):
+        nd, nr, total = s.meta
+        fs = s.h_fs[:nd].numpy() if nd else None
+        ac = s.h_ac[:nd].numpy() if nd else None
+        ac2 = s.h_ac2[:nr].numpy() if nr else None
+        mask = s.h_mask[:nr].numpy() if nr else None
+        ll = s.h_ll[:nr].numpy() if nr else None
+        now = time.perf_counter()
+        for i, r in enumerate(s.batch):
+            if i < nd:
+                r.result = (bool(ac[i]), int(fs[i]))
+            elif r.kind == "nfa":
+                r.result = (bool(ac2[i - nd]), int(mask[i - nd]) & 0xFFFFFFFFFFFFFFFF)
+            else:
+                r.result = (float(ll[i - nd]), bool(ac2[i - nd]))
+            r.t_done = now
+        with self._cv:
+            self._completed.extend(s.batch)
+            self._bytes_done += total
+            self._batches += 1
+            self._t_last = now
+        for r in s.batch:
+            r.done.set()
+        s.batch = None
+        s.meta = None
