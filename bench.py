@@ -14,6 +14,9 @@ Workloads (synthetic, seeded; the reference ships no dataset):
       writes the state of every position (2 bytes moved per character).
   nfa: random 64-state Boolean NFA over 20 symbols (bytes 0..19), per-symbol
       edge density 0.05, 256K strings x 4096 symbols, bit-parallel kernel.
+  serve: the serving mix (64 resident automata, Poisson arrivals at
+      --serve-rates) through trex_b200.serving.Server; reports throughput
+      and p50/p99 latency per rate and the plain per-request launch.
   pnfa: probabilistic 64-state NFA over 20 symbols (rows Dirichlet(0.5) x 0.9,
       ~30% kept), 64K strings x 2048 symbols, tcgen05 kernel with BF16 (or
       --pnfa-mode fp16 / fp32) operands; also reports the log-likelihood error
@@ -56,7 +59,15 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["trex", "reference"], default="trex")
-    ap.add_argument("--workload", choices=["ragged", "plain", "scan", "nfa", "pnfa"], default="ragged")
+    ap.add_argument("--workload", choices=["ragged", "plain", "scan", "nfa", "pnfa", "serve"],
+                    default="ragged")
+    ap.add_argument("--serve-rates", type=str, default="2000,8000,32000",
+                    help="offered request rates (requests/s) of the serve workload")
+    ap.add_argument("--serve-seconds", type=float, default=2.0)
+    ap.add_argument("--serve-no-graphs", action="store_true",
+                    help="launch the DFA batches directly instead of replaying CUDA graphs")
+    ap.add_argument("--serve-plain", type=int, default=2000,
+                    help="requests timed one by one for the plain per-request baseline")
     ap.add_argument("--pnfa-mode", choices=["bf16", "fp16", "fp32"], default="bf16",
                     help="operand type of the probabilistic NFA workload")
     ap.add_argument("--strings", type=int, default=None, help="override the number of strings")
@@ -503,6 +514,141 @@ class PNFAWorkload:
 
 
 # ---------------------------------------------------------------------------------
+# serving mix
+# ---------------------------------------------------------------------------------
+
+def serving_mix(seed: int):
+    """64 resident automata: 32 DFAs (16 states, 256 bytes), 24 Boolean NFAs and
+    8 probabilistic NFAs (64 states, 20 symbols)."""
+    from trex_b200.workloads import random_bool_nfa, random_dfa, random_prob_nfa
+    rng = np.random.default_rng(seed)
+    dfas = [random_dfa(16, np.arange(256), rng) for _ in range(32)]
+    nfas = [random_bool_nfa(rng, 64, 20, 0.05) for _ in range(24)]
+    pnfas = [random_prob_nfa(rng, 64, 20) for _ in range(8)]
+    return dfas, nfas, pnfas
+
+
+def serving_requests(seed: int, n: int):
+    """Request pool: automaton uniform over the 64, lengths log-normal (median
+    2 KiB, sigma 1.0, clipped to [16, 1 MiB]), bytes uniform over the automaton's
+    alphabet."""
+    rng = np.random.default_rng(seed + 11)
+    which = rng.integers(0, 64, size=n)
+    lens = np.clip(np.round(np.exp(rng.normal(np.log(2048), 1.0, size=n))), 16, 1 << 20).astype(np.int64)
+    pool = []
+    for w, L in zip(which.tolist(), lens.tolist()):
+        if w < 32:
+            pool.append(("dfa", w, rng.integers(0, 256, size=L, dtype=np.uint8).tobytes()))
+        elif w < 56:
+            pool.append(("nfa", w - 32, rng.integers(0, 20, size=L, dtype=np.uint8).tobytes()))
+        else:
+            pool.append(("pnfa", w - 56, rng.integers(0, 20, size=L, dtype=np.uint8).tobytes()))
+    return pool
+
+
+def poisson_run(srv, pool, rate: float, duration: float, seed: int):
+    """Open-loop Poisson load: request k arrives at the k-th point of a Poisson
+    process of `rate` requests/s over `duration` s. The client submits every
+    request whose arrival time has passed in one call (its latency is counted
+    from its arrival time), then sleeps briefly. Waits for all; returns the
+    server stats."""
+    rng = np.random.default_rng(seed + 17)
+    n = max(1, int(rate * duration))
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n))
+    arrivals = arrivals[arrivals <= duration]
+    srv.reset_stats()
+    reqs = []
+    t0 = time.perf_counter()
+    k = 0
+    while k < len(arrivals):
+        now = time.perf_counter() - t0
+        j = int(np.searchsorted(arrivals, now, side="right"))
+        if j > k:
+            items = [pool[i % len(pool)] for i in range(k, j)]
+            reqs += srv.submit_many(items, t_arrival=(t0 + arrivals[k:j]).tolist())
+            k = j
+        else:
+            time.sleep(min(5e-4, max(0.0, arrivals[k] - now)))
+    srv.wait(reqs, timeout=300)
+    st = srv.stats()
+    st["offered_req_s"] = rate
+    st["offered_gchar_s"] = rate * float(np.mean([len(p[2]) for p in pool])) / 1e9
+    return st
+
+
+def plain_run(engines, pool, n_req: int):
+    """Baseline: each request alone (host-to-device copy, one launch, device-to-
+    host copy, synchronise), one after another."""
+    import torch
+    dset, nfas, pnfas = engines
+    lat = []
+    nbytes = 0
+    t0 = time.perf_counter()
+    for kind, eng, data in pool[:n_req]:
+        ts = time.perf_counter()
+        d = torch.frombuffer(bytearray(data), dtype=torch.uint8).cuda(non_blocking=True)
+        off = torch.tensor([0, len(data)], dtype=torch.int64).cuda(non_blocking=True)
+        if kind == "dfa":
+            _, ac, _ = dset.run(d, off, torch.tensor([eng], dtype=torch.int32).cuda())
+            ac.cpu()
+        elif kind == "nfa":
+            _, ac = nfas[eng].run(d, off)
+            ac.cpu()
+        else:
+            ll, _ = pnfas[eng].run(d, off, "fp32")
+            ll.cpu()
+        lat.append((time.perf_counter() - ts) * 1e3)
+        nbytes += len(data)
+    span = time.perf_counter() - t0
+    lat = np.array(lat)
+    return {"requests": n_req, "gchar_s": nbytes / span / 1e9,
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))}
+
+
+def serve_arm(args):
+    import torch
+    from trex_b200.engine import NFA, PNFA, DFASet
+    from trex_b200.serving import Server
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    dfas, nfas, pnfas = serving_mix(args.seed)
+    pool = serving_requests(args.seed, 20000)
+    srv = Server(dfas, nfas, pnfas, hbm_budget=2 << 30, max_batch_requests=1 << 14, pnfa_mode="auto",
+                 use_graphs=not args.serve_no_graphs)
+    # warm-up (graphs captured per size bucket, first launches)
+    poisson_run(srv, pool, 20000, 0.5, args.seed)
+    rates = [float(r) for r in args.serve_rates.split(",")]
+    clocks = ClockSampler(gpu_index_for(0))
+    clocks.start()
+    runs = [poisson_run(srv, pool, r, args.serve_seconds, args.seed + k) for k, r in enumerate(rates)]
+    clock_info = clocks.stop()
+    srv.close()
+    engines = (DFASet(dfas), [NFA(*x, unknown_rejects=True) for x in nfas], [PNFA(*x) for x in pnfas])
+    plain_run(engines, pool, 200)   # warm
+    plain = plain_run(engines, pool, args.serve_plain)
+    best = max(runs, key=lambda r: r["gchar_s"])
+    line = {
+        "metric": METRIC, "value": best["gchar_s"], "unit": "Gchar/s", "n_gpus": 1,
+        "steps": len(rates), "warmup": 1, "ms_per_step": args.serve_seconds * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic (seeded request pool, Poisson arrivals)",
+        "config": {"workload": "serving mix: 64 resident automata (32 DFA16 over 256 bytes, 24 Boolean "
+                               "NFA64 and 8 probabilistic NFA64 over 20 symbols), lengths log-normal "
+                               "median 2 KiB sigma 1.0 clipped [16 B, 1 MiB], automaton uniform, "
+                               "Poisson arrivals at each offered rate",
+                   "parallelism": "1 GPU, continuous batching (2 lanes x 2 slots, "
+                                  + ("direct launches)" if args.serve_no_graphs
+                                     else "CUDA graphs for DFA batches)"),
+                   "hbm_budget_bytes": 2 << 30, "pnfa_mode": "auto (fp32 below 2048 strings a group)"},
+        "served": [{k: r[k] for k in ("offered_req_s", "offered_gchar_s", "gchar_s", "p50_ms", "p99_ms",
+                                      "requests", "batches", "by_kind")} for r in runs],
+        "plain_per_request": plain,
+        "clocks": clock_info,
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------
 # clocks
 # ---------------------------------------------------------------------------------
 
@@ -765,6 +911,10 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         reference_arm(args, rank)
+        return
+    if args.workload == "serve":
+        if rank == 0:
+            serve_arm(args)
         return
     if world > 1:
         import datetime

@@ -153,7 +153,9 @@ int trex_dfa_batch_run(trex_dfa_set *set, const uint8_t *data, const int64_t *of
 
 /* Error word of the last trex_dfa_batch_run that used `scratch` (NULL = the
  * set's own scratch): 0 = fine, bit 0 = malformed offsets, bit 1 = automaton
- * id out of range (the affected strings were skipped). Synchronises. */
+ * id out of range (the affected strings were skipped), bit 2 = offsets that
+ * overlap so far that the batch needs more work items than total_bytes allows
+ * for (no string of the batch was run). Synchronises. */
 int trex_dfa_batch_error(trex_dfa_set *set, void *scratch, int32_t *err_out);
 
 /* The same device-pointer batch without any allocation (no counterpart in the
@@ -202,7 +204,9 @@ int trex_dfa_scan_run(trex_dfa_set *set, int dfa_index, const uint8_t *data,
                       uint8_t *states, uint8_t *final_state, uint8_t *accept, void *scratch,
                       int64_t scratch_bytes, int32_t tile_len, void *stream);
 /* Error word of the last scan that used `scratch` (same sizes as the run):
- * bit 0 malformed offsets, bit 2 a look-back wait ran out. Synchronises. */
+ * bit 0 malformed offsets, bit 2 a look-back wait ran out, bit 3 offsets that
+ * overlap so far that the tiles exceed the scratch (no tile was scanned).
+ * Synchronises. */
 int trex_dfa_scan_error(void *scratch, int64_t n_strings, int64_t total_bytes, int32_t tile_len,
                         int32_t *err_out);
 

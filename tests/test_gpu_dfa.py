@@ -101,6 +101,25 @@ def test_malformed_offsets_are_reported(cuda):
     assert err & 1
 
 
+@pytest.mark.parametrize("seg_len", [0, 64])
+def test_overlapping_offsets_are_refused(cuda, seg_len):
+    # [0, T) twenty times (with the reversed strings [T, 0) between them): the
+    # valid strings alone hold 20 T bytes, more work items than total_bytes = T
+    # allows for, so the planner refuses the whole batch (bit 2) besides
+    # reporting the reversed strings (bit 0)
+    rng = np.random.default_rng(2)
+    d = random_dfa(8, np.arange(256), rng)
+    T = 2048 * 64
+    data = rng.integers(0, 256, size=T, dtype=np.uint8)
+    off = np.tile(np.array([0, T], dtype=np.int64), 20)
+    _, _, err = _run_set(cuda, [d], data, off, seg_len=seg_len)
+    assert err & 1 and err & 4
+    # the same automaton on a well-formed batch afterwards (same scratch sizes)
+    ok = np.array([0, T // 2, T], dtype=np.int64)
+    _, _, err = _run_set(cuda, [d], data, ok, seg_len=seg_len)
+    assert err == 0
+
+
 def test_golden_byte_dfas_on_gpu(cuda, golden):
     for rec in golden["byte_dfa"]:
         N = rec["n_states"]

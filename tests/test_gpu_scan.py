@@ -105,3 +105,16 @@ def test_scan_golden_positions(cuda, golden):
         for i in range(len(strs)):
             assert st[off[i]:off[i + 1]].tolist() == rec["positions"][i]
         assert fs.tolist() == rec["final_state"]
+
+
+def test_scan_malformed_and_overlapping_offsets(cuda):
+    rng = np.random.default_rng(4)
+    dfa = random_dfa(8, np.arange(256), rng)
+    T = 1 << 17
+    data = rng.integers(0, 256, size=T, dtype=np.uint8)
+    # a reversed string: bit 0
+    _, _, _, err = _scan(cuda, dfa, data, np.array([0, 100, 50, T], dtype=np.int64), 64)
+    assert err & 1
+    # [0, T) twenty times: more tiles than total_bytes allows for, nothing is scanned (bit 3)
+    _, _, _, err = _scan(cuda, dfa, data, np.tile(np.array([0, T], dtype=np.int64), 20), 64)
+    assert err & 1 and err & 8

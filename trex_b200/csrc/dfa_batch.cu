@@ -54,6 +54,7 @@ constexpr int kWarmBytes = 128;
 enum : uint32_t {
     kErrBadOffsets = 1u,
     kErrBadDfaId = 2u,
+    kErrCapacity = 4u,   // offsets overlap: more work items than the scratch holds
 };
 
 constexpr int kRaggedThreads = 1024;
@@ -63,8 +64,8 @@ constexpr int kLenClasses = 8;
 
 // ---- scratch layout -----------------------------------------------------------
 struct ScratchLayout {
-    size_t cls_count, cls_cursor, q_base, q_count, q_head, q_bytes, err, map_cursor, items, maps,
-        done, total;
+    size_t cls_count, cls_cursor, q_base, q_count, q_head, q_bytes, err, map_cursor, n_items,
+        items, maps, done, total;
     int64_t max_items;
 };
 
@@ -87,6 +88,7 @@ static ScratchLayout scratch_layout(int64_t n_strings, int64_t total_bytes, int3
     L.q_bytes = take(kMaxDfasPerSet * 8);
     L.err = take(4);
     L.map_cursor = take(4);
+    L.n_items = take(8);
     L.items = take((size_t)L.max_items * sizeof(WorkItem));
     L.maps = take((size_t)L.max_items * sizeof(uint32_t));
     L.done = take((size_t)std::max<int64_t>(n_strings, 1) * 4);
@@ -122,7 +124,8 @@ __device__ __forceinline__ int len_class(int64_t len) {
 // string is malformed; malformed strings get no work items.
 __device__ __forceinline__ int checked_dfa(const int64_t *offsets, const int32_t *dfa_id,
                                            int64_t i, int n_dfas, int64_t total_bytes,
-                                           uint32_t *err, int64_t *len_out) {
+                                           uint32_t *err, int64_t *len_out,
+                                           int64_t *start_out = nullptr) {
     int64_t a = offsets[i], b = offsets[i + 1];
     int d = dfa_id ? dfa_id[i] : 0;
     if (a < 0 || b < a || b > total_bytes) {
@@ -134,17 +137,21 @@ __device__ __forceinline__ int checked_dfa(const int64_t *offsets, const int32_t
         return -1;
     }
     *len_out = b - a;
+    if (start_out) *start_out = a;
     return d;
 }
 
 __global__ void plan_count_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n,
                                   int64_t total_bytes, const DfaDesc *desc, int n_dfas,
                                   int32_t seg_len, uint32_t *cls_count,
-                                  unsigned long long *q_bytes, uint32_t *err) {
+                                  unsigned long long *q_bytes, unsigned long long *n_items,
+                                  uint32_t *err) {
     __shared__ uint32_t cnt[kMaxDfasPerSet * kLenClasses];
     __shared__ unsigned long long byt[kMaxDfasPerSet];
+    __shared__ unsigned long long items;
     for (int t = threadIdx.x; t < n_dfas * kLenClasses; t += blockDim.x) cnt[t] = 0;
     for (int t = threadIdx.x; t < n_dfas; t += blockDim.x) byt[t] = 0;
+    if (threadIdx.x == 0) items = 0;
     __syncthreads();
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
@@ -156,16 +163,28 @@ __global__ void plan_count_kernel(const int64_t *offsets, const int32_t *dfa_id,
         if (k > 1) atomicAdd(&cnt[d * kLenClasses + len_class(seg)], k - 1);
         atomicAdd(&cnt[d * kLenClasses + len_class(len - (int64_t)(k - 1) * seg)], 1u);
         atomicAdd(&byt[d], (unsigned long long)len + 64ull);
+        atomicAdd(&items, (unsigned long long)k);
     }
     __syncthreads();
+    if (threadIdx.x == 0 && items) atomicAdd(n_items, items);
     for (int t = threadIdx.x; t < n_dfas * kLenClasses; t += blockDim.x)
         if (cnt[t]) atomicAdd(&cls_count[t], cnt[t]);
     for (int t = threadIdx.x; t < n_dfas; t += blockDim.x)
         if (byt[t]) atomicAdd(&q_bytes[t], byt[t]);
 }
 
+// Queue bases per (DFA, length class). Offsets that overlap (each string in
+// range, but their lengths summing past total_bytes) would need more items
+// than the scratch was sized for: then the error bit is set and every queue is
+// left empty, so neither the fill kernel nor the ragged kernel writes an item.
 __global__ void plan_scan_kernel(const uint32_t *cls_count, uint32_t *cls_cursor, uint32_t *q_base,
-                                 uint32_t *q_count, int n_dfas) {
+                                 uint32_t *q_count, int n_dfas, const unsigned long long *n_items,
+                                 int64_t max_items, uint32_t *err) {
+    if (threadIdx.x == 0 && *n_items > (unsigned long long)max_items) {
+        atomicOr(err, kErrCapacity);
+        for (int d = 0; d < n_dfas; ++d) q_base[d] = q_count[d] = 0;
+        return;
+    }
     if (threadIdx.x == 0) {
         uint32_t run = 0;
         for (int d = 0; d < n_dfas; ++d) {
@@ -185,22 +204,29 @@ __global__ void plan_scan_kernel(const uint32_t *cls_count, uint32_t *cls_cursor
 __global__ void __launch_bounds__(kPlanThreads)
 plan_fill_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n, int64_t total_bytes,
                  const DfaDesc *desc, int n_dfas, int32_t seg_len, uint32_t *cls_cursor,
-                 uint32_t *map_cursor, WorkItem *items, uint32_t *done, uint32_t *err) {
+                 uint32_t *map_cursor, WorkItem *items, int64_t max_items, uint32_t *done,
+                 uint32_t *err) {
     __shared__ uint32_t s_cnt[kMaxDfasPerSet * kLenClasses];
     __shared__ uint32_t s_base[kMaxDfasPerSet * kLenClasses];
     __shared__ uint32_t s_map, s_map_base;
     const int n_slots = n_dfas * kLenClasses;
+    if (*(volatile uint32_t *)err & kErrCapacity) {   // set by plan_scan_kernel: no items
+        for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+             i += (int64_t)gridDim.x * blockDim.x)
+            done[i] = 0;
+        return;
+    }
     for (int t = threadIdx.x; t < n_slots; t += blockDim.x) s_cnt[t] = 0;
     if (threadIdx.x == 0) s_map = 0;
     __syncthreads();
     for (int64_t tile = blockIdx.x; tile * kPlanThreads < n; tile += gridDim.x) {
         const int64_t i = tile * kPlanThreads + threadIdx.x;
         int d = -1;
-        int64_t len = 0, seg = 0;
+        int64_t len = 0, seg = 0, s0 = 0;
         uint32_t k = 0, cf = 0, cl = 0, r_full = 0, r_last = 0, r_map = 0;
         if (i < n) {
             done[i] = 0;
-            d = checked_dfa(offsets, dfa_id, i, n_dfas, total_bytes, err, &len);
+            d = checked_dfa(offsets, dfa_id, i, n_dfas, total_bytes, err, &len, &s0);
         }
         if (d >= 0) {
             k = n_items_of(len, desc[d].n_states, seg_len, &seg);
@@ -218,11 +244,21 @@ plan_fill_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n, int64
         if (threadIdx.x == 0 && s_map) s_map_base = atomicAdd(map_cursor, s_map);
         __syncthreads();
         if (d >= 0) {
-            const int64_t s0 = offsets[i];
             const uint32_t mb = k > 1 ? s_map_base + r_map : 0u;
             const uint32_t warm = (uint32_t)(seg < kWarmBytes ? seg : (int64_t)kWarmBytes);
+            // With the counts of plan_count_kernel every position and map slot is
+            // below max_items; offsets rewritten between the two planning kernels
+            // (a caller changing inputs in flight) could break that: refuse.
+            if ((int64_t)mb + (int64_t)k > max_items) {
+                atomicOr(err, kErrCapacity);
+                k = 0;
+            }
             for (uint32_t j = 0; j < k; ++j) {
                 const uint32_t pos = (j + 1 == k) ? s_base[cl] + r_last : s_base[cf] + r_full + j;
+                if ((int64_t)pos >= max_items) {
+                    atomicOr(err, kErrCapacity);
+                    continue;
+                }
                 const int64_t b0 = s0 + (int64_t)j * seg;
                 const int64_t b1 = (j + 1 == k) ? s0 + len : b0 + seg;
                 items[pos] = (j == 0)
@@ -252,6 +288,9 @@ struct RaggedParams {
     const uint32_t *q_count;
     uint32_t *q_head;
     const unsigned long long *q_bytes;
+    const uint32_t *cls_count;
+    const uint32_t *cls_cursor;
+    uint32_t *err;
     uint32_t *maps;
     uint32_t *done;
     uint8_t *final_state;
@@ -281,6 +320,10 @@ __device__ __forceinline__ void publish_item(const RaggedParams &P, const W &w, 
     if (prev != nseg - 1) return;
     __threadfence();
     const int64_t s0 = P.offsets[str], len = P.offsets[str + 1] - s0;
+    if (s0 < 0 || len < 0 || s0 + len > P.total_bytes) {   // offsets changed in flight
+        atomicOr(P.err, kErrBadOffsets);
+        return;
+    }
     int64_t seg_bytes;
     n_items_of(len, D.n_states, P.seg_len, &seg_bytes);
     uint32_t s = (uint32_t)D.start;
@@ -451,11 +494,24 @@ __device__ void drain_queue(const RaggedParams &P, const W &w, const DfaDesc &D,
 __global__ void __launch_bounds__(kRaggedThreads, 1) dfa_ragged_kernel(RaggedParams P) {
     __shared__ int s_dfa;
     if (threadIdx.x == 0) {
+        // The plan is complete when every (DFA, length class) cursor of the fill
+        // ended exactly at its class's end (reservations are disjoint, so every
+        // item slot was then written once); otherwise (capacity overflow, or
+        // offsets rewritten while the plan ran) no item is trusted.
+        bool planned = true;
+        for (int d = 0; d < P.n_dfas; ++d) {
+            uint32_t run = P.q_base[d];
+            for (int c = 0; c < kLenClasses; ++c) {
+                run += P.cls_count[d * kLenClasses + c];
+                planned &= P.cls_cursor[d * kLenClasses + c] == run;
+            }
+        }
+        if (!planned) atomicOr(P.err, kErrCapacity);
         // Home DFA: CTAs are spread over DFAs in proportion to their bytes.
         unsigned long long tot = 0;
         for (int d = 0; d < P.n_dfas; ++d) tot += P.q_bytes[d];
         int home = -1;
-        if (tot) {
+        if (tot && planned) {
             unsigned long long pos =
                 (unsigned long long)((double)tot * ((double)blockIdx.x + 0.5) / gridDim.x);
             unsigned long long run = 0;
@@ -470,6 +526,7 @@ __global__ void __launch_bounds__(kRaggedThreads, 1) dfa_ragged_kernel(RaggedPar
         s_dfa = home;
     }
     __syncthreads();
+    if (s_dfa < 0) return;
     const uint32_t lane = threadIdx.x & 31u;
     for (int round = 0; round <= P.n_dfas; ++round) {
         const int d = s_dfa;
@@ -561,24 +618,26 @@ int dfa_set_run(trex_dfa_set *set, const uint8_t *data, const int64_t *offsets,
     auto *q_bytes = reinterpret_cast<unsigned long long *>(sc + L.q_bytes);
     uint32_t *err = reinterpret_cast<uint32_t *>(sc + L.err);
     uint32_t *map_cursor = reinterpret_cast<uint32_t *>(sc + L.map_cursor);
+    auto *n_items = reinterpret_cast<unsigned long long *>(sc + L.n_items);
     WorkItem *items = reinterpret_cast<WorkItem *>(sc + L.items);
     uint32_t *maps = reinterpret_cast<uint32_t *>(sc + L.maps);
     uint32_t *done = reinterpret_cast<uint32_t *>(sc + L.done);
 
-    // Counters, bases, heads, cursors, byte counts, the error word and the
-    // map cursor are contiguous at the front of the scratch buffer.
+    // Counters, bases, heads, cursors, byte counts, the error word, the map
+    // cursor and the item count are contiguous at the front of the scratch buffer.
     TREX_CUDA(cudaMemsetAsync(sc, 0, L.items, stream));
     int plan_grid = (int)std::min<int64_t>((n + kPlanThreads - 1) / kPlanThreads,
                                            (int64_t)set->n_sms * 8);
     plan_count_kernel<<<plan_grid, kPlanThreads, 0, stream>>>(
         offsets, dfa_id, n, total_bytes, set->d_desc, set->n_dfas, seg_len, cls_count, q_bytes,
-        err);
+        n_items, err);
     TREX_CHECK_LAUNCH();
-    plan_scan_kernel<<<1, 32, 0, stream>>>(cls_count, cls_cursor, q_base, q_count, set->n_dfas);
+    plan_scan_kernel<<<1, 32, 0, stream>>>(cls_count, cls_cursor, q_base, q_count, set->n_dfas,
+                                           n_items, L.max_items, err);
     TREX_CHECK_LAUNCH();
     plan_fill_kernel<<<plan_grid, kPlanThreads, 0, stream>>>(
         offsets, dfa_id, n, total_bytes, set->d_desc, set->n_dfas, seg_len, cls_cursor,
-        map_cursor, items, done, err);
+        map_cursor, items, L.max_items, done, err);
     TREX_CHECK_LAUNCH();
 
     RaggedParams P;
@@ -595,6 +654,9 @@ int dfa_set_run(trex_dfa_set *set, const uint8_t *data, const int64_t *offsets,
     P.q_count = q_count;
     P.q_head = q_head;
     P.q_bytes = q_bytes;
+    P.cls_count = cls_count;
+    P.cls_cursor = cls_cursor;
+    P.err = err;
     P.maps = maps;
     P.done = done;
     P.final_state = final_state;

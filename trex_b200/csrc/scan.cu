@@ -43,7 +43,7 @@ constexpr int kSyncCap = 512;                 // bytes walked with 16 chains bef
 constexpr uint32_t kPollLimit = 1u << 24;     // polls of one look-back step before giving up
 
 enum : uint32_t { kStAgg = 1u, kStPrefix = 2u };
-enum : uint32_t { kScanErrOffsets = 1u, kScanErrTimeout = 4u };
+enum : uint32_t { kScanErrOffsets = 1u, kScanErrTimeout = 4u, kScanErrCapacity = 8u };
 
 // Tile length: the requested one (>= 64), or by default the length that gives
 // every resident warp one 32-tile chunk (1 KiB multiples, 1 KiB .. 64 KiB).
@@ -76,10 +76,15 @@ static ScanScratch scan_layout(int64_t n_strings, int64_t total_bytes, int32_t t
 
 // tile_base[i] = number of tiles of strings 0..i-1 (single block, sequential
 // per thread chunk then a block scan; fine for the few long strings this path
-// is for, and correct for any count).
+// is for, and correct for any count). The chunk buffers hold max_tiles tiles,
+// enough for well-formed offsets; overlapping offsets that need more set the
+// capacity bit and leave zero tiles, so the scan kernel touches nothing.
+// Sums saturate at max_tiles + 1 so that they cannot wrap.
 __global__ void scan_tile_base_kernel(const int64_t *offsets, int64_t n, int64_t total_bytes,
-                                      int32_t tile, int64_t *tile_base, uint32_t *err) {
+                                      int32_t tile, int64_t max_tiles, int64_t *tile_base,
+                                      uint32_t *err) {
     __shared__ int64_t part[1024];
+    __shared__ bool over;
     const int64_t per = (n + blockDim.x - 1) / blockDim.x;
     const int64_t lo = threadIdx.x * per, hi = min(n, lo + per);
     int64_t sum = 0;
@@ -89,7 +94,7 @@ __global__ void scan_tile_base_kernel(const int64_t *offsets, int64_t n, int64_t
             atomicOr(err, kScanErrOffsets);
             continue;
         }
-        sum += (b - a + tile - 1) / tile;
+        sum = min(sum + (b - a + tile - 1) / tile, max_tiles + 1);
     }
     part[threadIdx.x] = sum;
     __syncthreads();
@@ -98,10 +103,17 @@ __global__ void scan_tile_base_kernel(const int64_t *offsets, int64_t n, int64_t
         for (int t = 0; t < (int)blockDim.x; ++t) {
             const int64_t v = part[t];
             part[t] = run;
-            run += v;
+            run = min(run + v, max_tiles + 1);
         }
+        over = run > max_tiles;
+        if (over) atomicOr(err, kScanErrCapacity);
     }
     __syncthreads();
+    if (over) {
+        for (int64_t i = lo; i < hi; ++i) tile_base[i] = 0;
+        if (threadIdx.x == 0) tile_base[n] = 0;
+        return;
+    }
     int64_t run = part[threadIdx.x];
     for (int64_t i = lo; i < hi; ++i) {
         tile_base[i] = run;
@@ -450,7 +462,7 @@ int trex_dfa_scan_run(trex_dfa_set *set, int dfa_index, const uint8_t *data,
     int64_t *tile_base = reinterpret_cast<int64_t *>(sc + L.tile_base);
     uint32_t *err = reinterpret_cast<uint32_t *>(sc + L.err);
     scan_tile_base_kernel<<<1, 1024, 0, stream>>>(offsets, n_strings, total_bytes, tile_len,
-                                                  tile_base, err);
+                                                  max_tiles, tile_base, err);
     TREX_CHECK_LAUNCH();
     scan_empty_kernel<<<(int)std::min<int64_t>((n_strings + 255) / 256, 4096), 256, 0, stream>>>(
         offsets, n_strings, start, acc, final_state, accept);

@@ -7,14 +7,18 @@ engine:
 * tables stay in HBM: one DFA set for all byte DFAs (up to 64, one ragged
   launch carries any mix of them, a DFA id per string), a handle per Boolean
   NFA and per probabilistic NFA;
-* admission by memory footprint: the HBM budget is split over two batch
+* admission by memory footprint: the HBM budget is split over the batch
   slots; a request joins the forming batch while the slot's byte and request
   capacities allow, and waits otherwise (a request larger than a slot is
   refused at submit);
+* two lanes with two slots each: DFA and Boolean NFA requests (walked in
+  bulk, milliseconds even for long strings) and probabilistic NFA requests
+  (a sequential product chain per string, latency proportional to its
+  length), so a long probabilistic request never holds back the others;
 * continuous batching: while one slot's batch runs on its stream, the loop
-  packs the requests that arrived meanwhile into the other slot and launches
-  it; a finished slot is drained (results handed to their requests) and
-  reused at once;
+  packs the requests that arrived meanwhile into the lane's other slot and
+  launches it; a finished slot is drained (results handed to their requests)
+  and reused at once;
 * CUDA graphs: the DFA part of a batch (host-to-device copies, the planning
   and ragged kernels, device-to-host copies) is captured once per slot and
   size bucket (requests and bytes rounded up to powers of two, padded with
@@ -111,7 +115,8 @@ def _bucket(x: int, lo: int) -> int:
 class _Slot:
     """Device and pinned host buffers of one in-flight batch."""
 
-    def __init__(self, torch, dev, max_requests: int, max_bytes: int, dfa_scratch: int):
+    def __init__(self, torch, dev, lane: str, max_requests: int, max_bytes: int, dfa_scratch: int):
+        self.lane = lane
         u8, i32, i64, f64 = torch.uint8, torch.int32, torch.int64, torch.float64
         R, B = max_requests, max_bytes
         self.stream = torch.cuda.Stream(device=dev)
@@ -146,7 +151,7 @@ class Server:
 
     def __init__(self, dfas=(), nfas=(), pnfas=(), *, hbm_budget: int = 1 << 30,
                  max_batch_requests: int = 1 << 14, pnfa_mode: str = "bf16", use_graphs: bool = True,
-                 device: int = 0):
+                 device: int = 0, pnfa_auto_threshold: int = 2048):
         import torch
         from .engine import NFA, PNFA, DFASet
         self.torch = torch
@@ -155,26 +160,40 @@ class Server:
         self.dfa_set = DFASet(list(dfas)) if len(dfas) else None
         self.nfas = [NFA(T, s, a, unknown_rejects=True) for (T, s, a) in nfas]
         self.pnfas = [PNFA(T, s, a) for (T, s, a) in pnfas]
+        # "auto": the FP32 kernel for groups of fewer than pnfa_auto_threshold strings (its
+        # per-step latency is far lower than the tensor-core kernel's), BF16 tcgen05 above
+        if pnfa_mode not in ("bf16", "fp16", "fp32", "auto"):
+            raise ValueError("pnfa_mode must be bf16, fp16, fp32 or auto")
         self.pnfa_mode = pnfa_mode
+        self.pnfa_auto_threshold = pnfa_auto_threshold
         self.use_graphs = use_graphs and self.dfa_set is not None
-        # admission: two slots share the budget; besides its bytes a request holds
-        # 8+4+8 B of offsets/ids and 1+1+1+8+8 B of outputs, plus the DFA scratch
+        # admission: the budget is split 3:1 between the two lanes, each with two slots;
+        # besides its bytes a request holds 8+4+8 B of offsets/ids and 1+1+1+8+8 B of
+        # outputs, plus the DFA scratch in the fast lane
         per_req = 40
         self.max_requests = max_batch_requests
-        slot_budget = hbm_budget // 2
-        self.max_bytes = max(1 << 16, slot_budget - per_req * max_batch_requests)
-        scratch = DFASet.scratch_bytes(max_batch_requests, self.max_bytes, 0)
-        while (scratch + self.max_bytes + per_req * max_batch_requests > slot_budget
-               and self.max_bytes > (1 << 16)):
-            self.max_bytes //= 2
-            scratch = DFASet.scratch_bytes(max_batch_requests, self.max_bytes, 0)
-        self.slots = [_Slot(torch, self.dev, max_batch_requests, self.max_bytes, scratch) for _ in range(2)]
+
+        def slot_bytes(budget, scratch_fn):
+            b = max(1 << 16, budget - per_req * max_batch_requests)
+            sc = scratch_fn(b)
+            while sc + b + per_req * max_batch_requests > budget and b > (1 << 16):
+                b //= 2
+                sc = scratch_fn(b)
+            return b, sc
+
+        self.max_bytes, scratch = slot_bytes(hbm_budget * 3 // 8,
+                                             lambda b: DFASet.scratch_bytes(max_batch_requests, b, 0))
+        self.max_pnfa_bytes, _ = slot_bytes(hbm_budget // 8, lambda b: 0)
+        self.slots = [_Slot(torch, self.dev, "fast", max_batch_requests, self.max_bytes, scratch)
+                      for _ in range(2)]
+        self.slots += [_Slot(torch, self.dev, "pnfa", max_batch_requests, self.max_pnfa_bytes, 0)
+                       for _ in range(2)]
         if self.dfa_set is not None:   # first run outside any graph capture (one-time setup)
             s0 = self.slots[0]
             self.dfa_set.run(s0.d_data[:1], s0.d_doff[:2], s0.d_ids[:1], final_state=s0.d_fs,
                              accept=s0.d_ac, scratch=s0.d_scratch, stream=s0.stream)
             s0.stream.synchronize()
-        self._queue = collections.deque()
+        self._queues = {"fast": collections.deque(), "pnfa": collections.deque()}
         self._cv = threading.Condition()
         self._next = 0
         self._stop = False
@@ -196,16 +215,42 @@ class Server:
         if not 0 <= engine < n_eng:
             raise ValueError(f"no {kind} automaton {engine}")
         data = bytes(data)
-        if len(data) > self.max_bytes:
-            raise ValueError(f"request of {len(data)} bytes exceeds the slot capacity {self.max_bytes}")
+        cap = self.max_pnfa_bytes if kind == "pnfa" else self.max_bytes
+        if len(data) > cap:
+            raise ValueError(f"request of {len(data)} bytes exceeds the slot capacity {cap}")
         with self._cv:
             if self._error is not None:
                 raise RuntimeError("server loop failed") from self._error
             r = Request(self._next, kind, engine, data, t_submit=time.perf_counter())
             self._next += 1
-            self._queue.append(r)
+            self._queues["pnfa" if kind == "pnfa" else "fast"].append(r)
             self._cv.notify()
         return r
+
+    def submit_many(self, items, t_arrival: Optional[Sequence[float]] = None) -> list:
+        """Submit (kind, engine, data) triples under one lock. ``t_arrival`` gives
+        each request's arrival time (time.perf_counter clock) for open-loop load
+        generators that submit in bursts; latency is measured from it."""
+        reqs = []
+        now = time.perf_counter()
+        for i, (kind, engine, data) in enumerate(items):
+            if kind not in KINDS:
+                raise ValueError(f"kind must be one of {KINDS}")
+            data = bytes(data)
+            cap = self.max_pnfa_bytes if kind == "pnfa" else self.max_bytes
+            if len(data) > cap:
+                raise ValueError(f"request of {len(data)} bytes exceeds the slot capacity {cap}")
+            reqs.append(Request(0, kind, engine, data,
+                                t_submit=t_arrival[i] if t_arrival is not None else now))
+        with self._cv:
+            if self._error is not None:
+                raise RuntimeError("server loop failed") from self._error
+            for r in reqs:
+                r.rid = self._next
+                self._next += 1
+                self._queues["pnfa" if r.kind == "pnfa" else "fast"].append(r)
+            self._cv.notify()
+        return reqs
 
     def wait(self, reqs: Sequence[Request], timeout: float = 60.0) -> list:
         end = time.perf_counter() + timeout
@@ -217,14 +262,22 @@ class Server:
         return [r.result for r in reqs]
 
     def stats(self) -> dict:
+        """Requests, batches, bytes, throughput over the serving span and latency
+        percentiles (ms), overall and per kind."""
         with self._cv:
-            lat = np.array([r.latency_ms for r in self._completed]) if self._completed else np.zeros(1)
+            done = list(self._completed)
             span = (self._t_last - self._t_first) if self._t_first and self._t_last else 0.0
-            return {"requests": len(self._completed), "batches": self._batches,
-                    "bytes": self._bytes_done,
-                    "gchar_s": self._bytes_done / span / 1e9 if span > 0 else 0.0,
-                    "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-                    "mean_ms": float(lat.mean())}
+            nbytes, nb = self._bytes_done, self._batches
+
+        def pct(rs):
+            lat = np.array([r.latency_ms for r in rs]) if rs else np.zeros(1)
+            return {"n": len(rs), "p50_ms": float(np.percentile(lat, 50)),
+                    "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean())}
+
+        out = {"requests": len(done), "batches": nb, "bytes": nbytes,
+               "gchar_s": nbytes / span / 1e9 if span > 0 else 0.0, **pct(done)}
+        out["by_kind"] = {k: pct([r for r in done if r.kind == k]) for k in KINDS}
+        return out
 
     def reset_stats(self):
         with self._cv:
@@ -254,23 +307,31 @@ class Server:
                 for s in self.slots:
                     if s.batch is not None and s.event.query():
                         self._finish(s)
-                free = [s for s in self.slots if s.batch is None]
+                launches = []
                 with self._cv:
-                    if self._stop and not self._queue and len(free) == len(self.slots):
+                    idle = all(s.batch is None for s in self.slots)
+                    empty = not any(self._queues.values())
+                    if self._stop and empty and idle:
                         return
-                    batch = take_batch(self._queue, self.max_requests, self.max_bytes) if free else []
-                    if not batch and len(free) == len(self.slots) and not self._stop:
+                    for lane, cap in (("fast", self.max_bytes), ("pnfa", self.max_pnfa_bytes)):
+                        free = [s for s in self.slots if s.lane == lane and s.batch is None]
+                        if free and self._queues[lane]:
+                            launches.append((free[0], take_batch(self._queues[lane], self.max_requests, cap)))
+                    if not launches and idle and not self._stop:
                         self._cv.wait(timeout=0.05)
                         continue
-                if batch:
-                    self._launch(free[0], batch)
-                else:
+                for slot, batch in launches:
+                    if batch:
+                        self._launch(slot, batch)
+                if not launches:
                     time.sleep(20e-6)
         except BaseException as e:   # hand the failure to every waiting request
             with self._cv:
                 self._error = e
-                pending = list(self._queue) + [r for s in self.slots if s.batch for r in s.batch]
-                self._queue.clear()
+                pending = [r for q in self._queues.values() for r in q]
+                pending += [r for s in self.slots if s.batch for r in s.batch]
+                for q in self._queues.values():
+                    q.clear()
             for r in pending:
                 r.error = f"server loop failed: {e!r}"
                 r.done.set()
@@ -280,13 +341,15 @@ class Server:
         if nd == 0:
             return
         if not self.use_graphs:
-            s.d_data[:dfa_bytes].copy_(s.h_data[:dfa_bytes], non_blocking=True)
-            s.d_doff[:nd + 1].copy_(s.h_doff[:nd + 1], non_blocking=True)
-            s.d_ids[:nd].copy_(s.h_ids[:nd], non_blocking=True)
-            self.dfa_set.run(s.d_data[:max(dfa_bytes, 1)], s.d_doff[:nd + 1], s.d_ids[:nd],
-                             final_state=s.d_fs, accept=s.d_ac, scratch=s.d_scratch, stream=s.stream)
-            s.h_fs[:nd].copy_(s.d_fs[:nd], non_blocking=True)
-            s.h_ac[:nd].copy_(s.d_ac[:nd], non_blocking=True)
+            with torch.cuda.stream(s.stream):   # copies and kernels in one stream order
+                s.d_data[:dfa_bytes].copy_(s.h_data[:dfa_bytes], non_blocking=True)
+                s.d_doff[:nd + 1].copy_(s.h_doff[:nd + 1], non_blocking=True)
+                s.d_ids[:nd].copy_(s.h_ids[:nd], non_blocking=True)
+                self.dfa_set.run(s.d_data[:max(dfa_bytes, 1)], s.d_doff[:nd + 1], s.d_ids[:nd],
+                                 final_state=s.d_fs, accept=s.d_ac, scratch=s.d_scratch,
+                                 stream=s.stream)
+                s.h_fs[:nd].copy_(s.d_fs[:nd], non_blocking=True)
+                s.h_ac[:nd].copy_(s.d_ac[:nd], non_blocking=True)
             return
         nb = min(_bucket(nd, 64), self.max_requests)
         bb = min(_bucket(max(dfa_bytes, 1), 1 << 16), self.max_bytes)
@@ -328,7 +391,7 @@ class Server:
             # an NFA or PNFA handle keeps one work queue: its launches from the two slots
             # must not overlap, so this slot's stream waits for the other slot's batch
             for o in self.slots:
-                if o is not s and o.batch is not None:
+                if o is not s and o.lane == s.lane and o.batch is not None:
                     s.stream.wait_event(o.event)
             with torch.cuda.stream(s.stream):
                 if total > dfa_bytes:
@@ -341,7 +404,10 @@ class Server:
                         self.nfas[eng].run(data, off, final_mask=s.d_mask[first:first + cnt],
                                            accept=s.d_ac2[first:first + cnt], stream=s.stream)
                     else:
-                        self.pnfas[eng].run(data, off, self.pnfa_mode, loglik=s.d_ll[first:first + cnt],
+                        mode = self.pnfa_mode
+                        if mode == "auto":
+                            mode = "fp32" if cnt < self.pnfa_auto_threshold else "bf16"
+                        self.pnfas[eng].run(data, off, mode, loglik=s.d_ll[first:first + cnt],
                                             accept=s.d_ac2[first:first + cnt], stream=s.stream)
                 s.h_mask[:nr].copy_(s.d_mask[:nr], non_blocking=True)
                 s.h_ll[:nr].copy_(s.d_ll[:nr], non_blocking=True)
