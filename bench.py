@@ -227,7 +227,8 @@ class DFAWorkload:
 
     @property
     def launches_per_step(self):
-        return 3 if self.kind == "scan" else 4
+        # scan: tile bases, empty strings, scan; ragged: count, scan, fill, walk, compose
+        return 3 if self.kind == "scan" else 5
 
     def config(self):
         return {"workload": self.workload, "n_strings": self.n, "total_bytes_per_gpu": self.total,

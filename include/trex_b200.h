@@ -155,7 +155,8 @@ int trex_dfa_batch_run(trex_dfa_set *set, const uint8_t *data, const int64_t *of
  * set's own scratch): 0 = fine, bit 0 = malformed offsets, bit 1 = automaton
  * id out of range (the affected strings were skipped), bit 2 = offsets that
  * overlap so far that the batch needs more work items than total_bytes allows
- * for (no string of the batch was run). Synchronises. */
+ * for (no string of the batch was run), or a string longer than 64 GiB (that
+ * string was skipped). Synchronises. */
 int trex_dfa_batch_error(trex_dfa_set *set, void *scratch, int32_t *err_out);
 
 /* The same device-pointer batch without any allocation (no counterpart in the

@@ -48,6 +48,7 @@ struct WorkItem {
     uint32_t entry;      // start state (bits 0-7) | warm-up bytes (bits 8-15)
 };
 constexpr int64_t kMaxItemsPerString = 65535;
+constexpr int64_t kMaxWalkBytes = (int64_t)1 << 36;   // one item: a 32-bit count of windows
 constexpr int kWarmBytes = 128;
 
 // Error bits reported through the device error word.
@@ -60,12 +61,12 @@ enum : uint32_t {
 constexpr int kRaggedThreads = 1024;
 constexpr int kPlanThreads = 256;
 constexpr int kDefaultSegLen = 2048;
-constexpr int kLenClasses = 8;
+constexpr int kLenClasses = 64;
 
 // ---- scratch layout -----------------------------------------------------------
 struct ScratchLayout {
     size_t cls_count, cls_cursor, q_base, q_count, q_head, q_bytes, err, map_cursor, n_items,
-        items, maps, done, total;
+        items, maps, str_map, total;
     int64_t max_items;
 };
 
@@ -91,7 +92,7 @@ static ScratchLayout scratch_layout(int64_t n_strings, int64_t total_bytes, int3
     L.n_items = take(8);
     L.items = take((size_t)L.max_items * sizeof(WorkItem));
     L.maps = take((size_t)L.max_items * sizeof(uint32_t));
-    L.done = take((size_t)std::max<int64_t>(n_strings, 1) * 4);
+    L.str_map = take((size_t)std::max<int64_t>(n_strings, 1) * 4);
     L.total = o;
     return L;
 }
@@ -113,11 +114,28 @@ __device__ __forceinline__ uint32_t n_items_of(int64_t len, int n_states, int32_
     return (uint32_t)((len + seg - 1) / seg);
 }
 
-// Length class: 0 for >= 4096 bytes, then one class per halving, 7 for < 64.
+// Queue order of an item by the bytes it walks (warm-up included), longest
+// first: below 4 KiB one class per 128 bytes (class 32 + (4095 - len) / 128),
+// above one class per power of two (4-8 KiB: 31, 8-16 KiB: 30, ...). Items of
+// one class differ by at most 128 bytes, so a warp's batch of 32 consecutive
+// items spans nearly the same number of windows.
 __device__ __forceinline__ int len_class(int64_t len) {
-    int lg = len > 0 ? 63 - __clzll(len) : 0;
-    int c = 12 - lg;
-    return c < 0 ? 0 : (c > kLenClasses - 1 ? kLenClasses - 1 : c);
+    if (len < 4096) return 32 + (int)((4095 - len) >> 7);
+    const int c = 31 - ((63 - __clzll(len)) - 12);
+    return c < 0 ? 0 : c;
+}
+
+// Classes of the items of a string cut into k pieces of seg bytes: the first
+// piece (no warm-up), the k - 2 middle pieces and the last piece (both with
+// warm-up). A string of one piece has only the last class.
+struct ItemClasses {
+    int first, mid, last;
+};
+__device__ __forceinline__ ItemClasses item_classes(int64_t len, uint32_t k, int64_t seg) {
+    const int64_t warm = seg < kWarmBytes ? seg : (int64_t)kWarmBytes;
+    if (k == 1) return ItemClasses{0, 0, len_class(len)};
+    return ItemClasses{len_class(seg), len_class(seg + warm),
+                       len_class(len - (int64_t)(k - 1) * seg + warm)};
 }
 
 // Returns the DFA index of string i, or -1 (and raises an error bit) when the
@@ -134,6 +152,10 @@ __device__ __forceinline__ int checked_dfa(const int64_t *offsets, const int32_t
     }
     if (d < 0 || d >= n_dfas) {
         atomicOr(err, kErrBadDfaId);
+        return -1;
+    }
+    if (b - a > kMaxWalkBytes) {   // longer strings are refused (flagged, no result)
+        atomicOr(err, kErrCapacity);
         return -1;
     }
     *len_out = b - a;
@@ -160,8 +182,11 @@ __global__ void plan_count_kernel(const int64_t *offsets, const int32_t *dfa_id,
         if (d < 0) continue;
         int64_t seg;
         uint32_t k = n_items_of(len, desc[d].n_states, seg_len, &seg);
-        if (k > 1) atomicAdd(&cnt[d * kLenClasses + len_class(seg)], k - 1);
-        atomicAdd(&cnt[d * kLenClasses + len_class(len - (int64_t)(k - 1) * seg)], 1u);
+        const ItemClasses ic = item_classes(len, k, seg);
+        uint32_t *cd = cnt + d * kLenClasses;
+        if (k > 1) atomicAdd(&cd[ic.first], 1u);
+        if (k > 2) atomicAdd(&cd[ic.mid], k - 2);
+        atomicAdd(&cd[ic.last], 1u);
         atomicAdd(&byt[d], (unsigned long long)len + 64ull);
         atomicAdd(&items, (unsigned long long)k);
     }
@@ -173,27 +198,45 @@ __global__ void plan_count_kernel(const int64_t *offsets, const int32_t *dfa_id,
         if (byt[t]) atomicAdd(&q_bytes[t], byt[t]);
 }
 
-// Queue bases per (DFA, length class). Offsets that overlap (each string in
-// range, but their lengths summing past total_bytes) would need more items
-// than the scratch was sized for: then the error bit is set and every queue is
-// left empty, so neither the fill kernel nor the ragged kernel writes an item.
-__global__ void plan_scan_kernel(const uint32_t *cls_count, uint32_t *cls_cursor, uint32_t *q_base,
+// Queue bases per (DFA, length class), one thread per DFA (kMaxDfasPerSet
+// threads). cls_cursor gets each class's start and cls_count is overwritten
+// with each class's end, against which the ragged kernel checks the fill.
+// Offsets that overlap (each string in range, but their lengths summing past
+// total_bytes) would need more items than the scratch was sized for: then the
+// error bit is set and every queue is left empty, so neither the fill kernel
+// nor the ragged kernel writes an item.
+__global__ void plan_scan_kernel(uint32_t *cls_count, uint32_t *cls_cursor, uint32_t *q_base,
                                  uint32_t *q_count, int n_dfas, const unsigned long long *n_items,
                                  int64_t max_items, uint32_t *err) {
-    if (threadIdx.x == 0 && *n_items > (unsigned long long)max_items) {
-        atomicOr(err, kErrCapacity);
-        for (int d = 0; d < n_dfas; ++d) q_base[d] = q_count[d] = 0;
+    __shared__ uint32_t tot[kMaxDfasPerSet];
+    const int d = threadIdx.x;
+    if (*n_items > (unsigned long long)max_items) {
+        if (d == 0) atomicOr(err, kErrCapacity);
+        if (d < n_dfas) q_base[d] = q_count[d] = 0;
         return;
     }
-    if (threadIdx.x == 0) {
+    uint32_t sum = 0;
+    if (d < n_dfas)
+        for (int c = 0; c < kLenClasses; ++c) sum += cls_count[d * kLenClasses + c];
+    tot[d] = sum;
+    __syncthreads();
+    if (d == 0) {
         uint32_t run = 0;
-        for (int d = 0; d < n_dfas; ++d) {
-            q_base[d] = run;
-            for (int c = 0; c < kLenClasses; ++c) {
-                cls_cursor[d * kLenClasses + c] = run;
-                run += cls_count[d * kLenClasses + c];
-            }
-            q_count[d] = run - q_base[d];
+        for (int k = 0; k < n_dfas; ++k) {
+            const uint32_t v = tot[k];
+            tot[k] = run;
+            run += v;
+        }
+    }
+    __syncthreads();
+    if (d < n_dfas) {
+        uint32_t run = tot[d];
+        q_base[d] = run;
+        q_count[d] = sum;
+        for (int c = 0; c < kLenClasses; ++c) {
+            cls_cursor[d * kLenClasses + c] = run;
+            run += cls_count[d * kLenClasses + c];
+            cls_count[d * kLenClasses + c] = run;
         }
     }
 }
@@ -204,18 +247,13 @@ __global__ void plan_scan_kernel(const uint32_t *cls_count, uint32_t *cls_cursor
 __global__ void __launch_bounds__(kPlanThreads)
 plan_fill_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n, int64_t total_bytes,
                  const DfaDesc *desc, int n_dfas, int32_t seg_len, uint32_t *cls_cursor,
-                 uint32_t *map_cursor, WorkItem *items, int64_t max_items, uint32_t *done,
+                 uint32_t *map_cursor, WorkItem *items, int64_t max_items, uint32_t *str_map,
                  uint32_t *err) {
     __shared__ uint32_t s_cnt[kMaxDfasPerSet * kLenClasses];
     __shared__ uint32_t s_base[kMaxDfasPerSet * kLenClasses];
     __shared__ uint32_t s_map, s_map_base;
     const int n_slots = n_dfas * kLenClasses;
-    if (*(volatile uint32_t *)err & kErrCapacity) {   // set by plan_scan_kernel: no items
-        for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-             i += (int64_t)gridDim.x * blockDim.x)
-            done[i] = 0;
-        return;
-    }
+    if (*(volatile uint32_t *)err & kErrCapacity) return;   // set by plan_scan_kernel: no items
     for (int t = threadIdx.x; t < n_slots; t += blockDim.x) s_cnt[t] = 0;
     if (threadIdx.x == 0) s_map = 0;
     __syncthreads();
@@ -223,20 +261,21 @@ plan_fill_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n, int64
         const int64_t i = tile * kPlanThreads + threadIdx.x;
         int d = -1;
         int64_t len = 0, seg = 0, s0 = 0;
-        uint32_t k = 0, cf = 0, cl = 0, r_full = 0, r_last = 0, r_map = 0;
-        if (i < n) {
-            done[i] = 0;
-            d = checked_dfa(offsets, dfa_id, i, n_dfas, total_bytes, err, &len, &s0);
-        }
+        uint32_t k = 0, r0 = 0, rm = 0, r_last = 0, r_map = 0;
+        ItemClasses ic{0, 0, 0};
+        if (i < n) d = checked_dfa(offsets, dfa_id, i, n_dfas, total_bytes, err, &len, &s0);
         if (d >= 0) {
             k = n_items_of(len, desc[d].n_states, seg_len, &seg);
-            cf = d * kLenClasses + len_class(seg);
-            cl = d * kLenClasses + len_class(len - (int64_t)(k - 1) * seg);
+            ic = item_classes(len, k, seg);
+            ic.first += d * kLenClasses;
+            ic.mid += d * kLenClasses;
+            ic.last += d * kLenClasses;
             if (k > 1) {
-                r_full = atomicAdd(&s_cnt[cf], k - 1);
+                r0 = atomicAdd(&s_cnt[ic.first], 1u);
                 r_map = atomicAdd(&s_map, k);
             }
-            r_last = atomicAdd(&s_cnt[cl], 1u);
+            if (k > 2) rm = atomicAdd(&s_cnt[ic.mid], k - 2);
+            r_last = atomicAdd(&s_cnt[ic.last], 1u);
         }
         __syncthreads();
         for (int t = threadIdx.x; t < n_slots; t += blockDim.x)
@@ -253,8 +292,11 @@ plan_fill_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n, int64
                 atomicOr(err, kErrCapacity);
                 k = 0;
             }
+            if (k > 1) str_map[i] = mb;
             for (uint32_t j = 0; j < k; ++j) {
-                const uint32_t pos = (j + 1 == k) ? s_base[cl] + r_last : s_base[cf] + r_full + j;
+                const uint32_t pos = (j + 1 == k) ? s_base[ic.last] + r_last
+                                     : j == 0      ? s_base[ic.first] + r0
+                                                   : s_base[ic.mid] + rm + (j - 1);
                 if ((int64_t)pos >= max_items) {
                     atomicOr(err, kErrCapacity);
                     continue;
@@ -292,7 +334,10 @@ struct RaggedParams {
     const uint32_t *cls_cursor;
     uint32_t *err;
     uint32_t *maps;
-    uint32_t *done;
+    const uint32_t *str_map;
+    const int32_t *dfa_id;
+    int64_t n;
+    int64_t max_items;
     uint8_t *final_state;
     uint8_t *accept;
     int32_t *accept_i32;
@@ -306,206 +351,123 @@ __device__ __forceinline__ void write_result(const RaggedParams &P, uint32_t str
     if (P.accept_i32) P.accept_i32[str] = a ? 1 : 0;
 }
 
-// Records (guessed entry state, end state) of one item of a split string; the
-// last item of the string to finish composes the string in order and
-// re-walks every item whose guess was wrong.
+// Records (guessed entry state, end state) of one item of a split string;
+// compose_kernel chains the items of the string after the walk.
+__device__ __forceinline__ void publish_item(const RaggedParams &P, uint32_t segn, uint32_t mb,
+                                             uint32_t guess, uint32_t fin) {
+    P.maps[mb + (segn & 0xffffu)] = guess | (fin << 8);
+}
+
+// One item of a batch, as a lane holds it (segn == 0: no item).
+__device__ __forceinline__ WorkItem load_item(const RaggedParams &P, uint32_t base, uint32_t idx,
+                                              uint32_t count) {
+    if (idx < count) return P.items[base + idx];
+    return WorkItem{0, 0, 0, 0, 0, 0};
+}
+
+// Window walk with a byte mask (bit j: byte j of the window belongs to the
+// item) and a capture: when cpos > 0, cap_e takes the state after byte
+// cpos - 1 (the end of the warm-up).
 template <class W>
-__device__ __forceinline__ void publish_item(const RaggedParams &P, const W &w, uint32_t str,
-                                          uint32_t segn, uint32_t mb, uint32_t guess,
-                                          uint32_t fin, const DfaDesc &D) {
-    const uint32_t seg = segn & 0xffffu, nseg = segn >> 16;
-    P.maps[mb + seg] = guess | (fin << 8);
-    __threadfence();
-    uint32_t prev = atomicAdd(&P.done[str], 1u);
-    if (prev != nseg - 1) return;
-    __threadfence();
-    const int64_t s0 = P.offsets[str], len = P.offsets[str + 1] - s0;
-    if (s0 < 0 || len < 0 || s0 + len > P.total_bytes) {   // offsets changed in flight
-        atomicOr(P.err, kErrBadOffsets);
-        return;
+__device__ __forceinline__ uint32_t walk_masked(const W &w, uint32_t e, uint4 a, uint4 b, uint32_t m,
+                                                uint32_t cpos, uint32_t &cap_e) {
+    const uint32_t x[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        uint32_t n;
+#define TREX_MSTEP(J)                                       \
+        n = w.template step<J>(e, x[k]);                    \
+        e = (m >> (4 * k + J)) & 1u ? n : e;                \
+        cap_e = (4u * k + J + 1u == cpos) ? e : cap_e;
+        TREX_MSTEP(0) TREX_MSTEP(1) TREX_MSTEP(2) TREX_MSTEP(3)
+#undef TREX_MSTEP
     }
-    int64_t seg_bytes;
-    n_items_of(len, D.n_states, P.seg_len, &seg_bytes);
-    uint32_t s = (uint32_t)D.start;
-    for (uint32_t k = 0; k < nseg; ++k) {
-        const uint32_t v = ld_acquire_u32(P.maps + mb + k);
-        if (k == 0 || (v & 0xffu) == s) {
-            s = (v >> 8) & 0xffu;
-        } else {
-            // the chain had not synchronised: walk this item from the true state
-            const int64_t b0 = s0 + (int64_t)k * seg_bytes;
-            const int64_t b1 = (k + 1 == nseg) ? s0 + len : b0 + seg_bytes;
-            uint32_t e = w.enc(s);
-            for (int64_t q = b0; q < b1; ++q) e = w.template step<0>(e, (uint32_t)__ldg(P.data + q));
-            s = W::dec(e);
-        }
-    }
-    write_result(P, str, s, D.accept_off);
+    return e;
 }
 
-// Per-lane fields of the current item that are only touched when an item
-// starts or ends live in shared memory after the table (struct of arrays,
-// indexed by thread), which keeps the walking loop's registers free.
-constexpr int kColdOff = kRepTableBytes16;
-constexpr int kColdFields = 5;   // str, segn, map_base, guess, rest
-constexpr int kColdBytes = kColdFields * kRaggedThreads * 4;
-__device__ __forceinline__ uint32_t *cold(int field) {
-    return reinterpret_cast<uint32_t *>(g_dfa_tbl + kColdOff) + field * kRaggedThreads + threadIdx.x;
-}
-enum { kCStr = 0, kCSegn = 1, kCMb = 2, kCGuess = 3, kCRest = 4 };
-
-// Drains queue d with this warp. All lanes of the warp call it together.
+// Drains queue d with this warp, 32 items (one a lane) at a time. The items of
+// a queue are ordered by walked length (warm-up included), longest first, in
+// 128-byte classes, so the items of a batch span nearly the same number of
+// 32-byte windows: the lanes start and finish together, and every window
+// between a batch's first and last is walked without masks. The records of the
+// next batch are claimed and loaded while the current one is walked; the next
+// window of every lane is loaded while the current one is walked.
 template <class W>
 __device__ void drain_queue(const RaggedParams &P, const W &w, const DfaDesc &D, uint32_t base,
                             uint32_t count, uint32_t *head) {
     const uint32_t FULL = 0xffffffffu;
     const uint32_t lane = threadIdx.x & 31u;
     const uint8_t *const lo_ok = P.data, *const hi_ok = P.data + P.total_bytes;
-    // Walking state: the current 32-byte window starts at wp (32-aligned in
-    // memory); bytes [lo, lo + left) of the phase (warm-up or the item's own
-    // bytes) are still to be walked from there.
-    const uint8_t *wp = P.data;
-    uint32_t lo = 0, left = 0, e = 0;
-    // flags: bit 0 item live, bits 1-2 next slot (0 empty, 1 index requested,
-    // 2 record loaded), bit 3 queue exhausted for this lane, bit 4 warm-up,
-    // bit 5 lookahead (la) holds the next window to walk
-    uint32_t fl = 0;
-    WorkItem nx{0, 0, 0, 0, 0, 0};
-    uint32_t req_mask = 0, pending = 0;
-    uint4 la_a = make_uint4(0, 0, 0, 0), la_b = la_a;
+    uint32_t b0 = 0;
+    if (lane == 0) b0 = atomicAdd(head, 32u);
+    b0 = __shfl_sync(FULL, b0, 0);
+    if (b0 >= count) return;
+    WorkItem cur = load_item(P, base, b0 + lane, count);
     while (true) {
-        // A. resolve last iteration's request: item index -> record load
-        if (req_mask) {
-            const uint32_t b = __shfl_sync(FULL, pending, __ffs(req_mask) - 1);
-            if (req_mask & (1u << lane)) {
-                const uint32_t idx = b + (uint32_t)__popc(req_mask & ((1u << lane) - 1u));
-                if (idx < count) {
-                    nx = P.items[base + idx];
-                    fl = (fl & ~6u) | 4u;
-                } else {
-                    fl = (fl & ~6u) | 8u;
-                }
-            }
-            req_mask = 0;
+        uint32_t b1 = 0;
+        if (lane == 0) b1 = atomicAdd(head, 32u);
+        b1 = __shfl_sync(FULL, b1, 0);
+        const WorkItem nxt = load_item(P, base, b1 + lane, count);
+
+        // ---- this lane's item: windows [wp, wp + 32 nw), bytes [lo, lo + nbytes) of them
+        const uint32_t warm = (cur.entry >> 8) & 0xffu, entry = cur.entry & 0xffu;
+        const int64_t nbytes = cur.end - cur.p0;   // walked bytes, warm-up included
+        bool live = cur.segn != 0;
+        if (live && nbytes <= 0) {   // empty string: its final state is the start state
+            write_result(P, cur.str, entry, D.accept_off);
+            live = false;
         }
-        // B. end of a phase: warm-up -> the item's own bytes; item -> publish
-        //    it and start the next record
-        if (left == 0) {
-            if (fl & 16u) {
-                *cold(kCGuess) = W::dec(e);
-                left = *cold(kCRest);
-                fl &= ~16u;
-            } else {
-                if (fl & 1u) {
-                    const uint32_t segn = *cold(kCSegn);
-                    if ((segn >> 16) == 1)
-                        write_result(P, *cold(kCStr), W::dec(e), D.accept_off);
-                    else
-                        publish_item(P, w, *cold(kCStr), segn, *cold(kCMb), *cold(kCGuess),
-                                     W::dec(e), D);
-                    fl &= ~1u;
-                }
-                if (fl & 4u) {
-                    fl &= ~6u;
-                    const uint32_t warm = (nx.entry >> 8) & 0xffu;
-                    if (nx.p0 + warm < nx.end) {
-                        const uint8_t *q = P.data + nx.p0;
-                        wp = reinterpret_cast<const uint8_t *>((uintptr_t)q & ~(uintptr_t)31);
-                        lo = (uint32_t)(q - wp);
-                        *cold(kCStr) = nx.str;
-                        *cold(kCSegn) = nx.segn;
-                        *cold(kCMb) = nx.map_base;
-                        *cold(kCGuess) = nx.entry & 0xffu;
-                        e = w.enc(nx.entry & 0xffu);
-                        if (warm) {
-                            left = warm;
-                            *cold(kCRest) = (uint32_t)(nx.end - nx.p0 - warm);
-                            fl |= 17u;
-                        } else {
-                            left = (uint32_t)(nx.end - nx.p0);
-                            fl |= 1u;
-                        }
-                    } else {
-                        // empty string: its final state is the start state
-                        write_result(P, nx.str, nx.entry & 0xffu, D.accept_off);
-                        fl &= ~32u;
-                    }
-                } else {
-                    fl &= ~32u;
-                }
-            }
-        }
-        // C. request the next item for lanes with an empty slot
-        const uint32_t need = __ballot_sync(FULL, (fl & 14u) == 0u);
-        if (need) {
-            if ((int)lane == __ffs(need) - 1) pending = atomicAdd(head, (uint32_t)__popc(need));
-            if (need & (1u << lane)) fl |= 2u;
-            req_mask = need;
-        }
-        if (__all_sync(FULL, (fl & 15u) == 8u)) break;
-        // D. walk one window; load the next one ahead
+        const uint8_t *q0 = P.data + (live ? cur.p0 : 0);
+        const uint8_t *wp = reinterpret_cast<const uint8_t *>((uintptr_t)q0 & ~(uintptr_t)31);
+        const uint32_t lo = (uint32_t)(q0 - wp);
+        const uint32_t nw = live ? (uint32_t)((lo + nbytes + 31) >> 5) : 0u;
+        const uint32_t he = live ? (uint32_t)(lo + nbytes - 32 * (int64_t)(nw - 1)) : 0u;   // 1..32
+        const uint32_t cb = lo + warm;   // the item's own bytes start here (relative to wp)
+        const uint32_t cw = warm ? (cb >> 5) : 0xffffffffu, cpos = cb & 31u;
+        uint32_t e = w.enc(live ? entry : 0u);
+        uint32_t cap_e = e;
+        const uint32_t maxw = __reduce_max_sync(FULL, nw);
         uint4 a = make_uint4(0, 0, 0, 0), b = a;
-        uint32_t m = 0;
-        if (left) {
-            if (fl & 32u) {
-                a = la_a;
-                b = la_b;
+        if (nw) load_window(wp, lo_ok, hi_ok, a, b);
+        for (uint32_t it = 0; it < maxw; ++it) {
+            const uint4 ca = a, cbv = b;
+            if (it + 1 < nw) load_window(wp + 32 * (size_t)(it + 1), lo_ok, hi_ok, a, b);
+            const uint32_t mlo = it == 0 ? lo : 0u;
+            const uint32_t mhi = it + 1 < nw ? 32u : (it + 1 == nw ? he : 0u);
+            const uint32_t m = bit_range((int)mlo, (int)mhi);
+            const bool cap = it == cw;
+            if (cap && cpos == 0) cap_e = e;   // the warm-up ended with the previous window
+            const bool special = (it < nw && m != FULL) || (cap && cpos != 0);
+            if (!__any_sync(FULL, special)) {
+                e = step16(w, e, ca);
+                e = step16(w, e, cbv);
             } else {
-                load_window(wp, lo_ok, hi_ok, a, b);
+                e = walk_masked(w, e, ca, cbv, m, cap ? cpos : 0u, cap_e);
             }
-            const uint32_t h = min(32u, lo + left);
-            m = bit_range((int)lo, (int)h);
-            left -= h - lo;
-            fl |= 32u;
-            if (left) {
-                wp += 32;
-                lo = 0;
-                load_window(wp, lo_ok, hi_ok, la_a, la_b);
-            } else if (fl & 16u) {
-                // warm-up ends here; the item's own bytes follow
-                if (h < 32u) {
-                    lo = h;
-                    la_a = a;
-                    la_b = b;
-                } else {
-                    wp += 32;
-                    lo = 0;
-                    load_window(wp, lo_ok, hi_ok, la_a, la_b);
-                }
-            } else if ((fl & 6u) == 4u) {
-                // item ends here: fetch the first window of the next record
-                const uint8_t *q = reinterpret_cast<const uint8_t *>(
-                    (uintptr_t)(P.data + nx.p0) & ~(uintptr_t)31);
-                load_window(q, lo_ok, hi_ok, la_a, la_b);
-            } else {
-                fl &= ~32u;
+            if (it + 1 == nw) {   // this lane's item ends in this window
+                const uint32_t fin = W::dec(e);
+                if ((cur.segn >> 16) == 1)
+                    write_result(P, cur.str, fin, D.accept_off);
+                else
+                    publish_item(P, cur.segn, cur.map_base, warm ? W::dec(cap_e) : entry, fin);
             }
         }
-        if (__all_sync(FULL, m == FULL || m == 0u)) {
-            e = step16(w, e, a);
-            e = step16(w, e, b);
-        } else {
-            e = step16_masked(w, e, a, m);
-            e = step16_masked(w, e, b, m >> 16);
-        }
+        if (b1 >= count) break;
+        cur = nxt;
     }
 }
 
 __global__ void __launch_bounds__(kRaggedThreads, 1) dfa_ragged_kernel(RaggedParams P) {
     __shared__ int s_dfa;
+    // The plan is complete when every (DFA, length class) cursor of the fill
+    // ended exactly at its class's end (reservations are disjoint, so every item
+    // slot was then written once); otherwise (capacity overflow, or offsets
+    // rewritten while the plan ran) no item is trusted.
+    bool ok = true;
+    for (int t = threadIdx.x; t < P.n_dfas * kLenClasses; t += blockDim.x)
+        ok &= P.cls_cursor[t] == P.cls_count[t];
+    const bool planned = __syncthreads_and(ok) != 0;
     if (threadIdx.x == 0) {
-        // The plan is complete when every (DFA, length class) cursor of the fill
-        // ended exactly at its class's end (reservations are disjoint, so every
-        // item slot was then written once); otherwise (capacity overflow, or
-        // offsets rewritten while the plan ran) no item is trusted.
-        bool planned = true;
-        for (int d = 0; d < P.n_dfas; ++d) {
-            uint32_t run = P.q_base[d];
-            for (int c = 0; c < kLenClasses; ++c) {
-                run += P.cls_count[d * kLenClasses + c];
-                planned &= P.cls_cursor[d * kLenClasses + c] == run;
-            }
-        }
         if (!planned) atomicOr(P.err, kErrCapacity);
         // Home DFA: CTAs are spread over DFAs in proportion to their bytes.
         unsigned long long tot = 0;
@@ -551,6 +513,45 @@ __global__ void __launch_bounds__(kRaggedThreads, 1) dfa_ragged_kernel(RaggedPar
             s_dfa = best;
         }
         __syncthreads();
+    }
+}
+
+// Strings cut into several items: chains the items' (guessed entry, end state)
+// records in order. An item whose guessed entry differs from the true entry
+// state (its warm-up chain had not synchronised) is walked again from the true
+// state through the automaton's byte map in global memory; for synchronising
+// automata that is rare, for permutation automata it is every item after the
+// first. One thread per string.
+__global__ void compose_kernel(RaggedParams P) {
+    if (*(volatile uint32_t *)P.err & kErrCapacity) return;   // the plan was refused
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < P.n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        int64_t len, s0;
+        const int d = checked_dfa(P.offsets, P.dfa_id, i, P.n_dfas, P.total_bytes, P.err, &len, &s0);
+        if (d < 0) continue;
+        const DfaDesc D = P.desc[d];
+        int64_t seg;
+        const uint32_t k = n_items_of(len, D.n_states, P.seg_len, &seg);
+        if (k <= 1) continue;
+        const uint32_t mb = P.str_map[i];
+        if ((int64_t)mb + (int64_t)k > P.max_items) {   // offsets changed since the plan
+            atomicOr(P.err, kErrCapacity);
+            continue;
+        }
+        const uint8_t *tm = P.tmaps + D.tmap_off;
+        const uint32_t N = (uint32_t)D.n_states;
+        uint32_t s = (P.maps[mb] >> 8) & 0xffu;   // item 0 starts from the start state
+        for (uint32_t j = 1; j < k; ++j) {
+            const uint32_t v = P.maps[mb + j];
+            if ((v & 0xffu) == s) {
+                s = (v >> 8) & 0xffu;
+            } else {
+                const int64_t b0 = s0 + (int64_t)j * seg;
+                const int64_t b1 = (j + 1 == k) ? s0 + len : b0 + seg;
+                for (int64_t q = b0; q < b1; ++q) s = tm[(uint32_t)__ldg(P.data + q) * N + s];
+            }
+        }
+        write_result(P, (uint32_t)i, s, D.accept_off);
     }
 }
 
@@ -621,7 +622,7 @@ int dfa_set_run(trex_dfa_set *set, const uint8_t *data, const int64_t *offsets,
     auto *n_items = reinterpret_cast<unsigned long long *>(sc + L.n_items);
     WorkItem *items = reinterpret_cast<WorkItem *>(sc + L.items);
     uint32_t *maps = reinterpret_cast<uint32_t *>(sc + L.maps);
-    uint32_t *done = reinterpret_cast<uint32_t *>(sc + L.done);
+    uint32_t *str_map = reinterpret_cast<uint32_t *>(sc + L.str_map);
 
     // Counters, bases, heads, cursors, byte counts, the error word, the map
     // cursor and the item count are contiguous at the front of the scratch buffer.
@@ -632,12 +633,12 @@ int dfa_set_run(trex_dfa_set *set, const uint8_t *data, const int64_t *offsets,
         offsets, dfa_id, n, total_bytes, set->d_desc, set->n_dfas, seg_len, cls_count, q_bytes,
         n_items, err);
     TREX_CHECK_LAUNCH();
-    plan_scan_kernel<<<1, 32, 0, stream>>>(cls_count, cls_cursor, q_base, q_count, set->n_dfas,
+    plan_scan_kernel<<<1, kMaxDfasPerSet, 0, stream>>>(cls_count, cls_cursor, q_base, q_count, set->n_dfas,
                                            n_items, L.max_items, err);
     TREX_CHECK_LAUNCH();
     plan_fill_kernel<<<plan_grid, kPlanThreads, 0, stream>>>(
         offsets, dfa_id, n, total_bytes, set->d_desc, set->n_dfas, seg_len, cls_cursor,
-        map_cursor, items, L.max_items, done, err);
+        map_cursor, items, L.max_items, str_map, err);
     TREX_CHECK_LAUNCH();
 
     RaggedParams P;
@@ -658,7 +659,10 @@ int dfa_set_run(trex_dfa_set *set, const uint8_t *data, const int64_t *offsets,
     P.cls_cursor = cls_cursor;
     P.err = err;
     P.maps = maps;
-    P.done = done;
+    P.str_map = str_map;
+    P.dfa_id = dfa_id;
+    P.n = n;
+    P.max_items = L.max_items;
     P.final_state = final_state;
     P.accept = accept;
     P.accept_i32 = accept_i32;
@@ -666,6 +670,8 @@ int dfa_set_run(trex_dfa_set *set, const uint8_t *data, const int64_t *offsets,
     dfa_ragged_kernel<<<set->n_sms, kRaggedThreads, set->smem_bytes, stream>>>(P);
     TREX_CHECK_LAUNCH();
     profile_kernel_end(stream);
+    compose_kernel<<<plan_grid, kPlanThreads, 0, stream>>>(P);
+    TREX_CHECK_LAUNCH();
     if (err_word_out) *err_word_out = err;
     return TREX_OK;
 }
@@ -717,8 +723,8 @@ int trex_dfa_set_create(int n_dfas, const int32_t *n_states, const int32_t *star
         trex::set_last_error_msg("trex_dfa_set_create: no CUDA device");
         return TREX_ERR_SHAPE;
     }
-    // table region (sized for the largest layout) + per-lane cold state
-    set->smem_bytes = (size_t)trex::kColdOff + trex::kColdBytes;
+    // table region, sized for the largest layout
+    set->smem_bytes = (size_t)trex::kRepTableBytes16;
     auto fail = [&](cudaError_t e, const char *what) {
         trex::set_last_error(what, e);
         cudaFree(set->d_tmaps);
@@ -743,7 +749,7 @@ int trex_dfa_set_create(int n_dfas, const int32_t *n_states, const int32_t *star
     // table any set can need (128 KiB).
     if ((e = cudaFuncSetAttribute(trex::dfa_ragged_kernel,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  trex::kColdOff + trex::kColdBytes)) != cudaSuccess)
+                                  trex::kRepTableBytes16)) != cudaSuccess)
         return fail(e, "cudaFuncSetAttribute");
     *out = set;
     return TREX_OK;

@@ -155,8 +155,7 @@ __device__ __forceinline__ uint32_t bit_range(int lo, int hi) {
 __device__ __forceinline__ void load_window(const uint8_t *w, const uint8_t *lo,
                                             const uint8_t *hi, uint4 &a, uint4 &b) {
     if (w >= lo && w + 32 <= hi) {
-        a = ld_stream16(w);
-        b = ld_stream16(w + 16);
+        ld_stream32(w, a, b);   // one 32-byte load (the window is 32-byte aligned)
     } else {
         uint32_t r[8];
 #pragma unroll
