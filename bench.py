@@ -70,6 +70,8 @@ def parse_args():
                     help="requests timed one by one for the plain per-request baseline")
     ap.add_argument("--pnfa-mode", choices=["bf16", "fp16", "fp32"], default="bf16",
                     help="operand type of the probabilistic NFA workload")
+    ap.add_argument("--nfa-method", choices=["bitpar", "tc"], default="bitpar",
+                    help="nfa workload: bit-parallel kernel, or the Boolean NFA on the tensor cores")
     ap.add_argument("--strings", type=int, default=None, help="override the number of strings")
     ap.add_argument("--seg-len", type=int, default=0, help="bytes per work item / scan tile (0 = default)")
     ap.add_argument("--dfa-sizes", type=str, default=None,
@@ -514,6 +516,46 @@ class PNFAWorkload:
         return k, k * self.L, data
 
 
+class NFATcWorkload(PNFAWorkload):
+    """The Boolean NFA workload (64 states, 20 symbols, 4096 symbols a string) on the
+    tensor cores: 0/1 BF16 operands, FP32 sums thresholded to {0, 1} every step."""
+
+    kind = "nfa"
+    ref_dtype = "u64"
+
+    def __init__(self, args):
+        from trex_b200.workloads import random_bool_nfa
+        self.args = args
+        self.mode = "bool"
+        rng = np.random.default_rng(args.seed)
+        T, start, acc = random_bool_nfa(rng, n_states=64, sigma=20, density=0.05)
+        self.T, self.start, self.acc = (x.astype(np.float32) for x in (T, start, acc))
+        self.n = args.strings or 262144
+        self.L = 4096
+        self.off = np.arange(self.n + 1, dtype=np.int64) * self.L
+        self.kernel = "pnfa_tc_kernel"
+        self.dtype = "bf16"
+        self.workload = ("Boolean NFA: random 64-state NFA over 20 symbols (bytes 0..19), edge density "
+                         f"0.05, {self.n} strings x 4096 symbols; tensor cores (tcgen05), 0/1 BF16 "
+                         "operands, FP32 sums thresholded every step")
+
+    def config(self):
+        return {"workload": self.workload, "n_strings": self.n, "total_bytes_per_gpu": self.total,
+                "useful_ops_per_char": 2 * 64 * 64, "mode": "bool",
+                "selection_waste": "2x (each MMA computes both symbols of a pair; half is discarded)",
+                "l2": "inputs larger than L2 (126 MB), no flush"}
+
+    def exact_mismatches(self, orc, k=2048):
+        """Accept flags that differ from the bit-parallel oracle on the first k strings."""
+        data = self.data[:k * self.L].cpu().numpy()
+        _, ref = orc.nfa_bool(self.T != 0, self.start, self.acc, data, self.off[:k + 1],
+                              unknown_rejects=False)
+        return int(np.count_nonzero(self.ac[:k].cpu().numpy().astype(bool) != ref.astype(bool)))
+
+    def cpu_run(self, orc, data, k):
+        orc.nfa_bool(self.T != 0, self.start, self.acc, data, self.off[:k + 1], unknown_rejects=False)
+
+
 # ---------------------------------------------------------------------------------
 # serving mix
 # ---------------------------------------------------------------------------------
@@ -749,7 +791,7 @@ def committed_traffic(kernel: str, workload: str):
 
 def make_workload(args):
     if args.workload == "nfa":
-        return NFAWorkload(args)
+        return NFATcWorkload(args) if args.nfa_method == "tc" else NFAWorkload(args)
     if args.workload == "pnfa":
         return PNFAWorkload(args)
     return DFAWorkload(args)
@@ -893,7 +935,11 @@ def trex_arm(args, rank, world, local_rank):
         line = base_line(args, wl, value, ms_per_step, args.steps, warm, world)
         line["config"] = {**wl.config(), "parallelism": f"dp{world} (independent shards, no collective)"}
         line["roofline"] = roof
-        if hasattr(wl, "llerr"):
+        if hasattr(wl, "exact_mismatches"):
+            from oracle import oracle as orc
+            orc.build()
+            line["accept_mismatches_vs_oracle_first_2048"] = wl.exact_mismatches(orc)
+        elif hasattr(wl, "llerr"):
             from oracle import oracle as orc
             orc.build()
             line["loglik_max_rel_err_vs_fp64"] = wl.llerr(orc)

@@ -151,3 +151,41 @@ def test_pnfa_malformed_offsets_flagged(cuda):
     for mode in ("fp32", "bf16"):
         _, _, err = _run(cuda, T, start, acc, data, off, mode)
         assert err & 1
+
+
+@pytest.mark.parametrize("density", [0.02, 0.05, 0.12])
+def test_bool_mode_matches_boolean_nfa_oracle(cuda, oracle, density):
+    # Boolean NFA on the tensor cores: thresholded 0/1 products, bit-exact accept
+    # flags against the bit-parallel oracle with bytes >= sigma skipped
+    from trex_b200.workloads import random_bool_nfa
+    rng = np.random.default_rng(int(density * 1000))
+    T, start, acc = random_bool_nfa(rng, 64, 20, density=density)
+    T = T.astype(np.float32) * rng.uniform(0.1, 3.0, size=T.shape).astype(np.float32)  # any nonzero = edge
+    lens = rng.integers(0, 400, size=4000)
+    lens[:4] = [0, 1, 2, 3]
+    off = np.zeros(len(lens) + 1, dtype=np.int64)
+    np.cumsum(lens, out=off[1:])
+    data = rng.integers(0, 23, size=int(off[-1]), dtype=np.uint8)   # 20..22 skipped
+    _, ac, err = _run(cuda, T, start.astype(np.float32), acc.astype(np.float32), data, off, "bool")
+    _, ref = oracle.nfa_bool(T != 0, start, acc, data, off, unknown_rejects=False)
+    assert err == 0
+    assert np.array_equal(ac.astype(bool), ref.astype(bool)), np.flatnonzero(ac.astype(bool) != ref.astype(bool))[:8]
+
+
+def test_bool_mode_small_nfa_both_outcomes(cuda, oracle):
+    # 9 states, 5 symbols: strings both accepted and rejected
+    rng = np.random.default_rng(9)
+    T = (rng.random((5, 9, 9)) < 0.25).astype(np.float32)
+    start = np.zeros(9, np.float32)
+    start[0] = 1
+    acc = np.zeros(9, np.float32)
+    acc[[3, 7]] = 1
+    lens = rng.integers(0, 60, size=3000)
+    off = np.zeros(len(lens) + 1, dtype=np.int64)
+    np.cumsum(lens, out=off[1:])
+    data = rng.integers(0, 5, size=int(off[-1]), dtype=np.uint8)
+    _, ac, err = _run(cuda, T, start, acc, data, off, "bool")
+    _, ref = oracle.nfa_bool(T != 0, start, acc, data, off, unknown_rejects=False)
+    assert err == 0
+    assert 0 < ref.sum() < len(ref)
+    assert np.array_equal(ac.astype(bool), ref.astype(bool))

@@ -200,6 +200,7 @@ struct PnParams {
     const uint4 *start_img;    // [8] start vector, 16-bit, one B row
     const float *acc;          // [64] accept weights
     float start_max;
+    int boolean;               // Boolean NFA: threshold every product to {0, 1}, no rescale
     double ll_empty;
     int sigma;
     double *loglik;
@@ -783,6 +784,7 @@ __device__ void pn_epilogue(const PnParams &P, const PnShared &S, uint32_t tbase
     const float *rsym = reinterpret_cast<const float *>(S.misc() + kMRsym);
     const bool even = q < 2;
     const bool owner = (q & 1) == 0;
+    const bool bmode = P.boolean != 0;
     int32_t *E = S.E();
     const uint32_t nr = (uint32_t)L.nregions;
     uint32_t g = 0;
@@ -836,7 +838,7 @@ __device__ void pn_epilogue(const PnParams &P, const PnShared &S, uint32_t tbase
                             m = fmaxf(x2.x, x2.y);
                         }
                         int f = pn_ceil_exp(m * R);
-                        f = min(max(f, -125), 125);
+                        f = bmode ? 0 : min(max(f, -125), 125);
                         scl = pn_pow2(-f);
                         if (owner) {
                             const int e = (fresh ? 0 : E[jl]) + f;
@@ -867,6 +869,10 @@ __device__ void pn_epilogue(const PnParams &P, const PnShared &S, uint32_t tbase
                     x[i][1] = __uint_as_float(v0[ri + 2]) * sc[i];   // sg0 + 1
                     x[i][2] = __uint_as_float(v1[ri]) * sc[i];       // sg1
                     x[i][3] = __uint_as_float(v1[ri + 2]) * sc[i];   // sg1 + 1
+                    if (bmode) {   // reachability: exact, the sums are small integers
+#pragma unroll
+                        for (int z = 0; z < 4; ++z) x[i][z] = x[i][z] > 0.f ? 1.f : 0.f;
+                    }
                     const bool fin_i = (rc[i].x & kRecFinish) != 0;
                     const bool keep = valid[i] && !fin_i;
                     any_fin |= valid[i] && fin_i;
@@ -1081,12 +1087,12 @@ __global__ void __launch_bounds__(kPnPlainWarps * 32) pnfa_plain_kernel(PnPlainP
 // ---- handle -----------------------------------------------------------------------------------
 struct trex_pnfa {
     int n_states = 0, sigma = 0, npairs = 0, n_sms = 0;
-    double ll_empty = 0.0;
-    float start_max16[2] = {0.f, 0.f};   // [bf16, fp16]
-    float *d_T32 = nullptr, *d_start32 = nullptr, *d_acc = nullptr;
-    uint32_t *d_tpack[2] = {nullptr, nullptr};
-    float *d_rsym[2] = {nullptr, nullptr};
-    uint4 *d_simg[2] = {nullptr, nullptr};
+    double ll_empty = 0.0, ll_empty_bool = 0.0;
+    float start_max16[3] = {0.f, 0.f, 0.f};   // [bf16, fp16, Boolean (bf16 of 0/1)]
+    float *d_T32 = nullptr, *d_start32 = nullptr, *d_acc = nullptr, *d_acc_bool = nullptr;
+    uint32_t *d_tpack[3] = {nullptr, nullptr, nullptr};
+    float *d_rsym[3] = {nullptr, nullptr, nullptr};
+    uint4 *d_simg[3] = {nullptr, nullptr, nullptr};
     uint8_t *d_misc = nullptr;   // [0,8) queue, [8,12) error word
 };
 
@@ -1109,7 +1115,8 @@ static void pn_free(trex_pnfa *h) {
     cudaFree(h->d_T32);
     cudaFree(h->d_start32);
     cudaFree(h->d_acc);
-    for (int k = 0; k < 2; ++k) {
+    cudaFree(h->d_acc_bool);
+    for (int k = 0; k < 3; ++k) {
         cudaFree(h->d_tpack[k]);
         cudaFree(h->d_rsym[k]);
         cudaFree(h->d_simg[k]);
@@ -1170,11 +1177,23 @@ int trex_pnfa_create(int n_states, int sigma, const float *T, const float *start
         dot += (double)start[i] * (double)accept[i];
     }
     h->ll_empty = dot > 0.0 ? std::log(dot) : -INFINITY;
-    std::vector<uint32_t> tp[2];
-    std::vector<float> rs[2];
-    std::vector<uint4> simg[2];
-    for (int k = 0; k < 2; ++k) {
+    // Boolean form: every nonzero entry is an edge (1), start and accept are sets
+    std::vector<float> Tb(T32.size()), sb(64), ab(64);
+    for (size_t i = 0; i < T32.size(); ++i) Tb[i] = T32[i] != 0.f ? 1.f : 0.f;
+    int nacc = 0;
+    for (int i = 0; i < 64; ++i) {
+        sb[i] = s32[i] != 0.f ? 1.f : 0.f;
+        ab[i] = a32[i] != 0.f ? 1.f : 0.f;
+        nacc += sb[i] != 0.f && ab[i] != 0.f;
+    }
+    h->ll_empty_bool = nacc ? std::log((double)nacc) : -INFINITY;
+    std::vector<uint32_t> tp[3];
+    std::vector<float> rs[3];
+    std::vector<uint4> simg[3];
+    for (int k = 0; k < 3; ++k) {
         const bool fp16 = k == 1;
+        const std::vector<float> &Tk = k == 2 ? Tb : T32;
+        const std::vector<float> &sk = k == 2 ? sb : s32;
         tp[k].assign((size_t)h->npairs * 128 * 32, 0u);
         rs[k].assign(sigma, 0.f);
         for (int c = 0; c < sigma; ++c) {
@@ -1187,7 +1206,7 @@ int trex_pnfa_create(int n_states, int sigma, const float *T, const float *start
                 const int d = (rr & ~15) | ((rr & 7) << 1) | ((rr >> 3) & 1);
                 double rsum = 0.0;
                 for (int q = 0; q < 64; ++q) {
-                    const uint16_t v = pn_host16(T32[((size_t)c * 64 + d) * 64 + q], fp16);
+                    const uint16_t v = pn_host16(Tk[((size_t)c * 64 + d) * 64 + q], fp16);
                     rsum += std::fabs((double)pn_host16_to_f(v, fp16));
                     uint32_t &w = tp[k][((size_t)p * 128 + half_ * 64 + rr) * 32 + (q >> 1)];
                     w |= (uint32_t)v << (16 * (q & 1));
@@ -1200,7 +1219,7 @@ int trex_pnfa_create(int n_states, int sigma, const float *T, const float *start
         simg[k].assign(8, make_uint4(0, 0, 0, 0));
         float smax = 0.f;
         for (int i = 0; i < 64; ++i) {
-            const uint16_t v = pn_host16(s32[i], fp16);
+            const uint16_t v = pn_host16(sk[i], fp16);
             smax = std::max(smax, std::fabs(pn_host16_to_f(v, fp16)));
             uint32_t *w = reinterpret_cast<uint32_t *>(&simg[k][i >> 3]);
             w[(i & 7) >> 1] |= (uint32_t)v << (16 * (i & 1));
@@ -1216,7 +1235,8 @@ int trex_pnfa_create(int n_states, int sigma, const float *T, const float *start
     up((void **)&h->d_T32, T32.data(), T32.size() * 4);
     up((void **)&h->d_start32, s32.data(), 256);
     up((void **)&h->d_acc, a32.data(), 256);
-    for (int k = 0; k < 2; ++k) {
+    up((void **)&h->d_acc_bool, ab.data(), 256);
+    for (int k = 0; k < 3; ++k) {
         up((void **)&h->d_tpack[k], tp[k].data(), tp[k].size() * 4);
         up((void **)&h->d_rsym[k], rs[k].data(), rs[k].size() * 4);
         up((void **)&h->d_simg[k], simg[k].data(), 8 * sizeof(uint4));
@@ -1251,7 +1271,7 @@ int trex_pnfa_run(trex_pnfa *h, int mode, const uint8_t *data, const int64_t *of
     using namespace trex;
     if (!h) return TREX_ERR_NOT_INIT;
     if (n_strings < 0 || total_bytes < 0 || n_strings >= (int64_t)1 << 31) return TREX_ERR_ARG;
-    if (mode < TREX_PNFA_BF16 || mode > TREX_PNFA_FP32) return TREX_ERR_ARG;
+    if (mode < TREX_PNFA_BF16 || mode > TREX_PNFA_BOOL) return TREX_ERR_ARG;
     if (n_strings == 0) return TREX_OK;
     if (!offsets || (total_bytes > 0 && !data)) return TREX_ERR_ARG;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -1289,7 +1309,7 @@ int trex_pnfa_run(trex_pnfa *h, int mode, const uint8_t *data, const int64_t *of
     int grid = 0, p_sub = 0;
     int rc = pn_choose(h, n_strings, &grid, &p_sub);
     if (rc) return rc;
-    const int k = mode == TREX_PNFA_FP16 ? 1 : 0;
+    const int k = mode == TREX_PNFA_FP16 ? 1 : mode == TREX_PNFA_BOOL ? 2 : 0;
     PnParams P;
     P.data = data;
     P.total_bytes = total_bytes;
@@ -1298,9 +1318,10 @@ int trex_pnfa_run(trex_pnfa *h, int mode, const uint8_t *data, const int64_t *of
     P.tpack = h->d_tpack[k];
     P.rsym = h->d_rsym[k];
     P.start_img = h->d_simg[k];
-    P.acc = h->d_acc;
+    P.acc = k == 2 ? h->d_acc_bool : h->d_acc;
     P.start_max = h->start_max16[k];
-    P.ll_empty = h->ll_empty;
+    P.ll_empty = k == 2 ? h->ll_empty_bool : h->ll_empty;
+    P.boolean = k == 2;
     P.sigma = h->sigma;
     P.loglik = loglik;
     P.accept = accept;
@@ -1311,7 +1332,7 @@ int trex_pnfa_run(trex_pnfa *h, int mode, const uint8_t *data, const int64_t *of
     // one CTA per SM: it owns all 512 TMEM columns
     const uint32_t smem = std::max<uint32_t>(P.L.total, 120u * 1024u);
     profile_kernel_begin(st);
-    if (k) pnfa_tc_kernel<true><<<grid, kPnThreads, smem, st>>>(P);
+    if (k == 1) pnfa_tc_kernel<true><<<grid, kPnThreads, smem, st>>>(P);
     else pnfa_tc_kernel<false><<<grid, kPnThreads, smem, st>>>(P);
     profile_kernel_end(st);
     TREX_CHECK_LAUNCH();

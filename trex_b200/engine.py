@@ -233,7 +233,7 @@ class NFA:
         return v.value
 
 
-PNFA_MODES = {"bf16": 0, "fp16": 1, "fp32": 2}
+PNFA_MODES = {"bf16": 0, "fp16": 1, "fp32": 2, "bool": 3}
 
 
 class PNFA:
@@ -243,6 +243,11 @@ class PNFA:
 
     Modes: "bf16" / "fp16" run the tcgen05 tensor-core kernel (16-bit
     operands, FP32 accumulation, sigma <= 28); "fp32" the CUDA-core kernel.
+    "bool" runs the Boolean NFA of the same tables on the tensor cores (the
+    reference's FP16 WMMA nfa_tc_binary kernels, cuda/nfa_tc_evolution.cu:
+    59-442): nonzero entries are edges, each product is thresholded to {0, 1}
+    (exact), accept = some accepting state active; loglik is then the log of
+    the number of active accepting states. Bytes >= sigma are skipped.
     """
 
     def __init__(self, T, start_vec, accept_vec):
