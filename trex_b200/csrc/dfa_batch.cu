@@ -163,6 +163,29 @@ __device__ __forceinline__ int checked_dfa(const int64_t *offsets, const int32_t
     return d;
 }
 
+// Warp-aggregated shared-memory counting: lanes with pred set add 1 to
+// cnt[key]; one atomic per distinct key of the warp (all lanes call it).
+__device__ __forceinline__ void warp_count(uint32_t *cnt, bool pred, int key) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t grp = __match_any_sync(0xffffffffu, pred ? key : -1);
+    if (pred && (uint32_t)(__ffs(grp) - 1) == lane) atomicAdd(&cnt[key], (uint32_t)__popc(grp));
+}
+// Same, returning each lane's rank: the counter's old value plus the number
+// of lanes of the same key below this one.
+__device__ __forceinline__ uint32_t warp_rank(uint32_t *cnt, bool pred, int key) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t grp = __match_any_sync(0xffffffffu, pred ? key : -1);
+    const int leader = __ffs(grp) - 1;
+    uint32_t b = 0;
+    if (pred && (uint32_t)leader == lane) b = atomicAdd(&cnt[key], (uint32_t)__popc(grp));
+    b = __shfl_sync(0xffffffffu, b, leader);
+    return b + (uint32_t)__popc(grp & ((1u << lane) - 1u));
+}
+
+// Counts the items of every (DFA, length class), the items of the batch and,
+// per DFA, its bytes (in 64-byte units: they only weigh the CTAs' first
+// automaton). Warps walk tiles of consecutive strings, so all lanes take part
+// in the warp-level aggregation.
 __global__ void plan_count_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n,
                                   int64_t total_bytes, const DfaDesc *desc, int n_dfas,
                                   int32_t seg_len, uint32_t *cls_count,
@@ -171,24 +194,35 @@ __global__ void plan_count_kernel(const int64_t *offsets, const int32_t *dfa_id,
     __shared__ uint32_t cnt[kMaxDfasPerSet * kLenClasses];
     __shared__ unsigned long long byt[kMaxDfasPerSet];
     __shared__ unsigned long long items;
+    const uint32_t lane = threadIdx.x & 31u;
     for (int t = threadIdx.x; t < n_dfas * kLenClasses; t += blockDim.x) cnt[t] = 0;
     for (int t = threadIdx.x; t < n_dfas; t += blockDim.x) byt[t] = 0;
     if (threadIdx.x == 0) items = 0;
     __syncthreads();
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        int64_t len;
-        int d = checked_dfa(offsets, dfa_id, i, n_dfas, total_bytes, err, &len);
-        if (d < 0) continue;
-        int64_t seg;
-        uint32_t k = n_items_of(len, desc[d].n_states, seg_len, &seg);
-        const ItemClasses ic = item_classes(len, k, seg);
-        uint32_t *cd = cnt + d * kLenClasses;
-        if (k > 1) atomicAdd(&cd[ic.first], 1u);
-        if (k > 2) atomicAdd(&cd[ic.mid], k - 2);
-        atomicAdd(&cd[ic.last], 1u);
-        atomicAdd(&byt[d], (unsigned long long)len + 64ull);
-        atomicAdd(&items, (unsigned long long)k);
+    for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x; i0 < n; i0 += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = i0 + threadIdx.x;
+        int64_t len = 0, seg = 0;
+        int d = i < n ? checked_dfa(offsets, dfa_id, i, n_dfas, total_bytes, err, &len) : -1;
+        uint32_t k = 0;
+        ItemClasses ic{0, 0, 0};
+        if (d >= 0) {
+            k = n_items_of(len, desc[d].n_states, seg_len, &seg);
+            ic = item_classes(len, k, seg);
+        }
+        const int kb = d * kLenClasses;
+        warp_count(cnt, d >= 0 && k > 1, kb + ic.first);
+        warp_count(cnt, d >= 0, kb + ic.last);
+        if (d >= 0 && k > 2) atomicAdd(&cnt[kb + ic.mid], k - 2);
+        const uint32_t ksum = __reduce_add_sync(0xffffffffu, k);
+        if (lane == 0 && ksum) atomicAdd(&items, (unsigned long long)ksum);
+        const uint32_t units = d >= 0 ? (uint32_t)min((len + 127) >> 6, (int64_t)1 << 26) : 0u;
+        for (uint32_t rem = __ballot_sync(0xffffffffu, d >= 0); rem;) {   // one pass per DFA
+            const int leader = __ffs(rem) - 1;
+            const int dl = __shfl_sync(0xffffffffu, d, leader);
+            const uint32_t sum = __reduce_add_sync(0xffffffffu, d == dl ? units : 0u);
+            if ((int)lane == leader) atomicAdd(&byt[dl], (unsigned long long)sum << 6);
+            rem &= ~__ballot_sync(0xffffffffu, d == dl);
+        }
     }
     __syncthreads();
     if (threadIdx.x == 0 && items) atomicAdd(n_items, items);
@@ -270,12 +304,23 @@ plan_fill_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n, int64
             ic.first += d * kLenClasses;
             ic.mid += d * kLenClasses;
             ic.last += d * kLenClasses;
-            if (k > 1) {
-                r0 = atomicAdd(&s_cnt[ic.first], 1u);
-                r_map = atomicAdd(&s_map, k);
-            }
             if (k > 2) rm = atomicAdd(&s_cnt[ic.mid], k - 2);
-            r_last = atomicAdd(&s_cnt[ic.last], 1u);
+        }
+        r0 = warp_rank(s_cnt, d >= 0 && k > 1, ic.first);
+        r_last = warp_rank(s_cnt, d >= 0, ic.last);
+        {   // map slots of split strings: a warp prefix sum, one shared atomic a warp
+            const uint32_t lane = threadIdx.x & 31u;
+            const uint32_t want = (d >= 0 && k > 1) ? k : 0u;
+            uint32_t incl = want;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= (uint32_t)o) incl += v;
+            }
+            uint32_t wb = 0;
+            if (lane == 31 && incl) wb = atomicAdd(&s_map, incl);
+            wb = __shfl_sync(0xffffffffu, wb, 31);
+            r_map = wb + incl - want;
         }
         __syncthreads();
         for (int t = threadIdx.x; t < n_slots; t += blockDim.x)
@@ -516,42 +561,140 @@ __global__ void __launch_bounds__(kRaggedThreads, 1) dfa_ragged_kernel(RaggedPar
     }
 }
 
+// Re-walks bytes [b0, b1) of one item from state s_in with the whole warp:
+// lane l computes the map of all N (<= 16) states over its 1/32 of the bytes
+// (16 independent chains through the byte map in shared memory), then the 32
+// maps are applied in order. Returns the end state (every lane).
+__device__ __forceinline__ uint32_t warp_rewalk(const uint8_t *tbl, uint32_t N, const uint8_t *data,
+                                                int64_t b0, int64_t b1, uint32_t s_in) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const int64_t c = (b1 - b0 + 31) / 32;
+    const int64_t q0 = min(b1, b0 + (int64_t)lane * c), q1 = min(b1, q0 + c);
+    uint32_t st[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) st[j] = (uint32_t)j;
+    for (int64_t q = q0; q < q1; ++q) {
+        const uint8_t *row = tbl + (uint32_t)__ldg(data + q) * N;
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+            if ((uint32_t)j < N) st[j] = row[st[j]];
+    }
+    uint64_t map = 0;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) map |= (uint64_t)st[j] << (4 * j);
+    uint32_t s = s_in;
+    for (int l = 0; l < 32; ++l) {
+        const uint64_t ml = __shfl_sync(0xffffffffu, map, l);
+        s = (uint32_t)(ml >> (4 * s)) & 15u;
+    }
+    return s;
+}
+
+constexpr int kComposeThreads = 256;
+
 // Strings cut into several items: chains the items' (guessed entry, end state)
-// records in order. An item whose guessed entry differs from the true entry
-// state (its warm-up chain had not synchronised) is walked again from the true
-// state through the automaton's byte map in global memory; for synchronising
-// automata that is rare, for permutation automata it is every item after the
-// first. One thread per string.
-__global__ void compose_kernel(RaggedParams P) {
+// records in order, one warp per string. Item j's record is right when its
+// guessed entry equals the end state of item j - 1 (item 0 starts from the start
+// state); the first item whose guess is wrong (its warm-up chain had not
+// synchronised: rare for synchronising automata, every item after the first
+// for permutation automata) is walked again from the true state by the warp,
+// and the check goes on from there, 32 records at a time.
+__global__ void __launch_bounds__(kComposeThreads) compose_kernel(RaggedParams P) {
+    __shared__ __align__(16) uint8_t s_tbl[kComposeThreads / 32][256 * kSmallDfaStates];
     if (*(volatile uint32_t *)P.err & kErrCapacity) return;   // the plan was refused
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < P.n;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        int64_t len, s0;
-        const int d = checked_dfa(P.offsets, P.dfa_id, i, P.n_dfas, P.total_bytes, P.err, &len, &s0);
-        if (d < 0) continue;
-        const DfaDesc D = P.desc[d];
-        int64_t seg;
-        const uint32_t k = n_items_of(len, D.n_states, P.seg_len, &seg);
-        if (k <= 1) continue;
-        const uint32_t mb = P.str_map[i];
-        if ((int64_t)mb + (int64_t)k > P.max_items) {   // offsets changed since the plan
-            atomicOr(P.err, kErrCapacity);
-            continue;
-        }
-        const uint8_t *tm = P.tmaps + D.tmap_off;
-        const uint32_t N = (uint32_t)D.n_states;
-        uint32_t s = (P.maps[mb] >> 8) & 0xffu;   // item 0 starts from the start state
-        for (uint32_t j = 1; j < k; ++j) {
-            const uint32_t v = P.maps[mb + j];
-            if ((v & 0xffu) == s) {
-                s = (v >> 8) & 0xffu;
-            } else {
-                const int64_t b0 = s0 + (int64_t)j * seg;
-                const int64_t b1 = (j + 1 == k) ? s0 + len : b0 + seg;
-                for (int64_t q = b0; q < b1; ++q) s = tm[(uint32_t)__ldg(P.data + q) * N + s];
+    const uint32_t FULL = 0xffffffffu;
+    const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+    uint8_t *tbl = s_tbl[wib];
+    int tbl_dfa = -1;
+    const int64_t nwarps = (int64_t)gridDim.x * (kComposeThreads / 32);
+    for (int64_t base = ((int64_t)blockIdx.x * (kComposeThreads / 32) + wib) * 32; base < P.n;
+         base += nwarps * 32) {
+        const int64_t i = base + lane;
+        int64_t len = 0, s0 = 0, seg = 0;
+        const int d = i < P.n ? checked_dfa(P.offsets, P.dfa_id, i, P.n_dfas, P.total_bytes, P.err,
+                                            &len, &s0)
+                              : -1;
+        uint32_t k = 0, mb = 0;
+        if (d >= 0) {
+            k = n_items_of(len, P.desc[d].n_states, P.seg_len, &seg);
+            if (k > 1) {
+                mb = P.str_map[i];
+                if ((int64_t)mb + (int64_t)k > P.max_items) {   // offsets changed since the plan
+                    atomicOr(P.err, kErrCapacity);
+                    k = 0;
+                }
             }
         }
-        write_result(P, (uint32_t)i, s, D.accept_off);
+        // each lane chains its own string while every guess is right
+        uint32_t st = 0, jbad = 0;
+        bool help = false;
+        if (k > 1) {
+            st = (P.maps[mb] >> 8) & 0xffu;   // item 0 starts from the start state
+            for (uint32_t j0 = 1; j0 < k && !help; j0 += 4) {
+                uint32_t v[4];   // four records loaded together
+#pragma unroll
+                for (int u = 0; u < 4; ++u) v[u] = j0 + u < k ? P.maps[mb + j0 + u] : 0u;
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const uint32_t j = j0 + u;
+                    if (help || j >= k) continue;
+                    if ((v[u] & 0xffu) == st) st = (v[u] >> 8) & 0xffu;
+                    else { help = true; jbad = j; }
+                }
+            }
+            if (!help) {
+                if (st < (uint32_t)P.desc[d].n_states) write_result(P, (uint32_t)i, st, P.desc[d].accept_off);
+                else atomicOr(P.err, kErrCapacity);   // records not written by this plan
+            }
+        }
+        // strings with a wrong guess: the warp re-walks that item and goes on checking
+        for (uint32_t todo = __ballot_sync(FULL, help); todo; todo &= todo - 1) {
+            const int src = __ffs(todo) - 1;
+            const int sd = __shfl_sync(FULL, d, src);
+            const uint32_t sk = __shfl_sync(FULL, k, src), smb = __shfl_sync(FULL, mb, src);
+            const uint32_t sj = __shfl_sync(FULL, jbad, src), s_entry = __shfl_sync(FULL, st, src);
+            const int64_t ss0 = __shfl_sync(FULL, s0, src), slen = __shfl_sync(FULL, len, src);
+            const int64_t sseg = __shfl_sync(FULL, seg, src);
+            const DfaDesc D = P.desc[sd];
+            const uint32_t N = (uint32_t)D.n_states;
+            auto rewalk = [&](uint32_t jb, uint32_t s_in) {
+                if (tbl_dfa != sd) {   // this warp's copy of the automaton's byte map
+                    __syncwarp();
+                    const uint8_t *tm = P.tmaps + D.tmap_off;
+                    for (uint32_t t = lane; t < 256 * N; t += 32) tbl[t] = tm[t];
+                    __syncwarp();
+                    tbl_dfa = sd;
+                }
+                const int64_t b0 = ss0 + (int64_t)jb * sseg;
+                const int64_t b1 = (jb + 1 == sk) ? ss0 + slen : b0 + sseg;
+                return warp_rewalk(tbl, N, P.data, b0, b1, s_in);
+            };
+            uint32_t s = s_entry < N ? rewalk(sj, s_entry) : 0xffu;
+            for (uint32_t j0 = sj + 1; j0 < sk && s < N; j0 += 32) {
+                const uint32_t j = j0 + lane;
+                const bool in = j < sk;
+                const uint32_t v = in ? P.maps[smb + j] : 0u;
+                uint32_t g = v & 0xffu, f = (v >> 8) & 0xffu;
+                for (;;) {
+                    uint32_t pf = __shfl_up_sync(FULL, f, 1);
+                    if (lane == 0) pf = s;
+                    const uint32_t bad = __ballot_sync(FULL, in && g != pf);
+                    if (!bad) break;
+                    const int b = __ffs(bad) - 1;
+                    const uint32_t s_in = __shfl_sync(FULL, pf, b);
+                    const uint32_t s_out = s_in < N ? rewalk(j0 + (uint32_t)b, s_in) : s_in;
+                    if (lane == (uint32_t)b) {
+                        g = s_in;
+                        f = s_out;
+                    }
+                }
+                s = __shfl_sync(FULL, f, (int)min(31u, sk - 1 - j0));
+            }
+            if ((int)lane == src) {
+                if (s < N) write_result(P, (uint32_t)i, s, D.accept_off);
+                else atomicOr(P.err, kErrCapacity);   // records not written by this plan
+            }
+        }
     }
 }
 
@@ -670,7 +813,9 @@ int dfa_set_run(trex_dfa_set *set, const uint8_t *data, const int64_t *offsets,
     dfa_ragged_kernel<<<set->n_sms, kRaggedThreads, set->smem_bytes, stream>>>(P);
     TREX_CHECK_LAUNCH();
     profile_kernel_end(stream);
-    compose_kernel<<<plan_grid, kPlanThreads, 0, stream>>>(P);
+    compose_kernel<<<(int)std::min<int64_t>((n + kComposeThreads - 1) / kComposeThreads,
+                                            (int64_t)set->n_sms * 8),
+                     kComposeThreads, 0, stream>>>(P);
     TREX_CHECK_LAUNCH();
     if (err_word_out) *err_word_out = err;
     return TREX_OK;
