@@ -74,6 +74,9 @@ def parse_args():
                     help="nfa workload: bit-parallel kernel, or the Boolean NFA on the tensor cores")
     ap.add_argument("--strings", type=int, default=None, help="override the number of strings")
     ap.add_argument("--seg-len", type=int, default=0, help="bytes per work item / scan tile (0 = default)")
+    ap.add_argument("--kgram", type=int, default=None,
+                    help="K-gram width of every automaton of a DFA workload (0 = the largest each "
+                         "allows; default: byte walks, or the tuned choice with --tuned)")
     ap.add_argument("--dfa-sizes", type=str, default=None,
                     help="comma list of DFA state counts replacing the default 5x8,5x12,6x16")
     ap.add_argument("--seed", type=int, default=2024)
@@ -186,7 +189,8 @@ class DFAWorkload:
         self.data = device_bytes(torch, lens, is_sub, seed, dev)
         self.d_off = torch.from_numpy(self.off).to(dev)
         self.d_ids = torch.from_numpy(self.ids).to(dev)
-        self.set = DFASet(self.dfas)
+        self.set = DFASet(self.dfas, kgram=self.args.kgram)
+        self.kgram_used = [self.set.get_kgram(i) for i in range(len(self.dfas))]
         n = self.n
         if self.kind == "scan":
             self.scratch = torch.empty(DFASet.scan_scratch_bytes(n, self.total, self.args.seg_len),
@@ -235,6 +239,7 @@ class DFAWorkload:
     def config(self):
         return {"workload": self.workload, "n_strings": self.n, "total_bytes_per_gpu": self.total,
                 "seg_len": self.args.seg_len or (8192 if self.kind == "scan" else 2048),
+                "kgram": getattr(self, "kgram_used", None),
                 "l2": "inputs larger than L2 (126 MB), no flush" if self.total > 126e6 else
                       "inputs smaller than L2: L2 flushed by a 256 MB write between steps"}
 

@@ -135,6 +135,22 @@ int trex_dfa_set_create(int n_dfas, const int32_t *n_states, const int32_t *star
                         const uint8_t *tmaps, const uint8_t *accepts, trex_dfa_set **out);
 void trex_dfa_set_destroy(trex_dfa_set *set);
 
+/* K-gram walking (the reference's monoid K-gram path, src/kgram.py:29-231,
+ * cuda/monoid_batch.cu:103-125, re-designed): for an automaton with at most 16
+ * states whose bytes fall into at most 16 distinguished bytes plus one column
+ * shared by every other byte, k = 2, 4 or 8 consecutive input bytes advance
+ * the state with one table lookup (the codes of the k bytes form an 8-bit
+ * index: k <= 8 / bits for 1-, 2- or 4-bit codes). Windows holding any other
+ * byte are walked byte by byte; results are identical for every input.
+ * trex_dfa_kgram_max: the largest k automaton dfa_index allows (1: none).
+ * trex_dfa_set_kgram: k = 1 (byte walk, the default), 2, 4, 8, or 0 for the
+ * largest allowed; TREX_ERR_SHAPE when the automaton does not allow k. Call
+ * it between runs of the set (it updates the automaton's device descriptor
+ * with a synchronous copy). trex_dfa_get_kgram: the current k. */
+int trex_dfa_kgram_max(const trex_dfa_set *set, int dfa_index, int *k_max);
+int trex_dfa_set_kgram(trex_dfa_set *set, int dfa_index, int k);
+int trex_dfa_get_kgram(const trex_dfa_set *set, int dfa_index, int *k);
+
 /* Device scratch (bytes) needed by trex_dfa_batch_run for a batch. */
 int64_t trex_dfa_batch_scratch_bytes(int64_t n_strings, int64_t total_bytes, int32_t seg_len);
 

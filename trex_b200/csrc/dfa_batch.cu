@@ -430,6 +430,137 @@ __device__ __forceinline__ uint32_t walk_masked(const W &w, uint32_t e, uint4 a,
     return e;
 }
 
+// ---- window walkers ------------------------------------------------------------------------
+// A mode advances a state over one 32-byte window: fast() when all 32 bytes
+// belong to the item, masked() with a byte mask and the warm-up capture.
+template <class W>
+struct ByteMode {
+    W w;
+    __device__ __forceinline__ bool valid(uint4, uint4) const { return true; }
+    __device__ __forceinline__ uint32_t fast(uint32_t e, uint4 a, uint4 b) const {
+        e = step16(w, e, a);
+        return step16(w, e, b);
+    }
+    __device__ __forceinline__ uint32_t masked(uint32_t e, uint4 a, uint4 b, uint32_t m, uint32_t cpos,
+                                               uint32_t &cap_e) const {
+        return walk_masked(w, e, a, b, m, cpos, cap_e);
+    }
+};
+
+// Offset of the per-code fallback table (after the largest main table).
+constexpr uint32_t kFallbackOff = kRepTableBytes16;
+constexpr uint32_t kFallbackBytes = 17 * 512;
+
+// K-gram walking for an automaton whose bytes fall into at most 2^BITS
+// distinguished bytes ("letters", one code each) plus one shared column for
+// every other byte. A window whose 32 bytes are all letters is walked K bytes
+// per lookup: the codes of K consecutive bytes (first byte most significant)
+// form an 8-bit gram index into a table of K-step transitions in the same
+// layout as the byte table. Other windows are walked byte by byte through a
+// table of 2^BITS + 1 columns (the letters' codes, then the shared column).
+// Codes come from one shift and mask; a byte is a letter exactly when the
+// letter of its code equals it, which every window is checked for.
+template <class W, int BITS, int K>
+struct GramMode {
+    W w;
+    uint32_t sh;
+    uint32_t alpha[4];
+    static constexpr uint32_t kMask = BITS == 1 ? 0x01010101u : BITS == 2 ? 0x03030303u : 0x0F0F0F0Fu;
+    static constexpr uint32_t kOther = (1u << BITS) * 0x01010101u;   // the shared column, 4 bytes
+    __device__ __forceinline__ uint32_t codes(uint32_t x) const { return (x >> sh) & kMask; }
+    // the letter of each byte's code, in byte order
+    __device__ __forceinline__ uint32_t letters(uint32_t y) const {
+        if (BITS == 1) {
+            const uint32_t a0 = alpha[0] & 0xFFu, a1 = (alpha[0] >> 8) & 0xFFu;
+            return a0 * 0x01010101u ^ y * (a0 ^ a1);
+        } else if (BITS == 2) {
+            const uint32_t v = y | (y >> 12);   // selectors of bytes 0, 2, 1, 3 in nibbles 0-3
+            return __byte_perm(__byte_perm(alpha[0], 0, v), 0, 0x3120);
+        } else {
+            const uint32_t v = y | (y >> 12);
+            const uint32_t v7 = v & 0x7777u;
+            const uint32_t lo = __byte_perm(alpha[0], alpha[1], v7);
+            const uint32_t hi = __byte_perm(alpha[2], alpha[3], v7);
+            const uint32_t sel = __byte_perm(((y >> 3) & 0x01010101u) * 0xFFu, 0, 0x3120);
+            return __byte_perm((lo & ~sel) | (hi & sel), 0, 0x3120);
+        }
+    }
+    __device__ __forceinline__ bool word_ok(uint32_t x) const { return letters(codes(x)) == x; }
+    __device__ __forceinline__ bool valid(uint4 a, uint4 b) const {
+        return word_ok(a.x) & word_ok(a.y) & word_ok(a.z) & word_ok(a.w) & word_ok(b.x) &
+               word_ok(b.y) & word_ok(b.z) & word_ok(b.w);
+    }
+    __device__ __forceinline__ uint32_t grams_word(uint32_t e, uint32_t x) const {
+        const uint32_t y = codes(x);
+        if (BITS == 4) {   // K = 2: grams c0c1, c2c3 in bytes 1 and 3
+            const uint32_t p = y * 0x1001u;
+            e = w.template step<1>(e, p);
+            return w.template step<3>(e, p);
+        } else if (K == 2) {
+            const uint32_t p = y * (BITS == 2 ? 0x401u : 0x201u);
+            e = w.template step<1>(e, p);
+            return w.template step<3>(e, p);
+        } else {           // K = 4: one gram in byte 3
+            const uint32_t p = y * (BITS == 2 ? 0x40100401u : 0x08040201u);
+            return w.template step<3>(e, p);
+        }
+    }
+    __device__ __forceinline__ uint32_t fast(uint32_t e, uint4 a, uint4 b) const {
+        if (K == 8) {      // BITS = 1: the codes of two words make one gram
+            const uint32_t x[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+            for (int k = 0; k < 8; k += 2) {
+                const uint32_t h0 = ((codes(x[k]) * 0x08040201u) >> 20) & 0xF0u;
+                const uint32_t h1 = (codes(x[k + 1]) * 0x08040201u) >> 24;
+                e = w.template step<0>(e, h0 | h1);
+            }
+            return e;
+        }
+        e = grams_word(e, a.x); e = grams_word(e, a.y); e = grams_word(e, a.z); e = grams_word(e, a.w);
+        e = grams_word(e, b.x); e = grams_word(e, b.y); e = grams_word(e, b.z);
+        return grams_word(e, b.w);
+    }
+    // the fallback column of each byte: its code for a letter, else the shared column
+    __device__ __forceinline__ uint32_t columns(uint32_t x) const {
+        const uint32_t y = codes(x);
+        const uint32_t d = x ^ letters(y);
+        const uint32_t nz = (((d & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | d) & 0x80808080u;   // 0x80: byte differs
+        const uint32_t ne = (nz >> 7) * 0xFFu;
+        return (y & ~ne) | (kOther & ne);
+    }
+    __device__ __forceinline__ uint32_t masked(uint32_t e, uint4 a, uint4 b, uint32_t m, uint32_t cpos,
+                                               uint32_t &cap_e) const {
+        const uint32_t x[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const uint32_t col = columns(x[k]);
+            uint32_t n;
+#define TREX_GSTEP(J)                                               \
+            n = w.template step_off<J>(kFallbackOff, e, col);       \
+            e = (m >> (4 * k + J)) & 1u ? n : e;                    \
+            cap_e = (4u * k + J + 1u == cpos) ? e : cap_e;
+            TREX_GSTEP(0) TREX_GSTEP(1) TREX_GSTEP(2) TREX_GSTEP(3)
+#undef TREX_GSTEP
+        }
+        return e;
+    }
+};
+
+// Tables of a K-gram automaton: the gram table (256 columns) at 0 and the
+// fallback table at kFallbackOff.
+__device__ inline void build_gram_tables(const DfaDesc &D, const uint8_t *__restrict__ src) {
+    const int N = D.n_states, bits = D.kbits, K = D.kgram;
+    const uint32_t mask = (1u << bits) - 1u, ncode = 1u << bits;
+    const uint8_t *rep = D.krep;
+    build_layout(N, 256, 0, [&](uint32_t g, uint32_t s) {
+        uint32_t t = s;
+        for (int i = K - 1; i >= 0; --i) t = src[rep[(g >> (bits * i)) & mask] * N + t];
+        return t;
+    });
+    build_layout(N, (int)ncode + 1, kFallbackOff,
+                 [&](uint32_t c, uint32_t s) { return (uint32_t)src[rep[c] * N + s]; });
+}
+
 // Drains queue d with this warp, 32 items (one a lane) at a time. The items of
 // a queue are ordered by walked length (warm-up included), longest first, in
 // 128-byte classes, so the items of a batch span nearly the same number of
@@ -437,9 +568,11 @@ __device__ __forceinline__ uint32_t walk_masked(const W &w, uint32_t e, uint4 a,
 // between a batch's first and last is walked without masks. The records of the
 // next batch are claimed and loaded while the current one is walked; the next
 // window of every lane is loaded while the current one is walked.
-template <class W>
-__device__ void drain_queue(const RaggedParams &P, const W &w, const DfaDesc &D, uint32_t base,
+template <class M>
+__device__ void drain_queue(const RaggedParams &P, const M &md, const DfaDesc &D, uint32_t base,
                             uint32_t count, uint32_t *head) {
+    using W = decltype(md.w);
+    const W &w = md.w;
     const uint32_t FULL = 0xffffffffu;
     const uint32_t lane = threadIdx.x & 31u;
     const uint8_t *const lo_ok = P.data, *const hi_ok = P.data + P.total_bytes;
@@ -482,13 +615,10 @@ __device__ void drain_queue(const RaggedParams &P, const W &w, const DfaDesc &D,
             const uint32_t m = bit_range((int)mlo, (int)mhi);
             const bool cap = it == cw;
             if (cap && cpos == 0) cap_e = e;   // the warm-up ended with the previous window
-            const bool special = (it < nw && m != FULL) || (cap && cpos != 0);
-            if (!__any_sync(FULL, special)) {
-                e = step16(w, e, ca);
-                e = step16(w, e, cbv);
-            } else {
-                e = walk_masked(w, e, ca, cbv, m, cap ? cpos : 0u, cap_e);
-            }
+            const bool special =
+                (it < nw && (m != FULL || !md.valid(ca, cbv))) || (cap && cpos != 0);
+            if (!__any_sync(FULL, special)) e = md.fast(e, ca, cbv);
+            else e = md.masked(e, ca, cbv, m, cap ? cpos : 0u, cap_e);
             if (it + 1 == nw) {   // this lane's item ends in this window
                 const uint32_t fin = W::dec(e);
                 if ((cur.segn >> 16) == 1)
@@ -539,12 +669,28 @@ __global__ void __launch_bounds__(kRaggedThreads, 1) dfa_ragged_kernel(RaggedPar
         const int d = s_dfa;
         if (d < 0) break;
         const DfaDesc D = P.desc[d];
-        build_table(P.tmaps + D.tmap_off, D.n_states);
+        const bool gram = D.kgram > 1 && D.n_states <= kSmallDfaStates;
+        if (gram) build_gram_tables(D, P.tmaps + D.tmap_off);
+        else build_table(P.tmaps + D.tmap_off, D.n_states);
         __syncthreads();
         const uint32_t base = P.q_base[d], count = P.q_count[d];
-        if (D.n_states <= 8) drain_queue(P, Walker<8>{lane}, D, base, count, &P.q_head[d]);
-        else if (D.n_states <= 16) drain_queue(P, Walker<16>{lane}, D, base, count, &P.q_head[d]);
-        else drain_queue(P, Walker<0>{(uint32_t)D.n_states}, D, base, count, &P.q_head[d]);
+        uint32_t *head = &P.q_head[d];
+        if (gram) {
+            const uint32_t sh = (uint32_t)D.kshift;
+            const uint32_t *al = D.kalpha;
+#define TREX_GRAM(WT, B, KK)                                                                                 drain_queue(P, GramMode<WT, B, KK>{WT{lane}, sh, {al[0], al[1], al[2], al[3]}}, D, base,                         count, head)
+#define TREX_GRAMS(WT)                                                                                       switch (D.kbits * 16 + D.kgram) {                                                                    case 16 + 2: TREX_GRAM(WT, 1, 2); break;                                                          case 16 + 4: TREX_GRAM(WT, 1, 4); break;                                                          case 16 + 8: TREX_GRAM(WT, 1, 8); break;                                                          case 32 + 2: TREX_GRAM(WT, 2, 2); break;                                                          case 32 + 4: TREX_GRAM(WT, 2, 4); break;                                                          default: TREX_GRAM(WT, 4, 2); break;                                                          }
+            if (D.n_states <= 8) { TREX_GRAMS(Walker<8>) }
+            else { TREX_GRAMS(Walker<16>) }
+#undef TREX_GRAMS
+#undef TREX_GRAM
+        } else if (D.n_states <= 8) {
+            drain_queue(P, ByteMode<Walker<8>>{Walker<8>{lane}}, D, base, count, head);
+        } else if (D.n_states <= 16) {
+            drain_queue(P, ByteMode<Walker<16>>{Walker<16>{lane}}, D, base, count, head);
+        } else {
+            drain_queue(P, ByteMode<Walker<0>>{Walker<0>{(uint32_t)D.n_states}}, D, base, count, head);
+        }
         __syncthreads();
         if (threadIdx.x == 0) {
             int best = -1;
@@ -706,6 +852,8 @@ struct trex_dfa_set {
     std::vector<int32_t> n_states, starts;
     std::vector<int64_t> tmap_off, accept_off;
     std::vector<uint8_t> h_accepts;      // host copy for empty-batch answers
+    std::vector<uint8_t> h_tmaps;        // host copy: K-gram eligibility
+    std::vector<trex::DfaDesc> h_desc;
     uint8_t *d_tmaps = nullptr;
     uint8_t *d_accepts = nullptr;
     trex::DfaDesc *d_desc = nullptr;
@@ -862,14 +1010,16 @@ int trex_dfa_set_create(int n_dfas, const int32_t *n_states, const int32_t *star
             }
     }
     set->h_accepts.assign(accepts, accepts + asum);
+    set->h_tmaps.assign(tmaps, tmaps + tsum);
+    set->h_desc = desc;
     set->n_sms = trex::sm_count();
     if (set->n_sms <= 0) {
         delete set;
         trex::set_last_error_msg("trex_dfa_set_create: no CUDA device");
         return TREX_ERR_SHAPE;
     }
-    // table region, sized for the largest layout
-    set->smem_bytes = (size_t)trex::kRepTableBytes16;
+    // table region, sized for the largest layout, and the K-gram fallback table
+    set->smem_bytes = (size_t)trex::kFallbackOff + trex::kFallbackBytes;
     auto fail = [&](cudaError_t e, const char *what) {
         trex::set_last_error(what, e);
         cudaFree(set->d_tmaps);
@@ -894,7 +1044,7 @@ int trex_dfa_set_create(int n_dfas, const int32_t *n_states, const int32_t *star
     // table any set can need (128 KiB).
     if ((e = cudaFuncSetAttribute(trex::dfa_ragged_kernel,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  trex::kRepTableBytes16)) != cudaSuccess)
+                                  trex::kFallbackOff + trex::kFallbackBytes)) != cudaSuccess)
         return fail(e, "cudaFuncSetAttribute");
     *out = set;
     return TREX_OK;
@@ -1100,3 +1250,108 @@ extern "C" int trex_dfa_batch_run_static(trex_dfa_set *set, const uint8_t *data,
                              accept, accept_i32, scratch, trex::kStaticScratchBytes, seg_len,
                              static_cast<cudaStream_t>(stream), nullptr);
 }
+
+// ---- K-gram walking ---------------------------------------------------------------------------
+namespace trex {
+
+// The K-gram form of automaton d: its distinguished bytes are those whose
+// column (next state of every state) differs from the most common column;
+// they get codes (b >> sh) & (2^bits - 1) for the smallest bits in {1, 2, 4}
+// and shift sh that keep them apart. Returns the largest K (2^bits)^K <= 256
+// allows, or 1 when the automaton has more than 16 states or more than 16
+// distinguished bytes, or no shift separates them.
+static int kgram_plan(const trex_dfa_set *set, int d, DfaDesc *out) {
+    const int N = set->n_states[d];
+    if (N > kSmallDfaStates) return 1;
+    const uint8_t *t = set->h_tmaps.data() + set->tmap_off[d];
+    auto same = [&](int a, int b) { return std::memcmp(t + a * N, t + b * N, N) == 0; };
+    // the most common column
+    int other = 0, best = 0;
+    std::vector<int> cls(256, -1);
+    for (int b = 0; b < 256; ++b) {
+        if (cls[b] >= 0) continue;
+        int cnt = 0;
+        for (int c = b; c < 256; ++c)
+            if (cls[c] < 0 && same(b, c)) {
+                cls[c] = b;
+                ++cnt;
+            }
+        if (cnt > best) { best = cnt; other = b; }
+    }
+    std::vector<int> letters;
+    for (int b = 0; b < 256; ++b)
+        if (cls[b] != cls[other]) letters.push_back(b);
+    const int sigma = (int)letters.size();
+    if (sigma < 1 || sigma > 16) return 1;
+    for (int bits : {1, 2, 4}) {
+        if (sigma > (1 << bits)) continue;
+        for (int sh = 0; sh + bits <= 8; ++sh) {
+            const int mask = (1 << bits) - 1;
+            std::vector<int> owner(1 << bits, -1);
+            bool ok = true;
+            for (int b : letters) {
+                const int c = (b >> sh) & mask;
+                if (owner[c] >= 0) { ok = false; break; }
+                owner[c] = b;
+            }
+            if (!ok) continue;
+            DfaDesc D = set->h_desc[d];
+            D.kbits = bits;
+            D.kshift = sh;
+            uint8_t alpha[16];
+            for (int c = 0; c < 16; ++c) {
+                // an unused code's letter is a byte of another code: no input byte matches it
+                const int code_other = (c ^ 1) & mask;
+                alpha[c] = owner[c & mask] >= 0 && c <= mask ? (uint8_t)owner[c] : (uint8_t)(code_other << sh);
+                if (c <= mask) D.krep[c] = owner[c] >= 0 ? (uint8_t)owner[c] : (uint8_t)other;
+            }
+            D.krep[1 << bits] = (uint8_t)other;
+            std::memcpy(D.kalpha, alpha, 16);
+            *out = D;
+            return 8 / bits;
+        }
+    }
+    return 1;
+}
+
+}  // namespace trex
+
+extern "C" {
+
+int trex_dfa_kgram_max(const trex_dfa_set *set, int dfa_index, int *k_max) {
+    if (!set || !k_max || dfa_index < 0 || dfa_index >= set->n_dfas) return TREX_ERR_ARG;
+    trex::DfaDesc D{};
+    *k_max = trex::kgram_plan(set, dfa_index, &D);
+    return TREX_OK;
+}
+
+int trex_dfa_set_kgram(trex_dfa_set *set, int dfa_index, int k) {
+    if (!set || dfa_index < 0 || dfa_index >= set->n_dfas) return TREX_ERR_ARG;
+    if (k < 0 || (k > 1 && k != 2 && k != 4 && k != 8)) return TREX_ERR_ARG;
+    trex::DfaDesc D = set->h_desc[dfa_index];
+    if (k != 1) {
+        trex::DfaDesc P{};
+        const int kmax = trex::kgram_plan(set, dfa_index, &P);
+        if (k == 0) k = kmax;
+        if (k > kmax) {
+            trex::set_last_error_msg("trex_dfa_set_kgram: the automaton does not allow this K");
+            return TREX_ERR_SHAPE;
+        }
+        if (k > 1) D = P;
+    }
+    D.kgram = k > 1 ? k : 1;
+    if (D.kgram == 1) {
+        D.kbits = D.kshift = 0;
+    }
+    TREX_CUDA(cudaMemcpy(set->d_desc + dfa_index, &D, sizeof(D), cudaMemcpyHostToDevice));
+    set->h_desc[dfa_index] = D;
+    return TREX_OK;
+}
+
+int trex_dfa_get_kgram(const trex_dfa_set *set, int dfa_index, int *k) {
+    if (!set || !k || dfa_index < 0 || dfa_index >= set->n_dfas) return TREX_ERR_ARG;
+    *k = set->h_desc[dfa_index].kgram;
+    return TREX_OK;
+}
+
+}  // extern "C"

@@ -23,6 +23,13 @@ struct DfaDesc {
     int32_t start;
     int64_t tmap_off;
     int64_t accept_off;
+    // K-gram walking (kgram > 1): byte b has code (b >> kshift) & ((1 << kbits) - 1);
+    // b is one of the automaton's distinguished bytes when it equals byte `code` of
+    // kalpha; krep[c] is a byte of code c's column (the other column for unused
+    // codes) and krep[1 << kbits] a byte of the column every other byte shares.
+    int32_t kgram = 1, kbits = 0, kshift = 0, kpad = 0;
+    uint32_t kalpha[4] = {0, 0, 0, 0};
+    uint8_t krep[20] = {};
 };
 
 // Dynamic shared memory of every kernel that walks a table: the table sits
@@ -42,6 +49,11 @@ template <> struct Walker<8> {
     __device__ __forceinline__ uint32_t step(uint32_t e, uint32_t x) const {
         return tbl_u8(__byte_perm(e, x, 0x1100 | ((4 + I) << 4)));
     }
+    // the same layout for a second table `off` bytes into shared memory
+    template <int I>
+    __device__ __forceinline__ uint32_t step_off(uint32_t off, uint32_t e, uint32_t x) const {
+        return tbl_u8(off + __byte_perm(e, x, 0x1100 | ((4 + I) << 4)));
+    }
 };
 
 template <> struct Walker<16> {
@@ -53,6 +65,11 @@ template <> struct Walker<16> {
     __device__ __forceinline__ uint32_t step(uint32_t e, uint32_t x) const {
         uint32_t t = __byte_perm(e, x, 0x1100 | ((4 + I) << 4));
         return tbl_u8((lane << 2) + t + (t & 0xFFC0u));
+    }
+    template <int I>
+    __device__ __forceinline__ uint32_t step_off(uint32_t off, uint32_t e, uint32_t x) const {
+        uint32_t t = __byte_perm(e, x, 0x1100 | ((4 + I) << 4));
+        return tbl_u8(off + (lane << 2) + t + (t & 0xFFC0u));
     }
 };
 
@@ -71,6 +88,37 @@ template <> struct Walker<0> {
 // Shared-memory bytes a DFA of n states needs.
 __host__ __device__ inline int table_bytes_for(int n) {
     return n <= 8 ? 256 * 256 : n <= 16 ? 256 * 512 : 256 * n;
+}
+
+// Fills ncols columns of a replicated table (N <= 16) at byte `off` of shared
+// memory in the layout N selects; next(c, s) is the next state of state s < N
+// on column c (padded states loop).
+template <class F>
+__device__ inline void build_layout(int N, int ncols, uint32_t off, F next) {
+    uint32_t *w32 = reinterpret_cast<uint32_t *>(g_dfa_tbl + off);
+    if (N <= 8) {
+        for (int w = threadIdx.x; w < ncols * 64; w += blockDim.x) {
+            uint32_t c = w >> 6, q = (w >> 5) & 1u, ln = w & 31u, word = 0;
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                uint32_t s = q * 4 + b;
+                uint32_t t = s < (uint32_t)N ? next(c, s) : s;
+                word |= ((t & 3u) | (ln << 2) | ((t >> 2) << 7)) << (8 * b);
+            }
+            w32[w] = word;
+        }
+    } else {
+        for (int w = threadIdx.x; w < ncols * 128; w += blockDim.x) {
+            uint32_t c = w >> 7, q = (w >> 5) & 3u, word = 0;
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                uint32_t s = q * 4 + b;
+                uint32_t t = s < (uint32_t)N ? next(c, s) : s;
+                word |= ((t & 3u) | ((t >> 2) << 6)) << (8 * b);
+            }
+            w32[w] = word;
+        }
+    }
 }
 
 // Fills the shared table for `src` (256*N byte map) in the layout N selects.

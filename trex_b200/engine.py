@@ -48,9 +48,15 @@ def profile_end(capacity: int = 100000) -> list:
 
 
 class DFASet:
-    """Resident set of byte DFAs (N <= 256 each, at most 64)."""
+    """Resident set of byte DFAs (N <= 256 each, at most 64).
 
-    def __init__(self, dfas: Sequence[ByteDFA]):
+    kgram: None (byte walks), an int applied to every automaton, or one int
+    per automaton: K-gram width (1, 2, 4, 8, or 0 for the largest the
+    automaton allows; automata that allow none keep byte walks when 0 is
+    given). See kgram_max / set_kgram.
+    """
+
+    def __init__(self, dfas: Sequence[ByteDFA], kgram=None):
         self.lib = _lib.load()
         self.dfas = list(dfas)
         n = len(self.dfas)
@@ -64,6 +70,27 @@ class DFASet:
                                           ctypes.byref(h))
         _lib.check(rc, "trex_dfa_set_create")
         self._h = h
+        if kgram is not None:
+            ks = [kgram] * n if isinstance(kgram, int) else list(kgram)
+            for i, k in enumerate(ks):
+                if k == 0 and self.kgram_max(i) == 1:
+                    continue
+                self.set_kgram(i, k)
+
+    def kgram_max(self, index: int) -> int:
+        """Largest K-gram width automaton `index` allows (1: byte walks only)."""
+        k = ctypes.c_int()
+        _lib.check(self.lib.trex_dfa_kgram_max(self._h, index, ctypes.byref(k)), "trex_dfa_kgram_max")
+        return k.value
+
+    def set_kgram(self, index: int, k: int) -> None:
+        """K-gram width of automaton `index` (1 = bytes, 2/4/8, 0 = largest); between runs."""
+        _lib.check(self.lib.trex_dfa_set_kgram(self._h, index, k), "trex_dfa_set_kgram")
+
+    def get_kgram(self, index: int) -> int:
+        k = ctypes.c_int()
+        _lib.check(self.lib.trex_dfa_get_kgram(self._h, index, ctypes.byref(k)), "trex_dfa_get_kgram")
+        return k.value
 
     @property
     def handle(self):
