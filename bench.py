@@ -77,6 +77,9 @@ def parse_args():
     ap.add_argument("--kgram", type=int, default=None,
                     help="K-gram width of every automaton of a DFA workload (0 = the largest each "
                          "allows; default: byte walks, or the tuned choice with --tuned)")
+    ap.add_argument("--tuned", action="store_true",
+                    help="DFA workloads: run the autotuner (K-gram width per automaton, bytes per "
+                         "work item / scan tile) before the warm-up and report its sweep")
     ap.add_argument("--dfa-sizes", type=str, default=None,
                     help="comma list of DFA state counts replacing the default 5x8,5x12,6x16")
     ap.add_argument("--seed", type=int, default=2024)
@@ -190,6 +193,18 @@ class DFAWorkload:
         self.d_off = torch.from_numpy(self.off).to(dev)
         self.d_ids = torch.from_numpy(self.ids).to(dev)
         self.set = DFASet(self.dfas, kgram=self.args.kgram)
+        self.tune_info = None
+        if self.args.tuned:   # measured on a sample of this batch, before the warm-up
+            from trex_b200.autotune import Autotuner
+            tuner = Autotuner()
+            if self.kind == "scan":
+                tile, sweep = tuner.tune_scan(self.set, 0, self.data, self.d_off)
+                self.args.seg_len = tile
+                self.tune_info = {"scan_tile": tile, "sweep": sweep}
+            else:
+                rep = tuner.tune_batch(self.set, self.data, self.d_off, self.d_ids)
+                self.args.seg_len = rep.seg_len
+                self.tune_info = rep.as_dict()
         self.kgram_used = [self.set.get_kgram(i) for i in range(len(self.dfas))]
         n = self.n
         if self.kind == "scan":
@@ -940,6 +955,8 @@ def trex_arm(args, rank, world, local_rank):
         line = base_line(args, wl, value, ms_per_step, args.steps, warm, world)
         line["config"] = {**wl.config(), "parallelism": f"dp{world} (independent shards, no collective)"}
         line["roofline"] = roof
+        if getattr(wl, "tune_info", None) is not None:
+            line["autotune"] = wl.tune_info
         if hasattr(wl, "exact_mismatches"):
             from oracle import oracle as orc
             orc.build()

@@ -62,11 +62,12 @@ _ALL_CONFIGS = (None, "auto") + _CPU_CONFIGS + _REF_GPU_CONFIGS + _OWN_GPU_CONFI
 class _DfaEngine:
     """A DFA on the B200 ragged batch kernel (trex_dfa_batch_host)."""
 
-    def __init__(self, bdfa: ByteDFA, unknown_byte: Optional[int]):
+    def __init__(self, bdfa: ByteDFA, unknown_byte: Optional[int], kgram: int = 1):
         from .engine import DFASet
         self.bdfa = bdfa
         self.unknown_byte = unknown_byte
-        self.set = DFASet([bdfa])
+        self.set = DFASet([bdfa], kgram=kgram)
+        self.kgram = self.set.get_kgram(0)
 
     def _pack(self, strings):
         from ._batching import pack_strings
@@ -193,15 +194,15 @@ class OptimizedEngine:
     def _dfa_states(self) -> int:
         return self._bdfa.n_states if self._bdfa is not None else self._dfa.n_states
 
-    def _setup_gpu_dfa(self, backend: str, reason: str):
+    def _setup_gpu_dfa(self, backend: str, reason: str, kgram: int = 1):
         if self._bdfa is None:
             self._bdfa, unknown = _byte_dfa_from_dfa(self._dfa)
         else:
             unknown = None
-        self._gpu = _DfaEngine(self._bdfa, unknown)
+        self._gpu = _DfaEngine(self._bdfa, unknown, kgram)
         self._representation = "dfa"
         self._scan_backend = backend
-        self._kgram_k = 1
+        self._kgram_k = self._gpu.kgram
         self._selection_reason = reason
 
     def _setup_gpu_nfa(self, reason: str):
@@ -299,7 +300,11 @@ class OptimizedEngine:
             self._ref_gpu = PrefixComposeGPUSimulator().create_engine(
                 self._dm, max_total_chars=1 << 29, max_batch=1 << 19)
             self._selection_reason = f"GPU prefix compose (N={self._dm.n_states})"
-        else:   # batched+gpu, kgram+gpu, fp16_tc+gpu: the reference's WMMA engines
+        elif config == "kgram+gpu":   # K-gram walking, the largest width the automaton allows
+            self._setup_gpu_dfa(config, "config='kgram+gpu': B200 ragged batch DFA kernel with K-gram "
+                                        "walking (largest K the alphabet allows; K=1 when none)", kgram=0)
+            return
+        else:   # batched+gpu, fp16_tc+gpu: the reference's WMMA engines
             self._setup_gpu_dfa(config, f"config={config!r}: the reference's WMMA engine is not "
                                         f"rebuilt; B200 ragged batch DFA kernel (byte map, K=1)")
             return
