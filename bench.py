@@ -76,10 +76,13 @@ def parse_args():
     ap.add_argument("--seg-len", type=int, default=0, help="bytes per work item / scan tile (0 = default)")
     ap.add_argument("--kgram", type=int, default=None,
                     help="K-gram width of every automaton of a DFA workload (0 = the largest each "
-                         "allows; default: byte walks, or the tuned choice with --tuned)")
-    ap.add_argument("--tuned", action="store_true",
-                    help="DFA workloads: run the autotuner (K-gram width per automaton, bytes per "
-                         "work item / scan tile) before the warm-up and report its sweep")
+                         "allows; overrides the tuned choice)")
+    ap.add_argument("--no-tune", dest="tuned", action="store_false",
+                    help="DFA workloads: skip the autotuner (by default it picks the K-gram width "
+                         "per automaton and the bytes per work item / scan tile on a sample of the "
+                         "batch before the warm-up, outside the timed region, and the line reports "
+                         "its sweep)")
+    ap.set_defaults(tuned=True)
     ap.add_argument("--dfa-sizes", type=str, default=None,
                     help="comma list of DFA state counts replacing the default 5x8,5x12,6x16")
     ap.add_argument("--seed", type=int, default=2024)
@@ -205,6 +208,10 @@ class DFAWorkload:
                 rep = tuner.tune_batch(self.set, self.data, self.d_off, self.d_ids)
                 self.args.seg_len = rep.seg_len
                 self.tune_info = rep.as_dict()
+                if self.args.kgram is not None:   # an explicit width wins over the tuned one
+                    for i in range(len(self.dfas)):
+                        if self.args.kgram != 0 or self.set.kgram_max(i) > 1:
+                            self.set.set_kgram(i, self.args.kgram)
         self.kgram_used = [self.set.get_kgram(i) for i in range(len(self.dfas))]
         n = self.n
         if self.kind == "scan":

@@ -70,9 +70,12 @@ struct ScratchLayout {
     int64_t max_items;
 };
 
+// Bytes per work item: at least 64, a multiple of 32 (item cuts fall on window
+// boundaries).
 static int32_t effective_seg_len(int32_t seg_len) {
     if (seg_len <= 0) seg_len = kDefaultSegLen;
-    return seg_len < 64 ? 64 : seg_len;
+    seg_len = seg_len < 64 ? 64 : seg_len;
+    return (int32_t)std::min<int64_t>(((int64_t)seg_len + 31) & ~(int64_t)31, 1 << 30);
 }
 
 static ScratchLayout scratch_layout(int64_t n_strings, int64_t total_bytes, int32_t seg_len) {
@@ -98,20 +101,34 @@ static ScratchLayout scratch_layout(int64_t n_strings, int64_t total_bytes, int3
 }
 
 // ---- planning kernels -------------------------------------------------------------
-// Items of one string: its bytes are cut into pieces of seg bytes (seg grows
-// for strings that would need more than kMaxItemsPerString pieces); strings of
-// automata with more than 16 states are never cut.
-__device__ __forceinline__ uint32_t n_items_of(int64_t len, int n_states, int32_t seg_len,
-                                               int64_t *seg_out) {
-    if (len <= 0 || n_states > kSmallDfaStates) {
-        *seg_out = len;
-        return 1;
-    }
+// Items of one string, which starts at byte s0 of the batch (base_mis: the
+// address of the batch's first byte mod 32). The cuts fall on 32-byte aligned
+// addresses: the first item is seg bytes plus up to 31 up to the next aligned
+// address, the others seg bytes (a multiple of 32), the last the rest; so an
+// item after the first starts its warm-up, its own bytes and (but the last) its
+// end on window boundaries. seg grows for strings that would need more than
+// kMaxItemsPerString items; strings of automata with more than 16 states are
+// never cut.
+struct ItemGeom {
+    uint32_t k;
+    int64_t seg, first;
+};
+__device__ __forceinline__ ItemGeom item_geom(int64_t len, int64_t s0, int n_states, int32_t seg_len,
+                                              uint32_t base_mis) {
+    if (len <= 0 || n_states > kSmallDfaStates) return ItemGeom{1, len, len};
     int64_t seg = seg_len;
     if ((len + seg - 1) / seg > kMaxItemsPerString)
-        seg = (len + kMaxItemsPerString - 1) / kMaxItemsPerString;
-    *seg_out = seg;
-    return (uint32_t)((len + seg - 1) / seg);
+        seg = (((len + kMaxItemsPerString - 1) / kMaxItemsPerString) + 31) & ~(int64_t)31;
+    const int64_t pad = (int64_t)((32u - ((base_mis + (uint32_t)s0) & 31u)) & 31u);
+    const int64_t first = seg + pad;
+    if (len <= first) return ItemGeom{1, seg, len};
+    return ItemGeom{(uint32_t)(1 + (len - first + seg - 1) / seg), seg, first};
+}
+// Bytes [b0, b1) of item j of a string (s0, len).
+__device__ __forceinline__ void item_range(const ItemGeom &g, int64_t s0, int64_t len, uint32_t j,
+                                           int64_t *b0, int64_t *b1) {
+    *b0 = j == 0 ? s0 : s0 + g.first + (int64_t)(j - 1) * g.seg;
+    *b1 = (j + 1 == g.k) ? s0 + len : (j == 0 ? s0 + g.first : *b0 + g.seg);
 }
 
 // Queue order of an item by the bytes it walks (warm-up included), longest
@@ -131,11 +148,11 @@ __device__ __forceinline__ int len_class(int64_t len) {
 struct ItemClasses {
     int first, mid, last;
 };
-__device__ __forceinline__ ItemClasses item_classes(int64_t len, uint32_t k, int64_t seg) {
-    const int64_t warm = seg < kWarmBytes ? seg : (int64_t)kWarmBytes;
-    if (k == 1) return ItemClasses{0, 0, len_class(len)};
-    return ItemClasses{len_class(seg), len_class(seg + warm),
-                       len_class(len - (int64_t)(k - 1) * seg + warm)};
+__device__ __forceinline__ ItemClasses item_classes(int64_t len, const ItemGeom &g) {
+    const int64_t warm = g.seg < kWarmBytes ? g.seg : (int64_t)kWarmBytes;
+    if (g.k == 1) return ItemClasses{0, 0, len_class(len)};
+    return ItemClasses{len_class(g.first), len_class(g.seg + warm),
+                       len_class(len - g.first - (int64_t)(g.k - 2) * g.seg + warm)};
 }
 
 // Returns the DFA index of string i, or -1 (and raises an error bit) when the
@@ -188,7 +205,7 @@ __device__ __forceinline__ uint32_t warp_rank(uint32_t *cnt, bool pred, int key)
 // in the warp-level aggregation.
 __global__ void plan_count_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n,
                                   int64_t total_bytes, const DfaDesc *desc, int n_dfas,
-                                  int32_t seg_len, uint32_t *cls_count,
+                                  int32_t seg_len, uint32_t base_mis, uint32_t *cls_count,
                                   unsigned long long *q_bytes, unsigned long long *n_items,
                                   uint32_t *err) {
     __shared__ uint32_t cnt[kMaxDfasPerSet * kLenClasses];
@@ -201,13 +218,14 @@ __global__ void plan_count_kernel(const int64_t *offsets, const int32_t *dfa_id,
     __syncthreads();
     for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x; i0 < n; i0 += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = i0 + threadIdx.x;
-        int64_t len = 0, seg = 0;
-        int d = i < n ? checked_dfa(offsets, dfa_id, i, n_dfas, total_bytes, err, &len) : -1;
+        int64_t len = 0, s0 = 0;
+        int d = i < n ? checked_dfa(offsets, dfa_id, i, n_dfas, total_bytes, err, &len, &s0) : -1;
         uint32_t k = 0;
         ItemClasses ic{0, 0, 0};
         if (d >= 0) {
-            k = n_items_of(len, desc[d].n_states, seg_len, &seg);
-            ic = item_classes(len, k, seg);
+            const ItemGeom g = item_geom(len, s0, desc[d].n_states, seg_len, base_mis);
+            k = g.k;
+            ic = item_classes(len, g);
         }
         const int kb = d * kLenClasses;
         warp_count(cnt, d >= 0 && k > 1, kb + ic.first);
@@ -280,9 +298,9 @@ __global__ void plan_scan_kernel(uint32_t *cls_count, uint32_t *cls_cursor, uint
 // (DFA, length class) and ranks come from shared-memory atomics.
 __global__ void __launch_bounds__(kPlanThreads)
 plan_fill_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n, int64_t total_bytes,
-                 const DfaDesc *desc, int n_dfas, int32_t seg_len, uint32_t *cls_cursor,
-                 uint32_t *map_cursor, WorkItem *items, int64_t max_items, uint32_t *str_map,
-                 uint32_t *err) {
+                 const DfaDesc *desc, int n_dfas, int32_t seg_len, uint32_t base_mis,
+                 uint32_t *cls_cursor, uint32_t *map_cursor, WorkItem *items, int64_t max_items,
+                 uint32_t *str_map, uint32_t *err) {
     __shared__ uint32_t s_cnt[kMaxDfasPerSet * kLenClasses];
     __shared__ uint32_t s_base[kMaxDfasPerSet * kLenClasses];
     __shared__ uint32_t s_map, s_map_base;
@@ -294,13 +312,15 @@ plan_fill_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n, int64
     for (int64_t tile = blockIdx.x; tile * kPlanThreads < n; tile += gridDim.x) {
         const int64_t i = tile * kPlanThreads + threadIdx.x;
         int d = -1;
-        int64_t len = 0, seg = 0, s0 = 0;
+        int64_t len = 0, s0 = 0;
         uint32_t k = 0, r0 = 0, rm = 0, r_last = 0, r_map = 0;
         ItemClasses ic{0, 0, 0};
+        ItemGeom g{0, 0, 0};
         if (i < n) d = checked_dfa(offsets, dfa_id, i, n_dfas, total_bytes, err, &len, &s0);
         if (d >= 0) {
-            k = n_items_of(len, desc[d].n_states, seg_len, &seg);
-            ic = item_classes(len, k, seg);
+            g = item_geom(len, s0, desc[d].n_states, seg_len, base_mis);
+            k = g.k;
+            ic = item_classes(len, g);
             ic.first += d * kLenClasses;
             ic.mid += d * kLenClasses;
             ic.last += d * kLenClasses;
@@ -329,7 +349,7 @@ plan_fill_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n, int64
         __syncthreads();
         if (d >= 0) {
             const uint32_t mb = k > 1 ? s_map_base + r_map : 0u;
-            const uint32_t warm = (uint32_t)(seg < kWarmBytes ? seg : (int64_t)kWarmBytes);
+            const uint32_t warm = (uint32_t)(g.seg < kWarmBytes ? g.seg : (int64_t)kWarmBytes);
             // With the counts of plan_count_kernel every position and map slot is
             // below max_items; offsets rewritten between the two planning kernels
             // (a caller changing inputs in flight) could break that: refuse.
@@ -346,8 +366,8 @@ plan_fill_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n, int64
                     atomicOr(err, kErrCapacity);
                     continue;
                 }
-                const int64_t b0 = s0 + (int64_t)j * seg;
-                const int64_t b1 = (j + 1 == k) ? s0 + len : b0 + seg;
+                int64_t b0, b1;
+                item_range(g, s0, len, j, &b0, &b1);
                 items[pos] = (j == 0)
                     ? WorkItem{b0, b1, (uint32_t)i, j | (k << 16), mb, (uint32_t)desc[d].start}
                     : WorkItem{b0 - warm, b1, (uint32_t)i, j | (k << 16), mb, warm << 8};
@@ -383,6 +403,7 @@ struct RaggedParams {
     const int32_t *dfa_id;
     int64_t n;
     int64_t max_items;
+    uint32_t base_mis;
     uint8_t *final_state;
     uint8_t *accept;
     int32_t *accept_i32;
@@ -756,13 +777,15 @@ __global__ void __launch_bounds__(kComposeThreads) compose_kernel(RaggedParams P
     for (int64_t base = ((int64_t)blockIdx.x * (kComposeThreads / 32) + wib) * 32; base < P.n;
          base += nwarps * 32) {
         const int64_t i = base + lane;
-        int64_t len = 0, s0 = 0, seg = 0;
+        int64_t len = 0, s0 = 0;
         const int d = i < P.n ? checked_dfa(P.offsets, P.dfa_id, i, P.n_dfas, P.total_bytes, P.err,
                                             &len, &s0)
                               : -1;
         uint32_t k = 0, mb = 0;
+        ItemGeom g{0, 0, 0};
         if (d >= 0) {
-            k = n_items_of(len, P.desc[d].n_states, P.seg_len, &seg);
+            g = item_geom(len, s0, P.desc[d].n_states, P.seg_len, P.base_mis);
+            k = g.k;
             if (k > 1) {
                 mb = P.str_map[i];
                 if ((int64_t)mb + (int64_t)k > P.max_items) {   // offsets changed since the plan
@@ -800,7 +823,7 @@ __global__ void __launch_bounds__(kComposeThreads) compose_kernel(RaggedParams P
             const uint32_t sk = __shfl_sync(FULL, k, src), smb = __shfl_sync(FULL, mb, src);
             const uint32_t sj = __shfl_sync(FULL, jbad, src), s_entry = __shfl_sync(FULL, st, src);
             const int64_t ss0 = __shfl_sync(FULL, s0, src), slen = __shfl_sync(FULL, len, src);
-            const int64_t sseg = __shfl_sync(FULL, seg, src);
+            const ItemGeom sg{sk, __shfl_sync(FULL, g.seg, src), __shfl_sync(FULL, g.first, src)};
             const DfaDesc D = P.desc[sd];
             const uint32_t N = (uint32_t)D.n_states;
             auto rewalk = [&](uint32_t jb, uint32_t s_in) {
@@ -811,8 +834,8 @@ __global__ void __launch_bounds__(kComposeThreads) compose_kernel(RaggedParams P
                     __syncwarp();
                     tbl_dfa = sd;
                 }
-                const int64_t b0 = ss0 + (int64_t)jb * sseg;
-                const int64_t b1 = (jb + 1 == sk) ? ss0 + slen : b0 + sseg;
+                int64_t b0, b1;
+                item_range(sg, ss0, slen, jb, &b0, &b1);
                 return warp_rewalk(tbl, N, P.data, b0, b1, s_in);
             };
             uint32_t s = s_entry < N ? rewalk(sj, s_entry) : 0xffu;
@@ -914,6 +937,7 @@ int dfa_set_run(trex_dfa_set *set, const uint8_t *data, const int64_t *offsets,
     WorkItem *items = reinterpret_cast<WorkItem *>(sc + L.items);
     uint32_t *maps = reinterpret_cast<uint32_t *>(sc + L.maps);
     uint32_t *str_map = reinterpret_cast<uint32_t *>(sc + L.str_map);
+    const uint32_t base_mis = (uint32_t)((uintptr_t)data & 31u);
 
     // Counters, bases, heads, cursors, byte counts, the error word, the map
     // cursor and the item count are contiguous at the front of the scratch buffer.
@@ -921,14 +945,14 @@ int dfa_set_run(trex_dfa_set *set, const uint8_t *data, const int64_t *offsets,
     int plan_grid = (int)std::min<int64_t>((n + kPlanThreads - 1) / kPlanThreads,
                                            (int64_t)set->n_sms * 8);
     plan_count_kernel<<<plan_grid, kPlanThreads, 0, stream>>>(
-        offsets, dfa_id, n, total_bytes, set->d_desc, set->n_dfas, seg_len, cls_count, q_bytes,
-        n_items, err);
+        offsets, dfa_id, n, total_bytes, set->d_desc, set->n_dfas, seg_len, base_mis, cls_count,
+        q_bytes, n_items, err);
     TREX_CHECK_LAUNCH();
     plan_scan_kernel<<<1, kMaxDfasPerSet, 0, stream>>>(cls_count, cls_cursor, q_base, q_count, set->n_dfas,
                                            n_items, L.max_items, err);
     TREX_CHECK_LAUNCH();
     plan_fill_kernel<<<plan_grid, kPlanThreads, 0, stream>>>(
-        offsets, dfa_id, n, total_bytes, set->d_desc, set->n_dfas, seg_len, cls_cursor,
+        offsets, dfa_id, n, total_bytes, set->d_desc, set->n_dfas, seg_len, base_mis, cls_cursor,
         map_cursor, items, L.max_items, str_map, err);
     TREX_CHECK_LAUNCH();
 
@@ -954,6 +978,7 @@ int dfa_set_run(trex_dfa_set *set, const uint8_t *data, const int64_t *offsets,
     P.dfa_id = dfa_id;
     P.n = n;
     P.max_items = L.max_items;
+    P.base_mis = base_mis;
     P.final_state = final_state;
     P.accept = accept;
     P.accept_i32 = accept_i32;
