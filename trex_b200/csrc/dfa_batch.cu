@@ -8,27 +8,25 @@
 //
 // Design
 //  * Planning kernels cut every string into work items of at most seg_len
-//    bytes, bucket them by DFA (one CTA serves one DFA at a time) and, inside
-//    a DFA, order them by length class, longest first, so queues drain on
-//    short items. Queue slots are reserved per tile of strings with one
-//    global atomic per (DFA, class).
+//    bytes, the cuts on 32-byte aligned addresses, queue them by DFA (one CTA
+//    serves one DFA at a time) and, inside a DFA, by the bytes they walk in
+//    64 length classes, longest first. Queue slots are reserved per tile of
+//    strings with one global atomic per (DFA, class).
 //  * Speculative entry states: an item other than the first of its string
-//    does not know its entry state. It starts kWarmBytes earlier, inside the
-//    previous item, from state 0; for a synchronising DFA (random DFAs merge
-//    two chains with probability ~1/N per byte) the chain has then reached
-//    the true entry state. The item records that guess next to its end
-//    state; the last item of the string to finish composes the string
-//    (start -> end of item 0 -> ...), and wherever the true state differs
-//    from an item's guess it re-walks that item exactly. Results are exact
-//    for every DFA; only non-synchronising DFAs pay for re-walks.
+//    does not know its entry state. It starts warm_bytes(N) earlier, inside
+//    the previous item, from state 0; for a synchronising DFA (random DFAs
+//    merge two chains with probability ~1/N per byte) the chain has then
+//    reached the true entry state. The item records that guess next to its
+//    end state; compose_kernel chains each string's records and re-walks, with
+//    a whole warp, any item whose guess was wrong. Results are exact for every
+//    DFA; only non-synchronising DFAs pay for re-walks.
 //  * Main kernel: one persistent 1024-thread CTA per SM. The CTA expands the
-//    current DFA's byte map into a per-lane replicated shared-memory table
-//    (dfa_walk.cuh) so table lookups never conflict on banks. Each lane owns
-//    one item and the warp advances in lock step over 32-byte windows; edge
-//    windows apply bytes under a per-lane mask. Each lane holds the record of
-//    its next item (fetched one iteration ahead with a warp-aggregated atomic)
-//    and the next input window (across item boundaries), so refills do not
-//    stall the warp. No spin-waits anywhere.
+//    current DFA's byte map (or its K-gram tables) into a per-lane replicated
+//    shared-memory table (dfa_walk.cuh) so table lookups never conflict on
+//    banks. A warp walks 32 items of a queue together (their lengths match to
+//    128 bytes), one 32-byte window per lane per step with the next window
+//    loaded ahead; only a batch's first and last windows and warm-up capture
+//    windows apply bytes under a per-lane mask. No spin-waits anywhere.
 #include <algorithm>
 #include <cstring>
 #include <mutex>
@@ -49,7 +47,14 @@ struct WorkItem {
 };
 constexpr int64_t kMaxItemsPerString = 65535;
 constexpr int64_t kMaxWalkBytes = (int64_t)1 << 36;   // one item: a 32-bit count of windows
-constexpr int kWarmBytes = 128;
+// Warm-up bytes of an item after the first of its string: two chains of a
+// random N-state automaton merge with probability ~1/N per byte, so 32 bytes
+// per 4 states keep the miss rate near (1 - 1/N)^(8N) ~ 3e-4 (a multiple of 32,
+// which keeps aligned cuts aligned).
+__host__ __device__ __forceinline__ int64_t warm_bytes(int n_states, int64_t seg) {
+    const int64_t w = 32 * (int64_t)((n_states + 3) / 4);
+    return w < seg ? w : seg;
+}
 
 // Error bits reported through the device error word.
 enum : uint32_t {
@@ -148,8 +153,8 @@ __device__ __forceinline__ int len_class(int64_t len) {
 struct ItemClasses {
     int first, mid, last;
 };
-__device__ __forceinline__ ItemClasses item_classes(int64_t len, const ItemGeom &g) {
-    const int64_t warm = g.seg < kWarmBytes ? g.seg : (int64_t)kWarmBytes;
+__device__ __forceinline__ ItemClasses item_classes(int64_t len, const ItemGeom &g, int n_states) {
+    const int64_t warm = warm_bytes(n_states, g.seg);
     if (g.k == 1) return ItemClasses{0, 0, len_class(len)};
     return ItemClasses{len_class(g.first), len_class(g.seg + warm),
                        len_class(len - g.first - (int64_t)(g.k - 2) * g.seg + warm)};
@@ -225,7 +230,7 @@ __global__ void plan_count_kernel(const int64_t *offsets, const int32_t *dfa_id,
         if (d >= 0) {
             const ItemGeom g = item_geom(len, s0, desc[d].n_states, seg_len, base_mis);
             k = g.k;
-            ic = item_classes(len, g);
+            ic = item_classes(len, g, desc[d].n_states);
         }
         const int kb = d * kLenClasses;
         warp_count(cnt, d >= 0 && k > 1, kb + ic.first);
@@ -320,7 +325,7 @@ plan_fill_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n, int64
         if (d >= 0) {
             g = item_geom(len, s0, desc[d].n_states, seg_len, base_mis);
             k = g.k;
-            ic = item_classes(len, g);
+            ic = item_classes(len, g, desc[d].n_states);
             ic.first += d * kLenClasses;
             ic.mid += d * kLenClasses;
             ic.last += d * kLenClasses;
@@ -349,7 +354,7 @@ plan_fill_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n, int64
         __syncthreads();
         if (d >= 0) {
             const uint32_t mb = k > 1 ? s_map_base + r_map : 0u;
-            const uint32_t warm = (uint32_t)(g.seg < kWarmBytes ? g.seg : (int64_t)kWarmBytes);
+            const uint32_t warm = (uint32_t)warm_bytes(desc[d].n_states, g.seg);
             // With the counts of plan_count_kernel every position and map slot is
             // below max_items; offsets rewritten between the two planning kernels
             // (a caller changing inputs in flight) could break that: refuse.
