@@ -49,6 +49,8 @@ import numpy as np
 REPO = Path(__file__).resolve().parent
 sys.path.insert(0, str(REPO))
 
+from trex_b200.sharding import max_over_ranks, rank_seed  # noqa: E402
+
 METRIC = "Gchar/s vs HBM roofline, plain vs batched/served; served p50/p99 ms (1 B200)"
 SUB_ALPHABET = b"ACGT"
 
@@ -285,10 +287,7 @@ class DFAWorkload:
         for _ in range(steps):
             self.set.run_host(hd, ho, hi, self.args.seg_len, hf, ha)
         dt = time.perf_counter() - t0
-        if dist:
-            t = torch.tensor([dt], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            dt = float(t.item())
+        dt = max_over_ranks(dt, dist, dev)
         if not (np.array_equal(hf, self.fs.cpu().numpy()) and np.array_equal(ha, self.ac.cpu().numpy())):
             raise RuntimeError("host-buffer run disagrees with the device run")
         self.host_data = hd
@@ -401,10 +400,7 @@ class NFAWorkload:
         for _ in range(steps):
             _lib.check(L.nfa_tc_engine_dispatch(*args), "nfa_tc_engine_dispatch")
         dt = time.perf_counter() - t0
-        if dist:
-            t = torch.tensor([dt], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            dt = float(t.item())
+        dt = max_over_ranks(dt, dist, dev)
         L.nfa_tc_engine_destroy()
         if not np.array_equal(hr.astype(np.uint8), self.ac.cpu().numpy()):
             raise RuntimeError("host-buffer run disagrees with the device run")
@@ -519,10 +515,7 @@ class PNFAWorkload:
         for _ in range(steps):
             one()
         dt = time.perf_counter() - t0
-        if dist:
-            t = torch.tensor([dt], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            dt = float(t.item())
+        dt = max_over_ranks(dt, dist, dev)
         if not np.array_equal(h_ll.numpy(), self.ll.cpu().numpy()):
             raise RuntimeError("host-buffer run disagrees with the device run")
         return dt, int(self.total + self.off.nbytes), int(h_ll.numpy().nbytes)
@@ -877,7 +870,7 @@ def trex_arm(args, rank, world, local_rank):
     dist = None
     if world > 1:
         import torch.distributed as dist
-    seed = args.seed + 7919 * rank
+    seed = rank_seed(args.seed, rank)
     wl = make_workload(args)
     wl.setup(torch, dev, seed)
     stream = torch.cuda.current_stream(dev)
@@ -913,10 +906,7 @@ def trex_arm(args, rank, world, local_rank):
     if wl.error_word() != 0:
         raise RuntimeError("device reported an error during the timed steps")
     ms = ev0.elapsed_time(ev1)
-    if dist:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist, dev)
     ms_per_step = ms / args.steps
     chars_all = wl.chars * world
     value = chars_all / (ms_per_step * 1e-3) / 1e9
