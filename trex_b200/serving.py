@@ -35,7 +35,7 @@ from __future__ import annotations
 import collections
 import threading
 import time
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 from typing import Optional, Sequence
 
 import numpy as np
@@ -43,8 +43,15 @@ import numpy as np
 KINDS = ("dfa", "nfa", "pnfa")
 
 
-@dataclass
+@dataclass(slots=True)
 class Request:
+    """One match request. The server sets result (or error) and then t_done;
+    ``done`` is true from then on (Server.wait blocks until requests are done).
+    A request holds no lock or event of its own: under load the process
+    creates thousands of them a second, and every object the garbage
+    collector tracks lengthens its full passes (which showed up as p99
+    latency spikes of tens of milliseconds)."""
+
     rid: int
     kind: str
     engine: int
@@ -53,7 +60,10 @@ class Request:
     t_done: float = 0.0
     result: object = None
     error: Optional[str] = None
-    done: threading.Event = field(default_factory=threading.Event)
+
+    @property
+    def done(self) -> bool:
+        return self.t_done > 0.0 or self.error is not None
 
     @property
     def latency_ms(self) -> float:
@@ -151,7 +161,8 @@ class Server:
 
     def __init__(self, dfas=(), nfas=(), pnfas=(), *, hbm_budget: int = 1 << 30,
                  max_batch_requests: int = 1 << 14, pnfa_mode: str = "bf16", use_graphs: bool = True,
-                 device: int = 0, pnfa_auto_threshold: int = 2048):
+                 device: int = 0, pnfa_auto_threshold: int = 2048, precapture: bool = True,
+                 gc_freeze: bool = True):
         import torch
         from .engine import NFA, PNFA, DFASet
         self.torch = torch
@@ -193,16 +204,41 @@ class Server:
             self.dfa_set.run(s0.d_data[:1], s0.d_doff[:2], s0.d_ids[:1], final_state=s0.d_fs,
                              accept=s0.d_ac, scratch=s0.d_scratch, stream=s0.stream)
             s0.stream.synchronize()
+        if self.use_graphs and precapture:
+            # every size bucket's graph up front: a capture in the serving loop would stall
+            # the requests behind it
+            for s in self.slots:
+                if s.lane != "fast":
+                    continue
+                nb = 64
+                while True:
+                    bb = 1 << 16
+                    while True:
+                        self._graph(s, nb, bb)
+                        if bb >= self.max_bytes:
+                            break
+                        bb = min(bb * 2, self.max_bytes)
+                    if nb >= self.max_requests:
+                        break
+                    nb = min(nb * 2, self.max_requests)
+            torch.cuda.synchronize(self.dev)
         self._queues = {"fast": collections.deque(), "pnfa": collections.deque()}
         self._cv = threading.Condition()
+        self._fin = threading.Condition()   # notified when a batch's requests are done
+        self._lat = {k: [] for k in KINDS}   # latencies (ms) since reset_stats: plain floats
         self._next = 0
         self._stop = False
-        self._completed: list = []
         self._bytes_done = 0
         self._batches = 0
         self._t_first = None
         self._t_last = None
         self._error: Optional[BaseException] = None
+        if gc_freeze:
+            # the tables, buffers and graphs built above live as long as the server: move
+            # them (and everything else alive now) out of the collector's passes
+            import gc
+            gc.collect()
+            gc.freeze()
         self._thread = threading.Thread(target=self._loop, name="trex-serve", daemon=True)
         self._thread.start()
 
@@ -254,9 +290,14 @@ class Server:
 
     def wait(self, reqs: Sequence[Request], timeout: float = 60.0) -> list:
         end = time.perf_counter() + timeout
+        with self._fin:
+            for r in reqs:
+                while not r.done:
+                    left = end - time.perf_counter()
+                    if left <= 0:
+                        raise TimeoutError(f"request {r.rid} not served in time")
+                    self._fin.wait(min(left, 0.5))
         for r in reqs:
-            if not r.done.wait(max(0.0, end - time.perf_counter())):
-                raise TimeoutError(f"request {r.rid} not served in time")
             if r.error:
                 raise RuntimeError(r.error)
         return [r.result for r in reqs]
@@ -265,23 +306,24 @@ class Server:
         """Requests, batches, bytes, throughput over the serving span and latency
         percentiles (ms), overall and per kind."""
         with self._cv:
-            done = list(self._completed)
+            lat = {k: np.array(v, dtype=np.float64) for k, v in self._lat.items()}
             span = (self._t_last - self._t_first) if self._t_first and self._t_last else 0.0
             nbytes, nb = self._bytes_done, self._batches
 
-        def pct(rs):
-            lat = np.array([r.latency_ms for r in rs]) if rs else np.zeros(1)
-            return {"n": len(rs), "p50_ms": float(np.percentile(lat, 50)),
-                    "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean())}
+        def pct(a):
+            x = a if a.size else np.zeros(1)
+            return {"n": int(a.size), "p50_ms": float(np.percentile(x, 50)),
+                    "p99_ms": float(np.percentile(x, 99)), "mean_ms": float(x.mean())}
 
-        out = {"requests": len(done), "batches": nb, "bytes": nbytes,
-               "gchar_s": nbytes / span / 1e9 if span > 0 else 0.0, **pct(done)}
-        out["by_kind"] = {k: pct([r for r in done if r.kind == k]) for k in KINDS}
+        allv = np.concatenate(list(lat.values()))
+        out = {"requests": int(allv.size), "batches": nb, "bytes": nbytes,
+               "gchar_s": nbytes / span / 1e9 if span > 0 else 0.0, **pct(allv)}
+        out["by_kind"] = {k: pct(v) for k, v in lat.items()}
         return out
 
     def reset_stats(self):
         with self._cv:
-            self._completed = []
+            self._lat = {k: [] for k in KINDS}
             self._bytes_done = 0
             self._batches = 0
             self._t_first = self._t_last = None
@@ -334,7 +376,8 @@ class Server:
                     q.clear()
             for r in pending:
                 r.error = f"server loop failed: {e!r}"
-                r.done.set()
+            with self._fin:
+                self._fin.notify_all()
 
     def _dfa_part(self, s: _Slot, nd: int, dfa_bytes: int):
         torch = self.torch
@@ -356,6 +399,13 @@ class Server:
         # padding: empty strings on automaton 0 after the last real one
         s.h_doff[nd + 1:nb + 1] = int(s.h_doff[nd])
         s.h_ids[nd:nb] = 0
+        g = self._graph(s, nb, bb)
+        with torch.cuda.stream(s.stream):
+            g.replay()
+
+    def _graph(self, s: _Slot, nb: int, bb: int):
+        """The captured DFA part of slot s for nb strings and bb bytes (captured once)."""
+        torch = self.torch
         key = (nb, bb)
         g = s.graphs.get(key)
         if g is None:
@@ -370,8 +420,7 @@ class Server:
                 s.h_fs[:nb].copy_(s.d_fs[:nb], non_blocking=True)
                 s.h_ac[:nb].copy_(s.d_ac[:nb], non_blocking=True)
             s.graphs[key] = g
-        with torch.cuda.stream(s.stream):
-            g.replay()
+        return g
 
     def _launch(self, s: _Slot, batch: list):
         torch = self.torch
@@ -434,13 +483,15 @@ class Server:
                 r.result = (bool(ac2[i - nd]), int(mask[i - nd]) & 0xFFFFFFFFFFFFFFFF)
             else:
                 r.result = (float(ll[i - nd]), bool(ac2[i - nd]))
-            r.t_done = now
         with self._cv:
-            self._completed.extend(s.batch)
+            for r in s.batch:
+                self._lat[r.kind].append((now - r.t_submit) * 1e3)
             self._bytes_done += total
             self._batches += 1
             self._t_last = now
-        for r in s.batch:
-            r.done.set()
+        with self._fin:
+            for r in s.batch:
+                r.t_done = now
+            self._fin.notify_all()
         s.batch = None
         s.meta = None
