@@ -33,9 +33,14 @@ walk) with OpenMP on the host cores, on a bounded sample of the same workload.
 
 from __future__ import annotations
 
-import argparse
-import json
 import os
+
+# Many streams (the serving workload keeps 12): more hardware queues than the default 8, so
+# that independent streams do not serialise. Must be set before CUDA starts.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
+import argparse  # noqa: E402
+import json  # noqa: E402
 import re
 import statistics
 import subprocess

@@ -988,7 +988,14 @@ int dfa_set_run(trex_dfa_set *set, const uint8_t *data, const int64_t *offsets,
     P.accept = accept;
     P.accept_i32 = accept_i32;
     profile_kernel_begin(stream);
-    dfa_ragged_kernel<<<set->n_sms, kRaggedThreads, set->smem_bytes, stream>>>(P);
+    // one CTA per 64 KiB of input (and at least one per automaton the batch may
+    // use), at most one per SM: a small batch (a serving batch) then needs a few
+    // SMs and is not held back by other kernels running beside it; CTAs take
+    // work from the queues, so fewer CTAs just do more
+    const int ragged_grid = (int)std::min<int64_t>(
+        set->n_sms, std::max<int64_t>({(int64_t)1, (total_bytes + (64 << 10) - 1) >> 16,
+                                       std::min<int64_t>(n, set->n_dfas)}));
+    dfa_ragged_kernel<<<ragged_grid, kRaggedThreads, set->smem_bytes, stream>>>(P);
     TREX_CHECK_LAUNCH();
     profile_kernel_end(stream);
     compose_kernel<<<(int)std::min<int64_t>((n + kComposeThreads - 1) / kComposeThreads,

@@ -188,7 +188,9 @@ int nfa_run(trex_nfa *nfa, const uint8_t *data, const int64_t *offsets, int64_t 
     P.head = head;
     P.err = err;
     const size_t smem = nfa->smem ? nfa->table_words * 8 : 0;
-    const int grid = nfa->n_sms;
+    // a thread a string: a few strings need one CTA, so that batches of several
+    // automata launched on separate streams run side by side
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(nfa->n_sms, (n + 31) / 32));
     profile_kernel_begin(stream);
     switch (nfa->B) {
         case 6: nfa_bitpar_kernel<6, true><<<grid, kNfaThreads, smem, stream>>>(P); break;

@@ -41,6 +41,7 @@ from typing import Optional, Sequence
 import numpy as np
 
 KINDS = ("dfa", "nfa", "pnfa")
+kAuxStreams = 4   # extra streams of a fast-lane slot
 
 
 @dataclass(slots=True)
@@ -151,6 +152,13 @@ class _Slot:
         self.h_mask = torch.zeros(max(R, 1), dtype=i64, **pin)
         self.h_ll = torch.zeros(max(R, 1), dtype=f64, **pin)
         self.event = torch.cuda.Event()
+        # automaton groups of a fast-lane batch run side by side on these streams (each
+        # group's kernel is sized by its strings, so a few strings take one SM); the
+        # probabilistic lane runs its groups on its own stream
+        n_aux = kAuxStreams if lane == "fast" else 0
+        self.aux = [torch.cuda.Stream(device=dev) for _ in range(n_aux)]
+        self.aux_ev = [torch.cuda.Event() for _ in range(n_aux)]
+        self.ready = torch.cuda.Event()
         self.graphs = {}
         self.batch = None
         self.meta = None
@@ -162,7 +170,7 @@ class Server:
     def __init__(self, dfas=(), nfas=(), pnfas=(), *, hbm_budget: int = 1 << 30,
                  max_batch_requests: int = 1 << 14, pnfa_mode: str = "bf16", use_graphs: bool = True,
                  device: int = 0, pnfa_auto_threshold: int = 2048, precapture: bool = True,
-                 gc_freeze: bool = True):
+                 gc_freeze: bool = True, nfa_streams: int = kAuxStreams):
         import torch
         from .engine import NFA, PNFA, DFASet
         self.torch = torch
@@ -177,6 +185,12 @@ class Server:
             raise ValueError("pnfa_mode must be bf16, fp16, fp32 or auto")
         self.pnfa_mode = pnfa_mode
         self.pnfa_auto_threshold = pnfa_auto_threshold
+        # Boolean NFA groups of a batch run side by side on up to this many streams.
+        # The process keeps 2 x (1 + kAuxStreams) + 2 streams: CUDA maps streams onto
+        # CUDA_DEVICE_MAX_CONNECTIONS hardware queues (8 by default), and two streams on
+        # one queue serialise, so a serving process should raise it (to 32) before CUDA
+        # starts; otherwise a fast-lane kernel can wait behind a long probabilistic one.
+        self.nfa_streams = max(1, min(kAuxStreams, nfa_streams))
         self.use_graphs = use_graphs and self.dfa_set is not None
         # admission: the budget is split 3:1 between the two lanes, each with two slots;
         # besides its bytes a request holds 8+4+8 B of offsets/ids and 1+1+1+8+8 B of
@@ -446,18 +460,32 @@ class Server:
                 if total > dfa_bytes:
                     s.d_data[dfa_bytes:total].copy_(s.h_data[dfa_bytes:total], non_blocking=True)
                 s.d_roff[:nr + 1].copy_(s.h_roff[:nr + 1], non_blocking=True)
-                for kind, eng, first, cnt in groups:
-                    off = s.d_roff[first:first + cnt + 1]
-                    data = s.d_data[:max(total, 1)]
-                    if kind == "nfa":
-                        self.nfas[eng].run(data, off, final_mask=s.d_mask[first:first + cnt],
-                                           accept=s.d_ac2[first:first + cnt], stream=s.stream)
-                    else:
-                        mode = self.pnfa_mode
-                        if mode == "auto":
-                            mode = "fp32" if cnt < self.pnfa_auto_threshold else "bf16"
-                        self.pnfas[eng].run(data, off, mode, loglik=s.d_ll[first:first + cnt],
-                                            accept=s.d_ac2[first:first + cnt], stream=s.stream)
+                s.ready.record(s.stream)
+            used = set()
+            for gi, (kind, eng, first, cnt) in enumerate(groups):
+                if s.aux:
+                    k = gi % self.nfa_streams
+                    st = s.aux[k]
+                    if k not in used:
+                        st.wait_event(s.ready)
+                        used.add(k)
+                else:
+                    st = s.stream
+                off = s.d_roff[first:first + cnt + 1]
+                data = s.d_data[:max(total, 1)]
+                if kind == "nfa":
+                    self.nfas[eng].run(data, off, final_mask=s.d_mask[first:first + cnt],
+                                       accept=s.d_ac2[first:first + cnt], stream=st)
+                else:
+                    mode = self.pnfa_mode
+                    if mode == "auto":
+                        mode = "fp32" if cnt < self.pnfa_auto_threshold else "bf16"
+                    self.pnfas[eng].run(data, off, mode, loglik=s.d_ll[first:first + cnt],
+                                        accept=s.d_ac2[first:first + cnt], stream=st)
+            for k in used:
+                s.aux_ev[k].record(s.aux[k])
+                s.stream.wait_event(s.aux_ev[k])
+            with torch.cuda.stream(s.stream):
                 s.h_mask[:nr].copy_(s.d_mask[:nr], non_blocking=True)
                 s.h_ll[:nr].copy_(s.d_ll[:nr], non_blocking=True)
                 s.h_ac2[:nr].copy_(s.d_ac2[:nr], non_blocking=True)
