@@ -707,7 +707,7 @@ def serve_arm(args):
                    "parallelism": "1 GPU, continuous batching (2 lanes x 2 slots, "
                                   + ("direct launches)" if args.serve_no_graphs
                                      else "CUDA graphs for DFA batches)"),
-                   "hbm_budget_bytes": 2 << 30, "pnfa_mode": "auto (fp32 below 2048 strings a group)"},
+                   "hbm_budget_bytes": 2 << 30, "pnfa_mode": "auto (BF16 tables on CUDA cores below 2048 strings a group, tcgen05 above)"},
         "served": [{k: r[k] for k in ("offered_req_s", "offered_gchar_s", "gchar_s", "p50_ms", "p99_ms",
                                       "requests", "batches", "by_kind")} for r in runs],
         "plain_per_request": plain,

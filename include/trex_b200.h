@@ -251,7 +251,14 @@ int trex_nfa_error(trex_nfa *nfa, int32_t *err_out);
  * T[c][dst][src] (row-major, sigma x n x n), start[n], accept[n]. Bytes
  * >= sigma are skipped (the reference kernels leave the state unchanged). */
 typedef struct trex_pnfa trex_pnfa;
-enum { TREX_PNFA_BF16 = 0, TREX_PNFA_FP16 = 1, TREX_PNFA_FP32 = 2, TREX_PNFA_BOOL = 3 };
+enum {
+    TREX_PNFA_BF16 = 0,
+    TREX_PNFA_FP16 = 1,
+    TREX_PNFA_FP32 = 2,
+    TREX_PNFA_BOOL = 3,
+    TREX_PNFA_BF16_CC = 4,
+    TREX_PNFA_FP16_CC = 5
+};
 int trex_pnfa_create(int n_states, int sigma, const float *T, const float *start,
                      const float *accept, trex_pnfa **out);
 void trex_pnfa_destroy(trex_pnfa *pnfa);
@@ -265,7 +272,10 @@ void trex_pnfa_destroy(trex_pnfa *pnfa);
  * nonzero entries, and every product is thresholded to {0, 1}
  * (s' = min(T[c] s, 1), exact: operands are 0/1 in BF16, sums are small
  * integers in FP32); accept = some accepting state is active, and loglik is
- * the log of the number of active accepting states. sigma <= 28. DEVICE buffers;
+ * the log of the number of active accepting states. sigma <= 28.
+ * TREX_PNFA_BF16_CC / TREX_PNFA_FP16_CC: CUDA cores with the 16-bit tables in
+ * shared memory and an FP32 state, a warp per string: the low-latency form
+ * for few (possibly long) strings, sigma <= 28. DEVICE buffers;
  * loglik[n] (-inf when the likelihood is 0), accept[n], accept_i32[n]
  * (dot > 0.5) may each be NULL. One run at a time per handle. */
 int trex_pnfa_run(trex_pnfa *pnfa, int mode, const uint8_t *data, const int64_t *offsets,

@@ -22,8 +22,8 @@ from trex_b200.workloads import random_prob_nfa
 
 pytestmark = pytest.mark.gpu
 
-RTOL = {"fp32": 1e-5, "bf16": 1e-4, "fp16": 1e-4}
-U = {"fp32": 1e-7, "bf16": 2.0 ** -8, "fp16": 2.0 ** -11}
+RTOL = {"fp32": 1e-5, "bf16": 1e-4, "fp16": 1e-4, "bf16cc": 1e-4, "fp16cc": 1e-4}
+U = {"fp32": 1e-7, "bf16": 2.0 ** -8, "fp16": 2.0 ** -11, "bf16cc": 2.0 ** -8, "fp16cc": 2.0 ** -11}
 
 
 def _run(torch, T, start, acc, data, off, mode):
@@ -59,7 +59,7 @@ def _check(ll, ac, ref, mode, k, rtol=None):
     assert np.array_equal(ac[clear].astype(bool), (ref > np.log(0.5))[clear])
 
 
-@pytest.mark.parametrize("mode", ["fp32", "bf16", "fp16"])
+@pytest.mark.parametrize("mode", ["fp32", "bf16", "fp16", "bf16cc", "fp16cc"])
 def test_pnfa_ragged_matches_fp64(cuda, oracle, mode):
     rng = np.random.default_rng(7)
     T, start, acc = random_prob_nfa(rng, 64, 20)
@@ -74,7 +74,7 @@ def test_pnfa_ragged_matches_fp64(cuda, oracle, mode):
     _check(ll, ac, ref, mode, _symbols(data, off, 20))
 
 
-@pytest.mark.parametrize("mode", ["fp32", "bf16", "fp16"])
+@pytest.mark.parametrize("mode", ["fp32", "bf16", "fp16", "bf16cc", "fp16cc"])
 def test_pnfa_small_automaton_skips_unknown_bytes(cuda, oracle, mode):
     # 5 states, 7 symbols (odd: the last symbol pair is half empty), bytes >= 7 skipped
     rng = np.random.default_rng(11)
@@ -117,7 +117,7 @@ def test_pnfa_long_uniform_strings_error(cuda, oracle):
     off = np.arange(n + 1, dtype=np.int64) * L
     data = rng.integers(0, 20, size=n * L, dtype=np.uint8)
     ref = oracle.pnfa_fp64(T, start, acc, data, off)
-    for mode in ("bf16", "fp16", "fp32"):
+    for mode in ("bf16", "fp16", "fp32", "bf16cc", "fp16cc"):
         ll, ac, err = _run(cuda, T, start, acc, data, off, mode)
         assert err == 0
         _check(ll, ac, ref, mode, _symbols(data, off, 20), rtol=RTOL[mode])
@@ -137,7 +137,7 @@ def test_pnfa_reference_stochastic_matrices(cuda, oracle):
     np.cumsum(lens, out=off[1:])
     data = rng.integers(0, 2, size=int(off[-1]), dtype=np.uint8)
     ref = oracle.pnfa_fp64(T, start, acc, data, off)
-    for mode in ("fp32", "bf16", "fp16"):
+    for mode in ("fp32", "bf16", "fp16", "bf16cc", "fp16cc"):
         ll, ac, err = _run(cuda, T, start, acc, data, off, mode)
         assert err == 0
         _check(ll, ac, ref, mode, _symbols(data, off, 2))

@@ -1082,6 +1082,112 @@ __global__ void __launch_bounds__(kPnPlainWarps * 32) pnfa_plain_kernel(PnPlainP
     }
 }
 
+// CUDA-core form with 16-bit tables in shared memory (modes BF16_CC / FP16_CC):
+// the transition tables of all symbols (sigma x 8 KB) are copied into shared
+// memory once per CTA, so a step reads no global memory; the state stays in
+// FP32 with the plain kernel's exact power-of-two rescale. A warp per string,
+// lane l owns states l and l + 32. Its per-step latency is far below the
+// tensor-core kernel's (which advances many strings per step): the form for
+// few strings, long ones included (serving).
+template <bool FP16>
+__device__ __forceinline__ float pn_h2f(uint32_t h) {
+    if constexpr (FP16) return __half2float(__ushort_as_half((unsigned short)h));
+    else return __uint_as_float(h << 16);
+}
+
+template <bool FP16>
+__global__ void __launch_bounds__(kPnPlainWarps * 32) pnfa_cc_kernel(PnPlainParams P, const uint16_t *T16) {
+    extern __shared__ __align__(16) uint8_t pn_cc_smem[];
+    float *sv_all = reinterpret_cast<float *>(pn_cc_smem);                    // [warps][64]
+    uint16_t *tbl = reinterpret_cast<uint16_t *>(pn_cc_smem + kPnPlainWarps * 64 * 4);
+    {
+        const uint4 *src = reinterpret_cast<const uint4 *>(T16);
+        uint4 *dst = reinterpret_cast<uint4 *>(tbl);
+        const int words = P.sigma * 64 * 64 * 2 / 16;
+        for (int i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
+        __syncthreads();
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    float *v = sv_all + w * 64;
+    for (;;) {
+        unsigned long long idx = 0;
+        if (lane == 0) idx = atomicAdd(P.queue, 1ull);
+        idx = __shfl_sync(0xffffffffu, idx, 0);
+        if (idx >= (unsigned long long)P.n) break;
+        const int64_t p0 = P.offsets[idx], p1 = P.offsets[idx + 1];
+        if (p0 < 0 || p1 < p0 || p1 > P.total_bytes) {
+            if (lane == 0) atomicOr(P.err, kPnErrOffsets);
+            continue;
+        }
+        float s0 = P.start[lane], s1 = P.start[lane + 32];
+        int64_t E = 0;
+        for (int64_t base = p0; base < p1; base += 32) {
+            const int64_t pl = base + lane;
+            const uint32_t mybyte = pl < p1 ? P.data[pl] : 255u;
+            const int nb = (int)min((int64_t)32, p1 - base);
+            for (int k = 0; k < nb; ++k) {
+                const uint32_t c = __shfl_sync(0xffffffffu, mybyte, k);
+                if (c >= (uint32_t)P.sigma) continue;
+                v[lane] = s0;
+                v[lane + 32] = s1;
+                __syncwarp();
+                const uint4 *r0 = reinterpret_cast<const uint4 *>(tbl + ((size_t)c * 64 + lane) * 64);
+                const uint4 *r1 = reinterpret_cast<const uint4 *>(tbl + ((size_t)c * 64 + lane + 32) * 64);
+                const float4 *vv = reinterpret_cast<const float4 *>(v);
+                float a0 = 0.f, a1 = 0.f;
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {   // 8 source states per 16 bytes of a row
+                    const float4 xa = vv[2 * q], xb = vv[2 * q + 1];
+                    const uint4 t0 = r0[q], t1 = r1[q];
+                    const uint32_t u0[4] = {t0.x, t0.y, t0.z, t0.w}, u1[4] = {t1.x, t1.y, t1.z, t1.w};
+                    const float x[8] = {xa.x, xa.y, xa.z, xa.w, xb.x, xb.y, xb.z, xb.w};
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        a0 = fmaf(pn_h2f<FP16>(u0[j] & 0xFFFFu), x[2 * j], a0);
+                        a0 = fmaf(pn_h2f<FP16>(u0[j] >> 16), x[2 * j + 1], a0);
+                        a1 = fmaf(pn_h2f<FP16>(u1[j] & 0xFFFFu), x[2 * j], a1);
+                        a1 = fmaf(pn_h2f<FP16>(u1[j] >> 16), x[2 * j + 1], a1);
+                    }
+                }
+                __syncwarp();
+                float m = fmaxf(fabsf(a0), fabsf(a1));
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+                if (m > 0.f) {
+                    uint32_t bits = __float_as_uint(m);
+                    int pre = 0;
+                    if (((bits >> 23) & 0xFFu) == 0) {   // subnormal: lift by 2^64 first
+                        m *= 18446744073709551616.0f;
+                        bits = __float_as_uint(m);
+                        pre = 64;
+                    }
+                    const int e = (int)((bits >> 23) & 0xFFu) - 126 - pre;
+                    const int e1 = max(min(e, 126), -126);
+                    const float sc1 = pn_pow2(-e1);
+                    s0 = a0 * sc1;
+                    s1 = a1 * sc1;
+                    if (e != e1) {
+                        const float sc2 = pn_pow2(-(e - e1));
+                        s0 *= sc2;
+                        s1 *= sc2;
+                    }
+                    E += e;
+                } else {
+                    s0 = 0.f;
+                    s1 = 0.f;
+                }
+            }
+        }
+        float d = s0 * P.acc[lane] + s1 * P.acc[lane + 32];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+        if (lane == 0) {
+            const double ll = d > 0.f ? log((double)d) + (double)E * 0.69314718055994530942 : -INFINITY;
+            pn_write_result(P.loglik, P.accept, P.accept_i32, (int64_t)idx, ll);
+        }
+    }
+}
+
 }  // namespace trex
 
 // ---- handle -----------------------------------------------------------------------------------
@@ -1090,6 +1196,7 @@ struct trex_pnfa {
     double ll_empty = 0.0, ll_empty_bool = 0.0;
     float start_max16[3] = {0.f, 0.f, 0.f};   // [bf16, fp16, Boolean (bf16 of 0/1)]
     float *d_T32 = nullptr, *d_start32 = nullptr, *d_acc = nullptr, *d_acc_bool = nullptr;
+    uint16_t *d_T16[2] = {nullptr, nullptr};   // [sigma][64][64] row-major: bf16, fp16
     uint32_t *d_tpack[3] = {nullptr, nullptr, nullptr};
     float *d_rsym[3] = {nullptr, nullptr, nullptr};
     uint4 *d_simg[3] = {nullptr, nullptr, nullptr};
@@ -1113,6 +1220,8 @@ static float pn_host16_to_f(uint16_t v, bool fp16) {
 
 static void pn_free(trex_pnfa *h) {
     cudaFree(h->d_T32);
+    cudaFree(h->d_T16[0]);
+    cudaFree(h->d_T16[1]);
     cudaFree(h->d_start32);
     cudaFree(h->d_acc);
     cudaFree(h->d_acc_bool);
@@ -1233,6 +1342,11 @@ int trex_pnfa_create(int n_states, int sigma, const float *T, const float *start
         if (bytes) e = cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice);
     };
     up((void **)&h->d_T32, T32.data(), T32.size() * 4);
+    for (int k = 0; k < 2; ++k) {
+        std::vector<uint16_t> t16(T32.size());
+        for (size_t i = 0; i < T32.size(); ++i) t16[i] = pn_host16(T32[i], k == 1);
+        up((void **)&h->d_T16[k], t16.data(), t16.size() * 2);
+    }
     up((void **)&h->d_start32, s32.data(), 256);
     up((void **)&h->d_acc, a32.data(), 256);
     up((void **)&h->d_acc_bool, ab.data(), 256);
@@ -1245,6 +1359,12 @@ int trex_pnfa_create(int n_states, int sigma, const float *T, const float *start
     if (e == cudaSuccess) e = cudaMemset(h->d_misc, 0, 16);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(pnfa_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kPnSmemCap);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(pnfa_cc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kPnSmemCap);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(pnfa_cc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)kPnSmemCap);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(pnfa_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1271,14 +1391,14 @@ int trex_pnfa_run(trex_pnfa *h, int mode, const uint8_t *data, const int64_t *of
     using namespace trex;
     if (!h) return TREX_ERR_NOT_INIT;
     if (n_strings < 0 || total_bytes < 0 || n_strings >= (int64_t)1 << 31) return TREX_ERR_ARG;
-    if (mode < TREX_PNFA_BF16 || mode > TREX_PNFA_BOOL) return TREX_ERR_ARG;
+    if (mode < TREX_PNFA_BF16 || mode > TREX_PNFA_FP16_CC) return TREX_ERR_ARG;
     if (n_strings == 0) return TREX_OK;
     if (!offsets || (total_bytes > 0 && !data)) return TREX_ERR_ARG;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     unsigned long long *queue = reinterpret_cast<unsigned long long *>(h->d_misc);
     uint32_t *err = reinterpret_cast<uint32_t *>(h->d_misc + 8);
     TREX_CUDA(cudaMemsetAsync(h->d_misc, 0, 16, st));
-    if (mode == TREX_PNFA_FP32) {
+    if (mode == TREX_PNFA_FP32 || mode == TREX_PNFA_BF16_CC || mode == TREX_PNFA_FP16_CC) {
         PnPlainParams Q;
         Q.data = data;
         Q.total_bytes = total_bytes;
@@ -1294,6 +1414,23 @@ int trex_pnfa_run(trex_pnfa *h, int mode, const uint8_t *data, const int64_t *of
         Q.accept_i32 = accept_i32;
         Q.queue = queue;
         Q.err = err;
+        if (mode != TREX_PNFA_FP32) {
+            const size_t smem = (size_t)kPnPlainWarps * 64 * 4 + (size_t)h->sigma * 64 * 64 * 2;
+            if (smem > kPnSmemCap) {
+                set_last_error_msg("trex_pnfa_run: the shared-memory CUDA-core form takes at most 28 symbols");
+                return TREX_ERR_SHAPE;
+            }
+            // one CTA an SM (the tables fill its shared memory), 8 strings at a time each
+            const int64_t warps = std::min<int64_t>(n_strings, (int64_t)h->n_sms * kPnPlainWarps);
+            const int grid = (int)std::max<int64_t>(1, (warps + kPnPlainWarps - 1) / kPnPlainWarps);
+            const bool fp16 = mode == TREX_PNFA_FP16_CC;
+            profile_kernel_begin(st);
+            if (fp16) pnfa_cc_kernel<true><<<grid, kPnPlainWarps * 32, smem, st>>>(Q, h->d_T16[1]);
+            else pnfa_cc_kernel<false><<<grid, kPnPlainWarps * 32, smem, st>>>(Q, h->d_T16[0]);
+            profile_kernel_end(st);
+            TREX_CHECK_LAUNCH();
+            return TREX_OK;
+        }
         const int64_t warps = std::min<int64_t>(n_strings, (int64_t)h->n_sms * 64);
         const int grid = (int)std::max<int64_t>(1, (warps + kPnPlainWarps - 1) / kPnPlainWarps);
         profile_kernel_begin(st);

@@ -179,10 +179,11 @@ class Server:
         self.dfa_set = DFASet(list(dfas)) if len(dfas) else None
         self.nfas = [NFA(T, s, a, unknown_rejects=True) for (T, s, a) in nfas]
         self.pnfas = [PNFA(T, s, a) for (T, s, a) in pnfas]
-        # "auto": the FP32 kernel for groups of fewer than pnfa_auto_threshold strings (its
-        # per-step latency is far lower than the tensor-core kernel's), BF16 tcgen05 above
-        if pnfa_mode not in ("bf16", "fp16", "fp32", "auto"):
-            raise ValueError("pnfa_mode must be bf16, fp16, fp32 or auto")
+        # "auto": the CUDA-core kernel with BF16 tables in shared memory for groups of fewer
+        # than pnfa_auto_threshold strings (its per-step latency is far lower than the
+        # tensor-core kernel's), BF16 tcgen05 above
+        if pnfa_mode not in ("bf16", "fp16", "fp32", "bf16cc", "fp16cc", "auto"):
+            raise ValueError("pnfa_mode must be bf16, fp16, fp32, bf16cc, fp16cc or auto")
         self.pnfa_mode = pnfa_mode
         self.pnfa_auto_threshold = pnfa_auto_threshold
         # Boolean NFA groups of a batch run side by side on up to this many streams.
@@ -479,7 +480,7 @@ class Server:
                 else:
                     mode = self.pnfa_mode
                     if mode == "auto":
-                        mode = "fp32" if cnt < self.pnfa_auto_threshold else "bf16"
+                        mode = "bf16cc" if cnt < self.pnfa_auto_threshold else "bf16"
                     self.pnfas[eng].run(data, off, mode, loglik=s.d_ll[first:first + cnt],
                                         accept=s.d_ac2[first:first + cnt], stream=st)
             for k in used:
