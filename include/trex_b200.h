@@ -167,6 +167,19 @@ int trex_dfa_batch_run(trex_dfa_set *set, const uint8_t *data, const int64_t *of
                        uint8_t *final_state, uint8_t *accept, int32_t *accept_i32,
                        void *scratch, int64_t scratch_bytes, int32_t seg_len, void *stream);
 
+/* Multi-pattern batch (the reference's PackedEngine, src/packed_engine.py:
+ * 25-125 and 275-439, which packs the patterns block-diagonally and evolves
+ * one state vector): every one of n_strings strings is walked by every
+ * automaton of the set, reading the input once per automaton but no copy of
+ * it; results are automaton-major: final_state / accept / accept_i32 hold
+ * n_dfas * n_strings entries, entry d * n_strings + i for string i on
+ * automaton d. Scratch: trex_dfa_batch_scratch_bytes(n_strings * n_dfas,
+ * total_bytes * n_dfas, seg_len) bytes, or NULL for the set's own. */
+int trex_dfa_batch_run_multi(trex_dfa_set *set, const uint8_t *data, const int64_t *offsets,
+                             int64_t n_strings, int64_t total_bytes, uint8_t *final_state,
+                             uint8_t *accept, int32_t *accept_i32, void *scratch,
+                             int64_t scratch_bytes, int32_t seg_len, void *stream);
+
 /* Error word of the last trex_dfa_batch_run that used `scratch` (NULL = the
  * set's own scratch): 0 = fine, bit 0 = malformed offsets, bit 1 = automaton
  * id out of range (the affected strings were skipped), bit 2 = offsets that

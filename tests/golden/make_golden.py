@@ -214,13 +214,44 @@ def misc_section():
     }
 
 
+PACKED_SETS = [
+    ["(a|b)*abb", "a*b*"],
+    ["abc", "(a|b|c)*abc", "[a-z]+", "a(b|c)*d"],
+    ["x?y+z*"],
+    ["(ab|ba)*", "a.c", "\\d+\\.\\d*", "(a|b)*a(a|b)", "[^a-y]"],
+]
+
+
+def packed_section():
+    """The reference's multi-pattern PackedEngine (src/packed_engine.py, CPU path):
+    results[pattern][string] for a few pattern sets."""
+    from src.packed_engine import PackedEngine
+    rng = random.Random(29)
+    out = []
+    for regexes in PACKED_SETS:
+        eng = PackedEngine(regexes)
+        alpha = sorted(set("".join(eng._unified_alphabet)) | set(EXTRA_CHARS))
+        strings = _strings(alpha, 120, 40, rng) + ["", "abb", "abc", "aabb", "xyyz", "1.5"]
+        out.append({"regexes": regexes, "strings": strings,
+                    "results": [[bool(x) for x in row] for row in eng.match_batch(strings)],
+                    "NP": int(eng._NP), "state_counts": [int(n) for n in eng._state_counts]})
+    return out
+
+
 def main():
+    if "--only-packed" in sys.argv:   # add or refresh this section only
+        data = json.loads(OUT.read_text())
+        data["packed"] = packed_section()
+        OUT.write_text(json.dumps(data, separators=(",", ":")))
+        print(f"updated the packed section of {OUT}")
+        return
     data = {
         "generator": "tests/golden/make_golden.py",
         "regex": regex_section(),
         "byte_dfa": byte_dfa_section(),
         "nfa": nfa_section(),
         "misc": misc_section(),
+        "packed": packed_section(),
     }
     OUT.write_text(json.dumps(data, separators=(",", ":")))
     print(f"wrote {OUT} ({OUT.stat().st_size} bytes)")

@@ -74,6 +74,8 @@ SIGNATURES = {
     "trex_dfa_set_create": (ctypes.c_int, [ctypes.c_int, c_i32p, c_i32p, c_u8p, c_u8p,
                                            ctypes.POINTER(c_vp)]),
     "trex_dfa_set_destroy": (None, [c_vp]),
+    "trex_dfa_batch_run_multi": (ctypes.c_int, [c_vp, c_vp, c_vp, ctypes.c_int64, ctypes.c_int64, c_vp, c_vp,
+                                                c_vp, c_vp, ctypes.c_int64, ctypes.c_int32, c_vp]),
     "trex_dfa_kgram_max": (ctypes.c_int, [c_vp, ctypes.c_int, c_intp]),
     "trex_dfa_set_kgram": (ctypes.c_int, [c_vp, ctypes.c_int, ctypes.c_int]),
     "trex_dfa_get_kgram": (ctypes.c_int, [c_vp, ctypes.c_int, c_intp]),

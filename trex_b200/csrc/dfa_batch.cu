@@ -161,13 +161,16 @@ __device__ __forceinline__ ItemClasses item_classes(int64_t len, const ItemGeom 
 }
 
 // Returns the DFA index of string i, or -1 (and raises an error bit) when the
-// string is malformed; malformed strings get no work items.
+// string is malformed; malformed strings get no work items. Multi-pattern runs
+// (multi_n > 0) walk every one of multi_n strings with every automaton: string
+// i is then string i mod multi_n of the batch on automaton i / multi_n.
 __device__ __forceinline__ int checked_dfa(const int64_t *offsets, const int32_t *dfa_id,
                                            int64_t i, int n_dfas, int64_t total_bytes,
                                            uint32_t *err, int64_t *len_out,
-                                           int64_t *start_out = nullptr) {
-    int64_t a = offsets[i], b = offsets[i + 1];
-    int d = dfa_id ? dfa_id[i] : 0;
+                                           int64_t *start_out = nullptr, int64_t multi_n = 0) {
+    const int64_t ii = multi_n > 0 ? i % multi_n : i;
+    int64_t a = offsets[ii], b = offsets[ii + 1];
+    int d = multi_n > 0 ? (int)(i / multi_n) : dfa_id ? dfa_id[i] : 0;
     if (a < 0 || b < a || b > total_bytes) {
         atomicOr(err, kErrBadOffsets);
         return -1;
@@ -210,9 +213,9 @@ __device__ __forceinline__ uint32_t warp_rank(uint32_t *cnt, bool pred, int key)
 // in the warp-level aggregation.
 __global__ void plan_count_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n,
                                   int64_t total_bytes, const DfaDesc *desc, int n_dfas,
-                                  int32_t seg_len, uint32_t base_mis, uint32_t *cls_count,
-                                  unsigned long long *q_bytes, unsigned long long *n_items,
-                                  uint32_t *err) {
+                                  int32_t seg_len, uint32_t base_mis, int64_t multi_n,
+                                  uint32_t *cls_count, unsigned long long *q_bytes,
+                                  unsigned long long *n_items, uint32_t *err) {
     __shared__ uint32_t cnt[kMaxDfasPerSet * kLenClasses];
     __shared__ unsigned long long byt[kMaxDfasPerSet];
     __shared__ unsigned long long items;
@@ -224,7 +227,8 @@ __global__ void plan_count_kernel(const int64_t *offsets, const int32_t *dfa_id,
     for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x; i0 < n; i0 += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = i0 + threadIdx.x;
         int64_t len = 0, s0 = 0;
-        int d = i < n ? checked_dfa(offsets, dfa_id, i, n_dfas, total_bytes, err, &len, &s0) : -1;
+        int d = i < n ? checked_dfa(offsets, dfa_id, i, n_dfas, total_bytes, err, &len, &s0, multi_n)
+                      : -1;
         uint32_t k = 0;
         ItemClasses ic{0, 0, 0};
         if (d >= 0) {
@@ -304,8 +308,8 @@ __global__ void plan_scan_kernel(uint32_t *cls_count, uint32_t *cls_cursor, uint
 __global__ void __launch_bounds__(kPlanThreads)
 plan_fill_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n, int64_t total_bytes,
                  const DfaDesc *desc, int n_dfas, int32_t seg_len, uint32_t base_mis,
-                 uint32_t *cls_cursor, uint32_t *map_cursor, WorkItem *items, int64_t max_items,
-                 uint32_t *str_map, uint32_t *err) {
+                 int64_t multi_n, uint32_t *cls_cursor, uint32_t *map_cursor, WorkItem *items,
+                 int64_t max_items, uint32_t *str_map, uint32_t *err) {
     __shared__ uint32_t s_cnt[kMaxDfasPerSet * kLenClasses];
     __shared__ uint32_t s_base[kMaxDfasPerSet * kLenClasses];
     __shared__ uint32_t s_map, s_map_base;
@@ -321,7 +325,7 @@ plan_fill_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n, int64
         uint32_t k = 0, r0 = 0, rm = 0, r_last = 0, r_map = 0;
         ItemClasses ic{0, 0, 0};
         ItemGeom g{0, 0, 0};
-        if (i < n) d = checked_dfa(offsets, dfa_id, i, n_dfas, total_bytes, err, &len, &s0);
+        if (i < n) d = checked_dfa(offsets, dfa_id, i, n_dfas, total_bytes, err, &len, &s0, multi_n);
         if (d >= 0) {
             g = item_geom(len, s0, desc[d].n_states, seg_len, base_mis);
             k = g.k;
@@ -409,6 +413,7 @@ struct RaggedParams {
     int64_t n;
     int64_t max_items;
     uint32_t base_mis;
+    int64_t multi_n;
     uint8_t *final_state;
     uint8_t *accept;
     int32_t *accept_i32;
@@ -784,7 +789,7 @@ __global__ void __launch_bounds__(kComposeThreads) compose_kernel(RaggedParams P
         const int64_t i = base + lane;
         int64_t len = 0, s0 = 0;
         const int d = i < P.n ? checked_dfa(P.offsets, P.dfa_id, i, P.n_dfas, P.total_bytes, P.err,
-                                            &len, &s0)
+                                            &len, &s0, P.multi_n)
                               : -1;
         uint32_t k = 0, mb = 0;
         ItemGeom g{0, 0, 0};
@@ -901,17 +906,24 @@ struct trex_dfa_set {
 
 namespace trex {
 
-int dfa_set_run(trex_dfa_set *set, const uint8_t *data, const int64_t *offsets,
-                const int32_t *dfa_id, int64_t n, int64_t total_bytes, uint8_t *final_state,
-                uint8_t *accept, int32_t *accept_i32, void *scratch, int64_t scratch_bytes,
-                int32_t seg_len, cudaStream_t stream, uint32_t **err_word_out) {
+// Batch run; multi: every string against every automaton of the set (n
+// strings give n * n_dfas results, automaton-major; dfa_id unused).
+static int dfa_set_run_ex(trex_dfa_set *set, const uint8_t *data, const int64_t *offsets,
+                          const int32_t *dfa_id, int64_t n_strings, int64_t total_bytes,
+                          uint8_t *final_state, uint8_t *accept, int32_t *accept_i32, void *scratch,
+                          int64_t scratch_bytes, int32_t seg_len, cudaStream_t stream,
+                          uint32_t **err_word_out, bool multi) {
     if (!set) return TREX_ERR_NOT_INIT;
-    if (n < 0 || total_bytes < 0 || (n > 0 && !offsets) || (total_bytes > 0 && !data))
+    if (n_strings < 0 || total_bytes < 0 || (n_strings > 0 && !offsets) || (total_bytes > 0 && !data))
         return TREX_ERR_ARG;
+    const int64_t multi_n = multi ? n_strings : 0;
+    const int64_t n = multi ? n_strings * set->n_dfas : n_strings;   // strings walked
     if (n >= (int64_t)0x7fffffff) return TREX_ERR_CAPACITY;
     seg_len = effective_seg_len(seg_len);
     if (n == 0) return TREX_OK;
-    ScratchLayout L = scratch_layout(n, total_bytes, seg_len);
+    // bytes walked: every byte once per automaton in a multi-pattern run
+    const int64_t walked = multi ? total_bytes * set->n_dfas : total_bytes;
+    ScratchLayout L = scratch_layout(n, walked, seg_len);
     if (L.max_items >= (int64_t)0xffffffffLL) return TREX_ERR_CAPACITY;
     uint8_t *sc = static_cast<uint8_t *>(scratch);
     if (!sc) {
@@ -950,15 +962,15 @@ int dfa_set_run(trex_dfa_set *set, const uint8_t *data, const int64_t *offsets,
     int plan_grid = (int)std::min<int64_t>((n + kPlanThreads - 1) / kPlanThreads,
                                            (int64_t)set->n_sms * 8);
     plan_count_kernel<<<plan_grid, kPlanThreads, 0, stream>>>(
-        offsets, dfa_id, n, total_bytes, set->d_desc, set->n_dfas, seg_len, base_mis, cls_count,
-        q_bytes, n_items, err);
+        offsets, dfa_id, n, total_bytes, set->d_desc, set->n_dfas, seg_len, base_mis, multi_n,
+        cls_count, q_bytes, n_items, err);
     TREX_CHECK_LAUNCH();
     plan_scan_kernel<<<1, kMaxDfasPerSet, 0, stream>>>(cls_count, cls_cursor, q_base, q_count, set->n_dfas,
                                            n_items, L.max_items, err);
     TREX_CHECK_LAUNCH();
     plan_fill_kernel<<<plan_grid, kPlanThreads, 0, stream>>>(
-        offsets, dfa_id, n, total_bytes, set->d_desc, set->n_dfas, seg_len, base_mis, cls_cursor,
-        map_cursor, items, L.max_items, str_map, err);
+        offsets, dfa_id, n, total_bytes, set->d_desc, set->n_dfas, seg_len, base_mis, multi_n,
+        cls_cursor, map_cursor, items, L.max_items, str_map, err);
     TREX_CHECK_LAUNCH();
 
     RaggedParams P;
@@ -984,6 +996,7 @@ int dfa_set_run(trex_dfa_set *set, const uint8_t *data, const int64_t *offsets,
     P.n = n;
     P.max_items = L.max_items;
     P.base_mis = base_mis;
+    P.multi_n = multi_n;
     P.final_state = final_state;
     P.accept = accept;
     P.accept_i32 = accept_i32;
@@ -993,7 +1006,7 @@ int dfa_set_run(trex_dfa_set *set, const uint8_t *data, const int64_t *offsets,
     // SMs and is not held back by other kernels running beside it; CTAs take
     // work from the queues, so fewer CTAs just do more
     const int ragged_grid = (int)std::min<int64_t>(
-        set->n_sms, std::max<int64_t>({(int64_t)1, (total_bytes + (64 << 10) - 1) >> 16,
+        set->n_sms, std::max<int64_t>({(int64_t)1, (walked + (64 << 10) - 1) >> 16,
                                        std::min<int64_t>(n, set->n_dfas)}));
     dfa_ragged_kernel<<<ragged_grid, kRaggedThreads, set->smem_bytes, stream>>>(P);
     TREX_CHECK_LAUNCH();
@@ -1004,6 +1017,14 @@ int dfa_set_run(trex_dfa_set *set, const uint8_t *data, const int64_t *offsets,
     TREX_CHECK_LAUNCH();
     if (err_word_out) *err_word_out = err;
     return TREX_OK;
+}
+
+int dfa_set_run(trex_dfa_set *set, const uint8_t *data, const int64_t *offsets,
+                const int32_t *dfa_id, int64_t n, int64_t total_bytes, uint8_t *final_state,
+                uint8_t *accept, int32_t *accept_i32, void *scratch, int64_t scratch_bytes,
+                int32_t seg_len, cudaStream_t stream, uint32_t **err_word_out) {
+    return dfa_set_run_ex(set, data, offsets, dfa_id, n, total_bytes, final_state, accept,
+                          accept_i32, scratch, scratch_bytes, seg_len, stream, err_word_out, false);
 }
 
 }  // namespace trex
@@ -1217,6 +1238,15 @@ int trex_dfa_batch_run(trex_dfa_set *set, const uint8_t *data, const int64_t *of
     return trex::dfa_set_run(set, data, offsets, dfa_id, n_strings, total_bytes, final_state,
                              accept, accept_i32, scratch, scratch_bytes, seg_len,
                              static_cast<cudaStream_t>(stream), nullptr);
+}
+
+int trex_dfa_batch_run_multi(trex_dfa_set *set, const uint8_t *data, const int64_t *offsets,
+                             int64_t n_strings, int64_t total_bytes, uint8_t *final_state,
+                             uint8_t *accept, int32_t *accept_i32, void *scratch,
+                             int64_t scratch_bytes, int32_t seg_len, void *stream) {
+    return trex::dfa_set_run_ex(set, data, offsets, nullptr, n_strings, total_bytes, final_state,
+                                accept, accept_i32, scratch, scratch_bytes, seg_len,
+                                static_cast<cudaStream_t>(stream), nullptr, true);
 }
 
 }  // extern "C"

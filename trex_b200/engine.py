@@ -133,6 +133,25 @@ class DFASet:
         _lib.check(rc, "trex_dfa_batch_run")
         return final_state, accept, accept_i32
 
+    def run_all(self, data, offsets, *, final_state=None, accept=None, scratch=None,
+                seg_len: int = 0, stream=None):
+        """Every string against every automaton of the set (device tensors, as run).
+        Returns (final_state, accept) of shape [n_dfas, n] (automaton-major)."""
+        torch = _torch()
+        n = offsets.numel() - 1
+        P = len(self.dfas)
+        dev = offsets.device
+        if final_state is None:
+            final_state = torch.empty(max(P * n, 1), dtype=torch.uint8, device=dev)
+        if accept is None:
+            accept = torch.empty(max(P * n, 1), dtype=torch.uint8, device=dev)
+        sc_bytes = scratch.numel() if scratch is not None else 0
+        rc = self.lib.trex_dfa_batch_run_multi(
+            self._h, _dptr(data), _dptr(offsets), n, data.numel(), _dptr(final_state), _dptr(accept),
+            None, _dptr(scratch), sc_bytes, seg_len, _stream_handle(stream))
+        _lib.check(rc, "trex_dfa_batch_run_multi")
+        return final_state[:P * n].view(P, n), accept[:P * n].view(P, n)
+
     @staticmethod
     def scan_scratch_bytes(n_strings: int, total_bytes: int, tile_len: int = 0) -> int:
         return int(_lib.load().trex_dfa_scan_scratch_bytes(n_strings, total_bytes, tile_len))
