@@ -97,3 +97,30 @@ def test_mix_equals_alone_and_oracle(cuda, oracle):
             ll, ac = pnfa_h[q.engine].run(dd, do, "bf16")
             assert q.result == (float(ll.item()), bool(ac.item()))
     srv.close()
+
+
+@pytest.mark.gpu
+def test_server_from_file(cuda, oracle, tmp_path):
+    from trex_b200 import automata_io
+    from trex_b200.serving import Server
+    rng = np.random.default_rng(8)
+    dfas = [random_dfa(12, np.arange(256), rng), random_dfa(16, np.arange(256), rng)]
+    nfas = [random_bool_nfa(rng, 64, 20)]
+    pnfas = [random_prob_nfa(rng, 64, 20)]
+    path = automata_io.save(tmp_path / "served", dfas, nfas, pnfas)
+    srv = Server.from_file(path, hbm_budget=64 << 20, max_batch_requests=256)
+    items = [("dfa", i % 2, rng.integers(0, 256, size=int(rng.integers(0, 3000)), dtype=np.uint8).tobytes())
+             for i in range(40)]
+    items += [("nfa", 0, rng.integers(0, 20, size=500, dtype=np.uint8).tobytes()) for _ in range(10)]
+    reqs = srv.submit_many(items)
+    res = srv.wait(reqs, timeout=120)
+    srv.close()
+    for (kind, eng, data), r in zip(items, res):
+        d = np.frombuffer(data, np.uint8)
+        off = np.array([0, len(data)], np.int64)
+        if kind == "dfa":
+            fs, ac = oracle.dfa_walk([dfas[eng].tmap], [dfas[eng].n_states], [0], [dfas[eng].accept], d, off)
+            assert r == (bool(ac[0]), int(fs[0]))
+        else:
+            _, ac = oracle.nfa_bool(*nfas[0], d, off, unknown_rejects=True)
+            assert r[0] == bool(ac[0])

@@ -257,6 +257,13 @@ class Server:
         self._thread = threading.Thread(target=self._loop, name="trex-serve", daemon=True)
         self._thread.start()
 
+    @classmethod
+    def from_file(cls, path, **kw) -> "Server":
+        """A server over the automata of a file written by trex_b200.automata_io.save."""
+        from .automata_io import load
+        a = load(path)
+        return cls(a["dfas"], a["nfas"], a["pnfas"], **kw)
+
     # ---- client side ---------------------------------------------------------------------------
     def submit(self, kind: str, engine: int, data: bytes) -> Request:
         if kind not in KINDS:
