@@ -14,7 +14,8 @@
 // the set bits of v, so a step is ceil(64/B) table lookups ORed together.
 // Symbol index sigma is an extra table: the identity (skip) or all zeros
 // (reject), so bytes >= sigma need no branch. B is picked so all tables fit
-// in shared memory (B = 6 for sigma <= 35: 11 lookups a byte); larger
+// in shared memory: the widest of 8, 7, 6, 5, 4 bits that fits (8 lookups a
+// byte for sigma <= 12, 10 for sigma <= 21, 11 for sigma <= 39); larger
 // alphabets read 8-bit tables (8 lookups) from global memory through L1.
 // One persistent CTA per SM, a thread per string; threads take strings from
 // an atomic counter and walk them in 16-byte windows.
@@ -28,7 +29,7 @@
 namespace trex {
 
 constexpr int kNfaThreads = 1024;
-constexpr size_t kNfaSmemBudget = 200 * 1024;
+constexpr size_t kNfaSmemBudget = 220 * 1024;
 
 __host__ __device__ constexpr int nfa_groups(int B) { return (64 + B - 1) / B; }
 // Entries of symbol c are stored at v ^ swizzle(c): with dense states many
@@ -130,7 +131,8 @@ struct trex_nfa {
 namespace trex {
 
 static void nfa_choose_layout(int sigma, int *B, bool *smem) {
-    for (int b : {6, 5, 4}) {
+    // the widest groups (fewest lookups a byte) whose tables fit in shared memory
+    for (int b : {8, 7, 6, 5, 4}) {
         if ((size_t)(sigma + 1) * nfa_table_entries(b) * 8 <= kNfaSmemBudget) {
             *B = b;
             *smem = true;
@@ -193,10 +195,12 @@ int nfa_run(trex_nfa *nfa, const uint8_t *data, const int64_t *offsets, int64_t 
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(nfa->n_sms, (n + 31) / 32));
     profile_kernel_begin(stream);
     switch (nfa->B) {
+        case 8: nfa->smem ? nfa_bitpar_kernel<8, true><<<grid, kNfaThreads, smem, stream>>>(P)
+                          : nfa_bitpar_kernel<8, false><<<grid, kNfaThreads, 0, stream>>>(P); break;
+        case 7: nfa_bitpar_kernel<7, true><<<grid, kNfaThreads, smem, stream>>>(P); break;
         case 6: nfa_bitpar_kernel<6, true><<<grid, kNfaThreads, smem, stream>>>(P); break;
         case 5: nfa_bitpar_kernel<5, true><<<grid, kNfaThreads, smem, stream>>>(P); break;
-        case 4: nfa_bitpar_kernel<4, true><<<grid, kNfaThreads, smem, stream>>>(P); break;
-        default: nfa_bitpar_kernel<8, false><<<grid, kNfaThreads, 0, stream>>>(P); break;
+        default: nfa_bitpar_kernel<4, true><<<grid, kNfaThreads, smem, stream>>>(P); break;
     }
     TREX_CHECK_LAUNCH();
     profile_kernel_end(stream);
@@ -248,6 +252,8 @@ int trex_nfa_create(int n_states, int sigma, const uint64_t *cols, uint64_t star
     if (nfa->smem) {
         const int smem = (int)(t.size() * 8);
         switch (nfa->B) {
+            case 8: e = cudaFuncSetAttribute(nfa_bitpar_kernel<8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem); break;
+            case 7: e = cudaFuncSetAttribute(nfa_bitpar_kernel<7, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem); break;
             case 6: e = cudaFuncSetAttribute(nfa_bitpar_kernel<6, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem); break;
             case 5: e = cudaFuncSetAttribute(nfa_bitpar_kernel<5, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem); break;
             default: e = cudaFuncSetAttribute(nfa_bitpar_kernel<4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem); break;
