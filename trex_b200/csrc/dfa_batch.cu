@@ -23,10 +23,13 @@
 //  * Main kernel: one persistent 1024-thread CTA per SM. The CTA expands the
 //    current DFA's byte map (or its K-gram tables) into a per-lane replicated
 //    shared-memory table (dfa_walk.cuh) so table lookups never conflict on
-//    banks. A warp walks 32 items of a queue together (their lengths match to
-//    128 bytes), one 32-byte window per lane per step with the next window
-//    loaded ahead; only a batch's first and last windows and warm-up capture
-//    windows apply bytes under a per-lane mask. No spin-waits anywhere.
+//    banks. For automata of 9-256 states a warp walks 64 items of a queue
+//    together, two per lane as two independent chains (the items' records sit
+//    in shared memory, so the walk keeps its registers); for automata of at
+//    most 8 states 32 items, one per lane. Items of a batch have lengths within
+//    128 bytes of each other; one 32-byte window per chain per step, the next
+//    window loaded ahead; only a batch's first and last windows and warm-up
+//    capture windows apply bytes under per-lane masks. No spin-waits anywhere.
 #include <algorithm>
 #include <cstring>
 #include <mutex>
@@ -139,7 +142,7 @@ __device__ __forceinline__ void item_range(const ItemGeom &g, int64_t s0, int64_
 // Queue order of an item by the bytes it walks (warm-up included), longest
 // first: below 4 KiB one class per 128 bytes (class 32 + (4095 - len) / 128),
 // above one class per power of two (4-8 KiB: 31, 8-16 KiB: 30, ...). Items of
-// one class differ by at most 128 bytes, so a warp's batch of 32 consecutive
+// one class differ by at most 128 bytes, so a warp's batch of consecutive
 // items spans nearly the same number of windows.
 __device__ __forceinline__ int len_class(int64_t len) {
     if (len < 4096) return 32 + (int)((4095 - len) >> 7);
@@ -472,9 +475,45 @@ struct ByteMode {
         e = step16(w, e, a);
         return step16(w, e, b);
     }
+    // half a window (16 bytes) of two independent chains, interleaved byte by byte
+    __device__ __forceinline__ void fast2_half(uint32_t &e0, uint4 a0, uint32_t &e1, uint4 a1) const {
+        const uint32_t x0[4] = {a0.x, a0.y, a0.z, a0.w};
+        const uint32_t x1[4] = {a1.x, a1.y, a1.z, a1.w};
+        uint32_t s0 = e0, s1 = e1;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            s0 = w.template step<0>(s0, x0[k]); s1 = w.template step<0>(s1, x1[k]);
+            s0 = w.template step<1>(s0, x0[k]); s1 = w.template step<1>(s1, x1[k]);
+            s0 = w.template step<2>(s0, x0[k]); s1 = w.template step<2>(s1, x1[k]);
+            s0 = w.template step<3>(s0, x0[k]); s1 = w.template step<3>(s1, x1[k]);
+        }
+        e0 = s0;
+        e1 = s1;
+    }
     __device__ __forceinline__ uint32_t masked(uint32_t e, uint4 a, uint4 b, uint32_t m, uint32_t cpos,
                                                uint32_t &cap_e) const {
         return walk_masked(w, e, a, b, m, cpos, cap_e);
+    }
+    // two chains over one window each, byte j applied where bit j of the chain's mask is set
+    __device__ __forceinline__ void masked2(uint32_t &e0, uint4 a0, uint4 b0, uint32_t m0, uint32_t &e1,
+                                            uint4 a1, uint4 b1, uint32_t m1) const {
+        const uint32_t x0[8] = {a0.x, a0.y, a0.z, a0.w, b0.x, b0.y, b0.z, b0.w};
+        const uint32_t x1[8] = {a1.x, a1.y, a1.z, a1.w, b1.x, b1.y, b1.z, b1.w};
+        uint32_t s0 = e0, s1 = e1;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+#define TREX_MSTEP2(J)                                                  \
+            {                                                           \
+                const uint32_t n0 = w.template step<J>(s0, x0[k]);      \
+                const uint32_t n1 = w.template step<J>(s1, x1[k]);      \
+                s0 = (m0 >> (4 * k + J)) & 1u ? n0 : s0;                \
+                s1 = (m1 >> (4 * k + J)) & 1u ? n1 : s1;                \
+            }
+            TREX_MSTEP2(0) TREX_MSTEP2(1) TREX_MSTEP2(2) TREX_MSTEP2(3)
+#undef TREX_MSTEP2
+        }
+        e0 = s0;
+        e1 = s1;
     }
 };
 
@@ -551,6 +590,31 @@ struct GramMode {
         e = grams_word(e, b.x); e = grams_word(e, b.y); e = grams_word(e, b.z);
         return grams_word(e, b.w);
     }
+    // half a window (16 bytes) of two independent chains
+    __device__ __forceinline__ void fast2_half(uint32_t &e0, uint4 a0, uint32_t &e1, uint4 a1) const {
+        const uint32_t x0[4] = {a0.x, a0.y, a0.z, a0.w};
+        const uint32_t x1[4] = {a1.x, a1.y, a1.z, a1.w};
+        uint32_t s0 = e0, s1 = e1;
+        if (K == 8) {
+#pragma unroll
+            for (int k = 0; k < 4; k += 2) {
+                const uint32_t g0 = (((codes(x0[k]) * 0x08040201u) >> 20) & 0xF0u) |
+                                    ((codes(x0[k + 1]) * 0x08040201u) >> 24);
+                const uint32_t g1 = (((codes(x1[k]) * 0x08040201u) >> 20) & 0xF0u) |
+                                    ((codes(x1[k + 1]) * 0x08040201u) >> 24);
+                s0 = w.template step<0>(s0, g0);
+                s1 = w.template step<0>(s1, g1);
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                s0 = grams_word(s0, x0[k]);
+                s1 = grams_word(s1, x1[k]);
+            }
+        }
+        e0 = s0;
+        e1 = s1;
+    }
     // the fallback column of each byte: its code for a letter, else the shared column
     __device__ __forceinline__ uint32_t columns(uint32_t x) const {
         const uint32_t y = codes(x);
@@ -575,6 +639,28 @@ struct GramMode {
         }
         return e;
     }
+    // two chains through the per-code table, byte j where bit j of the chain's mask is set
+    __device__ __forceinline__ void masked2(uint32_t &e0, uint4 a0, uint4 b0, uint32_t m0, uint32_t &e1,
+                                            uint4 a1, uint4 b1, uint32_t m1) const {
+        const uint32_t x0[8] = {a0.x, a0.y, a0.z, a0.w, b0.x, b0.y, b0.z, b0.w};
+        const uint32_t x1[8] = {a1.x, a1.y, a1.z, a1.w, b1.x, b1.y, b1.z, b1.w};
+        uint32_t s0 = e0, s1 = e1;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const uint32_t col0 = columns(x0[k]), col1 = columns(x1[k]);
+#define TREX_GSTEP2(J)                                                          \
+            {                                                                   \
+                const uint32_t n0 = w.template step_off<J>(kFallbackOff, s0, col0); \
+                const uint32_t n1 = w.template step_off<J>(kFallbackOff, s1, col1); \
+                s0 = (m0 >> (4 * k + J)) & 1u ? n0 : s0;                        \
+                s1 = (m1 >> (4 * k + J)) & 1u ? n1 : s1;                        \
+            }
+            TREX_GSTEP2(0) TREX_GSTEP2(1) TREX_GSTEP2(2) TREX_GSTEP2(3)
+#undef TREX_GSTEP2
+        }
+        e0 = s0;
+        e1 = s1;
+    }
 };
 
 // Tables of a K-gram automaton: the gram table (256 columns) at 0 and the
@@ -592,16 +678,156 @@ __device__ inline void build_gram_tables(const DfaDesc &D, const uint8_t *__rest
                  [&](uint32_t c, uint32_t s) { return (uint32_t)src[rep[c] * N + s]; });
 }
 
-// Drains queue d with this warp, 32 items (one a lane) at a time. The items of
-// a queue are ordered by walked length (warm-up included), longest first, in
-// 128-byte classes, so the items of a batch span nearly the same number of
+// Shared memory after the tables: the two work items every thread walks (16
+// 32-bit words a thread).
+constexpr uint32_t kLaneItemsOff = kFallbackOff + kFallbackBytes;
+constexpr uint32_t kRaggedSmemBytes = kLaneItemsOff + kRaggedThreads * 2 * (uint32_t)sizeof(WorkItem);
+
+// A lane's item as the walk sees it: windows [wp, wp + 32 nw), the item's
+// bytes from byte lo of the first window to byte he - 1 of the last; the
+// warm-up ends at byte cpos of window cw (cw = ~0u: no warm-up).
+struct ItemView {
+    const uint8_t *wp;
+    uint32_t lo, nw, he, cw, cpos;
+};
+__device__ __forceinline__ bool item_live(const WorkItem &w) { return w.segn != 0 && w.end > w.p0; }
+__device__ __forceinline__ ItemView item_view(const RaggedParams &P, const WorkItem &w) {
+    ItemView v;
+    const bool live = item_live(w);
+    const uint32_t warm = (w.entry >> 8) & 0xffu;
+    const int64_t nbytes = w.end - w.p0;
+    const uint8_t *q0 = P.data + (live ? w.p0 : 0);
+    v.wp = reinterpret_cast<const uint8_t *>((uintptr_t)q0 & ~(uintptr_t)31);
+    v.lo = (uint32_t)(q0 - v.wp);
+    v.nw = live ? (uint32_t)((v.lo + nbytes + 31) >> 5) : 0u;
+    v.he = live ? (uint32_t)(v.lo + nbytes - 32 * (int64_t)(v.nw - 1)) : 0u;
+    const uint32_t cb = v.lo + warm;
+    v.cw = warm ? (cb >> 5) : 0xffffffffu;
+    v.cpos = cb & 31u;
+    return v;
+}
+// A thread's item slot in shared memory: the record's eight 32-bit words,
+// word k at slot[k * kRaggedThreads], so the lanes of a warp read and write
+// consecutive words (no bank conflicts).
+__device__ __forceinline__ void write_slot(uint32_t *slot, const WorkItem &w) {
+    slot[0] = (uint32_t)w.p0;
+    slot[kRaggedThreads] = (uint32_t)((uint64_t)w.p0 >> 32);
+    slot[2 * kRaggedThreads] = (uint32_t)w.end;
+    slot[3 * kRaggedThreads] = (uint32_t)((uint64_t)w.end >> 32);
+    slot[4 * kRaggedThreads] = w.str;
+    slot[5 * kRaggedThreads] = w.segn;
+    slot[6 * kRaggedThreads] = w.map_base;
+    slot[7 * kRaggedThreads] = w.entry;
+}
+// Read again at every use (volatile: the compiler keeps none of the fields in
+// registers across the unmasked walk).
+__device__ __forceinline__ WorkItem read_slot(const uint32_t *slot) {
+    const volatile uint32_t *v = slot;
+    WorkItem w;
+    w.p0 = (int64_t)(((uint64_t)v[kRaggedThreads] << 32) | v[0]);
+    w.end = (int64_t)(((uint64_t)v[3 * kRaggedThreads] << 32) | v[2 * kRaggedThreads]);
+    w.str = v[4 * kRaggedThreads];
+    w.segn = v[5 * kRaggedThreads];
+    w.map_base = v[6 * kRaggedThreads];
+    w.entry = v[7 * kRaggedThreads];
+    return w;
+}
+
+// One window of one chain with per-lane masks: window `it` of the slot's item
+// is (a, b); the next window is loaded into (a, b). A lane whose item ended
+// before this window keeps its state.
+template <class M>
+__device__ __forceinline__ void masked_window(const RaggedParams &P, const M &md, const DfaDesc &D,
+                                              const uint32_t *slot, uint32_t it, uint32_t &e,
+                                              uint32_t &cap_e, uint4 &a, uint4 &b) {
+    const uint32_t FULL = 0xffffffffu;
+    const WorkItem w = read_slot(slot);
+    const ItemView v = item_view(P, w);
+    const uint4 ca = a, cb = b;
+    if (it + 1 < v.nw) load_window(v.wp + 32 * (size_t)(it + 1), P.data, P.data + P.total_bytes, a, b);
+    const uint32_t mlo = it == 0 ? v.lo : 0u;
+    const uint32_t mhi = it + 1 < v.nw ? 32u : (it + 1 == v.nw ? v.he : 0u);
+    const uint32_t m = bit_range((int)mlo, (int)mhi);
+    const bool cap = it == v.cw;
+    if (cap && v.cpos == 0) cap_e = e;   // the warm-up ended with the previous window
+    const bool special = (it < v.nw && (m != FULL || !md.valid(ca, cb))) || (cap && v.cpos != 0);
+    const uint32_t e_in = e;
+    if (!__any_sync(FULL, special)) e = md.fast(e, ca, cb);
+    else e = md.masked(e, ca, cb, m, cap ? v.cpos : 0u, cap_e);
+    e = it < v.nw ? e : e_in;
+}
+
+// After a batch: the final state of the slot's item (or the split item's
+// record).
+template <class W>
+__device__ __forceinline__ void finish_item(const RaggedParams &P, const DfaDesc &D, const uint32_t *slot,
+                                            uint32_t e, uint32_t cap_e) {
+    const WorkItem w = read_slot(slot);
+    if (!item_live(w)) return;
+    const uint32_t fin = W::dec(e);
+    if ((w.segn >> 16) == 1)
+        write_result(P, w.str, fin, D.accept_off);
+    else
+        publish_item(P, w.segn, w.map_base, (w.entry >> 8) & 0xffu ? W::dec(cap_e) : w.entry & 0xffu, fin);
+}
+
+// Queue d's first item and item count, read again at each batch (volatile:
+// no register holds them across the walk).
+__device__ __forceinline__ uint32_t q_base_of(const RaggedParams &P, int d) {
+    return *(const volatile uint32_t *)&P.q_base[d];
+}
+__device__ __forceinline__ uint32_t q_count_of(const RaggedParams &P, int d) {
+    return *(const volatile uint32_t *)&P.q_count[d];
+}
+
+// Both chains of a batch over the windows [it, end) that every lane walks
+// whole (the next windows as well); CAPTURE: some warm-up ends in this range.
+template <bool CAPTURE, class M>
+__device__ __forceinline__ void whole_windows(const M &md, uint32_t &it, uint32_t end,
+                                              const uint8_t *wp0, const uint8_t *wp1, uint32_t cw0,
+                                              uint32_t cw1, uint32_t &e0, uint32_t &e1, uint32_t &cap0,
+                                              uint32_t &cap1, uint4 &a0, uint4 &c0, uint4 &a1,
+                                              uint4 &c1) {
+    const uint32_t FULL = 0xffffffffu;
+    for (; it < end; ++it) {
+        if (CAPTURE) {
+            cap0 = it == cw0 ? e0 : cap0;
+            cap1 = it == cw1 ? e1 : cap1;
+        }
+        if (__all_sync(FULL, md.valid(a0, c0) && md.valid(a1, c1))) {
+            // the next windows are loaded once the first halves are walked, so
+            // that their registers are free
+            md.fast2_half(e0, a0, e1, a1);
+            const uint4 y0 = c0, y1 = c1;
+            ld_stream32(wp0 + 32 * (size_t)(it + 1), a0, c0);
+            ld_stream32(wp1 + 32 * (size_t)(it + 1), a1, c1);
+            md.fast2_half(e0, y0, e1, y1);
+        } else {
+            const uint4 x0 = a0, y0 = c0, x1 = a1, y1 = c1;
+            ld_stream32(wp0 + 32 * (size_t)(it + 1), a0, c0);
+            ld_stream32(wp1 + 32 * (size_t)(it + 1), a1, c1);
+            uint32_t unused = 0;
+            if (__all_sync(FULL, md.valid(x0, y0))) e0 = md.fast(e0, x0, y0);
+            else e0 = md.masked(e0, x0, y0, FULL, 0u, unused);
+            if (__all_sync(FULL, md.valid(x1, y1))) e1 = md.fast(e1, x1, y1);
+            else e1 = md.masked(e1, x1, y1, FULL, 0u, unused);
+        }
+    }
+}
+
+// Drains queue d with this warp, 32 items (one a lane, one chain a thread) at
+// a time; automata of at most 8 states take this path (their two-instruction
+// step gains nothing from a second chain on ragged batches, measured). The
+// items of a queue are ordered by walked length (warm-up included), longest
+// first, in 128-byte classes, so the items of a batch span nearly the same number of
 // 32-byte windows: the lanes start and finish together, and every window
 // between a batch's first and last is walked without masks. The records of the
 // next batch are claimed and loaded while the current one is walked; the next
 // window of every lane is loaded while the current one is walked.
 template <class M>
-__device__ void drain_queue(const RaggedParams &P, const M &md, const DfaDesc &D, uint32_t base,
-                            uint32_t count, uint32_t *head) {
+__device__ void drain_queue_one(const RaggedParams &P, const M &md, const DfaDesc &D, int d) {
+    const uint32_t base = P.q_base[d], count = P.q_count[d];
+    uint32_t *const head = &P.q_head[d];
     using W = decltype(md.w);
     const W &w = md.w;
     const uint32_t FULL = 0xffffffffu;
@@ -663,6 +889,160 @@ __device__ void drain_queue(const RaggedParams &P, const M &md, const DfaDesc &D
     }
 }
 
+// Bits of the bytes of window `it` that belong to the item (0 past its end).
+__device__ __forceinline__ uint32_t window_mask(uint32_t it, const ItemView &v) {
+    const uint32_t mlo = it == 0 ? v.lo : 0u;
+    const uint32_t mhi = it + 1 < v.nw ? 32u : (it + 1 == v.nw ? v.he : 0u);
+    return bit_range((int)mlo, (int)mhi);
+}
+
+// Windows [it, end) of both chains with per-lane masks (a batch's first and
+// last windows): the two chains are walked together, byte by byte, each byte
+// applied where it belongs to the lane's item; a warm-up that ends at a window
+// boundary is captured before the window. A window where a warm-up ends inside
+// (cuts off the 32-byte grid) goes through the one-chain masked step.
+template <class M>
+__device__ __forceinline__ void edge_windows(const RaggedParams &P, const M &md, const DfaDesc &D,
+                                             const uint32_t *slot0, const uint32_t *slot1, uint32_t &it,
+                                             uint32_t end, uint32_t &e0, uint32_t &cap0, uint4 &a0,
+                                             uint4 &c0, uint32_t &e1, uint32_t &cap1, uint4 &a1,
+                                             uint4 &c1) {
+    const uint32_t FULL = 0xffffffffu;
+    for (; it < end; ++it) {
+        const ItemView v0 = item_view(P, read_slot(slot0)), v1 = item_view(P, read_slot(slot1));
+        if (__any_sync(FULL, (it == v0.cw && v0.cpos != 0) || (it == v1.cw && v1.cpos != 0))) {
+            masked_window(P, md, D, slot0, it, e0, cap0, a0, c0);
+            masked_window(P, md, D, slot1, it, e1, cap1, a1, c1);
+            continue;
+        }
+        cap0 = it == v0.cw ? e0 : cap0;
+        cap1 = it == v1.cw ? e1 : cap1;
+        const uint32_t m0 = window_mask(it, v0), m1 = window_mask(it, v1);
+        const uint4 x0 = a0, y0 = c0, x1 = a1, y1 = c1;
+        if (it + 1 < v0.nw) load_window(v0.wp + 32 * (size_t)(it + 1), P.data, P.data + P.total_bytes, a0, c0);
+        if (it + 1 < v1.nw) load_window(v1.wp + 32 * (size_t)(it + 1), P.data, P.data + P.total_bytes, a1, c1);
+        if (__all_sync(FULL, (m0 & m1) == FULL && md.valid(x0, y0) && md.valid(x1, y1))) {
+            md.fast2_half(e0, x0, e1, x1);
+            md.fast2_half(e0, y0, e1, y1);
+        } else {
+            md.masked2(e0, x0, y0, m0, e1, x1, y1, m1);
+        }
+    }
+}
+
+// Drains queue d with this warp, 64 items at a time: lane l walks items l and
+// 32 + l of the batch as two independent chains, so every thread keeps two
+// table lookups in flight (with one chain a thread, the walk is bound by the
+// latency of its dependent lookups, not by the table's bandwidth). The items
+// of a queue are ordered by walked length (warm-up included), longest first,
+// in 128-byte classes, so the 64 items of a batch span nearly the same number
+// of 32-byte windows. The windows every lane of both chains walks whole (from
+// the latest first whole window to the earliest last whole window of the
+// batch) go through an unmasked loop whose loads need no bounds checks; the
+// batch's first and last windows go through the masked step. Results are
+// written after the batch. The next batch's records are prefetched into L2
+// while the current one is walked.
+template <class M>
+__device__ void drain_queue(const RaggedParams &P, const M &md, const DfaDesc &D, int d) {
+    using W = decltype(md.w);
+    const W &w = md.w;
+    const uint32_t FULL = 0xffffffffu;
+    const uint32_t lane = threadIdx.x & 31u;
+    // per warp: the next batch, then the batch's fl, cwmax and the windows of
+    // each chain (below)
+    __shared__ uint32_t s_warp[kRaggedThreads / 32][5];
+    volatile uint32_t *const wv = s_warp[threadIdx.x >> 5];
+    uint32_t *const slot0 = reinterpret_cast<uint32_t *>(g_dfa_tbl + kLaneItemsOff) + threadIdx.x;
+    uint32_t *const slot1 = slot0 + 8 * kRaggedThreads;
+    uint32_t b0 = 0;
+    if (lane == 0) b0 = atomicAdd(&P.q_head[d], 64u);
+    b0 = __shfl_sync(FULL, b0, 0);
+    {
+        const uint32_t base = q_base_of(P, d), count = q_count_of(P, d);
+        if (b0 >= count) return;
+        write_slot(slot0, load_item(P, base, b0 + lane, count));
+        write_slot(slot1, load_item(P, base, b0 + 32 + lane, count));
+    }
+    while (true) {
+        {
+            uint32_t b1 = 0;
+            if (lane == 0) b1 = atomicAdd(&P.q_head[d], 64u);
+            b1 = __shfl_sync(FULL, b1, 0);
+            const uint32_t base = q_base_of(P, d), count = q_count_of(P, d);
+            if (b1 + lane < count) prefetch_l2(P.items + base + b1 + lane);
+            if (b1 + 32 + lane < count) prefetch_l2(P.items + base + b1 + 32 + lane);
+            __syncwarp();
+            if (lane == 0) wv[0] = b1;
+        }
+
+        // ---- both chains: entry state, first window, whole-window range [ff, fl)
+        uint32_t e0, e1, ff;
+        uint4 a0 = make_uint4(0, 0, 0, 0), c0 = a0, a1 = a0, c1 = a0;
+        {
+            const WorkItem w0 = read_slot(slot0), w1 = read_slot(slot1);
+            // empty strings: the final state is the start state
+            if (w0.segn != 0 && w0.end <= w0.p0) write_result(P, w0.str, w0.entry & 0xffu, D.accept_off);
+            if (w1.segn != 0 && w1.end <= w1.p0) write_result(P, w1.str, w1.entry & 0xffu, D.accept_off);
+            const ItemView v0 = item_view(P, w0), v1 = item_view(P, w1);
+            e0 = w.enc(item_live(w0) ? (w0.entry & 0xffu) : 0u);
+            e1 = w.enc(item_live(w1) ? (w1.entry & 0xffu) : 0u);
+            if (v0.nw) load_window(v0.wp, P.data, P.data + P.total_bytes, a0, c0);
+            if (v1.nw) load_window(v1.wp, P.data, P.data + P.total_bytes, a1, c1);
+            // window j of an item is whole when j >= (lo != 0) and j < nw - (he != 32); a
+            // warm-up that ends inside a window needs the masked step there
+            uint32_t f0 = v0.lo != 0 ? 1u : 0u, f1 = v1.lo != 0 ? 1u : 0u;
+            if (v0.cw != 0xffffffffu && v0.cpos != 0) f0 = max(f0, v0.cw + 1u);
+            if (v1.cw != 0xffffffffu && v1.cpos != 0) f1 = max(f1, v1.cw + 1u);
+            const uint32_t l0 = v0.nw == 0 ? 0u : v0.nw - (v0.he != 32 ? 1u : 0u);
+            const uint32_t l1 = v1.nw == 0 ? 0u : v1.nw - (v1.he != 32 ? 1u : 0u);
+            ff = __reduce_max_sync(FULL, max(f0, f1));
+            const uint32_t fl = __reduce_min_sync(FULL, min(l0, l1));
+            const uint32_t nw0 = __reduce_max_sync(FULL, v0.nw), nw1 = __reduce_max_sync(FULL, v1.nw);
+            const uint32_t nwmax = max(nw0, nw1);
+            const uint32_t cwmax = __reduce_max_sync(FULL, max(v0.cw == 0xffffffffu ? 0u : v0.cw + 1u,
+                                                               v1.cw == 0xffffffffu ? 0u : v1.cw + 1u));
+            if (lane == 0) {
+                wv[1] = fl;
+                wv[2] = cwmax;
+                wv[3] = nw0;
+                wv[4] = nw1;
+            }
+            __syncwarp();
+            ff = min(ff, nwmax);
+        }
+        // Warp-uniform values live in shared memory and the windows' addresses are
+        // derived again after the first windows, so that the masked steps have
+        // the registers to themselves.
+        uint32_t cap0 = e0, cap1 = e1;
+        uint32_t it = 0;
+        edge_windows(P, md, D, slot0, slot1, it, ff, e0, cap0, a0, c0, e1, cap1, a1, c1);
+        // windows it and it + 1 are whole for every lane of both chains, inside
+        // the items' bytes and so inside the batch buffer; the warm-ups end
+        // before window cwmax
+        if (const uint32_t fl = wv[1]; fl > 0) {
+            const ItemView v0 = item_view(P, read_slot(slot0)), v1 = item_view(P, read_slot(slot1));
+            whole_windows<true>(md, it, min(fl - 1u, wv[2]), v0.wp, v1.wp, v0.cw, v1.cw, e0, e1, cap0,
+                                cap1, a0, c0, a1, c1);
+            whole_windows<false>(md, it, fl - 1u, v0.wp, v1.wp, v0.cw, v1.cw, e0, e1, cap0, cap1, a0, c0,
+                                 a1, c1);
+        }
+        edge_windows(P, md, D, slot0, slot1, it, max(wv[3], wv[4]), e0, cap0, a0, c0, e1, cap1, a1, c1);
+        finish_item<W>(P, D, slot0, e0, cap0);
+        finish_item<W>(P, D, slot1, e1, cap1);
+        const uint32_t b1 = wv[0], base = q_base_of(P, d), count = q_count_of(P, d);
+        if (b1 >= count) break;
+        write_slot(slot0, load_item(P, base, b1 + lane, count));
+        write_slot(slot1, load_item(P, base, b1 + 32 + lane, count));
+    }
+}
+
+// One chain a thread for automata of at most 8 states, two for larger ones.
+template <class M>
+__device__ __forceinline__ void drain(const RaggedParams &P, const M &md, const DfaDesc &D, int d) {
+    if constexpr (decltype(md.w)::kChains == 8) drain_queue_one(P, md, D, d);
+    else drain_queue(P, md, D, d);
+}
+
 __global__ void __launch_bounds__(kRaggedThreads, 1) dfa_ragged_kernel(RaggedParams P) {
     __shared__ int s_dfa;
     // The plan is complete when every (DFA, length class) cursor of the fill
@@ -704,23 +1084,21 @@ __global__ void __launch_bounds__(kRaggedThreads, 1) dfa_ragged_kernel(RaggedPar
         if (gram) build_gram_tables(D, P.tmaps + D.tmap_off);
         else build_table(P.tmaps + D.tmap_off, D.n_states);
         __syncthreads();
-        const uint32_t base = P.q_base[d], count = P.q_count[d];
-        uint32_t *head = &P.q_head[d];
         if (gram) {
             const uint32_t sh = (uint32_t)D.kshift;
             const uint32_t *al = D.kalpha;
-#define TREX_GRAM(WT, B, KK)                                                                                 drain_queue(P, GramMode<WT, B, KK>{WT{lane}, sh, {al[0], al[1], al[2], al[3]}}, D, base,                         count, head)
+#define TREX_GRAM(WT, B, KK)                                                                                 drain(P, GramMode<WT, B, KK>{WT{lane}, sh, {al[0], al[1], al[2], al[3]}}, D, d)
 #define TREX_GRAMS(WT)                                                                                       switch (D.kbits * 16 + D.kgram) {                                                                    case 16 + 2: TREX_GRAM(WT, 1, 2); break;                                                          case 16 + 4: TREX_GRAM(WT, 1, 4); break;                                                          case 16 + 8: TREX_GRAM(WT, 1, 8); break;                                                          case 32 + 2: TREX_GRAM(WT, 2, 2); break;                                                          case 32 + 4: TREX_GRAM(WT, 2, 4); break;                                                          default: TREX_GRAM(WT, 4, 2); break;                                                          }
             if (D.n_states <= 8) { TREX_GRAMS(Walker<8>) }
             else { TREX_GRAMS(Walker<16>) }
 #undef TREX_GRAMS
 #undef TREX_GRAM
         } else if (D.n_states <= 8) {
-            drain_queue(P, ByteMode<Walker<8>>{Walker<8>{lane}}, D, base, count, head);
+            drain(P, ByteMode<Walker<8>>{Walker<8>{lane}}, D, d);
         } else if (D.n_states <= 16) {
-            drain_queue(P, ByteMode<Walker<16>>{Walker<16>{lane}}, D, base, count, head);
+            drain(P, ByteMode<Walker<16>>{Walker<16>{lane}}, D, d);
         } else {
-            drain_queue(P, ByteMode<Walker<0>>{Walker<0>{(uint32_t)D.n_states}}, D, base, count, head);
+            drain(P, ByteMode<Walker<0>>{Walker<0>{(uint32_t)D.n_states}}, D, d);
         }
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -1077,7 +1455,7 @@ int trex_dfa_set_create(int n_dfas, const int32_t *n_states, const int32_t *star
         return TREX_ERR_SHAPE;
     }
     // table region, sized for the largest layout, and the K-gram fallback table
-    set->smem_bytes = (size_t)trex::kFallbackOff + trex::kFallbackBytes;
+    set->smem_bytes = (size_t)trex::kRaggedSmemBytes;
     auto fail = [&](cudaError_t e, const char *what) {
         trex::set_last_error(what, e);
         cudaFree(set->d_tmaps);
@@ -1098,11 +1476,11 @@ int trex_dfa_set_create(int n_dfas, const int32_t *n_states, const int32_t *star
     if ((e = cudaMemcpy(set->d_desc, desc.data(), sizeof(trex::DfaDesc) * n_dfas,
                         cudaMemcpyHostToDevice)) != cudaSuccess)
         return fail(e, "copy desc");
-    // The attribute is per kernel, so it is always raised to the largest
-    // table any set can need (128 KiB).
+    // The attribute is per kernel, so it is always raised to what any set can
+    // need (the largest tables and the threads' work items).
     if ((e = cudaFuncSetAttribute(trex::dfa_ragged_kernel,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  trex::kFallbackOff + trex::kFallbackBytes)) != cudaSuccess)
+                                  trex::kRaggedSmemBytes)) != cudaSuccess)
         return fail(e, "cudaFuncSetAttribute");
     *out = set;
     return TREX_OK;
