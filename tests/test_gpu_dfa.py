@@ -65,6 +65,26 @@ def test_segment_maps_compose_exactly(cuda, oracle, seg_len):
     assert np.array_equal(ac, rac)
 
 
+@pytest.mark.parametrize("n_states", [8, 12, 100])
+@pytest.mark.parametrize("length", [32, 1024, 2080])
+def test_whole_window_batches(cuda, oracle, n_states, length):
+    # Strings whose bytes fill whole 32-byte windows: every batch but the last
+    # (1000 items: not a multiple of 64) runs entirely through the unmasked
+    # loop; 2080-byte strings are cut into pieces whose warm-ups end on window
+    # boundaries.
+    rng = np.random.default_rng(n_states * 7 + length)
+    d = random_dfa(n_states, np.arange(256), rng)
+    lens = np.full(1000, length, dtype=np.int64)
+    off = np.zeros(len(lens) + 1, dtype=np.int64)
+    np.cumsum(lens, out=off[1:])
+    data = rng.integers(0, 256, size=int(off[-1]), dtype=np.uint8)
+    fs, ac, err = _run_set(cuda, [d], data, off, seg_len=1024)
+    rfs, rac = oracle.dfa_walk([d.tmap], [d.n_states], [0], [d.accept], data, off)
+    assert err == 0
+    assert np.array_equal(fs, rfs)
+    assert np.array_equal(ac, rac)
+
+
 def test_ragged_multi_dfa_batch(cuda, oracle):
     rng = np.random.default_rng(42)
     sizes = (8,) * 5 + (12,) * 5 + (16,) * 6

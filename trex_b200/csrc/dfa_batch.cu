@@ -469,6 +469,7 @@ __device__ __forceinline__ uint32_t walk_masked(const W &w, uint32_t e, uint4 a,
 // belong to the item, masked() with a byte mask and the warm-up capture.
 template <class W>
 struct ByteMode {
+    static constexpr bool kWideLetters = false;
     W w;
     __device__ __forceinline__ bool valid(uint4, uint4) const { return true; }
     __device__ __forceinline__ uint32_t fast(uint32_t e, uint4 a, uint4 b) const {
@@ -535,6 +536,7 @@ struct GramMode {
     W w;
     uint32_t sh;
     uint32_t alpha[4];
+    static constexpr bool kWideLetters = BITS == 4;
     static constexpr uint32_t kMask = BITS == 1 ? 0x01010101u : BITS == 2 ? 0x03030303u : 0x0F0F0F0Fu;
     static constexpr uint32_t kOther = (1u << BITS) * 0x01010101u;   // the shared column, 4 bytes
     __device__ __forceinline__ uint32_t codes(uint32_t x) const { return (x >> sh) & kMask; }
@@ -1036,10 +1038,12 @@ __device__ void drain_queue(const RaggedParams &P, const M &md, const DfaDesc &D
     }
 }
 
-// One chain a thread for automata of at most 8 states, two for larger ones.
+// One chain a thread for automata of at most 8 states (and for K-gram walks
+// over 16 letters, whose letter table leaves no registers for a second chain),
+// two for larger ones.
 template <class M>
 __device__ __forceinline__ void drain(const RaggedParams &P, const M &md, const DfaDesc &D, int d) {
-    if constexpr (decltype(md.w)::kChains == 8) drain_queue_one(P, md, D, d);
+    if constexpr (decltype(md.w)::kChains == 8 || M::kWideLetters) drain_queue_one(P, md, D, d);
     else drain_queue(P, md, D, d);
 }
 
