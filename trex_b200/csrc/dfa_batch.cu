@@ -359,9 +359,11 @@ plan_fill_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n, int64
             if (s_cnt[t]) s_base[t] = atomicAdd(&cls_cursor[t], s_cnt[t]);
         if (threadIdx.x == 0 && s_map) s_map_base = atomicAdd(map_cursor, s_map);
         __syncthreads();
+        // this string's item positions: first, first middle and last item
+        uint32_t mb = 0, warm = 0, p_first = 0, p_mid = 0, p_last = 0, start = 0;
         if (d >= 0) {
-            const uint32_t mb = k > 1 ? s_map_base + r_map : 0u;
-            const uint32_t warm = (uint32_t)warm_bytes(desc[d].n_states, g.seg);
+            mb = k > 1 ? s_map_base + r_map : 0u;
+            warm = (uint32_t)warm_bytes(desc[d].n_states, g.seg);
             // With the counts of plan_count_kernel every position and map slot is
             // below max_items; offsets rewritten between the two planning kernels
             // (a caller changing inputs in flight) could break that: refuse.
@@ -370,19 +372,50 @@ plan_fill_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n, int64
                 k = 0;
             }
             if (k > 1) str_map[i] = mb;
-            for (uint32_t j = 0; j < k; ++j) {
-                const uint32_t pos = (j + 1 == k) ? s_base[ic.last] + r_last
-                                     : j == 0      ? s_base[ic.first] + r0
-                                                   : s_base[ic.mid] + rm + (j - 1);
+            if (k > 1) p_first = s_base[ic.first] + r0;
+            if (k > 2) p_mid = s_base[ic.mid] + rm;
+            if (k > 0) p_last = s_base[ic.last] + r_last;
+            start = (uint32_t)desc[d].start;
+        } else {
+            k = 0;
+        }
+        // The warp writes its strings' items together, 32 at a time (a string
+        // of many pieces would otherwise keep its lane busy while the others
+        // idle): item t of the warp belongs to the lane whose inclusive prefix
+        // sum of item counts first exceeds t.
+        {
+            const uint32_t FULL = 0xffffffffu, lane = threadIdx.x & 31u;
+            uint32_t incl = k;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t v = __shfl_up_sync(FULL, incl, o);
+                if (lane >= (uint32_t)o) incl += v;
+            }
+            const uint32_t total = __shfl_sync(FULL, incl, 31);
+            for (uint32_t t0 = 0; t0 < total; t0 += 32) {
+                const uint32_t t = t0 + lane;
+                uint32_t o = 0;   // lanes whose inclusive count is <= t
+#pragma unroll
+                for (uint32_t step = 16; step >= 1; step >>= 1)
+                    if (__shfl_sync(FULL, incl, o + step - 1) <= t) o += step;
+                const uint32_t ko = __shfl_sync(FULL, k, o), io = __shfl_sync(FULL, incl, o);
+                const int64_t so = __shfl_sync(FULL, s0, o), lo_ = __shfl_sync(FULL, len, o);
+                const ItemGeom go{ko, __shfl_sync(FULL, g.seg, o), __shfl_sync(FULL, g.first, o)};
+                const uint32_t pf = __shfl_sync(FULL, p_first, o), pm = __shfl_sync(FULL, p_mid, o);
+                const uint32_t pl = __shfl_sync(FULL, p_last, o), mbo = __shfl_sync(FULL, mb, o);
+                const uint32_t wo = __shfl_sync(FULL, warm, o), sto = __shfl_sync(FULL, start, o);
+                const uint32_t stro = __shfl_sync(FULL, (uint32_t)i, o);
+                if (t >= total) continue;
+                const uint32_t j = t - (io - ko);   // the item's index in its string
+                const uint32_t pos = (j + 1 == ko) ? pl : j == 0 ? pf : pm + (j - 1);
                 if ((int64_t)pos >= max_items) {
                     atomicOr(err, kErrCapacity);
                     continue;
                 }
                 int64_t b0, b1;
-                item_range(g, s0, len, j, &b0, &b1);
-                items[pos] = (j == 0)
-                    ? WorkItem{b0, b1, (uint32_t)i, j | (k << 16), mb, (uint32_t)desc[d].start}
-                    : WorkItem{b0 - warm, b1, (uint32_t)i, j | (k << 16), mb, warm << 8};
+                item_range(go, so, lo_, j, &b0, &b1);
+                items[pos] = (j == 0) ? WorkItem{b0, b1, stro, j | (ko << 16), mbo, sto}
+                                      : WorkItem{b0 - wo, b1, stro, j | (ko << 16), mbo, wo << 8};
             }
         }
         __syncthreads();
