@@ -1224,12 +1224,12 @@ __global__ void __launch_bounds__(kComposeThreads) compose_kernel(RaggedParams P
         bool help = false;
         if (k > 1) {
             st = (P.maps[mb] >> 8) & 0xffu;   // item 0 starts from the start state
-            for (uint32_t j0 = 1; j0 < k && !help; j0 += 4) {
-                uint32_t v[4];   // four records loaded together
+            for (uint32_t j0 = 1; j0 < k && !help; j0 += 8) {
+                uint32_t v[8];   // eight records loaded together (one load latency for most strings)
 #pragma unroll
-                for (int u = 0; u < 4; ++u) v[u] = j0 + u < k ? P.maps[mb + j0 + u] : 0u;
+                for (int u = 0; u < 8; ++u) v[u] = j0 + u < k ? P.maps[mb + j0 + u] : 0u;
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
+                for (int u = 0; u < 8; ++u) {
                     const uint32_t j = j0 + u;
                     if (help || j >= k) continue;
                     if ((v[u] & 0xffu) == st) st = (v[u] >> 8) & 0xffu;
