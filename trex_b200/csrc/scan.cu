@@ -38,7 +38,6 @@
 namespace trex {
 
 constexpr int kScanThreads = 1024;
-constexpr int kScanDefaultTile = 8192;
 constexpr int kSyncCap = 512;                 // bytes walked with 16 chains before giving up
 constexpr uint32_t kPollLimit = 1u << 24;     // polls of one look-back step before giving up
 
