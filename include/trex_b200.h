@@ -42,6 +42,16 @@ const char *trex_last_error(void);
 /* Library version string. */
 const char *trex_version(void);
 
+/* Limits of the bounded device waits (no counterpart in the reference, whose
+ * look-back spins without a limit, cuda/monoid_scan.cu:187-193): scan_polls =
+ * polls of one look-back step of trex_dfa_scan_run, mbar_cycles = clock cycles
+ * of one hand-off wait inside the tensor-core NFA kernel (trex_pnfa_run modes
+ * BF16, FP16, BOOL, BOOL8). A wait that runs out sets the timeout bit (4) of
+ * the run's error word and the kernel returns; the results of that run are
+ * then invalid. 0 restores a default (2^24 polls; 4e9 cycles, about 2 s).
+ * Process-wide, read at each launch; meant for tests of the give-up paths. */
+int trex_set_wait_limits(int64_t scan_polls, int64_t mbar_cycles);
+
 /* Launch profiler: after trex_profile_begin(n), the main kernel of each of the
  * next n runs is bracketed by CUDA events on its stream. trex_profile_end
  * stops recording, waits for the events and writes up to `capacity`
@@ -194,22 +204,33 @@ int trex_dfa_batch_error(trex_dfa_set *set, void *scratch, int32_t *err_out);
  * caching allocator, a memory pool with a fixed budget), a real-time serving
  * loop that must not enter the driver's allocator (cudaMalloc / cudaFree can
  * synchronise the device). This entry point takes no scratch argument: its
- * scratch is a
- * file-scope device array of 8 MiB (every GPU that loads the library holds it
- * until the process exits), so a batch whose trex_dfa_batch_scratch_bytes is
- * above 8 MiB is refused with TREX_ERR_CAPACITY (about 200K strings at the
- * default segment length). The caller still passes inputs and outputs. The
- * first call on each device looks up the array's device address
- * (cudaGetSymbolAddress); make that first call before any stream capture.
- * Every call on a device shares the one array and it keeps the last call's
- * contents (the counters it needs zeroed are cleared at the start of each
- * call), so calls whose work overlaps on the GPU -- different streams, or
- * other host threads -- race: serialise them. Strings with malformed offsets
- * are skipped (their outputs are not written). */
+ * scratch is a file-scope device array of 8 MiB (every GPU that loads the
+ * library holds it until the process exits), so a batch whose
+ * trex_dfa_batch_scratch_bytes is above 8 MiB is refused with
+ * TREX_ERR_CAPACITY (about 200K strings at the default segment length). The
+ * caller still passes inputs and outputs, and calls it with the set's device
+ * current (else TREX_ERR_ARG). The first call on each device (and again after
+ * a cudaDeviceReset, which makes a new context) looks up the array's device
+ * address (cudaGetSymbolAddress); make that first call before any stream
+ * capture. Every call on a device shares the one array and it keeps the last
+ * call's contents (the counters it needs zeroed are cleared at the start of
+ * each call), so calls whose work overlaps on the GPU -- different streams,
+ * or other host threads -- race: serialise them. Errors are reported as by
+ * trex_dfa_batch_run, through trex_dfa_batch_static_error: strings with
+ * malformed offsets or automaton ids are skipped (their outputs are not
+ * written), and offsets that overlap so far that the batch needs more work
+ * items than total_bytes allows for skip the whole batch (no output is
+ * written). */
 int trex_dfa_batch_run_static(trex_dfa_set *set, const uint8_t *data, const int64_t *offsets,
                               const int32_t *dfa_id, int64_t n_strings, int64_t total_bytes,
                               uint8_t *final_state, uint8_t *accept, int32_t *accept_i32,
                               int32_t seg_len, void *stream);
+
+/* Error word (bits as trex_dfa_batch_error) of the last
+ * trex_dfa_batch_run_static on the set's device, read from the static array
+ * with a copy from the symbol (no allocation; no counterpart in the
+ * reference). Call it with the set's device current; synchronises. */
+int trex_dfa_batch_static_error(trex_dfa_set *set, int32_t *err_out);
 
 /* The same batch from HOST buffers (64-bit offsets): copies the inputs in,
  * runs, copies the requested outputs (each may be NULL) back and reports
@@ -270,7 +291,8 @@ enum {
     TREX_PNFA_FP32 = 2,
     TREX_PNFA_BOOL = 3,
     TREX_PNFA_BF16_CC = 4,
-    TREX_PNFA_FP16_CC = 5
+    TREX_PNFA_FP16_CC = 5,
+    TREX_PNFA_BOOL8 = 6
 };
 int trex_pnfa_create(int n_states, int sigma, const float *T, const float *start,
                      const float *accept, trex_pnfa **out);
@@ -286,6 +308,9 @@ void trex_pnfa_destroy(trex_pnfa *pnfa);
  * (s' = min(T[c] s, 1), exact: operands are 0/1 in BF16, sums are small
  * integers in FP32); accept = some accepting state is active, and loglik is
  * the log of the number of active accepting states. sigma <= 28.
+ * TREX_PNFA_BOOL8: the same Boolean NFA with 0/1 int8 operands and int32
+ * sums (tcgen05 kind::i8: K = 32 an instruction, so half the MMA
+ * instructions of TREX_PNFA_BOOL), thresholded to {0, 1} every step (exact).
  * TREX_PNFA_BF16_CC / TREX_PNFA_FP16_CC: CUDA cores with the 16-bit tables in
  * shared memory and an FP32 state, a warp per string: the low-latency form
  * for few (possibly long) strings, sigma <= 28. DEVICE buffers;

@@ -153,10 +153,12 @@ def test_pnfa_malformed_offsets_flagged(cuda):
         assert err & 1
 
 
+@pytest.mark.parametrize("mode", ["bool", "bool8"])
 @pytest.mark.parametrize("density", [0.02, 0.05, 0.12])
-def test_bool_mode_matches_boolean_nfa_oracle(cuda, oracle, density):
-    # Boolean NFA on the tensor cores: thresholded 0/1 products, bit-exact accept
-    # flags against the bit-parallel oracle with bytes >= sigma skipped
+def test_bool_mode_matches_boolean_nfa_oracle(cuda, oracle, density, mode):
+    # Boolean NFA on the tensor cores (0/1 BF16 operands with FP32 sums, or 0/1 int8
+    # operands with int32 sums): thresholded products, bit-exact accept flags against
+    # the bit-parallel oracle with bytes >= sigma skipped
     from trex_b200.workloads import random_bool_nfa
     rng = np.random.default_rng(int(density * 1000))
     T, start, acc = random_bool_nfa(rng, 64, 20, density=density)
@@ -166,13 +168,21 @@ def test_bool_mode_matches_boolean_nfa_oracle(cuda, oracle, density):
     off = np.zeros(len(lens) + 1, dtype=np.int64)
     np.cumsum(lens, out=off[1:])
     data = rng.integers(0, 23, size=int(off[-1]), dtype=np.uint8)   # 20..22 skipped
-    _, ac, err = _run(cuda, T, start.astype(np.float32), acc.astype(np.float32), data, off, "bool")
-    _, ref = oracle.nfa_bool(T != 0, start, acc, data, off, unknown_rejects=False)
+    ll, ac, err = _run(cuda, T, start.astype(np.float32), acc.astype(np.float32), data, off, mode)
+    rfm, ref = oracle.nfa_bool(T != 0, start, acc, data, off, unknown_rejects=False)
     assert err == 0
     assert np.array_equal(ac.astype(bool), ref.astype(bool)), np.flatnonzero(ac.astype(bool) != ref.astype(bool))[:8]
+    # loglik = log(number of active accepting states): exact for the Boolean forms
+    accmask = np.uint64(sum(1 << int(i) for i in np.flatnonzero(acc)))
+    n_act = np.array([bin(int(m)).count("1") for m in (rfm & accmask)], dtype=np.float64)
+    want = np.where(n_act > 0, np.log(np.maximum(n_act, 1)), -np.inf)
+    assert np.array_equal(np.isfinite(ll), np.isfinite(want))
+    fin = np.isfinite(want)
+    assert np.allclose(ll[fin], want[fin], rtol=0, atol=1e-6)
 
 
-def test_bool_mode_small_nfa_both_outcomes(cuda, oracle):
+@pytest.mark.parametrize("mode", ["bool", "bool8"])
+def test_bool_mode_small_nfa_both_outcomes(cuda, oracle, mode):
     # 9 states, 5 symbols: strings both accepted and rejected
     rng = np.random.default_rng(9)
     T = (rng.random((5, 9, 9)) < 0.25).astype(np.float32)
@@ -184,7 +194,7 @@ def test_bool_mode_small_nfa_both_outcomes(cuda, oracle):
     off = np.zeros(len(lens) + 1, dtype=np.int64)
     np.cumsum(lens, out=off[1:])
     data = rng.integers(0, 5, size=int(off[-1]), dtype=np.uint8)
-    _, ac, err = _run(cuda, T, start, acc, data, off, "bool")
+    _, ac, err = _run(cuda, T, start, acc, data, off, mode)
     _, ref = oracle.nfa_bool(T != 0, start, acc, data, off, unknown_rejects=False)
     assert err == 0
     assert 0 < ref.sum() < len(ref)

@@ -29,6 +29,7 @@ SIGNATURES = {
     "trex_last_error": (ctypes.c_char_p, []),
     "trex_version": (ctypes.c_char_p, []),
     "trex_profile_begin": (ctypes.c_int, [ctypes.c_int]),
+    "trex_set_wait_limits": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int64]),
     "trex_profile_end": (ctypes.c_int, [c_f32p, ctypes.c_int, c_intp]),
     # reference C ABI
     "monoid_batch_engine_device_check": (ctypes.c_int, []),
@@ -87,6 +88,7 @@ SIGNATURES = {
     "trex_dfa_batch_run_static": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, ctypes.c_int64,
                                                  ctypes.c_int64, c_vp, c_vp, c_vp, ctypes.c_int32,
                                                  c_vp]),
+    "trex_dfa_batch_static_error": (ctypes.c_int, [c_vp, c_i32p]),
     "trex_dfa_scan_scratch_bytes": (ctypes.c_int64, [ctypes.c_int64, ctypes.c_int64, ctypes.c_int32]),
     "trex_dfa_scan_run": (ctypes.c_int, [c_vp, ctypes.c_int, c_vp, c_vp, ctypes.c_int64,
                                          ctypes.c_int64, c_vp, c_vp, c_vp, c_vp, ctypes.c_int64,

@@ -1,4 +1,5 @@
 // Error strings, device queries and the library version.
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <vector>
@@ -24,6 +25,12 @@ int sm_count() {
     if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
     return n;
 }
+
+// ---- wait limits -------------------------------------------------------------------
+static std::atomic<uint32_t> g_scan_polls{kDefaultScanPolls};
+static std::atomic<long long> g_mbar_cycles{kDefaultMbarCycles};
+uint32_t scan_poll_limit() { return g_scan_polls.load(std::memory_order_relaxed); }
+long long mbar_wait_cycles() { return g_mbar_cycles.load(std::memory_order_relaxed); }
 
 // ---- launch profiler: CUDA events around the main kernel of each run -----------
 struct Profiler {
@@ -72,6 +79,13 @@ extern "C" int trex_profile_end(float *ms_out, int capacity, int *count) {
         TREX_CUDA(cudaEventElapsedTime(&ms_out[i], g_prof.start[i], g_prof.stop[i]));
     }
     g_prof.used = 0;
+    return TREX_OK;
+}
+
+extern "C" int trex_set_wait_limits(int64_t scan_polls, int64_t mbar_cycles) {
+    if (scan_polls < 0 || mbar_cycles < 0 || scan_polls > 0xffffffffll) return TREX_ERR_ARG;
+    trex::g_scan_polls.store(scan_polls ? (uint32_t)scan_polls : trex::kDefaultScanPolls);
+    trex::g_mbar_cycles.store(mbar_cycles ? (long long)mbar_cycles : trex::kDefaultMbarCycles);
     return TREX_OK;
 }
 

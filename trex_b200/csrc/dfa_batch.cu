@@ -33,6 +33,8 @@
 #include <algorithm>
 #include <cstring>
 #include <mutex>
+
+#include <cuda.h>
 #include <new>
 #include <vector>
 
@@ -50,13 +52,16 @@ struct WorkItem {
 };
 constexpr int64_t kMaxItemsPerString = 65535;
 constexpr int64_t kMaxWalkBytes = (int64_t)1 << 36;   // one item: a 32-bit count of windows
-// Warm-up bytes of an item after the first of its string: two chains of a
-// random N-state automaton merge with probability ~1/N per byte, so 32 bytes
-// per 4 states keep the miss rate near (1 - 1/N)^(8N) ~ 3e-4 (a multiple of 32,
-// which keeps aligned cuts aligned).
+// Warm-up bytes of an item after the first of its string: one window (a
+// multiple of 32 keeps aligned cuts aligned). Two chains of a random N-state
+// automaton merge with probability ~1/N per byte, so the warm-up chain has
+// reached the true entry state with probability 1 - (1 - 1/N)^32 (87% for
+// N = 16, 99% for N = 8). When it has not, the item's checkpoints (its chain's
+// state 1, 2, 4 and 8 windows into its own bytes) let compose_kernel walk from
+// the true entry state only until the two chains meet (about one window).
 __host__ __device__ __forceinline__ int64_t warm_bytes(int n_states, int64_t seg) {
-    const int64_t w = 32 * (int64_t)((n_states + 3) / 4);
-    return w < seg ? w : seg;
+    (void)n_states;
+    return 32 < seg ? 32 : seg;
 }
 
 // Error bits reported through the device error word.
@@ -67,14 +72,15 @@ enum : uint32_t {
 };
 
 constexpr int kRaggedThreads = 1024;
-constexpr int kPlanThreads = 256;
+constexpr int kPlanThreads = 1024;
+constexpr int kMaxPlanCtas = 148;   // planning CTAs (one per SM on a B200)
 constexpr int kDefaultSegLen = 2048;
 constexpr int kLenClasses = 64;
 
 // ---- scratch layout -----------------------------------------------------------
 struct ScratchLayout {
-    size_t cls_count, cls_cursor, q_base, q_count, q_head, q_bytes, err, map_cursor, n_items,
-        items, maps, str_map, total;
+    size_t q_base, q_count, q_head, q_bytes, err, n_items, items, maps, str_map, cta_bins, bin_base,
+        bin_end, cta_maps, total;
     int64_t max_items;
 };
 
@@ -92,18 +98,22 @@ static ScratchLayout scratch_layout(int64_t n_strings, int64_t total_bytes, int3
     L.max_items = n_strings + total_bytes / seg_len + 1;
     size_t o = 0;
     auto take = [&](size_t bytes) { size_t at = o; o = (o + bytes + 255) & ~size_t(255); return at; };
-    L.cls_count = take(kMaxDfasPerSet * kLenClasses * 4);
-    L.cls_cursor = take(kMaxDfasPerSet * kLenClasses * 4);
+    // the front (up to items) is cleared before every run
     L.q_base = take(kMaxDfasPerSet * 4);
     L.q_count = take(kMaxDfasPerSet * 4);
     L.q_head = take(kMaxDfasPerSet * 4);
     L.q_bytes = take(kMaxDfasPerSet * 8);
     L.err = take(4);
-    L.map_cursor = take(4);
     L.n_items = take(8);
     L.items = take((size_t)L.max_items * sizeof(WorkItem));
-    L.maps = take((size_t)L.max_items * sizeof(uint32_t));
+    L.maps = take((size_t)L.max_items * sizeof(uint64_t));
     L.str_map = take((size_t)std::max<int64_t>(n_strings, 1) * 4);
+    // planning: items per (planning CTA, DFA x length class), then those CTAs' first
+    // queue positions; each class's end; map slots per planning CTA, then its first slot
+    L.cta_bins = take((size_t)kMaxPlanCtas * kMaxDfasPerSet * kLenClasses * 4);
+    L.bin_base = take(kMaxDfasPerSet * kLenClasses * 4);
+    L.bin_end = take(kMaxDfasPerSet * kLenClasses * 4);
+    L.cta_maps = take((kMaxPlanCtas + 1) * 4);
     L.total = o;
     return L;
 }
@@ -210,25 +220,33 @@ __device__ __forceinline__ uint32_t warp_rank(uint32_t *cnt, bool pred, int key)
     return b + (uint32_t)__popc(grp & ((1u << lane) - 1u));
 }
 
-// Counts the items of every (DFA, length class), the items of the batch and,
+// The planning kernels run with the same grid of at most kMaxPlanCtas CTAs of
+// kPlanThreads threads, and CTA c takes the tiles of kPlanThreads consecutive
+// strings t = c, c + G, c + 2G, ... in both: so the fill meets exactly the
+// items the count saw, and each CTA writes its items into a range of every
+// queue class reserved for it alone (no global atomics on the hot counters).
+
+// Counts the items of every (DFA, length class) and the map slots of this CTA's
+// strings into its row of cta_bins / cta_maps, and the items of the batch and,
 // per DFA, its bytes (in 64-byte units: they only weigh the CTAs' first
-// automaton). Warps walk tiles of consecutive strings, so all lanes take part
-// in the warp-level aggregation.
-__global__ void plan_count_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n,
-                                  int64_t total_bytes, const DfaDesc *desc, int n_dfas,
-                                  int32_t seg_len, uint32_t base_mis, int64_t multi_n,
-                                  uint32_t *cls_count, unsigned long long *q_bytes,
-                                  unsigned long long *n_items, uint32_t *err) {
+// automaton).
+__global__ void __launch_bounds__(kPlanThreads)
+plan_count_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n, int64_t total_bytes,
+                  const DfaDesc *desc, int n_dfas, int32_t seg_len, uint32_t base_mis, int64_t multi_n,
+                  uint32_t *cta_bins, uint32_t *cta_maps, unsigned long long *q_bytes,
+                  unsigned long long *n_items, uint32_t *err) {
     __shared__ uint32_t cnt[kMaxDfasPerSet * kLenClasses];
     __shared__ unsigned long long byt[kMaxDfasPerSet];
     __shared__ unsigned long long items;
+    __shared__ uint32_t maps;
     const uint32_t lane = threadIdx.x & 31u;
-    for (int t = threadIdx.x; t < n_dfas * kLenClasses; t += blockDim.x) cnt[t] = 0;
+    const int n_bins = n_dfas * kLenClasses;
+    for (int t = threadIdx.x; t < n_bins; t += blockDim.x) cnt[t] = 0;
     for (int t = threadIdx.x; t < n_dfas; t += blockDim.x) byt[t] = 0;
-    if (threadIdx.x == 0) items = 0;
+    if (threadIdx.x == 0) { items = 0; maps = 0; }
     __syncthreads();
-    for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x; i0 < n; i0 += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t i = i0 + threadIdx.x;
+    for (int64_t tile = blockIdx.x; tile * kPlanThreads < n; tile += gridDim.x) {
+        const int64_t i = tile * kPlanThreads + threadIdx.x;
         int64_t len = 0, s0 = 0;
         int d = i < n ? checked_dfa(offsets, dfa_id, i, n_dfas, total_bytes, err, &len, &s0, multi_n)
                       : -1;
@@ -244,7 +262,9 @@ __global__ void plan_count_kernel(const int64_t *offsets, const int32_t *dfa_id,
         warp_count(cnt, d >= 0, kb + ic.last);
         if (d >= 0 && k > 2) atomicAdd(&cnt[kb + ic.mid], k - 2);
         const uint32_t ksum = __reduce_add_sync(0xffffffffu, k);
+        const uint32_t msum = __reduce_add_sync(0xffffffffu, k > 1 ? k : 0u);
         if (lane == 0 && ksum) atomicAdd(&items, (unsigned long long)ksum);
+        if (lane == 0 && msum) atomicAdd(&maps, msum);
         const uint32_t units = d >= 0 ? (uint32_t)min((len + 127) >> 6, (int64_t)1 << 26) : 0u;
         for (uint32_t rem = __ballot_sync(0xffffffffu, d >= 0); rem;) {   // one pass per DFA
             const int leader = __ffs(rem) - 1;
@@ -255,77 +275,142 @@ __global__ void plan_count_kernel(const int64_t *offsets, const int32_t *dfa_id,
         }
     }
     __syncthreads();
-    if (threadIdx.x == 0 && items) atomicAdd(n_items, items);
-    for (int t = threadIdx.x; t < n_dfas * kLenClasses; t += blockDim.x)
-        if (cnt[t]) atomicAdd(&cls_count[t], cnt[t]);
+    uint32_t *row = cta_bins + (size_t)blockIdx.x * n_bins;
+    for (int t = threadIdx.x; t < n_bins; t += blockDim.x) row[t] = cnt[t];
+    if (threadIdx.x == 0) {
+        cta_maps[blockIdx.x] = maps;
+        if (items) atomicAdd(n_items, items);
+    }
     for (int t = threadIdx.x; t < n_dfas; t += blockDim.x)
         if (byt[t]) atomicAdd(&q_bytes[t], byt[t]);
 }
 
-// Queue bases per (DFA, length class), one thread per DFA (kMaxDfasPerSet
-// threads). cls_cursor gets each class's start and cls_count is overwritten
-// with each class's end, against which the ragged kernel checks the fill.
-// Offsets that overlap (each string in range, but their lengths summing past
-// total_bytes) would need more items than the scratch was sized for: then the
-// error bit is set and every queue is left empty, so neither the fill kernel
-// nor the ragged kernel writes an item.
-__global__ void plan_scan_kernel(uint32_t *cls_count, uint32_t *cls_cursor, uint32_t *q_base,
-                                 uint32_t *q_count, int n_dfas, const unsigned long long *n_items,
-                                 int64_t max_items, uint32_t *err) {
-    __shared__ uint32_t tot[kMaxDfasPerSet];
-    const int d = threadIdx.x;
+// One CTA of kPlanThreads threads. Turns the per-CTA counts of the G planning
+// CTAs into positions: over each class b, the exclusive prefix of the CTAs'
+// counts (written over cta_bins), so that class b of CTA c starts at
+// bin_base[b] + cta_bins[c][b]; classes follow each other by DFA and, inside a
+// DFA, by class (each DFA's queue is one range, longest items first). bin_end
+// gets each class's end and cta_maps each CTA's first map slot (cta_maps[G]:
+// the total). Offsets that overlap (each string in range, but their lengths
+// summing past total_bytes) would need more items than the scratch was sized
+// for: then the error bit is set and every queue is left empty, so neither the
+// fill kernel nor the ragged kernel writes an item.
+__global__ void __launch_bounds__(kPlanThreads)
+plan_scan_kernel(uint32_t *cta_bins, uint32_t *bin_base, uint32_t *bin_end, uint32_t *cta_maps, int G,
+                 int n_dfas, uint32_t *q_base, uint32_t *q_count, const unsigned long long *n_items,
+                 int64_t max_items, uint32_t *err) {
+    constexpr int kPer = kMaxDfasPerSet * kLenClasses / kPlanThreads;   // classes a thread (pass 2)
+    constexpr int kRows = 16;                                           // CTAs' counts in flight
+    __shared__ uint32_t s_tot[kMaxDfasPerSet * kLenClasses];
+    __shared__ uint32_t s_warp[kPlanThreads / 32];
+    const int n_bins = n_dfas * kLenClasses;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     if (*n_items > (unsigned long long)max_items) {
-        if (d == 0) atomicOr(err, kErrCapacity);
-        if (d < n_dfas) q_base[d] = q_count[d] = 0;
+        if (threadIdx.x == 0) atomicOr(err, kErrCapacity);
+        if ((int)threadIdx.x < n_dfas) q_base[threadIdx.x] = q_count[threadIdx.x] = 0;
         return;
     }
-    uint32_t sum = 0;
-    if (d < n_dfas)
-        for (int c = 0; c < kLenClasses; ++c) sum += cls_count[d * kLenClasses + c];
-    tot[d] = sum;
-    __syncthreads();
-    if (d == 0) {
+    // pass 1: per class, the exclusive prefix over the CTAs (kRows loads in flight)
+    for (int b = threadIdx.x; b < n_bins; b += kPlanThreads) {
         uint32_t run = 0;
-        for (int k = 0; k < n_dfas; ++k) {
-            const uint32_t v = tot[k];
-            tot[k] = run;
-            run += v;
+        for (int c0 = 0; c0 < G; c0 += kRows) {
+            uint32_t v[kRows];
+#pragma unroll
+            for (int u = 0; u < kRows; ++u) v[u] = c0 + u < G ? cta_bins[(size_t)(c0 + u) * n_bins + b] : 0u;
+#pragma unroll
+            for (int u = 0; u < kRows; ++u)
+                if (c0 + u < G) {
+                    cta_bins[(size_t)(c0 + u) * n_bins + b] = run;
+                    run += v[u];
+                }
         }
+        s_tot[b] = run;
     }
     __syncthreads();
-    if (d < n_dfas) {
-        uint32_t run = tot[d];
-        q_base[d] = run;
-        q_count[d] = sum;
-        for (int c = 0; c < kLenClasses; ++c) {
-            cls_cursor[d * kLenClasses + c] = run;
-            run += cls_count[d * kLenClasses + c];
-            cls_count[d * kLenClasses + c] = run;
+    // pass 2: exclusive scan of the class totals in class order (thread t: classes kPer t ..)
+    uint32_t tot[kPer], mine = 0;
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+        const int b = kPer * (int)threadIdx.x + j;
+        tot[j] = b < n_bins ? s_tot[b] : 0u;
+        mine += tot[j];
+    }
+    uint32_t incl = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (uint32_t)o) incl += v;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t w = s_warp[lane];
+        uint32_t wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= (uint32_t)o) wi += v;
         }
+        s_warp[lane] = wi - w;
+    }
+    __syncthreads();
+    uint32_t base = s_warp[warp] + incl - mine;
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+        const int b = kPer * (int)threadIdx.x + j;
+        if (b < n_bins) {
+            bin_base[b] = base;
+            bin_end[b] = base + tot[j];
+            if (b % kLenClasses == 0) q_base[b / kLenClasses] = base;
+            if (b % kLenClasses == kLenClasses - 1) q_count[b / kLenClasses] = base + tot[j];
+        }
+        base += tot[j];
+    }
+    __syncthreads();
+    if ((int)threadIdx.x < n_dfas) q_count[threadIdx.x] -= q_base[threadIdx.x];
+    if (threadIdx.x == 0) {
+        uint32_t run = 0;
+        for (int c = 0; c < G; ++c) {
+            const uint32_t v = cta_maps[c];
+            cta_maps[c] = run;
+            run += v;
+        }
+        cta_maps[G] = run;
     }
 }
 
-// Writes the work items. Strings are handled in tiles of kPlanThreads; the
-// queue positions of a tile are reserved with one global atomic per
-// (DFA, length class) and ranks come from shared-memory atomics.
+// Writes the work items. CTA c takes the same tiles as in plan_count_kernel and
+// hands out positions from its own ranges (shared-memory counters starting at
+// its bases). A position outside the CTA's range of a class, or a range not
+// filled exactly at the end (offsets rewritten while the plan ran), raises the
+// capacity bit: the ragged kernel then trusts no item.
 __global__ void __launch_bounds__(kPlanThreads)
 plan_fill_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n, int64_t total_bytes,
                  const DfaDesc *desc, int n_dfas, int32_t seg_len, uint32_t base_mis,
-                 int64_t multi_n, uint32_t *cls_cursor, uint32_t *map_cursor, WorkItem *items,
-                 int64_t max_items, uint32_t *str_map, uint32_t *err) {
-    __shared__ uint32_t s_cnt[kMaxDfasPerSet * kLenClasses];
-    __shared__ uint32_t s_base[kMaxDfasPerSet * kLenClasses];
-    __shared__ uint32_t s_map, s_map_base;
-    const int n_slots = n_dfas * kLenClasses;
+                 int64_t multi_n, const uint32_t *cta_bins, const uint32_t *bin_base,
+                 const uint32_t *bin_end, const uint32_t *cta_maps, WorkItem *items, int64_t max_items,
+                 uint32_t *str_map, uint32_t *err) {
+    __shared__ uint32_t s_pos[kMaxDfasPerSet * kLenClasses];
+    __shared__ uint32_t s_end[kMaxDfasPerSet * kLenClasses];
+    __shared__ uint32_t s_map, s_map_end;
+    const int n_bins = n_dfas * kLenClasses;
+    const int G = gridDim.x, c = blockIdx.x;
     if (*(volatile uint32_t *)err & kErrCapacity) return;   // set by plan_scan_kernel: no items
-    for (int t = threadIdx.x; t < n_slots; t += blockDim.x) s_cnt[t] = 0;
-    if (threadIdx.x == 0) s_map = 0;
+    for (int t = threadIdx.x; t < n_bins; t += blockDim.x) {
+        s_pos[t] = bin_base[t] + cta_bins[(size_t)c * n_bins + t];
+        s_end[t] = c + 1 < G ? bin_base[t] + cta_bins[(size_t)(c + 1) * n_bins + t] : bin_end[t];
+    }
+    if (threadIdx.x == 0) {
+        s_map = cta_maps[c];
+        s_map_end = cta_maps[c + 1];
+    }
     __syncthreads();
+    bool bad = false;
     for (int64_t tile = blockIdx.x; tile * kPlanThreads < n; tile += gridDim.x) {
         const int64_t i = tile * kPlanThreads + threadIdx.x;
         int d = -1;
         int64_t len = 0, s0 = 0;
-        uint32_t k = 0, r0 = 0, rm = 0, r_last = 0, r_map = 0;
+        uint32_t k = 0, p_first = 0, p_mid = 0, p_last = 0, mb = 0;
         ItemClasses ic{0, 0, 0};
         ItemGeom g{0, 0, 0};
         if (i < n) d = checked_dfa(offsets, dfa_id, i, n_dfas, total_bytes, err, &len, &s0, multi_n);
@@ -336,10 +421,10 @@ plan_fill_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n, int64
             ic.first += d * kLenClasses;
             ic.mid += d * kLenClasses;
             ic.last += d * kLenClasses;
-            if (k > 2) rm = atomicAdd(&s_cnt[ic.mid], k - 2);
+            if (k > 2) p_mid = atomicAdd(&s_pos[ic.mid], k - 2);
         }
-        r0 = warp_rank(s_cnt, d >= 0 && k > 1, ic.first);
-        r_last = warp_rank(s_cnt, d >= 0, ic.last);
+        p_first = warp_rank(s_pos, d >= 0 && k > 1, ic.first);
+        p_last = warp_rank(s_pos, d >= 0, ic.last);
         {   // map slots of split strings: a warp prefix sum, one shared atomic a warp
             const uint32_t lane = threadIdx.x & 31u;
             const uint32_t want = (d >= 0 && k > 1) ? k : 0u;
@@ -352,29 +437,22 @@ plan_fill_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n, int64
             uint32_t wb = 0;
             if (lane == 31 && incl) wb = atomicAdd(&s_map, incl);
             wb = __shfl_sync(0xffffffffu, wb, 31);
-            r_map = wb + incl - want;
+            mb = wb + incl - want;
         }
-        __syncthreads();
-        for (int t = threadIdx.x; t < n_slots; t += blockDim.x)
-            if (s_cnt[t]) s_base[t] = atomicAdd(&cls_cursor[t], s_cnt[t]);
-        if (threadIdx.x == 0 && s_map) s_map_base = atomicAdd(map_cursor, s_map);
-        __syncthreads();
-        // this string's item positions: first, first middle and last item
-        uint32_t mb = 0, warm = 0, p_first = 0, p_mid = 0, p_last = 0, start = 0;
+        uint32_t warm = 0, start = 0;
         if (d >= 0) {
-            mb = k > 1 ? s_map_base + r_map : 0u;
             warm = (uint32_t)warm_bytes(desc[d].n_states, g.seg);
-            // With the counts of plan_count_kernel every position and map slot is
-            // below max_items; offsets rewritten between the two planning kernels
-            // (a caller changing inputs in flight) could break that: refuse.
-            if ((int64_t)mb + (int64_t)k > max_items) {
-                atomicOr(err, kErrCapacity);
+            // every position must lie in this CTA's ranges (true when the offsets did not
+            // change since the count): else no item of this string is written
+            const bool in = (k <= 1 || (uint64_t)p_first < s_end[ic.first]) &&
+                            (k <= 2 || (uint64_t)p_mid + (k - 2) <= s_end[ic.mid]) &&
+                            p_last < s_end[ic.last] &&
+                            (k <= 1 || ((uint64_t)mb + k <= s_map_end && (int64_t)mb + k <= max_items));
+            if (!in) {
+                bad = true;
                 k = 0;
             }
             if (k > 1) str_map[i] = mb;
-            if (k > 1) p_first = s_base[ic.first] + r0;
-            if (k > 2) p_mid = s_base[ic.mid] + rm;
-            if (k > 0) p_last = s_base[ic.last] + r_last;
             start = (uint32_t)desc[d].start;
         } else {
             k = 0;
@@ -409,7 +487,7 @@ plan_fill_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n, int64
                 const uint32_t j = t - (io - ko);   // the item's index in its string
                 const uint32_t pos = (j + 1 == ko) ? pl : j == 0 ? pf : pm + (j - 1);
                 if ((int64_t)pos >= max_items) {
-                    atomicOr(err, kErrCapacity);
+                    bad = true;
                     continue;
                 }
                 int64_t b0, b1;
@@ -418,11 +496,12 @@ plan_fill_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n, int64
                                       : WorkItem{b0 - wo, b1, stro, j | (ko << 16), mbo, wo << 8};
             }
         }
-        __syncthreads();
-        for (int t = threadIdx.x; t < n_slots; t += blockDim.x) s_cnt[t] = 0;
-        if (threadIdx.x == 0) s_map = 0;
-        __syncthreads();
     }
+    __syncthreads();
+    // every range of this CTA must have been filled exactly
+    for (int t = threadIdx.x; t < n_bins; t += blockDim.x) bad |= s_pos[t] != s_end[t];
+    if (threadIdx.x == 0) bad |= s_map != s_map_end;
+    if (bad) atomicOr(err, kErrCapacity);
 }
 
 // ---- main kernel -------------------------------------------------------------------------
@@ -440,10 +519,8 @@ struct RaggedParams {
     const uint32_t *q_count;
     uint32_t *q_head;
     const unsigned long long *q_bytes;
-    const uint32_t *cls_count;
-    const uint32_t *cls_cursor;
     uint32_t *err;
-    uint32_t *maps;
+    uint64_t *maps;
     const uint32_t *str_map;
     const int32_t *dfa_id;
     int64_t n;
@@ -463,11 +540,13 @@ __device__ __forceinline__ void write_result(const RaggedParams &P, uint32_t str
     if (P.accept_i32) P.accept_i32[str] = a ? 1 : 0;
 }
 
-// Records (guessed entry state, end state) of one item of a split string;
-// compose_kernel chains the items of the string after the walk.
+// Record of one item of a split string, for compose_kernel, which chains the
+// items of the string after the walk: bits 0-7 the guessed entry state (the
+// state after the warm-up; the start state for the first item), 8-15 the end
+// state, 16-47 the checkpoints (four states, see capture_cp).
 __device__ __forceinline__ void publish_item(const RaggedParams &P, uint32_t segn, uint32_t mb,
-                                             uint32_t guess, uint32_t fin) {
-    P.maps[mb + (segn & 0xffffu)] = guess | (fin << 8);
+                                             uint32_t guess, uint32_t fin, uint32_t cps) {
+    P.maps[mb + (segn & 0xffffu)] = (uint64_t)(guess | (fin << 8)) | ((uint64_t)cps << 16);
 }
 
 // One item of a batch, as a lane holds it (segn == 0: no item).
@@ -716,7 +795,34 @@ __device__ inline void build_gram_tables(const DfaDesc &D, const uint8_t *__rest
 // Shared memory after the tables: the two work items every thread walks (16
 // 32-bit words a thread).
 constexpr uint32_t kLaneItemsOff = kFallbackOff + kFallbackBytes;
-constexpr uint32_t kRaggedSmemBytes = kLaneItemsOff + kRaggedThreads * 2 * (uint32_t)sizeof(WorkItem);
+// Then one 32-bit word a thread and chain: the checkpoints of the chain's item.
+constexpr uint32_t kCpOff = kLaneItemsOff + kRaggedThreads * 2 * (uint32_t)sizeof(WorkItem);
+constexpr uint32_t kRaggedSmemBytes = kCpOff + kRaggedThreads * 2 * 4;
+
+// Checkpoints of an item after the first of its string: its chain's state at
+// the start of windows cw + 1, cw + 2, cw + 4 and cw + 8 (32, 64, 128 and 256
+// bytes into the item's own bytes, which start on a window boundary), one byte
+// each (encoded) of the thread's word for the chain. Called at the start of
+// window `it`; any other window stores nothing.
+__device__ __forceinline__ void capture_cp(int chain, uint32_t it, uint32_t cw, uint32_t e) {
+    const uint32_t d = it - cw;
+    if (d - 1u < 8u && (d & (d - 1u)) == 0u)
+        g_dfa_tbl[kCpOff + (chain * kRaggedThreads + threadIdx.x) * 4 + (__ffs(d) - 1)] = (uint8_t)e;
+}
+// The four checkpoints of a finished item, decoded, packed one byte each; a
+// checkpoint at or past the item's last window is its end state.
+template <class W>
+__device__ __forceinline__ uint32_t checkpoints(int chain, uint32_t cw, uint32_t nw, uint32_t fin) {
+    const uint32_t raw =
+        *reinterpret_cast<volatile uint32_t *>(g_dfa_tbl + kCpOff + (chain * kRaggedThreads + threadIdx.x) * 4);
+    uint32_t cps = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const uint32_t v = cw + (1u << k) < nw ? W::dec((raw >> (8 * k)) & 0xffu) : fin;
+        cps |= v << (8 * k);
+    }
+    return cps;
+}
 
 // A lane's item as the walk sees it: windows [wp, wp + 32 nw), the item's
 // bytes from byte lo of the first window to byte he - 1 of the last; the
@@ -773,7 +879,7 @@ __device__ __forceinline__ WorkItem read_slot(const uint32_t *slot) {
 // before this window keeps its state.
 template <class M>
 __device__ __forceinline__ void masked_window(const RaggedParams &P, const M &md, const DfaDesc &D,
-                                              const uint32_t *slot, uint32_t it, uint32_t &e,
+                                              const uint32_t *slot, int chain, uint32_t it, uint32_t &e,
                                               uint32_t &cap_e, uint4 &a, uint4 &b) {
     const uint32_t FULL = 0xffffffffu;
     const WorkItem w = read_slot(slot);
@@ -785,6 +891,7 @@ __device__ __forceinline__ void masked_window(const RaggedParams &P, const M &md
     const uint32_t m = bit_range((int)mlo, (int)mhi);
     const bool cap = it == v.cw;
     if (cap && v.cpos == 0) cap_e = e;   // the warm-up ended with the previous window
+    capture_cp(chain, it, v.cw, e);
     const bool special = (it < v.nw && (m != FULL || !md.valid(ca, cb))) || (cap && v.cpos != 0);
     const uint32_t e_in = e;
     if (!__any_sync(FULL, special)) e = md.fast(e, ca, cb);
@@ -796,14 +903,18 @@ __device__ __forceinline__ void masked_window(const RaggedParams &P, const M &md
 // record).
 template <class W>
 __device__ __forceinline__ void finish_item(const RaggedParams &P, const DfaDesc &D, const uint32_t *slot,
-                                            uint32_t e, uint32_t cap_e) {
+                                            int chain, uint32_t e, uint32_t cap_e) {
     const WorkItem w = read_slot(slot);
     if (!item_live(w)) return;
     const uint32_t fin = W::dec(e);
-    if ((w.segn >> 16) == 1)
+    if ((w.segn >> 16) == 1) {
         write_result(P, w.str, fin, D.accept_off);
-    else
-        publish_item(P, w.segn, w.map_base, (w.entry >> 8) & 0xffu ? W::dec(cap_e) : w.entry & 0xffu, fin);
+    } else if ((w.entry >> 8) & 0xffu) {
+        const ItemView v = item_view(P, w);
+        publish_item(P, w.segn, w.map_base, W::dec(cap_e), fin, checkpoints<W>(chain, v.cw, v.nw, fin));
+    } else {
+        publish_item(P, w.segn, w.map_base, w.entry & 0xffu, fin, 0u);
+    }
 }
 
 // Queue d's first item and item count, read again at each batch (volatile:
@@ -828,6 +939,8 @@ __device__ __forceinline__ void whole_windows(const M &md, uint32_t &it, uint32_
         if (CAPTURE) {
             cap0 = it == cw0 ? e0 : cap0;
             cap1 = it == cw1 ? e1 : cap1;
+            capture_cp(0, it, cw0, e0);
+            capture_cp(1, it, cw1, e1);
         }
         if (__all_sync(FULL, md.valid(a0, c0) && md.valid(a1, c1))) {
             // the next windows are loaded once the first halves are walked, so
@@ -907,6 +1020,7 @@ __device__ void drain_queue_one(const RaggedParams &P, const M &md, const DfaDes
             const uint32_t m = bit_range((int)mlo, (int)mhi);
             const bool cap = it == cw;
             if (cap && cpos == 0) cap_e = e;   // the warm-up ended with the previous window
+            capture_cp(0, it, cw, e);
             const bool special =
                 (it < nw && (m != FULL || !md.valid(ca, cbv))) || (cap && cpos != 0);
             if (!__any_sync(FULL, special)) e = md.fast(e, ca, cbv);
@@ -915,8 +1029,11 @@ __device__ void drain_queue_one(const RaggedParams &P, const M &md, const DfaDes
                 const uint32_t fin = W::dec(e);
                 if ((cur.segn >> 16) == 1)
                     write_result(P, cur.str, fin, D.accept_off);
+                else if (warm)
+                    publish_item(P, cur.segn, cur.map_base, W::dec(cap_e), fin,
+                                 checkpoints<W>(0, cw, nw, fin));
                 else
-                    publish_item(P, cur.segn, cur.map_base, warm ? W::dec(cap_e) : entry, fin);
+                    publish_item(P, cur.segn, cur.map_base, entry, fin, 0u);
             }
         }
         if (b1 >= count) break;
@@ -946,12 +1063,14 @@ __device__ __forceinline__ void edge_windows(const RaggedParams &P, const M &md,
     for (; it < end; ++it) {
         const ItemView v0 = item_view(P, read_slot(slot0)), v1 = item_view(P, read_slot(slot1));
         if (__any_sync(FULL, (it == v0.cw && v0.cpos != 0) || (it == v1.cw && v1.cpos != 0))) {
-            masked_window(P, md, D, slot0, it, e0, cap0, a0, c0);
-            masked_window(P, md, D, slot1, it, e1, cap1, a1, c1);
+            masked_window(P, md, D, slot0, 0, it, e0, cap0, a0, c0);
+            masked_window(P, md, D, slot1, 1, it, e1, cap1, a1, c1);
             continue;
         }
         cap0 = it == v0.cw ? e0 : cap0;
         cap1 = it == v1.cw ? e1 : cap1;
+        capture_cp(0, it, v0.cw, e0);
+        capture_cp(1, it, v1.cw, e1);
         const uint32_t m0 = window_mask(it, v0), m1 = window_mask(it, v1);
         const uint4 x0 = a0, y0 = c0, x1 = a1, y1 = c1;
         if (it + 1 < v0.nw) load_window(v0.wp + 32 * (size_t)(it + 1), P.data, P.data + P.total_bytes, a0, c0);
@@ -1034,8 +1153,9 @@ __device__ void drain_queue(const RaggedParams &P, const M &md, const DfaDesc &D
             const uint32_t fl = __reduce_min_sync(FULL, min(l0, l1));
             const uint32_t nw0 = __reduce_max_sync(FULL, v0.nw), nw1 = __reduce_max_sync(FULL, v1.nw);
             const uint32_t nwmax = max(nw0, nw1);
-            const uint32_t cwmax = __reduce_max_sync(FULL, max(v0.cw == 0xffffffffu ? 0u : v0.cw + 1u,
-                                                               v1.cw == 0xffffffffu ? 0u : v1.cw + 1u));
+            // the capture phase ends after the last checkpoint (window cw + 8) of any lane
+            const uint32_t cwmax = __reduce_max_sync(FULL, max(v0.cw == 0xffffffffu ? 0u : v0.cw + 9u,
+                                                               v1.cw == 0xffffffffu ? 0u : v1.cw + 9u));
             if (lane == 0) {
                 wv[1] = fl;
                 wv[2] = cwmax;
@@ -1062,8 +1182,8 @@ __device__ void drain_queue(const RaggedParams &P, const M &md, const DfaDesc &D
                                  a1, c1);
         }
         edge_windows(P, md, D, slot0, slot1, it, max(wv[3], wv[4]), e0, cap0, a0, c0, e1, cap1, a1, c1);
-        finish_item<W>(P, D, slot0, e0, cap0);
-        finish_item<W>(P, D, slot1, e1, cap1);
+        finish_item<W>(P, D, slot0, 0, e0, cap0);
+        finish_item<W>(P, D, slot1, 1, e1, cap1);
         const uint32_t b1 = wv[0], base = q_base_of(P, d), count = q_count_of(P, d);
         if (b1 >= count) break;
         write_slot(slot0, load_item(P, base, b1 + lane, count));
@@ -1082,16 +1202,12 @@ __device__ __forceinline__ void drain(const RaggedParams &P, const M &md, const 
 
 __global__ void __launch_bounds__(kRaggedThreads, 1) dfa_ragged_kernel(RaggedParams P) {
     __shared__ int s_dfa;
-    // The plan is complete when every (DFA, length class) cursor of the fill
-    // ended exactly at its class's end (reservations are disjoint, so every item
-    // slot was then written once); otherwise (capacity overflow, or offsets
-    // rewritten while the plan ran) no item is trusted.
-    bool ok = true;
-    for (int t = threadIdx.x; t < P.n_dfas * kLenClasses; t += blockDim.x)
-        ok &= P.cls_cursor[t] == P.cls_count[t];
-    const bool planned = __syncthreads_and(ok) != 0;
+    // The plan is complete when no planning CTA raised the capacity bit: each
+    // filled its disjoint ranges exactly (so every item slot was written once);
+    // otherwise (capacity overflow, or offsets rewritten while the plan ran) no
+    // item is trusted.
+    const bool planned = (*(volatile uint32_t *)P.err & kErrCapacity) == 0;
     if (threadIdx.x == 0) {
-        if (!planned) atomicOr(P.err, kErrCapacity);
         // Home DFA: CTAs are spread over DFAs in proportion to their walking
         // time, estimated as bytes x 7/8 for automata of at most 8 states (their
         // step is two instructions instead of four; measured 0.86 of the time per
@@ -1188,13 +1304,53 @@ __device__ __forceinline__ uint32_t warp_rewalk(const uint8_t *tbl, uint32_t N, 
 
 constexpr int kComposeThreads = 256;
 
-// Strings cut into several items: chains the items' (guessed entry, end state)
-// records in order, one warp per string. Item j's record is right when its
-// guessed entry equals the end state of item j - 1 (item 0 starts from the start
-// state); the first item whose guess is wrong (its warm-up chain had not
-// synchronised: rare for synchronising automata, every item after the first
-// for permutation automata) is walked again from the true state by the warp,
-// and the check goes on from there, 32 records at a time.
+// Walks bytes [p, q) of the batch from state s through a byte map in global
+// memory (L1-cached): one lane, aligned 32-byte windows.
+__device__ __forceinline__ uint32_t lane_walk(const RaggedParams &P, const uint8_t *__restrict__ tm,
+                                              uint32_t N, int64_t p, int64_t q, uint32_t s) {
+    const uint8_t *lo = P.data + p, *hi = P.data + q;
+    for (const uint8_t *w = reinterpret_cast<const uint8_t *>((uintptr_t)lo & ~(uintptr_t)31); w < hi;
+         w += 32) {
+        uint4 a, b;
+        load_window(w, lo, hi, a, b);
+        const uint32_t x[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+        for (int j = 0; j < 32; ++j)
+            if (w + j >= lo && w + j < hi) s = __ldg(tm + ((x[j >> 2] >> (8 * (j & 3))) & 0xffu) * N + s);
+    }
+    return s;
+}
+
+// Item j (> 0) of a split string whose warm-up chain missed the true entry
+// state s_in: walks the item from s_in until its state equals the recorded
+// chain's at one of the checkpoints (after 1, 2, 4 and 8 windows of its own
+// bytes); from there the two chains are one, so the item ends in the recorded
+// end state. Returns the item's end state, or 0xFFFF when the chains had not
+// met by the last checkpoint (the caller then walks the item whole).
+__device__ __noinline__ uint32_t fix_item(const RaggedParams &P, const uint8_t *__restrict__ tm, uint32_t N,
+                                          int64_t b0, int64_t b1, uint32_t s_in, uint64_t rec) {
+    // the item's own bytes start on a window boundary (aligned cuts, whole-window warm-up)
+    const int64_t a0 = b0 - (int64_t)((P.base_mis + (uint32_t)b0) & 31u);
+    int64_t p = b0;
+    uint32_t s = s_in;
+    for (int k = 0; k < 4; ++k) {
+        const int64_t q = min(a0 + ((int64_t)32 << k), b1);
+        s = lane_walk(P, tm, N, p, q, s);
+        if (q == b1) return s;
+        if (s == ((uint32_t)(rec >> (16 + 8 * k)) & 0xffu)) return (uint32_t)(rec >> 8) & 0xffu;
+        p = q;
+    }
+    return 0xFFFFu;
+}
+
+// Strings cut into several items: chains the items' records in order, one lane
+// per string. Item j's record is right when its guessed entry equals the end
+// state of item j - 1 (item 0 starts from the start state); otherwise the lane
+// walks the item from the true entry state until it meets the recorded chain at
+// a checkpoint (fix_item: about one window for synchronising automata). The
+// first item whose chains never meet (automata that do not synchronise, such
+// as permutations) is walked again whole by the warp, and the check goes on
+// from there, 32 records at a time.
 __global__ void __launch_bounds__(kComposeThreads) compose_kernel(RaggedParams P) {
     __shared__ __align__(16) uint8_t s_tbl[kComposeThreads / 32][256 * kSmallDfaStates];
     if (*(volatile uint32_t *)P.err & kErrCapacity) return;   // the plan was refused
@@ -1223,21 +1379,30 @@ __global__ void __launch_bounds__(kComposeThreads) compose_kernel(RaggedParams P
                 }
             }
         }
-        // each lane chains its own string while every guess is right
+        // each lane chains its own string, fixing wrong guesses from the checkpoints
         uint32_t st = 0, jbad = 0;
         bool help = false;
         if (k > 1) {
-            st = (P.maps[mb] >> 8) & 0xffu;   // item 0 starts from the start state
+            const uint8_t *tm = P.tmaps + P.desc[d].tmap_off;
+            const uint32_t N = (uint32_t)P.desc[d].n_states;
+            st = (uint32_t)(P.maps[mb] >> 8) & 0xffu;   // item 0 starts from the start state
             for (uint32_t j0 = 1; j0 < k && !help; j0 += 8) {
-                uint32_t v[8];   // eight records loaded together (one load latency for most strings)
+                uint64_t v[8];   // eight records loaded together (one load latency for most strings)
 #pragma unroll
-                for (int u = 0; u < 8; ++u) v[u] = j0 + u < k ? P.maps[mb + j0 + u] : 0u;
+                for (int u = 0; u < 8; ++u) v[u] = j0 + u < k ? P.maps[mb + j0 + u] : 0ull;
 #pragma unroll
                 for (int u = 0; u < 8; ++u) {
                     const uint32_t j = j0 + u;
                     if (help || j >= k) continue;
-                    if ((v[u] & 0xffu) == st) st = (v[u] >> 8) & 0xffu;
-                    else { help = true; jbad = j; }
+                    if (((uint32_t)v[u] & 0xffu) == st) {
+                        st = (uint32_t)(v[u] >> 8) & 0xffu;
+                    } else {
+                        int64_t b0, b1;
+                        item_range(g, s0, len, j, &b0, &b1);
+                        const uint32_t f = st < N ? fix_item(P, tm, N, b0, b1, st, v[u]) : 0xFFFFu;
+                        if (f != 0xFFFFu) st = f;
+                        else { help = true; jbad = j; }
+                    }
                 }
             }
             if (!help) {
@@ -1271,7 +1436,7 @@ __global__ void __launch_bounds__(kComposeThreads) compose_kernel(RaggedParams P
             for (uint32_t j0 = sj + 1; j0 < sk && s < N; j0 += 32) {
                 const uint32_t j = j0 + lane;
                 const bool in = j < sk;
-                const uint32_t v = in ? P.maps[smb + j] : 0u;
+                const uint32_t v = in ? (uint32_t)P.maps[smb + j] : 0u;
                 uint32_t g = v & 0xffu, f = (v >> 8) & 0xffu;
                 for (;;) {
                     uint32_t pf = __shfl_up_sync(FULL, f, 1);
@@ -1312,6 +1477,7 @@ struct trex_dfa_set {
     void *own_scratch = nullptr;
     size_t own_scratch_bytes = 0;
     int n_sms = 0;
+    int device = -1;   // the set's tables live on this device
     size_t smem_bytes = 0;
     // Device staging for trex_dfa_batch_host (grown on demand).
     uint8_t *st_data = nullptr;
@@ -1335,6 +1501,14 @@ static int dfa_set_run_ex(trex_dfa_set *set, const uint8_t *data, const int64_t 
     if (!set) return TREX_ERR_NOT_INIT;
     if (n_strings < 0 || total_bytes < 0 || (n_strings > 0 && !offsets) || (total_bytes > 0 && !data))
         return TREX_ERR_ARG;
+    {   // the kernels read the set's tables: they must run on the set's device
+        int dev = -1;
+        TREX_CUDA(cudaGetDevice(&dev));
+        if (dev != set->device) {
+            set_last_error_msg("trex_dfa_batch: the current device is not the device the set was created on");
+            return TREX_ERR_ARG;
+        }
+    }
     const int64_t multi_n = multi ? n_strings : 0;
     const int64_t n = multi ? n_strings * set->n_dfas : n_strings;   // strings walked
     if (n >= (int64_t)0x7fffffff) return TREX_ERR_CAPACITY;
@@ -1361,35 +1535,37 @@ static int dfa_set_run_ex(trex_dfa_set *set, const uint8_t *data, const int64_t 
     } else if ((size_t)scratch_bytes < L.total) {
         return TREX_ERR_ARG;
     }
-    uint32_t *cls_count = reinterpret_cast<uint32_t *>(sc + L.cls_count);
-    uint32_t *cls_cursor = reinterpret_cast<uint32_t *>(sc + L.cls_cursor);
     uint32_t *q_count = reinterpret_cast<uint32_t *>(sc + L.q_count);
     uint32_t *q_base = reinterpret_cast<uint32_t *>(sc + L.q_base);
     uint32_t *q_head = reinterpret_cast<uint32_t *>(sc + L.q_head);
     auto *q_bytes = reinterpret_cast<unsigned long long *>(sc + L.q_bytes);
     uint32_t *err = reinterpret_cast<uint32_t *>(sc + L.err);
-    uint32_t *map_cursor = reinterpret_cast<uint32_t *>(sc + L.map_cursor);
     auto *n_items = reinterpret_cast<unsigned long long *>(sc + L.n_items);
     WorkItem *items = reinterpret_cast<WorkItem *>(sc + L.items);
-    uint32_t *maps = reinterpret_cast<uint32_t *>(sc + L.maps);
+    uint64_t *maps = reinterpret_cast<uint64_t *>(sc + L.maps);
     uint32_t *str_map = reinterpret_cast<uint32_t *>(sc + L.str_map);
+    uint32_t *cta_bins = reinterpret_cast<uint32_t *>(sc + L.cta_bins);
+    uint32_t *bin_base = reinterpret_cast<uint32_t *>(sc + L.bin_base);
+    uint32_t *bin_end = reinterpret_cast<uint32_t *>(sc + L.bin_end);
+    uint32_t *cta_maps = reinterpret_cast<uint32_t *>(sc + L.cta_maps);
     const uint32_t base_mis = (uint32_t)((uintptr_t)data & 31u);
 
-    // Counters, bases, heads, cursors, byte counts, the error word, the map
-    // cursor and the item count are contiguous at the front of the scratch buffer.
+    // Queue bases, counts and heads, byte counts, the error word and the item
+    // count are contiguous at the front of the scratch buffer.
     TREX_CUDA(cudaMemsetAsync(sc, 0, L.items, stream));
-    int plan_grid = (int)std::min<int64_t>((n + kPlanThreads - 1) / kPlanThreads,
-                                           (int64_t)set->n_sms * 8);
+    const int plan_grid = (int)std::min<int64_t>({(n + kPlanThreads - 1) / kPlanThreads,
+                                                  (int64_t)set->n_sms, (int64_t)kMaxPlanCtas});
     plan_count_kernel<<<plan_grid, kPlanThreads, 0, stream>>>(
         offsets, dfa_id, n, total_bytes, set->d_desc, set->n_dfas, seg_len, base_mis, multi_n,
-        cls_count, q_bytes, n_items, err);
+        cta_bins, cta_maps, q_bytes, n_items, err);
     TREX_CHECK_LAUNCH();
-    plan_scan_kernel<<<1, kMaxDfasPerSet, 0, stream>>>(cls_count, cls_cursor, q_base, q_count, set->n_dfas,
-                                           n_items, L.max_items, err);
+    plan_scan_kernel<<<1, kPlanThreads, 0, stream>>>(cta_bins, bin_base, bin_end, cta_maps, plan_grid,
+                                                     set->n_dfas, q_base, q_count, n_items, L.max_items,
+                                                     err);
     TREX_CHECK_LAUNCH();
     plan_fill_kernel<<<plan_grid, kPlanThreads, 0, stream>>>(
         offsets, dfa_id, n, total_bytes, set->d_desc, set->n_dfas, seg_len, base_mis, multi_n,
-        cls_cursor, map_cursor, items, L.max_items, str_map, err);
+        cta_bins, bin_base, bin_end, cta_maps, items, L.max_items, str_map, err);
     TREX_CHECK_LAUNCH();
 
     RaggedParams P;
@@ -1406,8 +1582,6 @@ static int dfa_set_run_ex(trex_dfa_set *set, const uint8_t *data, const int64_t 
     P.q_count = q_count;
     P.q_head = q_head;
     P.q_bytes = q_bytes;
-    P.cls_count = cls_count;
-    P.cls_cursor = cls_cursor;
     P.err = err;
     P.maps = maps;
     P.str_map = str_map;
@@ -1490,7 +1664,8 @@ int trex_dfa_set_create(int n_dfas, const int32_t *n_states, const int32_t *star
     set->h_tmaps.assign(tmaps, tmaps + tsum);
     set->h_desc = desc;
     set->n_sms = trex::sm_count();
-    if (set->n_sms <= 0) {
+    if (set->n_sms <= 0 || cudaGetDevice(&set->device) != cudaSuccess) {
+        cudaGetLastError();
         delete set;
         trex::set_last_error_msg("trex_dfa_set_create: no CUDA device");
         return TREX_ERR_SHAPE;
@@ -1686,28 +1861,74 @@ constexpr int kMaxStaticDevices = 64;
 static __device__ __align__(256) uint8_t g_static_scratch[kStaticScratchBytes];
 
 // Device address of g_static_scratch on each device, looked up once per device
-// (in host code the symbol name is only a stand-in, not a device address).
-static void *g_static_scratch_ptr[kMaxStaticDevices] = {};
+// and CUDA context (in host code the symbol name is only a stand-in, not a
+// device address). The cache is keyed on the context's unique id as well as
+// the device ordinal: after cudaDeviceReset the primary context, and with it
+// the module that holds the array, is made again, and the address is looked up
+// again.
+struct StaticScratchSlot {
+    unsigned long long ctx_id = 0;
+    void *ptr = nullptr;
+};
+static StaticScratchSlot g_static_scratch_slot[kMaxStaticDevices];
 static std::mutex g_static_scratch_mu;
 
-static int static_scratch_address(void **out) {
+// The driver's context calls are reached through the runtime's entry-point
+// query, so the library keeps loading without libcuda (CPU-only hosts).
+static int current_context_id(unsigned long long *id) {
+    using GetCurrent = CUresult (*)(CUcontext *);
+    using GetId = CUresult (*)(CUcontext, unsigned long long *);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    if (!get_current || !get_id) {
+        void *a = nullptr, *b = nullptr;
+        cudaDriverEntryPointQueryResult qa, qb;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa) != cudaSuccess ||
+            cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb) != cudaSuccess ||
+            qa != cudaDriverEntryPointSuccess || qb != cudaDriverEntryPointSuccess || !a || !b) {
+            cudaGetLastError();
+            return TREX_ERR_CUDA;
+        }
+        get_current = reinterpret_cast<GetCurrent>(a);
+        get_id = reinterpret_cast<GetId>(b);
+    }
+    CUcontext ctx = nullptr;
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return TREX_ERR_CUDA;
+    return get_id(ctx, id) == CUDA_SUCCESS ? TREX_OK : TREX_ERR_CUDA;
+}
+
+static int static_scratch_address(const trex_dfa_set *set, void **out) {
     int dev = 0;
     TREX_CUDA(cudaGetDevice(&dev));
+    if (dev != set->device) {
+        set_last_error_msg("trex_dfa_batch_run_static: the current device is not the device the set "
+                           "was created on");
+        return TREX_ERR_ARG;
+    }
     if (dev < 0 || dev >= kMaxStaticDevices) {
         set_last_error_msg("trex_dfa_batch_run_static: device ordinal out of range");
         return TREX_ERR_SHAPE;
     }
     std::lock_guard<std::mutex> lock(g_static_scratch_mu);
-    if (!g_static_scratch_ptr[dev]) {
+    StaticScratchSlot &slot = g_static_scratch_slot[dev];
+    unsigned long long id = 0;
+    // no context current yet on this thread: the lookup below makes the primary one current
+    const bool known = current_context_id(&id) == TREX_OK;
+    if (!known || slot.ptr == nullptr || slot.ctx_id != id) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
         if (e != cudaSuccess || !p) {
             set_last_error("trex_dfa_batch_run_static: cudaGetSymbolAddress", e);
             return TREX_ERR_CUDA;
         }
-        g_static_scratch_ptr[dev] = p;
+        if (current_context_id(&id) != TREX_OK) {
+            set_last_error_msg("trex_dfa_batch_run_static: no current CUDA context");
+            return TREX_ERR_CUDA;
+        }
+        slot.ptr = p;
+        slot.ctx_id = id;
     }
-    *out = g_static_scratch_ptr[dev];
+    *out = slot.ptr;
     return TREX_OK;
 }
 
@@ -1728,13 +1949,33 @@ extern "C" int trex_dfa_batch_run_static(trex_dfa_set *set, const uint8_t *data,
         return TREX_ERR_CAPACITY;
     }
     void *scratch = nullptr;
-    const int rc = trex::static_scratch_address(&scratch);
+    const int rc = trex::static_scratch_address(set, &scratch);
     if (rc) return rc;
     // dfa_set_run clears the counters at the front of the scratch before use
     // and writes every item / map slot before reading it.
     return trex::dfa_set_run(set, data, offsets, dfa_id, n_strings, total_bytes, final_state,
                              accept, accept_i32, scratch, trex::kStaticScratchBytes, seg_len,
                              static_cast<cudaStream_t>(stream), nullptr);
+}
+
+extern "C" int trex_dfa_batch_static_error(trex_dfa_set *set, int32_t *err_out) {
+    // Reads the error word of the last trex_dfa_batch_run_static on the set's
+    // device straight from the static array (a copy from the symbol, no
+    // allocation); synchronises with the device.
+    if (!set) return TREX_ERR_NOT_INIT;
+    if (!err_out) return TREX_ERR_ARG;
+    int dev = 0;
+    TREX_CUDA(cudaGetDevice(&dev));
+    if (dev != set->device) {
+        trex::set_last_error_msg("trex_dfa_batch_static_error: the current device is not the device "
+                                 "the set was created on");
+        return TREX_ERR_ARG;
+    }
+    const trex::ScratchLayout L = trex::scratch_layout(0, 0, 0);
+    uint32_t v = 0;
+    TREX_CUDA(cudaMemcpyFromSymbol(&v, trex::g_static_scratch, sizeof(v), L.err, cudaMemcpyDeviceToHost));
+    *err_out = (int32_t)v;
+    return TREX_OK;
 }
 
 // ---- K-gram walking ---------------------------------------------------------------------------

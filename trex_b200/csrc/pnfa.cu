@@ -96,7 +96,10 @@ constexpr int kPnMiscBytes = 2048;
 constexpr uint32_t kPnSmemCap = 232448;
 constexpr int32_t kPnTerminate = -1;
 constexpr uint32_t kPnErrOffsets = 1u, kPnErrTimeout = 4u;
-constexpr long long kPnWaitCycles = 4000000000ll;   // about 2 s
+// The drain of committed MMAs before the TMEM is freed always waits up to the
+// default limit (an MMA still writing TMEM must not outlive the allocation);
+// the hand-off waits use PnParams::wait_cycles.
+constexpr long long kPnDrainCycles = kDefaultMbarCycles;
 
 constexpr uint32_t kRecFinish = 1u << 31;
 // slot flags (planner)
@@ -129,11 +132,13 @@ struct PnLayout {
 
 __host__ __device__ inline uint32_t pn_align16(uint32_t x) { return (x + 15u) & ~15u; }
 
-static PnLayout pn_layout(int p_sub, int sigma) {
+// acols: TMEM columns of a symbol pair's A operand (32 for 16-bit operands: 64 K
+// values of 2 bytes a lane; 16 for int8 operands: 4 K values a 32-bit column).
+static PnLayout pn_layout(int p_sub, int sigma, int acols = 32) {
     PnLayout L{};
     L.p_sub = p_sub;
     L.npairs = (sigma + 1) / 2;
-    L.ring_base = 32 * L.npairs;
+    L.ring_base = acols * L.npairs;
     L.nregions = std::min(kPnMaxRegions, (512 - L.ring_base) / kPnRegionCols);
     int rows = p_sub + 16;
     while (rows % 8 != 1) ++rows;
@@ -201,6 +206,8 @@ struct PnParams {
     const float *acc;          // [64] accept weights
     float start_max;
     int boolean;               // Boolean NFA: threshold every product to {0, 1}, no rescale
+    int kcols;                 // 16-byte core-matrix columns of a B row: 8 (16-bit), 4 (int8)
+    long long wait_cycles;     // limit of one hand-off wait
     double ll_empty;
     int sigma;
     double *loglik;
@@ -250,13 +257,13 @@ __device__ __forceinline__ void pn_mbar_arrive(uint32_t addr) {
 // given parity; bounded; the result is broadcast to the warp. Spins on the
 // non-suspending test: the hand-offs of this kernel are on its critical path.
 __device__ __forceinline__ bool pn_wait(uint32_t addr, uint32_t parity, volatile uint32_t *abort_flag,
-                                        uint32_t *err) {
+                                        uint32_t *err, long long limit) {
     int ok = 1;
     if ((threadIdx.x & 31) == 0) {
         const long long t0 = clock64();
         while (!pn_mbar_poll(addr, parity)) {
             if (*abort_flag) { ok = 0; break; }
-            if (clock64() - t0 > kPnWaitCycles) {
+            if (clock64() - t0 > limit) {
                 atomicOr(err, kPnErrTimeout);
                 *abort_flag = 1u;
                 ok = 0;
@@ -341,6 +348,16 @@ __device__ __forceinline__ void pn_tmem_st32(uint32_t taddr, const uint32_t (&r)
         : "memory");
 }
 
+__device__ __forceinline__ void pn_tmem_st16(uint32_t taddr, const uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+        "%14,%15,%16};"
+        :: "r"(taddr), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]),
+           "r"(r[7]), "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]),
+           "r"(r[14]), "r"(r[15])
+        : "memory");
+}
+
 // ---- shared-memory view -------------------------------------------------------------------------
 struct PnShared {
     uint8_t *base;
@@ -396,7 +413,7 @@ __device__ void pn_loader(const PnParams &P, const PnShared &S, volatile uint32_
     for (int blk = 0;; ++blk) {
         const int buf = blk & 1;
         if (blk >= 2 && !pn_wait(S.bar(kBarConsumed + buf), (uint32_t)((blk - 2) >> 1) & 1u,
-                                 abort_flag, P.err))
+                                 abort_flag, P.err, P.wait_cycles))
             break;
         uint8_t *sym = S.sym(buf);
         PnHdr *hd = S.hdr(buf);
@@ -483,7 +500,7 @@ __device__ void pn_loader(const PnParams &P, const PnShared &S, volatile uint32_
         }
         __syncwarp();
         // both loader warps have written the block: its active count decides the end
-        if (!pn_wait(S.bar(kBarLoaded + buf), (uint32_t)(blk >> 1) & 1u, abort_flag, P.err)) break;
+        if (!pn_wait(S.bar(kBarLoaded + buf), (uint32_t)(blk >> 1) & 1u, abort_flag, P.err, P.wait_cycles)) break;
         const volatile int32_t *ba = reinterpret_cast<const volatile int32_t *>(S.misc() + kMBlkAct);
         if (ba[buf * 2] + ba[buf * 2 + 1] == 0) break;
     }
@@ -538,11 +555,11 @@ __device__ void pn_planner(const PnParams &P, const PnShared &S, volatile uint32
         if (tid < 32) {
             bool ok = true;
             if (s >= 4)
-                ok = pn_wait(S.bar(kBarEpi + ((s - 4) & 3)), pn_par(s - 4, 4), abort_flag, P.err);
+                ok = pn_wait(S.bar(kBarEpi + ((s - 4) & 3)), pn_par(s - 4, 4), abort_flag, P.err, P.wait_cycles);
             if (ok && s % kPnBlk == 0) {
                 const int blk = s / kPnBlk;
                 if (leader && blk >= 1) pn_mbar_arrive(S.bar(kBarConsumed + ((blk - 1) & 1)));
-                ok = pn_wait(S.bar(kBarLoaded + (blk & 1)), (uint32_t)(blk >> 1) & 1u, abort_flag, P.err);
+                ok = pn_wait(S.bar(kBarLoaded + (blk & 1)), (uint32_t)(blk >> 1) & 1u, abort_flag, P.err, P.wait_cycles);
                 if (ok && leader) {
                     const volatile int32_t *ba =
                         reinterpret_cast<const volatile int32_t *>(S.misc() + kMBlkAct);
@@ -658,7 +675,7 @@ __device__ void pn_planner(const PnParams &P, const PnShared &S, volatile uint32
         // ---------------- stage 2 ----------------
         if (tid < 32) {
             bool ok = true;
-            if (s >= 2) ok = pn_wait(S.bar(kBarEpi + ((s - 2) & 3)), pn_par(s - 2, 4), abort_flag, P.err);
+            if (s >= 2) ok = pn_wait(S.bar(kBarEpi + ((s - 2) & 3)), pn_par(s - 2, 4), abort_flag, P.err, P.wait_cycles);
             if (leader) *plan_ok = ok ? 1u : 0u;
         }
         pn_plan_sync();
@@ -671,7 +688,7 @@ __device__ void pn_planner(const PnParams &P, const PnShared &S, volatile uint32
                 if ((sl.flags & kSlotFresh) == 0) continue;
                 uint8_t *dst = S.base + sb + (uint32_t)sl.row * 16u;
 #pragma unroll
-                for (int c = 0; c < 8; ++c) *reinterpret_cast<uint4 *>(dst + c * L.lbo) = simg[c];
+                for (int c = 0; c < P.kcols; ++c) *reinterpret_cast<uint4 *>(dst + c * L.lbo) = simg[c];
             }
         }
         pn_fence_async_smem();
@@ -681,7 +698,7 @@ __device__ void pn_planner(const PnParams &P, const PnShared &S, volatile uint32
             if (s >= 1) {
                 if (tid < 32) {
                     const bool ok = pn_wait(S.bar(kBarEpi + ((s - 1) & 3)), pn_par(s - 1, 4), abort_flag,
-                                            P.err);
+                                            P.err, P.wait_cycles);
                     if (leader) *plan_ok = ok ? 1u : 0u;
                 }
                 pn_plan_sync();
@@ -693,48 +710,65 @@ __device__ void pn_planner(const PnParams &P, const PnShared &S, volatile uint32
 }
 
 // ---- MMA issuer: warp 8 ----------------------------------------------------------------------------
-template <bool FP16>
+// KIND: 0 = BF16, 1 = FP16 operands (kind::f16, FP32 sums), 2 = 0/1 int8 operands
+// (kind::i8, unsigned, int32 sums: K = 32 an instruction, half the instructions).
+template <int KIND>
 __device__ void pn_mma(const PnParams &P, const PnShared &S, uint32_t tbase,
                        volatile uint32_t *abort_flag) {
+    constexpr bool I8 = KIND == 2;
+    constexpr int kKSteps = I8 ? 2 : 4;              // K = 64 as 2 x K32 or 4 x K16
+    constexpr uint32_t kACols = I8 ? 16u : 32u;      // TMEM columns of a pair's A
     const int lane = threadIdx.x & 31;
     const PnLayout &L = S.L;
-    const uint32_t fmt = FP16 ? 0u : 1u;
+    const uint32_t fmt = KIND == 1 ? 0u : 1u;
     const uint32_t smem_base = pn_smem_u32(S.base);
     const uint32_t desc_hi = (128u >> 4) | (1u << 14);   // SBO = 128 B, descriptor version 1
     const uint32_t nr = (uint32_t)L.nregions;
     uint32_t g = 0;
     for (int t = 0;; ++t) {
-        if (!pn_wait(S.bar(kBarPlan2 + (t & 1)), pn_par(t, 2), abort_flag, P.err)) break;
+        if (!pn_wait(S.bar(kBarPlan2 + (t & 1)), pn_par(t, 2), abort_flag, P.err, P.wait_cycles)) break;
         const int nch = *S.nch(t);
         if (nch == kPnTerminate) break;
-        if (t >= 1 && !pn_wait(S.bar(kBarEpi + ((t - 1) & 3)), pn_par(t - 1, 4), abort_flag, P.err)) break;
+        if (t >= 1 && !pn_wait(S.bar(kBarEpi + ((t - 1) & 3)), pn_par(t - 1, 4), abort_flag, P.err, P.wait_cycles)) break;
         const PnChunk *ch = S.chunks(t);
         const uint32_t sb = smem_base + S.sbuf(t & 1);
         bool aborted = false;
         for (int k = 0; k < nch; ++k) {
             const PnChunk d = ch[k];
             const uint32_t r = g % nr, u = g / nr;
-            if (u > 0 && !pn_wait(S.bar(kBarEmpty + (int)r), (u - 1) & 1u, abort_flag, P.err)) {
+            if (u > 0 && !pn_wait(S.bar(kBarEmpty + (int)r), (u - 1) & 1u, abort_flag, P.err, P.wait_cycles)) {
                 aborted = true;
                 break;
             }
             pn_tc_after();
             if (lane == 0) {
                 const uint32_t n16 = ((uint32_t)d.ncols + 15u) & ~15u;
-                const uint32_t idesc = (1u << 4) | (fmt << 7) | (fmt << 10) | ((n16 >> 3) << 17) |
-                                       ((128u >> 4) << 24);
+                // instruction descriptor: D format (bits 4-5: F32 = 1, S32 = 2), A and B
+                // formats (bits 7-9, 10-12: F16 = 0 / BF16 = 1; U8 = 0), N / 8 (17-22),
+                // M / 16 (24-28); both operands K-major
+                const uint32_t idesc = I8 ? ((2u << 4) | ((n16 >> 3) << 17) | ((128u >> 4) << 24))
+                                          : ((1u << 4) | (fmt << 7) | (fmt << 10) | ((n16 >> 3) << 17) |
+                                             ((128u >> 4) << 24));
                 const uint32_t td = tbase + (uint32_t)L.ring_base + r * kPnRegionCols;
+                // every K step spans two 16-byte core-matrix columns of B (16 states of
+                // 16 bits, or 32 states of 8 bits) and 8 TMEM columns of A
 #pragma unroll
-                for (int kk = 0; kk < 4; ++kk) {
+                for (int kk = 0; kk < kKSteps; ++kk) {
                     const uint32_t saddr = sb + (uint32_t)d.row0 * 16u + (uint32_t)kk * 2u * L.lbo;
                     const uint64_t desc = (uint64_t)(((saddr >> 4) & 0x3FFFu) | ((L.lbo >> 4) << 16)) |
                                           ((uint64_t)desc_hi << 32);
-                    const uint32_t ta = tbase + 32u * d.pair + 8u * kk;
+                    const uint32_t ta = tbase + kACols * d.pair + 8u * kk;
                     const uint32_t acc = kk > 0;
-                    asm volatile(
-                        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}"
-                        :: "r"(td), "r"(ta), "l"(desc), "r"(idesc), "r"(acc) : "memory");
+                    if constexpr (I8)
+                        asm volatile(
+                            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                            "tcgen05.mma.cta_group::1.kind::i8 [%0], [%1], %2, %3, p;\n\t}"
+                            :: "r"(td), "r"(ta), "l"(desc), "r"(idesc), "r"(acc) : "memory");
+                    else
+                        asm volatile(
+                            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                            "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}"
+                            :: "r"(td), "r"(ta), "l"(desc), "r"(idesc), "r"(acc) : "memory");
                 }
                 asm volatile(
                     "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
@@ -751,7 +785,7 @@ __device__ void pn_mma(const PnParams &P, const PnShared &S, uint32_t tbase,
         if (lane == 0) {                               // completion of the last one
             const long long t0 = clock64();
             while (!pn_mbar_test(S.bar(kBarFull + (int)r), (uses - 1) & 1u)) {
-                if (clock64() - t0 > kPnWaitCycles) { atomicOr(P.err, kPnErrTimeout); break; }
+                if (clock64() - t0 > kPnDrainCycles) { atomicOr(P.err, kPnErrTimeout); break; }
             }
         }
         __syncwarp();
@@ -767,9 +801,10 @@ __device__ void pn_mma(const PnParams &P, const PnShared &S, uint32_t tbase,
 // threads holding the same columns. The scale of a column, 2^-f with f the exponent of
 // max|s_t| * R_c (max|s_t| left by the previous step's epilogue), is computed by one lane per
 // column and shuffled to the others; warps q = 0, 2 keep the exponent sums.
-template <bool FP16>
+template <int KIND>
 __device__ void pn_epilogue(const PnParams &P, const PnShared &S, uint32_t tbase,
                             volatile uint32_t *abort_flag) {
+    constexpr bool I8 = KIND == 2, FP16 = KIND == 1;
     const int lane = threadIdx.x & 31;
     const int ew = threadIdx.x >> 5;
     const int q = ew & 3;                           // TMEM lane quadrant
@@ -777,8 +812,12 @@ __device__ void pn_epilogue(const PnParams &P, const PnShared &S, uint32_t tbase
     const PnLayout &L = S.L;
     const int j = lane >> 2, cp = lane & 3;
     const int sg0 = 32 * (q & 1) + 2 * j, sg1 = sg0 + 16;   // first states of the two pairs
-    const uint32_t toff0 = (uint32_t)(sg0 >> 3) * L.lbo + (uint32_t)(sg0 & 7) * 2u;
-    const uint32_t toff1 = (uint32_t)(sg1 >> 3) * L.lbo + (uint32_t)(sg1 & 7) * 2u;
+    // byte offsets of states sg0 and sg1 in a B row: 8 states of 16 bits, or 16 of 8 bits, a
+    // core-matrix column
+    const uint32_t toff0 = I8 ? (uint32_t)(sg0 >> 4) * L.lbo + (uint32_t)(sg0 & 15)
+                              : (uint32_t)(sg0 >> 3) * L.lbo + (uint32_t)(sg0 & 7) * 2u;
+    const uint32_t toff1 = I8 ? (uint32_t)(sg1 >> 4) * L.lbo + (uint32_t)(sg1 & 15)
+                              : (uint32_t)(sg1 >> 3) * L.lbo + (uint32_t)(sg1 & 7) * 2u;
     const float *accv = reinterpret_cast<const float *>(S.misc() + kMAcc);
     const float a00 = accv[sg0], a01 = accv[sg0 + 1], a10 = accv[sg1], a11 = accv[sg1 + 1];
     const float *rsym = reinterpret_cast<const float *>(S.misc() + kMRsym);
@@ -788,13 +827,13 @@ __device__ void pn_epilogue(const PnParams &P, const PnShared &S, uint32_t tbase
     int32_t *E = S.E();
     const uint32_t nr = (uint32_t)L.nregions;
     uint32_t g = 0;
-    if (!pn_wait(S.bar(kBarPlan1), 0u, abort_flag, P.err)) return;
+    if (!pn_wait(S.bar(kBarPlan1), 0u, abort_flag, P.err, P.wait_cycles)) return;
     for (int t = 0;; ++t) {
         const int nch = *S.nch(t);   // plan of step t: waited for in the previous iteration
         if (nch == kPnTerminate) break;
         // records of step t come with the plan of step t+1; the maxima of step t from both sets
-        if (!pn_wait(S.bar(kBarPlan1 + ((t + 1) & 3)), pn_par(t + 1, 4), abort_flag, P.err)) break;
-        if (t >= 1 && !pn_wait(S.bar(kBarEpi + ((t - 1) & 3)), pn_par(t - 1, 4), abort_flag, P.err)) break;
+        if (!pn_wait(S.bar(kBarPlan1 + ((t + 1) & 3)), pn_par(t + 1, 4), abort_flag, P.err, P.wait_cycles)) break;
+        if (t >= 1 && !pn_wait(S.bar(kBarEpi + ((t - 1) & 3)), pn_par(t - 1, 4), abort_flag, P.err, P.wait_cycles)) break;
         const PnChunk *ch = S.chunks(t);
         const uint2 *rec = S.rec(t);
         const float2 *xm = S.xmax(t);
@@ -807,7 +846,7 @@ __device__ void pn_epilogue(const PnParams &P, const PnShared &S, uint32_t tbase
             if ((g & 1u) != set) continue;
             const PnChunk d = ch[k];
             const uint32_t r = g % nr, u = g / nr;
-            if (!pn_wait(S.bar(kBarFull + (int)r), u & 1u, abort_flag, P.err)) {
+            if (!pn_wait(S.bar(kBarFull + (int)r), u & 1u, abort_flag, P.err, P.wait_cycles)) {
                 aborted = true;
                 break;
             }
@@ -865,11 +904,18 @@ __device__ void pn_epilogue(const PnParams &P, const PnShared &S, uint32_t tbase
 #pragma unroll
                 for (int i = 0; i < 4; ++i) {
                     const int ri = (i >> 1) * 4 + (i & 1);
-                    x[i][0] = __uint_as_float(v0[ri]) * sc[i];       // state sg0
-                    x[i][1] = __uint_as_float(v0[ri + 2]) * sc[i];   // sg0 + 1
-                    x[i][2] = __uint_as_float(v1[ri]) * sc[i];       // sg1
-                    x[i][3] = __uint_as_float(v1[ri + 2]) * sc[i];   // sg1 + 1
-                    if (bmode) {   // reachability: exact, the sums are small integers
+                    if constexpr (I8) {   // int32 path counts: reachable when nonzero
+                        x[i][0] = v0[ri] != 0u ? 1.f : 0.f;
+                        x[i][1] = v0[ri + 2] != 0u ? 1.f : 0.f;
+                        x[i][2] = v1[ri] != 0u ? 1.f : 0.f;
+                        x[i][3] = v1[ri + 2] != 0u ? 1.f : 0.f;
+                    } else {
+                        x[i][0] = __uint_as_float(v0[ri]) * sc[i];       // state sg0
+                        x[i][1] = __uint_as_float(v0[ri + 2]) * sc[i];   // sg0 + 1
+                        x[i][2] = __uint_as_float(v1[ri]) * sc[i];       // sg1
+                        x[i][3] = __uint_as_float(v1[ri + 2]) * sc[i];   // sg1 + 1
+                    }
+                    if (!I8 && bmode) {   // reachability: exact, the sums are small integers
 #pragma unroll
                         for (int z = 0; z < 4; ++z) x[i][z] = x[i][z] > 0.f ? 1.f : 0.f;
                     }
@@ -878,8 +924,15 @@ __device__ void pn_epilogue(const PnParams &P, const PnShared &S, uint32_t tbase
                     any_fin |= valid[i] && fin_i;
                     if (keep) {
                         uint8_t *dst = snext + rc[i].x;
-                        *reinterpret_cast<uint32_t *>(dst + toff0) = pn_pack2<FP16>(x[i][0], x[i][1]);
-                        *reinterpret_cast<uint32_t *>(dst + toff1) = pn_pack2<FP16>(x[i][2], x[i][3]);
+                        if constexpr (I8) {   // two adjacent states, one byte each
+                            *reinterpret_cast<uint16_t *>(dst + toff0) =
+                                (uint16_t)((x[i][0] != 0.f ? 1u : 0u) | (x[i][1] != 0.f ? 0x100u : 0u));
+                            *reinterpret_cast<uint16_t *>(dst + toff1) =
+                                (uint16_t)((x[i][2] != 0.f ? 1u : 0u) | (x[i][3] != 0.f ? 0x100u : 0u));
+                        } else {
+                            *reinterpret_cast<uint32_t *>(dst + toff0) = pn_pack2<FP16>(x[i][0], x[i][1]);
+                            *reinterpret_cast<uint32_t *>(dst + toff1) = pn_pack2<FP16>(x[i][2], x[i][3]);
+                        }
                     }
                     m[i] = keep ? fmaxf(fmaxf(fabsf(x[i][0]), fabsf(x[i][1])),
                                         fmaxf(fabsf(x[i][2]), fabsf(x[i][3])))
@@ -922,7 +975,7 @@ __device__ void pn_epilogue(const PnParams &P, const PnShared &S, uint32_t tbase
     }
 }
 
-template <bool FP16>
+template <int KIND>
 __global__ void __launch_bounds__(kPnThreads, 1) pnfa_tc_kernel(PnParams P) {
     extern __shared__ __align__(1024) uint8_t pn_smem[];
     PnShared S{pn_smem, P.L};
@@ -956,14 +1009,23 @@ __global__ void __launch_bounds__(kPnThreads, 1) pnfa_tc_kernel(PnParams P) {
     __syncthreads();
     pn_tc_after();
     const uint32_t tbase = *reinterpret_cast<volatile uint32_t *>(misc + kMTmem);
-    // A operands: pair p -> TMEM columns [32p, 32p + 32), lane = row of [T[2p]; T[2p+1]]
+    // A operands: pair p -> TMEM columns [32p, 32p + 32) (16-bit values, two a column) or
+    // [16p, 16p + 16) (int8, four a column), lane = row of [T[2p]; T[2p+1]]
     if (warp < 4) {
         for (int p = 0; p < P.L.npairs; ++p) {
-            const uint32_t *src = P.tpack + ((size_t)p * 128 + 32 * warp + lane) * 32;
-            uint32_t r[32];
+            if constexpr (KIND == 2) {
+                const uint32_t *src = P.tpack + ((size_t)p * 128 + 32 * warp + lane) * 16;
+                uint32_t r[16];
 #pragma unroll
-            for (int k = 0; k < 32; ++k) r[k] = __ldg(src + k);
-            pn_tmem_st32(tbase + ((uint32_t)(32 * warp) << 16) + 32u * p, r);
+                for (int k = 0; k < 16; ++k) r[k] = __ldg(src + k);
+                pn_tmem_st16(tbase + ((uint32_t)(32 * warp) << 16) + 16u * p, r);
+            } else {
+                const uint32_t *src = P.tpack + ((size_t)p * 128 + 32 * warp + lane) * 32;
+                uint32_t r[32];
+#pragma unroll
+                for (int k = 0; k < 32; ++k) r[k] = __ldg(src + k);
+                pn_tmem_st32(tbase + ((uint32_t)(32 * warp) << 16) + 32u * p, r);
+            }
         }
         asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
     }
@@ -971,8 +1033,8 @@ __global__ void __launch_bounds__(kPnThreads, 1) pnfa_tc_kernel(PnParams P) {
     __syncthreads();
     pn_tc_after();
     volatile uint32_t *abort_flag = S.u32(kMAbort);
-    if (warp < kPnEpiWarps) pn_epilogue<FP16>(P, S, tbase, abort_flag);
-    else if (warp == kPnMmaWarp) pn_mma<FP16>(P, S, tbase, abort_flag);
+    if (warp < kPnEpiWarps) pn_epilogue<KIND>(P, S, tbase, abort_flag);
+    else if (warp == kPnMmaWarp) pn_mma<KIND>(P, S, tbase, abort_flag);
     else if (warp < kPnLoadWarp0) pn_planner(P, S, abort_flag);
     else pn_loader(P, S, abort_flag);
     pn_tc_before();
@@ -1194,12 +1256,13 @@ __global__ void __launch_bounds__(kPnPlainWarps * 32) pnfa_cc_kernel(PnPlainPara
 struct trex_pnfa {
     int n_states = 0, sigma = 0, npairs = 0, n_sms = 0;
     double ll_empty = 0.0, ll_empty_bool = 0.0;
-    float start_max16[3] = {0.f, 0.f, 0.f};   // [bf16, fp16, Boolean (bf16 of 0/1)]
+    // tensor-core tables: [bf16, fp16, Boolean 0/1 in bf16, Boolean 0/1 in int8]
+    float start_max16[4] = {0.f, 0.f, 0.f, 0.f};
     float *d_T32 = nullptr, *d_start32 = nullptr, *d_acc = nullptr, *d_acc_bool = nullptr;
     uint16_t *d_T16[2] = {nullptr, nullptr};   // [sigma][64][64] row-major: bf16, fp16
-    uint32_t *d_tpack[3] = {nullptr, nullptr, nullptr};
-    float *d_rsym[3] = {nullptr, nullptr, nullptr};
-    uint4 *d_simg[3] = {nullptr, nullptr, nullptr};
+    uint32_t *d_tpack[4] = {nullptr, nullptr, nullptr, nullptr};
+    float *d_rsym[4] = {nullptr, nullptr, nullptr, nullptr};
+    uint4 *d_simg[4] = {nullptr, nullptr, nullptr, nullptr};
     uint8_t *d_misc = nullptr;   // [0,8) queue, [8,12) error word
 };
 
@@ -1225,7 +1288,7 @@ static void pn_free(trex_pnfa *h) {
     cudaFree(h->d_start32);
     cudaFree(h->d_acc);
     cudaFree(h->d_acc_bool);
-    for (int k = 0; k < 3; ++k) {
+    for (int k = 0; k < 4; ++k) {
         cudaFree(h->d_tpack[k]);
         cudaFree(h->d_rsym[k]);
         cudaFree(h->d_simg[k]);
@@ -1296,9 +1359,9 @@ int trex_pnfa_create(int n_states, int sigma, const float *T, const float *start
         nacc += sb[i] != 0.f && ab[i] != 0.f;
     }
     h->ll_empty_bool = nacc ? std::log((double)nacc) : -INFINITY;
-    std::vector<uint32_t> tp[3];
-    std::vector<float> rs[3];
-    std::vector<uint4> simg[3];
+    std::vector<uint32_t> tp[4];
+    std::vector<float> rs[4];
+    std::vector<uint4> simg[4];
     for (int k = 0; k < 3; ++k) {
         const bool fp16 = k == 1;
         const std::vector<float> &Tk = k == 2 ? Tb : T32;
@@ -1335,6 +1398,23 @@ int trex_pnfa_create(int n_states, int sigma, const float *T, const float *start
         }
         h->start_max16[k] = smax;
     }
+    {   // int8 Boolean tables: the same A rows as above with 0/1 bytes, four K values a word
+        tp[3].assign((size_t)h->npairs * 128 * 16, 0u);
+        for (int c = 0; c < sigma; ++c) {
+            const int p = c >> 1, half_ = c & 1;
+            for (int rr = 0; rr < 64; ++rr) {
+                const int d = (rr & ~15) | ((rr & 7) << 1) | ((rr >> 3) & 1);
+                for (int q = 0; q < 64; ++q)
+                    if (Tb[((size_t)c * 64 + d) * 64 + q] != 0.f)
+                        tp[3][((size_t)p * 128 + half_ * 64 + rr) * 16 + (q >> 2)] |= 1u << (8 * (q & 3));
+            }
+        }
+        rs[3] = rs[2];
+        simg[3].assign(8, make_uint4(0, 0, 0, 0));   // a B row: 16 states a 16-byte column
+        uint8_t *b = reinterpret_cast<uint8_t *>(simg[3].data());
+        for (int i = 0; i < 64; ++i) b[(i >> 4) * 16 + (i & 15)] = sb[i] != 0.f ? 1 : 0;
+        h->start_max16[3] = 1.f;
+    }
     cudaError_t e = cudaSuccess;
     auto up = [&](void **dst, const void *src, size_t bytes) {
         if (e != cudaSuccess) return;
@@ -1350,7 +1430,7 @@ int trex_pnfa_create(int n_states, int sigma, const float *T, const float *start
     up((void **)&h->d_start32, s32.data(), 256);
     up((void **)&h->d_acc, a32.data(), 256);
     up((void **)&h->d_acc_bool, ab.data(), 256);
-    for (int k = 0; k < 3; ++k) {
+    for (int k = 0; k < 4; ++k) {
         up((void **)&h->d_tpack[k], tp[k].data(), tp[k].size() * 4);
         up((void **)&h->d_rsym[k], rs[k].data(), rs[k].size() * 4);
         up((void **)&h->d_simg[k], simg[k].data(), 8 * sizeof(uint4));
@@ -1358,7 +1438,10 @@ int trex_pnfa_create(int n_states, int sigma, const float *T, const float *start
     if (e == cudaSuccess) e = cudaMalloc(&h->d_misc, 16);
     if (e == cudaSuccess) e = cudaMemset(h->d_misc, 0, 16);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(pnfa_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        e = cudaFuncSetAttribute(pnfa_tc_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kPnSmemCap);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(pnfa_tc_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)kPnSmemCap);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(pnfa_cc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1367,7 +1450,7 @@ int trex_pnfa_create(int n_states, int sigma, const float *T, const float *start
         e = cudaFuncSetAttribute(pnfa_cc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)kPnSmemCap);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(pnfa_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        e = cudaFuncSetAttribute(pnfa_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)kPnSmemCap);
     if (e != cudaSuccess) {
         set_last_error("trex_pnfa_create", e);
@@ -1391,7 +1474,7 @@ int trex_pnfa_run(trex_pnfa *h, int mode, const uint8_t *data, const int64_t *of
     using namespace trex;
     if (!h) return TREX_ERR_NOT_INIT;
     if (n_strings < 0 || total_bytes < 0 || n_strings >= (int64_t)1 << 31) return TREX_ERR_ARG;
-    if (mode < TREX_PNFA_BF16 || mode > TREX_PNFA_FP16_CC) return TREX_ERR_ARG;
+    if (mode < TREX_PNFA_BF16 || mode > TREX_PNFA_BOOL8) return TREX_ERR_ARG;
     if (n_strings == 0) return TREX_OK;
     if (!offsets || (total_bytes > 0 && !data)) return TREX_ERR_ARG;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -1446,7 +1529,7 @@ int trex_pnfa_run(trex_pnfa *h, int mode, const uint8_t *data, const int64_t *of
     int grid = 0, p_sub = 0;
     int rc = pn_choose(h, n_strings, &grid, &p_sub);
     if (rc) return rc;
-    const int k = mode == TREX_PNFA_FP16 ? 1 : mode == TREX_PNFA_BOOL ? 2 : 0;
+    const int k = mode == TREX_PNFA_FP16 ? 1 : mode == TREX_PNFA_BOOL ? 2 : mode == TREX_PNFA_BOOL8 ? 3 : 0;
     PnParams P;
     P.data = data;
     P.total_bytes = total_bytes;
@@ -1455,22 +1538,25 @@ int trex_pnfa_run(trex_pnfa *h, int mode, const uint8_t *data, const int64_t *of
     P.tpack = h->d_tpack[k];
     P.rsym = h->d_rsym[k];
     P.start_img = h->d_simg[k];
-    P.acc = k == 2 ? h->d_acc_bool : h->d_acc;
+    P.acc = k >= 2 ? h->d_acc_bool : h->d_acc;
     P.start_max = h->start_max16[k];
-    P.ll_empty = k == 2 ? h->ll_empty_bool : h->ll_empty;
-    P.boolean = k == 2;
+    P.ll_empty = k >= 2 ? h->ll_empty_bool : h->ll_empty;
+    P.boolean = k >= 2;
+    P.kcols = k == 3 ? 4 : 8;
+    P.wait_cycles = mbar_wait_cycles();
     P.sigma = h->sigma;
     P.loglik = loglik;
     P.accept = accept;
     P.accept_i32 = accept_i32;
     P.queue = queue;
     P.err = err;
-    P.L = pn_layout(p_sub, h->sigma);
+    P.L = pn_layout(p_sub, h->sigma, k == 3 ? 16 : 32);
     // one CTA per SM: it owns all 512 TMEM columns
     const uint32_t smem = std::max<uint32_t>(P.L.total, 120u * 1024u);
     profile_kernel_begin(st);
-    if (k == 1) pnfa_tc_kernel<true><<<grid, kPnThreads, smem, st>>>(P);
-    else pnfa_tc_kernel<false><<<grid, kPnThreads, smem, st>>>(P);
+    if (k == 1) pnfa_tc_kernel<1><<<grid, kPnThreads, smem, st>>>(P);
+    else if (k == 3) pnfa_tc_kernel<2><<<grid, kPnThreads, smem, st>>>(P);
+    else pnfa_tc_kernel<0><<<grid, kPnThreads, smem, st>>>(P);
     profile_kernel_end(st);
     TREX_CHECK_LAUNCH();
     return TREX_OK;

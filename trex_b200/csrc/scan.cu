@@ -39,7 +39,6 @@ namespace trex {
 
 constexpr int kScanThreads = 1024;
 constexpr int kSyncCap = 512;                 // bytes walked with 16 chains before giving up
-constexpr uint32_t kPollLimit = 1u << 24;     // polls of one look-back step before giving up
 
 enum : uint32_t { kStAgg = 1u, kStPrefix = 2u };
 enum : uint32_t { kScanErrOffsets = 1u, kScanErrTimeout = 4u, kScanErrCapacity = 8u };
@@ -167,6 +166,7 @@ struct ScanParams {
     uint64_t *chunk_map;
     unsigned long long *head;
     uint32_t *err;
+    uint32_t poll_limit;   // polls of one look-back step before giving up
 };
 
 // Decodes four encoded states packed in a word into four plain states.
@@ -358,7 +358,7 @@ __device__ void scan_chunk(const ScanParams &P, const W &w, int64_t chunk, int64
             uint32_t st = 0;
             uint32_t polls = 0;
             while (((st = ld_acquire_u32(P.chunk_status + j)) & 3u) == 0u) {
-                if (++polls >= kPollLimit) break;
+                if (++polls >= P.poll_limit) break;
                 __nanosleep(64);
             }
             if ((st & 3u) == 0u) {
@@ -484,6 +484,7 @@ int trex_dfa_scan_run(trex_dfa_set *set, int dfa_index, const uint8_t *data,
     P.chunk_map = reinterpret_cast<uint64_t *>(sc + L.chunk_map);
     P.head = reinterpret_cast<unsigned long long *>(sc + L.head);
     P.err = err;
+    P.poll_limit = scan_poll_limit();
     static bool attr_set = false;
     if (!attr_set) {
         TREX_CUDA(cudaFuncSetAttribute(dfa_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -93,6 +93,15 @@ constexpr int kRepTableBytes16 = 256 * 512;   // 128 KiB
 
 int sm_count();
 
+// Limits of the kernels' bounded waits: polls of one look-back step of the
+// per-position scan, and clock cycles of one mbarrier hand-off of the
+// tensor-core NFA kernel. Process-wide; trex_set_wait_limits changes them (for
+// tests of the give-up paths), 0 restores the defaults.
+constexpr uint32_t kDefaultScanPolls = 1u << 24;
+constexpr long long kDefaultMbarCycles = 4000000000ll;   // about 2 s
+uint32_t scan_poll_limit();
+long long mbar_wait_cycles();
+
 // Launch profiler hooks (no-ops unless trex_profile_begin was called).
 void profile_kernel_begin(cudaStream_t s);
 void profile_kernel_end(cudaStream_t s);

@@ -279,7 +279,7 @@ class NFA:
         return v.value
 
 
-PNFA_MODES = {"bf16": 0, "fp16": 1, "fp32": 2, "bool": 3, "bf16cc": 4, "fp16cc": 5}
+PNFA_MODES = {"bf16": 0, "fp16": 1, "fp32": 2, "bool": 3, "bf16cc": 4, "fp16cc": 5, "bool8": 6}
 
 
 class PNFA:
@@ -294,6 +294,8 @@ class PNFA:
     59-442): nonzero entries are edges, each product is thresholded to {0, 1}
     (exact), accept = some accepting state active; loglik is then the log of
     the number of active accepting states. Bytes >= sigma are skipped.
+    "bool8": the same Boolean NFA with 0/1 int8 operands and int32 sums (tcgen05
+    kind::i8, K = 32 an instruction: half the MMA instructions of "bool").
     "bf16cc" / "fp16cc": CUDA cores with the 16-bit tables in shared memory and an
     FP32 state, a warp per string: the low-latency form for few strings.
     """
