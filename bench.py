@@ -1,7 +1,8 @@
 """Benchmark: automaton simulation on B200 (one JSON line on stdout, rank 0).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl trex|reference]
-                    [--workload ragged|plain|scan] [--strings S]
+                    [--workload ragged|plain|scan|nfa|pnfa|serve] [--strings S]
+                    [--no-extras] [--extras a,b,...]
 
 Workloads (synthetic, seeded; the reference ships no dataset):
   ragged (default, the headline case): 16 random DFAs (5 x 8, 5 x 12, 6 x 16
@@ -13,14 +14,29 @@ Workloads (synthetic, seeded; the reference ships no dataset):
   scan: one random 16-state DFA over 256 bytes, 8 strings x 256 MiB; one step
       writes the state of every position (2 bytes moved per character).
   nfa: random 64-state Boolean NFA over 20 symbols (bytes 0..19), per-symbol
-      edge density 0.05, 256K strings x 4096 symbols, bit-parallel kernel.
+      edge density 0.05, 256K strings x 4096 symbols; bit-parallel kernel, or
+      --nfa-method tc (0/1 BF16 tensor cores) / tc8 (0/1 int8 tensor cores).
   serve: the serving mix (64 resident automata, Poisson arrivals at
       --serve-rates) through trex_b200.serving.Server; reports throughput
       and p50/p99 latency per rate and the plain per-request launch.
   pnfa: probabilistic 64-state NFA over 20 symbols (rows Dirichlet(0.5) x 0.9,
       ~30% kept), 64K strings x 2048 symbols, tcgen05 kernel with BF16 (or
       --pnfa-mode fp16 / fp32) operands; also reports the log-likelihood error
-      against the FP64 oracle on 256 strings.
+      against the FP64 oracle.
+
+Every workload's results are checked against the C oracle (oracle/oracle.c)
+on the same bytes, outside the timed region: the line carries
+"mismatches_vs_oracle" (all strings of the batch; every position for the
+scan) and the run exits non-zero on any mismatch.
+
+The default run (ragged headline, one GPU) also measures the other
+configurations and the plain per-pattern form in the same process and adds
+them under "configs": cfg1_plain, plain_per_pattern (the ragged batch as 16
+per-automaton launches, device buffers and through the reference's
+prefix_engine_* ABI with host buffers), cfg3a_scan, cfg3b_nfa (bit-parallel and
+tensor-core forms), cfg4_pnfa (with the one-string chain latency per
+position), cfg5_served (a Poisson sweep up to saturation, with the limiter
+named). --no-extras skips them.
 
 Multi-GPU: one process per GPU (torchrun); every rank runs its own seeded
 batch (weak scaling, no data-path collective); times are the max over ranks
@@ -41,15 +57,15 @@ os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 import argparse  # noqa: E402
 import json  # noqa: E402
-import re
-import statistics
-import subprocess
-import sys
-import threading
-import time
-from pathlib import Path
+import re  # noqa: E402
+import statistics  # noqa: E402
+import subprocess  # noqa: E402
+import sys  # noqa: E402
+import threading  # noqa: E402
+import time  # noqa: E402
+from pathlib import Path  # noqa: E402
 
-import numpy as np
+import numpy as np  # noqa: E402
 
 REPO = Path(__file__).resolve().parent
 sys.path.insert(0, str(REPO))
@@ -58,9 +74,10 @@ from trex_b200.sharding import max_over_ranks, rank_seed  # noqa: E402
 
 METRIC = "Gchar/s vs HBM roofline, plain vs batched/served; served p50/p99 ms (1 B200)"
 SUB_ALPHABET = b"ACGT"
+EXTRAS = ("cfg1_plain", "plain_per_pattern", "cfg3a_scan", "cfg3b_nfa", "cfg4_pnfa", "cfg5_served")
 
 
-def parse_args():
+def parse_args(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=400)
@@ -68,8 +85,9 @@ def parse_args():
     ap.add_argument("--impl", choices=["trex", "reference"], default="trex")
     ap.add_argument("--workload", choices=["ragged", "plain", "scan", "nfa", "pnfa", "serve"],
                     default="ragged")
-    ap.add_argument("--serve-rates", type=str, default="2000,8000,32000",
-                    help="offered request rates (requests/s) of the serve workload")
+    ap.add_argument("--serve-rates", type=str, default="2000,8000,32000,64000,128000",
+                    help="offered request rates (requests/s) of the serve workload, swept upwards "
+                         "until the served rate falls below 90%% of the offered one")
     ap.add_argument("--serve-seconds", type=float, default=2.0)
     ap.add_argument("--serve-no-graphs", action="store_true",
                     help="launch the DFA batches directly instead of replaying CUDA graphs")
@@ -77,8 +95,9 @@ def parse_args():
                     help="requests timed one by one for the plain per-request baseline")
     ap.add_argument("--pnfa-mode", choices=["bf16", "fp16", "fp32"], default="bf16",
                     help="operand type of the probabilistic NFA workload")
-    ap.add_argument("--nfa-method", choices=["bitpar", "tc"], default="bitpar",
-                    help="nfa workload: bit-parallel kernel, or the Boolean NFA on the tensor cores")
+    ap.add_argument("--nfa-method", choices=["bitpar", "tc", "tc8"], default="bitpar",
+                    help="nfa workload: bit-parallel kernel, or the Boolean NFA on the tensor cores "
+                         "with 0/1 BF16 (tc) or int8 (tc8) operands")
     ap.add_argument("--strings", type=int, default=None, help="override the number of strings")
     ap.add_argument("--seg-len", type=int, default=0, help="bytes per work item / scan tile (0 = default)")
     ap.add_argument("--kgram", type=int, default=None,
@@ -95,9 +114,16 @@ def parse_args():
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
-                    help="CPU budget of the cpu_baseline sample (trex arm) / of the whole run (reference arm)")
+                    help="CPU budget of the reference arm's samples")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    return ap.parse_args()
+    ap.add_argument("--no-verify", action="store_true",
+                    help="skip the oracle check of the results (profiling runs only)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="default run: skip the other configurations")
+    ap.add_argument("--extras", type=str, default=",".join(EXTRAS),
+                    help="configurations measured after the headline (comma list of "
+                         + ", ".join(EXTRAS) + ")")
+    return ap.parse_args(argv)
 
 
 # ---------------------------------------------------------------------------------
@@ -148,6 +174,13 @@ def host_bytes(lens, is_sub, seed):
     return data
 
 
+def host_copy(torch, t):
+    """A pinned host copy of a device tensor, as numpy."""
+    h = torch.empty(t.numel(), dtype=t.dtype, pin_memory=True)
+    h.copy_(t)
+    return h.numpy()
+
+
 class DFAWorkload:
     """ragged / plain / scan: byte DFAs over CSR strings."""
 
@@ -157,6 +190,7 @@ class DFAWorkload:
         from trex_b200.workloads import ACGT, random_dfa
         self.kind = args.workload
         self.args = args
+        self.host_data = None
         rng = np.random.default_rng(args.seed)
         if self.kind == "plain":
             self.n = args.strings or 4096
@@ -298,7 +332,36 @@ class DFAWorkload:
         self.host_data = hd
         return dt, int(self.total + self.off.nbytes + self.ids.nbytes), int(2 * self.n + 4)
 
-    # ---- CPU (oracle) sample
+    # ---- the oracle on the same bytes, every string (every position for the scan)
+    def verify(self, orc):
+        torch = self.torch
+        if self.host_data is None:
+            self.host_data = host_copy(torch, self.data)
+        d = self.dfas
+        fs = self.fs.cpu().numpy()
+        ac = self.ac.cpu().numpy()
+        t0 = time.perf_counter()
+        if self.kind == "scan":
+            ref = orc.dfa_positions(d[0].tmap, d[0].n_states, d[0].start, self.host_data, self.off)
+            dt = time.perf_counter() - t0
+            got = host_copy(torch, self.states)
+            last = self.off[1:] - 1
+            rfs = ref[last]
+            mism = {"states": int(np.count_nonzero(got != ref)),
+                    "final_state": int(np.count_nonzero(fs != rfs)),
+                    "accept": int(np.count_nonzero(ac != d[0].accept[rfs])),
+                    "strings": self.n, "positions": int(self.total)}
+        else:
+            rfs, rac = orc.dfa_walk([x.tmap for x in d], [x.n_states for x in d],
+                                    [x.start for x in d], [x.accept for x in d], self.host_data,
+                                    self.off, self.ids)
+            dt = time.perf_counter() - t0
+            mism = {"final_state": int(np.count_nonzero(fs != rfs)),
+                    "accept": int(np.count_nonzero(ac != rac)), "strings": self.n,
+                    "bytes": int(self.total)}
+        return mism, dt, self.total
+
+    # ---- CPU (oracle) sample, reference arm
     def cpu_run(self, orc, data, k):
         d = self.dfas
         if self.kind == "scan":
@@ -327,6 +390,9 @@ class DFAWorkload:
         data = host_bytes(lens[:k], None if is_sub is None else is_sub[:k], seed)
         return k, int(self.off_cpu[k]), data
 
+    def close(self):
+        self.set.close()
+
 
 class NFAWorkload:
     """Boolean NFA, 64 states, 20 symbols (bit-parallel kernel)."""
@@ -339,6 +405,7 @@ class NFAWorkload:
     def __init__(self, args):
         from trex_b200.workloads import random_bool_nfa
         self.args = args
+        self.host_data = None
         rng = np.random.default_rng(args.seed)
         self.T, self.start, self.acc = random_bool_nfa(rng, n_states=64, sigma=20, density=0.05)
         self.n = args.strings or 262144
@@ -412,20 +479,36 @@ class NFAWorkload:
         self.host_data = hd
         return dt, int(self.total + ho.nbytes), int(hr.nbytes)
 
+    def verify(self, orc):
+        if self.host_data is None:
+            self.host_data = host_copy(self.torch, self.data)
+        t0 = time.perf_counter()
+        rfm, rac = orc.nfa_bool(self.T, self.start, self.acc, self.host_data, self.off,
+                                unknown_rejects=True)
+        dt = time.perf_counter() - t0
+        fm = self.fm.cpu().numpy().view(np.uint64)
+        ac = self.ac.cpu().numpy()
+        return ({"final_mask": int(np.count_nonzero(fm != rfm)),
+                 "accept": int(np.count_nonzero(ac != rac)), "strings": self.n,
+                 "bytes": int(self.total)}, dt, self.total)
+
     def cpu_run(self, orc, data, k):
         orc.nfa_bool(self.T, self.start, self.acc, data, self.off[:k + 1], unknown_rejects=True)
 
     def cpu_sample(self, seed, seconds, threads):
-        from oracle import oracle as orc
         rng = np.random.default_rng(seed + 3)
         k0 = max(1, min(self.n, threads * 4))
         data0 = rng.integers(0, 20, size=k0 * self.L, dtype=np.uint8)
+        from oracle import oracle as orc
         t0 = time.perf_counter()
         self.cpu_run(orc, data0, k0)
         rate = k0 * self.L / max(time.perf_counter() - t0, 1e-6)
         k = max(1, min(self.n, int(seconds * rate / self.L)))
         data = rng.integers(0, 20, size=k * self.L, dtype=np.uint8)
         return k, k * self.L, data
+
+    def close(self):
+        self.nfa.close()
 
 
 class PNFAWorkload:
@@ -435,6 +518,7 @@ class PNFAWorkload:
     launches_per_step = 1
     bound = "tensor"
     ref_dtype = "f64"
+    verify_strings = 1024
 
     def __init__(self, args):
         from trex_b200.workloads import random_prob_nfa
@@ -488,12 +572,24 @@ class PNFAWorkload:
                 "useful_flops_per_char": 2 * 64 * 64, "mode": self.mode,
                 "l2": "inputs (134 MB) larger than L2 (126 MB), no flush"}
 
-    def llerr(self, orc, k=256):
-        """Max relative log-likelihood error vs the FP64 oracle on the first k strings."""
+    def verify(self, orc):
+        """Log-likelihoods of the first verify_strings strings against the FP64 oracle:
+        the largest relative error (the tolerance of the tests: 1e-4 relative for
+        strings of this length) and the accept flags that differ."""
+        k = min(self.n, self.verify_strings)
         data = self.data[:k * self.L].cpu().numpy()
+        t0 = time.perf_counter()
         ref = orc.pnfa_fp64(self.T, self.start, self.acc, data, self.off[:k + 1])
+        dt = time.perf_counter() - t0
         got = self.ll[:k].cpu().numpy()
-        return float(np.max(np.abs(got - ref) / np.maximum(1.0, np.abs(ref))))
+        rel = float(np.max(np.abs(got - ref) / np.maximum(1.0, np.abs(ref))))
+        ac = self.ac[:k].cpu().numpy().astype(bool)
+        return ({"loglik_max_rel_err_vs_fp64": rel, "loglik_tolerance": 1e-4,
+                 "loglik_over_tolerance": int(np.count_nonzero(
+                     np.abs(got - ref) > 1e-4 * np.maximum(1.0, np.abs(ref)))),
+                 "accept_flags_differ": int(np.count_nonzero(ac != (ref > np.log(0.5)))),
+                 "strings": k},
+                dt, k * self.L)
 
     def e2e(self, torch, steps, dist, dev):
         # the public API with host buffers: pinned H2D of the step's bytes and offsets,
@@ -540,10 +636,14 @@ class PNFAWorkload:
         data = rng.integers(0, 20, size=k * self.L, dtype=np.uint8)
         return k, k * self.L, data
 
+    def close(self):
+        self.pnfa.close()
+
 
 class NFATcWorkload(PNFAWorkload):
     """The Boolean NFA workload (64 states, 20 symbols, 4096 symbols a string) on the
-    tensor cores: 0/1 BF16 operands, FP32 sums thresholded to {0, 1} every step."""
+    tensor cores: 0/1 operands (BF16, or int8 with int32 sums), each product
+    thresholded to {0, 1} every step."""
 
     kind = "nfa"
     ref_dtype = "u64"
@@ -551,7 +651,7 @@ class NFATcWorkload(PNFAWorkload):
     def __init__(self, args):
         from trex_b200.workloads import random_bool_nfa
         self.args = args
-        self.mode = "bool"
+        self.mode = "bool8" if args.nfa_method == "tc8" else "bool"
         rng = np.random.default_rng(args.seed)
         T, start, acc = random_bool_nfa(rng, n_states=64, sigma=20, density=0.05)
         self.T, self.start, self.acc = (x.astype(np.float32) for x in (T, start, acc))
@@ -559,23 +659,29 @@ class NFATcWorkload(PNFAWorkload):
         self.L = 4096
         self.off = np.arange(self.n + 1, dtype=np.int64) * self.L
         self.kernel = "pnfa_tc_kernel"
-        self.dtype = "bf16"
+        self.dtype = "s8" if self.mode == "bool8" else "bf16"
+        ops = ("0/1 int8 operands, int32 sums (tcgen05 kind::i8)" if self.mode == "bool8"
+               else "0/1 BF16 operands, FP32 sums (tcgen05 kind::f16)")
         self.workload = ("Boolean NFA: random 64-state NFA over 20 symbols (bytes 0..19), edge density "
-                         f"0.05, {self.n} strings x 4096 symbols; tensor cores (tcgen05), 0/1 BF16 "
-                         "operands, FP32 sums thresholded every step")
+                         f"0.05, {self.n} strings x 4096 symbols; tensor cores, {ops} thresholded "
+                         "every step")
 
     def config(self):
         return {"workload": self.workload, "n_strings": self.n, "total_bytes_per_gpu": self.total,
-                "useful_ops_per_char": 2 * 64 * 64, "mode": "bool",
+                "useful_ops_per_char": 2 * 64 * 64, "mode": self.mode,
                 "selection_waste": "2x (each MMA computes both symbols of a pair; half is discarded)",
                 "l2": "inputs larger than L2 (126 MB), no flush"}
 
-    def exact_mismatches(self, orc, k=2048):
-        """Accept flags that differ from the bit-parallel oracle on the first k strings."""
-        data = self.data[:k * self.L].cpu().numpy()
-        _, ref = orc.nfa_bool(self.T != 0, self.start, self.acc, data, self.off[:k + 1],
+    def verify(self, orc):
+        """Accept flags of every string against the bit-parallel oracle."""
+        data = host_copy(self.torch, self.data)
+        t0 = time.perf_counter()
+        _, ref = orc.nfa_bool(self.T != 0, self.start, self.acc, data, self.off,
                               unknown_rejects=False)
-        return int(np.count_nonzero(self.ac[:k].cpu().numpy().astype(bool) != ref.astype(bool)))
+        dt = time.perf_counter() - t0
+        got = self.ac.cpu().numpy().astype(bool)
+        return ({"accept": int(np.count_nonzero(got != ref.astype(bool))), "strings": self.n,
+                 "bytes": int(self.total)}, dt, self.total)
 
     def cpu_run(self, orc, data, k):
         orc.nfa_bool(self.T != 0, self.start, self.acc, data, self.off[:k + 1], unknown_rejects=False)
@@ -619,19 +725,21 @@ def poisson_run(srv, pool, rate: float, duration: float, seed: int):
     process of `rate` requests/s over `duration` s. The client submits every
     request whose arrival time has passed in one call (its latency is counted
     from its arrival time), then sleeps briefly. Waits for all; returns the
-    server stats."""
+    server stats, plus how far the client fell behind the arrival schedule."""
     rng = np.random.default_rng(seed + 17)
     n = max(1, int(rate * duration))
     arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n))
     arrivals = arrivals[arrivals <= duration]
     srv.reset_stats()
     reqs = []
+    lag = 0.0
     t0 = time.perf_counter()
     k = 0
     while k < len(arrivals):
         now = time.perf_counter() - t0
         j = int(np.searchsorted(arrivals, now, side="right"))
         if j > k:
+            lag = max(lag, now - arrivals[k])
             items = [pool[i % len(pool)] for i in range(k, j)]
             reqs += srv.submit_many(items, t_arrival=(t0 + arrivals[k:j]).tolist())
             k = j
@@ -641,6 +749,7 @@ def poisson_run(srv, pool, rate: float, duration: float, seed: int):
     st = srv.stats()
     st["offered_req_s"] = rate
     st["offered_gchar_s"] = rate * float(np.mean([len(p[2]) for p in pool])) / 1e9
+    st["client_max_lag_ms"] = lag * 1e3
     return st
 
 
@@ -673,7 +782,9 @@ def plain_run(engines, pool, n_req: int):
             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))}
 
 
-def serve_arm(args):
+def serve_measure(args) -> dict:
+    """Poisson sweep over the serving mix, upwards until the served rate falls
+    below 90% of the offered one; the plain per-request launch beside it."""
     import torch
     from trex_b200.engine import NFA, PNFA, DFASet
     from trex_b200.serving import Server
@@ -688,30 +799,62 @@ def serve_arm(args):
     rates = [float(r) for r in args.serve_rates.split(",")]
     clocks = ClockSampler(gpu_index_for(0))
     clocks.start()
-    runs = [poisson_run(srv, pool, r, args.serve_seconds, args.seed + k) for k, r in enumerate(rates)]
+    runs = []
+    for k, r in enumerate(rates):
+        util = UtilSampler(gpu_index_for(0))
+        util.start()
+        runs.append(poisson_run(srv, pool, r, args.serve_seconds, args.seed + k))
+        runs[-1]["gpu_busy_frac"] = util.stop()
+        if runs[-1]["gchar_s"] < 0.9 * runs[-1]["offered_gchar_s"]:
+            break
     clock_info = clocks.stop()
     srv.close()
     engines = (DFASet(dfas), [NFA(*x, unknown_rejects=True) for x in nfas], [PNFA(*x) for x in pnfas])
     plain_run(engines, pool, 200)   # warm
     plain = plain_run(engines, pool, args.serve_plain)
-    best = max(runs, key=lambda r: r["gchar_s"])
+    engines[0].close()
+    for m in engines[1] + engines[2]:
+        m.close()
+    sustained = [r for r in runs if r["gchar_s"] >= 0.9 * r["offered_gchar_s"]]
+    top = max(sustained, key=lambda r: r["offered_req_s"]) if sustained else runs[0]
+    last = runs[-1]
+    # the limiter at the last rate: the device (busy most of the span) or the host loop
+    gpu_busy = last.get("gpu_busy_frac") or 0.0
+    loop_busy = last.get("loop_busy_frac") or 0.0
+    if last is top:
+        limiter = "not reached (served >= 90% of offered at the highest rate tried)"
+    elif gpu_busy >= 0.8:
+        limiter = "GPU (device busy {:.0%} of the span)".format(gpu_busy)
+    else:
+        limiter = ("host: the Python request loop and client (loop busy {:.0%}, device busy {:.0%} of "
+                   "the span)".format(loop_busy, gpu_busy))
+    keys = ("offered_req_s", "offered_gchar_s", "gchar_s", "p50_ms", "p99_ms", "requests", "batches",
+            "by_kind", "client_max_lag_ms", "loop_busy_frac", "gpu_busy_frac")
+    return {
+        "workload": "serving mix: 64 resident automata (32 DFA16 over 256 bytes, 24 Boolean NFA64 and "
+                    "8 probabilistic NFA64 over 20 symbols), lengths log-normal median 2 KiB sigma 1.0 "
+                    "clipped [16 B, 1 MiB], automaton uniform, Poisson arrivals at each offered rate",
+        "parallelism": "1 GPU, continuous batching (2 lanes x 2 slots, "
+                       + ("direct launches)" if args.serve_no_graphs else "CUDA graphs for DFA batches)"),
+        "hbm_budget_bytes": 2 << 30,
+        "pnfa_mode": "auto (BF16 tables on CUDA cores below 2048 strings a group, tcgen05 above)",
+        "value": top["gchar_s"], "unit": "Gchar/s",
+        "sustained_req_s": top["offered_req_s"], "p50_ms_at_sustained": top["p50_ms"],
+        "p99_ms_at_sustained": top["p99_ms"], "limiter": limiter,
+        "sweep": [{k: r.get(k) for k in keys} for r in runs],
+        "plain_per_request": plain, "clocks": clock_info,
+    }
+
+
+def serve_arm(args):
+    r = serve_measure(args)
     line = {
-        "metric": METRIC, "value": best["gchar_s"], "unit": "Gchar/s", "n_gpus": 1,
-        "steps": len(rates), "warmup": 1, "ms_per_step": args.serve_seconds * 1e3,
+        "metric": METRIC, "value": r["value"], "unit": "Gchar/s", "n_gpus": 1,
+        "steps": len(r["sweep"]), "warmup": 1, "ms_per_step": args.serve_seconds * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
         "data": "synthetic (seeded request pool, Poisson arrivals)",
-        "config": {"workload": "serving mix: 64 resident automata (32 DFA16 over 256 bytes, 24 Boolean "
-                               "NFA64 and 8 probabilistic NFA64 over 20 symbols), lengths log-normal "
-                               "median 2 KiB sigma 1.0 clipped [16 B, 1 MiB], automaton uniform, "
-                               "Poisson arrivals at each offered rate",
-                   "parallelism": "1 GPU, continuous batching (2 lanes x 2 slots, "
-                                  + ("direct launches)" if args.serve_no_graphs
-                                     else "CUDA graphs for DFA batches)"),
-                   "hbm_budget_bytes": 2 << 30, "pnfa_mode": "auto (BF16 tables on CUDA cores below 2048 strings a group, tcgen05 above)"},
-        "served": [{k: r[k] for k in ("offered_req_s", "offered_gchar_s", "gchar_s", "p50_ms", "p99_ms",
-                                      "requests", "batches", "by_kind")} for r in runs],
-        "plain_per_request": plain,
-        "clocks": clock_info,
+        "config": {k: r[k] for k in ("workload", "parallelism", "hbm_budget_bytes", "pnfa_mode")},
+        "served": r, "clocks": r["clocks"],
     }
     print(json.dumps(line), flush=True)
 
@@ -775,6 +918,29 @@ class ClockSampler:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
+class UtilSampler(ClockSampler):
+    """Mean of nvidia-smi's utilization.gpu (the share of each sample period in
+    which a kernel ran) while it runs, as a fraction."""
+    QUERY = "utilization.gpu"
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        v = []
+        for ln in self.lines:
+            try:
+                v.append(float(ln.split(",")[0]))
+            except ValueError:
+                continue
+        return float(np.mean(v)) / 100.0 if v else None
+
+
 def gpu_index_for(local_rank: int) -> str:
     cvd = os.environ.get("CUDA_VISIBLE_DEVICES")
     if cvd:
@@ -811,15 +977,118 @@ def committed_traffic(kernel: str, workload: str):
 
 
 # ---------------------------------------------------------------------------------
-# arms
+# measurement
 # ---------------------------------------------------------------------------------
 
 def make_workload(args):
     if args.workload == "nfa":
-        return NFATcWorkload(args) if args.nfa_method == "tc" else NFAWorkload(args)
+        return NFATcWorkload(args) if args.nfa_method in ("tc", "tc8") else NFAWorkload(args)
     if args.workload == "pnfa":
         return PNFAWorkload(args)
     return DFAWorkload(args)
+
+
+def sub_args(args, **kw):
+    """A copy of the command line for one sub-configuration (defaults for it)."""
+    d = dict(vars(args))
+    d.update({"strings": None, "seg_len": 0, "kgram": None, "dfa_sizes": None})
+    d.update(kw)
+    return argparse.Namespace(**d)
+
+
+def measure(wl, args, torch, dev, *, steps, warmup, rank=0, world=1, local_rank=0, dist=None,
+            e2e_steps=3, verify=True, roof_tag=None):
+    """Set up, warm, time `steps` steps between synchronisations on the device
+    (CUDA events on the launching stream, max over ranks), the main kernel's
+    own time (library events), the end-to-end host-buffer form, and the oracle
+    check on the same bytes. Returns a dict (the line's fields)."""
+    from trex_b200.engine import profile_begin, profile_end
+    seed = rank_seed(args.seed, rank)
+    wl.setup(torch, dev, seed)
+    stream = torch.cuda.current_stream(dev)
+    flush = None
+    if wl.chars < 126e6:
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    warm = max(3, warmup)
+    for _ in range(warm):
+        wl.step(stream)
+    torch.cuda.synchronize()
+    if wl.error_word() != 0:
+        raise RuntimeError("device reported malformed input or a look-back timeout")
+    clocks = ClockSampler(gpu_index_for(local_rank))
+    clocks.start()
+    time.sleep(0.3)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    profile_begin(steps)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(steps):
+        if flush is not None:
+            flush.fill_(1)
+        wl.step(stream)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    kern_ms = profile_end(steps)
+    clock_info = clocks.stop()
+    if wl.error_word() != 0:
+        raise RuntimeError("device reported an error during the timed steps")
+    ms = ev0.elapsed_time(ev1)
+    ms = max_over_ranks(ms, dist, dev)
+    ms_per_step = ms / steps
+    chars_all = wl.chars * world
+    value = chars_all / (ms_per_step * 1e-3) / 1e9
+
+    kmean = sum(kern_ms) / max(1, len(kern_ms))
+    traffic = committed_traffic(wl.kernel, roof_tag or args.workload)
+    if getattr(wl, "bound", "hbm") == "tensor":
+        peak, peak_kind = measured_tensor_peak()
+        achieved = wl.alg_flops / (kmean * 1e-3) / 1e12
+        roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak, "traffic": traffic, "kernel": wl.kernel,
+                "kernel_ms_mean": kmean, "algorithmic_flops_per_launch": wl.alg_flops,
+                "peak_source": f"MEASURED_PEAKS.json bf16_tflops_sustained ({peak_kind}); "
+                               "useful flops 2*64*64 per symbol (the pair layout issues 2x)"}
+    else:
+        peak, peak_kind = measured_peaks()
+        achieved = wl.alg_bytes / (kmean * 1e-3) / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "kernel": wl.kernel,
+                "kernel_ms_mean": kmean, "algorithmic_bytes_per_launch": wl.alg_bytes,
+                "step_frac": wl.alg_bytes / (ms_per_step * 1e-3) / 1e9 / peak,
+                "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})"}
+
+    e2e = None
+    if e2e_steps > 0:
+        res = wl.e2e(torch, e2e_steps, dist, dev)
+        if res is not None:
+            dt, h2d, d2h = res
+            e2e = {"value": chars_all * e2e_steps / dt / 1e9, "unit": "Gchar/s",
+                   "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
+    out = {"value": value, "unit": "Gchar/s", "ms_per_step": ms_per_step, "steps": steps,
+           "warmup": warm, "roofline": roof, "e2e": e2e, "clocks": clock_info,
+           "gpu_launches": wl.launches_per_step * steps,
+           "config": {**wl.config(), "parallelism": f"dp{world} (independent shards, no collective)"}}
+    if getattr(wl, "tune_info", None) is not None:
+        out["autotune"] = wl.tune_info
+    if verify:
+        from oracle import oracle as orc
+        orc.build()
+        mism, secs, nbytes = wl.verify(orc)
+        out["mismatches_vs_oracle"] = mism
+        out["oracle"] = {"seconds": secs, "gchar_s": nbytes / max(secs, 1e-9) / 1e9,
+                         "threads": orc.threads(), "bytes": int(nbytes)}
+    return out
+
+
+def failed_checks(m: dict) -> bool:
+    mm = m.get("mismatches_vs_oracle") or {}
+    bad = any(v for k, v in mm.items() if k in ("final_state", "accept", "states", "final_mask"))
+    return bad or mm.get("loglik_over_tolerance", 0) > 0
 
 
 def base_line(args, wl, value, ms_per_step, steps, warmup, world):
@@ -867,112 +1136,230 @@ def reference_arm(args, rank):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------------
+# extra configurations (default run, one GPU)
+# ---------------------------------------------------------------------------------
+
+def plain_per_pattern(args, torch, dev, wl):
+    """The ragged batch as one launch per automaton (the plain form): each
+    automaton's strings gathered once (outside the timed region), then
+    (device) 16 single-automaton sets run back to back on device buffers, and
+    (host) 16 reference-style singleton engines, prefix_engine_init + one
+    prefix_engine_dispatch per automaton, from pinned host buffers with int32
+    offsets. Results are checked against the batched run of the same strings."""
+    import ctypes
+    from trex_b200 import _lib
+    from trex_b200.engine import DFASet
+    L = _lib.load()
+    hd = wl.host_data if wl.host_data is not None else host_copy(torch, wl.data)
+    off, ids = wl.off, wl.ids
+    fs_b, ac_b = wl.fs.cpu().numpy(), wl.ac.cpu().numpy()
+    lens = np.diff(off)
+    pats = []
+    for d in range(len(wl.dfas)):
+        idx = np.flatnonzero(ids == d)
+        starts, ends = off[idx], off[idx + 1]
+        blob = np.concatenate([hd[a:b] for a, b in zip(starts.tolist(), ends.tolist())])
+        h = torch.from_numpy(blob).pin_memory()
+        o = offsets_of(lens[idx])
+        pats.append({"idx": idx, "h": h, "off": o, "off32": torch.from_numpy(o.astype(np.int32)).pin_memory(),
+                     "d": h.to(dev), "d_off": torch.from_numpy(o).to(dev),
+                     "set": DFASet([wl.dfas[d]]),
+                     "fs": torch.empty(len(idx), dtype=torch.uint8, device=dev),
+                     "ac": torch.empty(len(idx), dtype=torch.uint8, device=dev)})
+    for p in pats:
+        p["scratch"] = torch.empty(DFASet.scratch_bytes(len(p["idx"]), int(p["off"][-1]), args.seg_len),
+                                   dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def dev_step():
+        for p in pats:
+            p["set"].run(p["d"], p["d_off"], None, final_state=p["fs"], accept=p["ac"],
+                         scratch=p["scratch"], seg_len=args.seg_len, stream=stream)
+
+    for _ in range(3):
+        dev_step()
+    torch.cuda.synchronize()
+    steps = 20
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(steps):
+        dev_step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    dev_ms = ev0.elapsed_time(ev1) / steps
+    mism = 0
+    for p in pats:
+        mism += int(np.count_nonzero(p["fs"].cpu().numpy() != fs_b[p["idx"]]))
+        mism += int(np.count_nonzero(p["ac"].cpu().numpy() != ac_b[p["idx"]]))
+
+    # through the reference ABI (one resident automaton per library): init + dispatch each
+    u8 = ctypes.c_uint8
+    res = [np.zeros(len(p["idx"]), dtype=np.int32) for p in pats]
+
+    def host_step():
+        disp_ms = 0.0
+        for d, p in enumerate(pats):
+            D = wl.dfas[d]
+            tm = np.ascontiguousarray(D.tmap)
+            ac = np.ascontiguousarray(D.accept)
+            _lib.check(L.prefix_engine_init(_lib.ptr(tm, u8), _lib.ptr(ac, u8), int(D.start), D.n_states, 1,
+                                            int(p["off"][-1]), len(p["idx"])), "prefix_engine_init")
+            km, tm_ = ctypes.c_float(), ctypes.c_float()
+            hdp, hop = p["h"].numpy(), p["off32"].numpy()
+            _lib.check(L.prefix_engine_dispatch(_lib.ptr(hdp, u8), _lib.ptr(hop, ctypes.c_int),
+                                                _lib.ptr(res[d], ctypes.c_int), len(p["idx"]),
+                                                int(p["off"][-1]), ctypes.byref(km), ctypes.byref(tm_)),
+                       "prefix_engine_dispatch")
+            disp_ms += tm_.value
+        L.prefix_engine_destroy()
+        return disp_ms
+
+    host_step()
+    hsteps = 2
+    t0 = time.perf_counter()
+    disp = [host_step() for _ in range(hsteps)]
+    host_s = (time.perf_counter() - t0) / hsteps
+    for d, p in enumerate(pats):
+        mism += int(np.count_nonzero(res[d].astype(np.uint8) != ac_b[p["idx"]]))
+    for p in pats:
+        p["set"].close()
+    chars = int(wl.total)
+    return {"workload": "the ragged batch (same strings and automata) as 16 per-automaton launches",
+            "value": chars / (dev_ms * 1e-3) / 1e9, "unit": "Gchar/s", "ms_per_step": dev_ms,
+            "steps": steps, "launches_per_step": 16 * 5,
+            "e2e_reference_abi": {"value": chars / host_s / 1e9, "unit": "Gchar/s",
+                                  "ms_per_step": host_s * 1e3,
+                                  "dispatch_only_value": chars / (np.mean(disp) * 1e-3) / 1e9,
+                                  "form": "per automaton: prefix_engine_init (table upload, buffer "
+                                          "allocation) + prefix_engine_dispatch (pinned H2D, run, D2H of "
+                                          "int results)"},
+            "mismatches_vs_batched": mism}
+
+
+def pnfa_latency(args, torch, dev):
+    """One string through the probabilistic NFA chain (64 states, 20 symbols):
+    the step latency per position of the tensor-core and CUDA-core kernels."""
+    from trex_b200.engine import PNFA
+    from trex_b200.workloads import random_prob_nfa
+    rng = np.random.default_rng(args.seed)
+    T, s, a = random_prob_nfa(rng, 64, 20)
+    L = 1 << 16
+    data = torch.randint(0, 20, (L,), dtype=torch.uint8, device=dev,
+                         generator=torch.Generator(device=dev).manual_seed(args.seed + 9))
+    off = torch.tensor([0, L], dtype=torch.int64, device=dev)
+    m = PNFA(T, s, a)
+    out = {}
+    clocks = ClockSampler(gpu_index_for(0))
+    clocks.start()
+    for mode in ("bf16", "bf16cc", "fp32"):
+        for _ in range(2):
+            m.run(data, off, mode)
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        reps = 3
+        for _ in range(reps):
+            m.run(data, off, mode)
+        ev1.record()
+        torch.cuda.synchronize()
+        ns = ev0.elapsed_time(ev1) / reps * 1e6 / L
+        out[mode] = {"ns_per_position": ns}
+    ci = clocks.stop()
+    mhz = ci.get("sm_mhz") or 1965.0
+    for v in out.values():
+        v["cycles_per_position"] = v["ns_per_position"] * mhz / 1e3
+    m.close()
+    return {"workload": f"one string of {L} symbols, 64-state probabilistic NFA over 20 symbols",
+            "by_mode": out, "sm_mhz": mhz,
+            "reference": "82.7 cycles/position: wgmma RS chain, 1 string per warpgroup, H200 "
+                         "(cuda/probe_wgmma_layout.cu)"}
+
+
+def run_extras(args, torch, dev, main_wl, names):
+    extras = {}
+    if "plain_per_pattern" in names and isinstance(main_wl, DFAWorkload) and main_wl.kind == "ragged":
+        try:
+            extras["plain_per_pattern"] = plain_per_pattern(args, torch, dev, main_wl)
+        except Exception as e:   # keep the headline; record what failed
+            extras["plain_per_pattern"] = {"error": repr(e)[:400]}
+    main_wl.close()
+    for k in ("data", "d_off", "d_ids", "scratch", "fs", "ac", "states", "host_data"):
+        if hasattr(main_wl, k):
+            setattr(main_wl, k, None)
+    torch.cuda.empty_cache()
+    subs = [("cfg1_plain", lambda: DFAWorkload(sub_args(args, workload="plain")), 200, "plain"),
+            ("cfg3a_scan", lambda: DFAWorkload(sub_args(args, workload="scan")), 20, "scan"),
+            ("cfg3b_nfa", lambda: NFAWorkload(sub_args(args, workload="nfa")), 10, "nfa"),
+            ("cfg3b_nfa_tensor_bf16", lambda: NFATcWorkload(sub_args(args, workload="nfa", nfa_method="tc")),
+             2, "nfa_tc"),
+            ("cfg3b_nfa_tensor_int8", lambda: NFATcWorkload(sub_args(args, workload="nfa", nfa_method="tc8")),
+             2, "nfa_tc8"),
+            ("cfg4_pnfa", lambda: PNFAWorkload(sub_args(args, workload="pnfa", pnfa_mode="bf16")), 5, "pnfa")]
+    for name, make, steps, tag in subs:
+        if name.split("_tensor")[0] not in names:
+            continue
+        try:
+            wl = make()
+            extras[name] = measure(wl, wl.args, torch, dev, steps=steps, warmup=3,
+                                   e2e_steps=0 if "tensor" in name else 2, roof_tag=tag)
+            wl.close()
+            del wl
+        except Exception as e:
+            extras[name] = {"error": repr(e)[:400]}
+        torch.cuda.empty_cache()
+    if "cfg4_pnfa" in names:
+        try:
+            extras["cfg4_pnfa_latency"] = pnfa_latency(args, torch, dev)
+        except Exception as e:
+            extras["cfg4_pnfa_latency"] = {"error": repr(e)[:400]}
+    if "cfg5_served" in names:
+        try:
+            extras["cfg5_served"] = serve_measure(args)
+        except Exception as e:
+            extras["cfg5_served"] = {"error": repr(e)[:400]}
+    return extras
+
+
 def trex_arm(args, rank, world, local_rank):
     import torch
-    from trex_b200.engine import profile_begin, profile_end
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
     dist = None
     if world > 1:
         import torch.distributed as dist
-    seed = rank_seed(args.seed, rank)
     wl = make_workload(args)
-    wl.setup(torch, dev, seed)
-    stream = torch.cuda.current_stream(dev)
-    flush = None
-    if wl.chars < 126e6:
-        flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    warm = max(3, args.warmup)
-    for _ in range(warm):
-        wl.step(stream)
-    torch.cuda.synchronize()
-    if wl.error_word() != 0:
-        raise RuntimeError("device reported malformed input or a look-back timeout")
-    clocks = ClockSampler(gpu_index_for(local_rank))
-    clocks.start()
-    time.sleep(0.3)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    profile_begin(args.steps)
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    for _ in range(args.steps):
-        if flush is not None:
-            flush.fill_(1)
-        wl.step(stream)
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    kern_ms = profile_end(args.steps)
-    clock_info = clocks.stop()
-    if wl.error_word() != 0:
-        raise RuntimeError("device reported an error during the timed steps")
-    ms = ev0.elapsed_time(ev1)
-    ms = max_over_ranks(ms, dist, dev)
-    ms_per_step = ms / args.steps
-    chars_all = wl.chars * world
-    value = chars_all / (ms_per_step * 1e-3) / 1e9
-
-    kmean = sum(kern_ms) / max(1, len(kern_ms))
-    traffic = committed_traffic(wl.kernel, args.workload)
-    if getattr(wl, "bound", "hbm") == "tensor":
-        peak, peak_kind = measured_tensor_peak()
-        achieved = wl.alg_flops / (kmean * 1e-3) / 1e12
-        roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": achieved / peak, "traffic": traffic, "kernel": wl.kernel,
-                "kernel_ms_mean": kmean, "algorithmic_flops_per_launch": wl.alg_flops,
-                "peak_source": f"MEASURED_PEAKS.json bf16_tflops_sustained ({peak_kind}); "
-                               "useful flops 2*64*64 per symbol (the pair layout issues 2x)"}
-    else:
-        peak, peak_kind = measured_peaks()
-        achieved = wl.alg_bytes / (kmean * 1e-3) / 1e9
-        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": traffic, "kernel": wl.kernel,
-                "kernel_ms_mean": kmean, "algorithmic_bytes_per_launch": wl.alg_bytes,
-                "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})"}
-
-    e2e = None
-    res = wl.e2e(torch, args.e2e_steps, dist, dev)
-    if res is not None:
-        dt, h2d, d2h = res
-        e2e = {"value": chars_all * args.e2e_steps / dt / 1e9, "unit": "Gchar/s",
-               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
-
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        from oracle import oracle as orc
-        orc.build()
-        threads = orc.threads()
-        k, chars, data = wl.cpu_sample(seed, args.cpu_seconds, threads)
-        t0 = time.perf_counter()
-        wl.cpu_run(orc, data, k)
-        dt = time.perf_counter() - t0
-        cpu = {"value": chars / dt / 1e9, "unit": "Gchar/s", "cores": threads, "kind": "port",
-               "sample": f"first {k} strings ({chars} bytes) of the same workload, OpenMP over {threads} threads"}
-
+    verify = not args.no_verify and rank == 0 and world == 1
+    m = measure(wl, args, torch, dev, steps=args.steps, warmup=args.warmup, rank=rank, world=world,
+                local_rank=local_rank, dist=dist, e2e_steps=args.e2e_steps, verify=verify)
+    failed = failed_checks(m)
     if rank == 0:
-        line = base_line(args, wl, value, ms_per_step, args.steps, warm, world)
-        line["config"] = {**wl.config(), "parallelism": f"dp{world} (independent shards, no collective)"}
-        line["roofline"] = roof
-        if getattr(wl, "tune_info", None) is not None:
-            line["autotune"] = wl.tune_info
-        if hasattr(wl, "exact_mismatches"):
-            from oracle import oracle as orc
-            orc.build()
-            line["accept_mismatches_vs_oracle_first_2048"] = wl.exact_mismatches(orc)
-        elif hasattr(wl, "llerr"):
-            from oracle import oracle as orc
-            orc.build()
-            line["loglik_max_rel_err_vs_fp64"] = wl.llerr(orc)
-        line["e2e"] = e2e
+        line = base_line(args, wl, m["value"], m["ms_per_step"], args.steps, m["warmup"], world)
+        for k in ("config", "roofline", "autotune", "mismatches_vs_oracle", "e2e"):
+            if k in m:
+                line[k] = m[k]
+        cpu = None
+        if verify and not args.no_cpu_baseline:
+            o = m["oracle"]
+            cpu = {"value": o["gchar_s"], "unit": "Gchar/s", "cores": o["threads"], "kind": "port",
+                   "sample": (f"the oracle check of this run: {o['bytes']} bytes of the batch (every "
+                              f"string checked where the workload is a DFA, NFA or scan batch), the "
+                              f"same bytes as the GPU run, OpenMP over {o['threads']} threads")}
         line["cpu_baseline"] = cpu
-        line["gpu_launches"] = wl.launches_per_step * args.steps
-        line["clocks"] = clock_info
+        line["gpu_launches"] = m["gpu_launches"]
+        line["clocks"] = m["clocks"]
+        if world == 1 and not args.no_extras:
+            names = set(x.strip() for x in args.extras.split(",") if x.strip())
+            line["configs"] = run_extras(args, torch, dev, wl, names)
+            for v in line["configs"].values():
+                failed |= isinstance(v, dict) and (failed_checks(v) or bool(v.get("mismatches_vs_batched")))
+        else:
+            wl.close()
         print(json.dumps(line), flush=True)
-    wl.set.close()
+    else:
+        wl.close()
+    if failed:
+        raise SystemExit("results differ from the oracle (see mismatches_vs_oracle)")
 
 
 def main():
@@ -987,6 +1374,8 @@ def main():
         if rank == 0:
             serve_arm(args)
         return
+    if args.workload != "ragged":
+        args.no_extras = True
     if world > 1:
         import datetime
         import torch

@@ -245,6 +245,7 @@ class Server:
         self._stop = False
         self._bytes_done = 0
         self._batches = 0
+        self._loop_busy = 0.0   # seconds the loop spent packing, launching and handing out results
         self._t_first = None
         self._t_last = None
         self._error: Optional[BaseException] = None
@@ -330,7 +331,7 @@ class Server:
         with self._cv:
             lat = {k: np.array(v, dtype=np.float64) for k, v in self._lat.items()}
             span = (self._t_last - self._t_first) if self._t_first and self._t_last else 0.0
-            nbytes, nb = self._bytes_done, self._batches
+            nbytes, nb, busy = self._bytes_done, self._batches, self._loop_busy
 
         def pct(a):
             x = a if a.size else np.zeros(1)
@@ -339,7 +340,8 @@ class Server:
 
         allv = np.concatenate(list(lat.values()))
         out = {"requests": int(allv.size), "batches": nb, "bytes": nbytes,
-               "gchar_s": nbytes / span / 1e9 if span > 0 else 0.0, **pct(allv)}
+               "gchar_s": nbytes / span / 1e9 if span > 0 else 0.0,
+               "loop_busy_frac": busy / span if span > 0 else 0.0, **pct(allv)}
         out["by_kind"] = {k: pct(v) for k, v in lat.items()}
         return out
 
@@ -348,6 +350,7 @@ class Server:
             self._lat = {k: [] for k in KINDS}
             self._bytes_done = 0
             self._batches = 0
+            self._loop_busy = 0.0
             self._t_first = self._t_last = None
 
     def close(self):
@@ -446,6 +449,7 @@ class Server:
 
     def _launch(self, s: _Slot, batch: list):
         torch = self.torch
+        t_busy = time.perf_counter()
         order, blob, doff, ids, roff, groups = pack_batch(batch)
         nd = len(doff) - 1
         total = len(blob)
@@ -503,8 +507,10 @@ class Server:
         with self._cv:
             if self._t_first is None:
                 self._t_first = time.perf_counter()
+            self._loop_busy += time.perf_counter() - t_busy
 
     def _finish(self, s: _Slot):
+        t_busy = time.perf_counter()
         nd, nr, total = s.meta
         fs = s.h_fs[:nd].numpy() if nd else None
         ac = s.h_ac[:nd].numpy() if nd else None
@@ -525,6 +531,7 @@ class Server:
             self._bytes_done += total
             self._batches += 1
             self._t_last = now
+            self._loop_busy += time.perf_counter() - t_busy
         with self._fin:
             for r in s.batch:
                 r.t_done = now
