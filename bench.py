@@ -35,8 +35,10 @@ them under "configs": cfg1_plain, plain_per_pattern (the ragged batch as 16
 per-automaton launches, device buffers and through the reference's
 prefix_engine_* ABI with host buffers), cfg3a_scan, cfg3b_nfa (bit-parallel and
 tensor-core forms), cfg4_pnfa (with the one-string chain latency per
-position), cfg5_served (a Poisson sweep up to saturation, with the limiter
-named). --no-extras skips them.
+position), dfa_n32_64 (the ragged batch shape, 250K strings, on 32- and
+64-state automata), kgram_sweep (K = 1, 2, 4 on 4 GB of ACGT strings, where
+gram tables apply), cfg5_served (a Poisson sweep up to saturation, with the
+limiter named). --no-extras skips them.
 
 Multi-GPU: one process per GPU (torchrun); every rank runs its own seeded
 batch (weak scaling, no data-path collective); times are the max over ranks
@@ -74,7 +76,8 @@ from trex_b200.sharding import max_over_ranks, rank_seed  # noqa: E402
 
 METRIC = "Gchar/s vs HBM roofline, plain vs batched/served; served p50/p99 ms (1 B200)"
 SUB_ALPHABET = b"ACGT"
-EXTRAS = ("cfg1_plain", "plain_per_pattern", "cfg3a_scan", "cfg3b_nfa", "cfg4_pnfa", "cfg5_served")
+EXTRAS = ("cfg1_plain", "plain_per_pattern", "cfg3a_scan", "cfg3b_nfa", "cfg4_pnfa", "dfa_n32_64",
+          "kgram_sweep", "cfg5_served")
 
 
 def parse_args(argv=None):
@@ -1276,6 +1279,27 @@ def pnfa_latency(args, torch, dev):
                          "(cuda/probe_wgmma_layout.cu)"}
 
 
+def kgram_sweep(args, torch, dev):
+    """K-gram widths where grams apply: one 16-state automaton over the bytes
+    ACGT, 4M strings x 1024 bytes (4 GB), each width timed like the headline
+    (K = 8 needs two letters). The headline batch's automata distinguish all
+    256 bytes, so no gram table applies to them (kgram_max 1 each)."""
+    out = {}
+    for k in (1, 2, 4):
+        wl = DFAWorkload(sub_args(args, workload="plain", strings=4 << 20, kgram=k, tuned=False))
+        m = measure(wl, wl.args, torch, dev, steps=20, warmup=3, e2e_steps=0, verify=(k == 4),
+                    roof_tag="kgram")
+        out[f"k{k}"] = {"value": m["value"], "kernel_ms": m["roofline"]["kernel_ms_mean"],
+                        "frac": m["roofline"]["frac"], "kgram": m["config"]["kgram"]}
+        if "mismatches_vs_oracle" in m:
+            out[f"k{k}"]["mismatches_vs_oracle"] = m["mismatches_vs_oracle"]
+        wl.close()
+        del wl
+        torch.cuda.empty_cache()
+    return {"workload": "one random 16-state DFA over bytes ACGT, 4M strings x 1024 bytes (4 GB), "
+                        "K-gram width forced per run", "by_k": out}
+
+
 def run_extras(args, torch, dev, main_wl, names):
     extras = {}
     if "plain_per_pattern" in names and isinstance(main_wl, DFAWorkload) and main_wl.kind == "ragged":
@@ -1295,7 +1319,9 @@ def run_extras(args, torch, dev, main_wl, names):
              2, "nfa_tc"),
             ("cfg3b_nfa_tensor_int8", lambda: NFATcWorkload(sub_args(args, workload="nfa", nfa_method="tc8")),
              2, "nfa_tc8"),
-            ("cfg4_pnfa", lambda: PNFAWorkload(sub_args(args, workload="pnfa", pnfa_mode="bf16")), 5, "pnfa")]
+            ("cfg4_pnfa", lambda: PNFAWorkload(sub_args(args, workload="pnfa", pnfa_mode="bf16")), 5, "pnfa"),
+            ("dfa_n32_64", lambda: DFAWorkload(sub_args(args, workload="ragged", dfa_sizes="32,64",
+                                                        strings=250_000)), 5, "ragged_n32_64")]
     for name, make, steps, tag in subs:
         if name.split("_tensor")[0] not in names:
             continue
@@ -1313,6 +1339,11 @@ def run_extras(args, torch, dev, main_wl, names):
             extras["cfg4_pnfa_latency"] = pnfa_latency(args, torch, dev)
         except Exception as e:
             extras["cfg4_pnfa_latency"] = {"error": repr(e)[:400]}
+    if "kgram_sweep" in names:
+        try:
+            extras["kgram_sweep"] = kgram_sweep(args, torch, dev)
+        except Exception as e:
+            extras["kgram_sweep"] = {"error": repr(e)[:400]}
     if "cfg5_served" in names:
         try:
             extras["cfg5_served"] = serve_measure(args)

@@ -1,9 +1,10 @@
 """Generate golden vectors by importing the reference's own Python modules.
 
-Run from the repository root in a checkout where the reference project is
-available (default location below, override with TREX_REFERENCE):
+Run from the repository root, naming the reference project's checkout (the
+directory that holds its ``src/`` package) on the command line or in
+TREX_REFERENCE:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py <reference checkout>
 
 It writes ``tests/golden/reference_golden.json`` (small, committed). The
 tests read only that JSON file; they never import the reference.
@@ -34,7 +35,17 @@ from pathlib import Path
 
 import numpy as np
 
-REF = Path(os.environ.get("TREX_REFERENCE", "/root/reference"))
+def _reference_dir() -> Path:
+    arg = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("TREX_REFERENCE")
+    if not arg:
+        sys.exit("usage: make_golden.py <reference checkout> (or set TREX_REFERENCE)")
+    ref = Path(arg)
+    if not (ref / "src" / "regex_to_dfa.py").exists():
+        sys.exit(f"{ref} does not hold the reference's src/ package")
+    return ref
+
+
+REF = _reference_dir()
 OUT = Path(__file__).resolve().parent / "reference_golden.json"
 
 sys.path.insert(0, str(REF))

@@ -56,13 +56,14 @@ class TuneReport:
     """What a tuning call chose and what it measured (milliseconds per run)."""
 
     kgram: list = field(default_factory=list)       # per automaton
+    kgram_max: list = field(default_factory=list)   # per automaton: the largest K it allows
     seg_len: int = 0
     sweep: list = field(default_factory=list)       # [{"what": ..., "value": ..., "ms": ...}]
     cached: bool = False
 
     def as_dict(self) -> dict:
-        return {"kgram": self.kgram, "seg_len": self.seg_len, "sweep": self.sweep,
-                "cached": self.cached}
+        return {"kgram": self.kgram, "kgram_max": self.kgram_max, "seg_len": self.seg_len,
+                "sweep": self.sweep, "cached": self.cached}
 
 
 class Autotuner:
@@ -151,6 +152,7 @@ class Autotuner:
         # K-gram width per automaton, on its own strings
         for d in range(n_dfas):
             kmax = dfa_set.kgram_max(d)
+            rep.kgram_max.append(kmax)
             rows = np.flatnonzero(ids == d)
             med = _pow2_ceil(np.median(lens[rows])) if rows.size else 1
             N = dfa_set.dfas[d].n_states

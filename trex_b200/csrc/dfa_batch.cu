@@ -227,22 +227,17 @@ __device__ __forceinline__ uint32_t warp_rank(uint32_t *cnt, bool pred, int key)
 // queue class reserved for it alone (no global atomics on the hot counters).
 
 // Counts the items of every (DFA, length class) and the map slots of this CTA's
-// strings into its row of cta_bins / cta_maps, and the items of the batch and,
-// per DFA, its bytes (in 64-byte units: they only weigh the CTAs' first
-// automaton).
+// strings into its row of cta_bins / cta_maps, and the items of the batch.
 __global__ void __launch_bounds__(kPlanThreads)
 plan_count_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n, int64_t total_bytes,
                   const DfaDesc *desc, int n_dfas, int32_t seg_len, uint32_t base_mis, int64_t multi_n,
-                  uint32_t *cta_bins, uint32_t *cta_maps, unsigned long long *q_bytes,
-                  unsigned long long *n_items, uint32_t *err) {
+                  uint32_t *cta_bins, uint32_t *cta_maps, unsigned long long *n_items, uint32_t *err) {
     __shared__ uint32_t cnt[kMaxDfasPerSet * kLenClasses];
-    __shared__ unsigned long long byt[kMaxDfasPerSet];
     __shared__ unsigned long long items;
     __shared__ uint32_t maps;
     const uint32_t lane = threadIdx.x & 31u;
     const int n_bins = n_dfas * kLenClasses;
     for (int t = threadIdx.x; t < n_bins; t += blockDim.x) cnt[t] = 0;
-    for (int t = threadIdx.x; t < n_dfas; t += blockDim.x) byt[t] = 0;
     if (threadIdx.x == 0) { items = 0; maps = 0; }
     __syncthreads();
     for (int64_t tile = blockIdx.x; tile * kPlanThreads < n; tile += gridDim.x) {
@@ -265,14 +260,6 @@ plan_count_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n, int6
         const uint32_t msum = __reduce_add_sync(0xffffffffu, k > 1 ? k : 0u);
         if (lane == 0 && ksum) atomicAdd(&items, (unsigned long long)ksum);
         if (lane == 0 && msum) atomicAdd(&maps, msum);
-        const uint32_t units = d >= 0 ? (uint32_t)min((len + 127) >> 6, (int64_t)1 << 26) : 0u;
-        for (uint32_t rem = __ballot_sync(0xffffffffu, d >= 0); rem;) {   // one pass per DFA
-            const int leader = __ffs(rem) - 1;
-            const int dl = __shfl_sync(0xffffffffu, d, leader);
-            const uint32_t sum = __reduce_add_sync(0xffffffffu, d == dl ? units : 0u);
-            if ((int)lane == leader) atomicAdd(&byt[dl], (unsigned long long)sum << 6);
-            rem &= ~__ballot_sync(0xffffffffu, d == dl);
-        }
     }
     __syncthreads();
     uint32_t *row = cta_bins + (size_t)blockIdx.x * n_bins;
@@ -281,8 +268,14 @@ plan_count_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n, int6
         cta_maps[blockIdx.x] = maps;
         if (items) atomicAdd(n_items, items);
     }
-    for (int t = threadIdx.x; t < n_dfas; t += blockDim.x)
-        if (byt[t]) atomicAdd(&q_bytes[t], byt[t]);
+}
+
+// A length class's typical walked bytes (its middle; only weighs the CTAs' first
+// automaton): classes 32-63 hold 128-byte ranges below 4 KiB, 0-31 powers of two.
+__device__ __forceinline__ unsigned long long class_bytes(int c) {
+    if (c >= 32) return (unsigned long long)(4032 - 128 * (c - 32));
+    const int e = min(12 + 31 - c, 40);
+    return 3ull << (e - 1);
 }
 
 // One CTA of kPlanThreads threads. Turns the per-CTA counts of the G planning
@@ -297,8 +290,8 @@ plan_count_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n, int6
 // fill kernel nor the ragged kernel writes an item.
 __global__ void __launch_bounds__(kPlanThreads)
 plan_scan_kernel(uint32_t *cta_bins, uint32_t *bin_base, uint32_t *bin_end, uint32_t *cta_maps, int G,
-                 int n_dfas, uint32_t *q_base, uint32_t *q_count, const unsigned long long *n_items,
-                 int64_t max_items, uint32_t *err) {
+                 int n_dfas, uint32_t *q_base, uint32_t *q_count, unsigned long long *q_bytes,
+                 const unsigned long long *n_items, int64_t max_items, uint32_t *err) {
     constexpr int kPer = kMaxDfasPerSet * kLenClasses / kPlanThreads;   // classes a thread (pass 2)
     constexpr int kRows = 16;                                           // CTAs' counts in flight
     __shared__ uint32_t s_tot[kMaxDfasPerSet * kLenClasses];
@@ -363,6 +356,7 @@ plan_scan_kernel(uint32_t *cta_bins, uint32_t *bin_base, uint32_t *bin_end, uint
             bin_end[b] = base + tot[j];
             if (b % kLenClasses == 0) q_base[b / kLenClasses] = base;
             if (b % kLenClasses == kLenClasses - 1) q_count[b / kLenClasses] = base + tot[j];
+            if (tot[j]) atomicAdd(&q_bytes[b / kLenClasses], tot[j] * class_bytes(b % kLenClasses));
         }
         base += tot[j];
     }
@@ -1345,17 +1339,20 @@ __device__ __noinline__ uint32_t fix_item(const RaggedParams &P, const uint8_t *
 
 // Strings cut into several items: chains the items' records in order, one lane
 // per string. Item j's record is right when its guessed entry equals the end
-// state of item j - 1 (item 0 starts from the start state); otherwise the lane
-// walks the item from the true entry state until it meets the recorded chain at
-// a checkpoint (fix_item: about one window for synchronising automata). The
-// first item whose chains never meet (automata that do not synchronise, such
-// as permutations) is walked again whole by the warp, and the check goes on
-// from there, 32 records at a time.
+// state of item j - 1 (item 0 starts from the start state); otherwise the item
+// is walked from the true entry state until it meets the recorded chain at a
+// checkpoint (fix_item: about one window for synchronising automata), by any
+// lane of the warp. The first item whose chains never meet (automata that do
+// not synchronise, such as permutations) is walked again whole by the warp, and
+// the check goes on from there, 32 records at a time.
 __global__ void __launch_bounds__(kComposeThreads) compose_kernel(RaggedParams P) {
     __shared__ __align__(16) uint8_t s_tbl[kComposeThreads / 32][256 * kSmallDfaStates];
+    __shared__ uint32_t s_bad[kComposeThreads / 32][32];   // per string of a warp: first failed fix-up
     if (*(volatile uint32_t *)P.err & kErrCapacity) return;   // the plan was refused
     const uint32_t FULL = 0xffffffffu;
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+    s_bad[wib][lane] = 0xFFFFFFFFu;
+    __syncwarp();
     uint8_t *tbl = s_tbl[wib];
     int tbl_dfa = -1;
     const int64_t nwarps = (int64_t)gridDim.x * (kComposeThreads / 32);
@@ -1379,36 +1376,80 @@ __global__ void __launch_bounds__(kComposeThreads) compose_kernel(RaggedParams P
                 }
             }
         }
-        // each lane chains its own string, fixing wrong guesses from the checkpoints
+        // Each lane chains its own string's records, as if every wrong guess were fixed by
+        // meeting the recorded chain at a checkpoint (true unless the automaton does not
+        // synchronise): the entry of item j is then the recorded end state of item j - 1.
+        // The fix-ups of eight records of the warp's 32 strings are shared out over the
+        // lanes, one a lane at a time (a lane per string would run them one after another:
+        // SIMT serialises divergent calls). A fix-up that does not end in the recorded end
+        // state hands the string to the warp re-walk below from that item.
         uint32_t st = 0, jbad = 0;
         bool help = false;
-        if (k > 1) {
-            const uint8_t *tm = P.tmaps + P.desc[d].tmap_off;
-            const uint32_t N = (uint32_t)P.desc[d].n_states;
-            st = (uint32_t)(P.maps[mb] >> 8) & 0xffu;   // item 0 starts from the start state
-            for (uint32_t j0 = 1; j0 < k && !help; j0 += 8) {
+        if (k > 1) st = (uint32_t)(P.maps[mb] >> 8) & 0xffu;   // item 0 starts from the start state
+        for (uint32_t j0 = 1; __any_sync(FULL, k > 1 && j0 < k && !help); j0 += 8) {
+            const bool act = k > 1 && j0 < k && !help;
+            uint32_t tmask = 0, elo = 0, ehi = 0;   // records needing a fix-up, their entry states
+            if (act) {
                 uint64_t v[8];   // eight records loaded together (one load latency for most strings)
 #pragma unroll
                 for (int u = 0; u < 8; ++u) v[u] = j0 + u < k ? P.maps[mb + j0 + u] : 0ull;
 #pragma unroll
                 for (int u = 0; u < 8; ++u) {
-                    const uint32_t j = j0 + u;
-                    if (help || j >= k) continue;
-                    if (((uint32_t)v[u] & 0xffu) == st) {
-                        st = (uint32_t)(v[u] >> 8) & 0xffu;
-                    } else {
-                        int64_t b0, b1;
-                        item_range(g, s0, len, j, &b0, &b1);
-                        const uint32_t f = st < N ? fix_item(P, tm, N, b0, b1, st, v[u]) : 0xFFFFu;
-                        if (f != 0xFFFFu) st = f;
-                        else { help = true; jbad = j; }
+                    if (j0 + u >= k) continue;
+                    if (((uint32_t)v[u] & 0xffu) != st) {
+                        tmask |= 1u << u;
+                        if (u < 4) elo |= st << (8 * u);
+                        else ehi |= st << (8 * (u - 4));
                     }
+                    st = (uint32_t)(v[u] >> 8) & 0xffu;
                 }
             }
-            if (!help) {
-                if (st < (uint32_t)P.desc[d].n_states) write_result(P, (uint32_t)i, st, P.desc[d].accept_off);
-                else atomicOr(P.err, kErrCapacity);   // records not written by this plan
+            const uint32_t cnt = __popc(tmask);
+            uint32_t incl = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t x = __shfl_up_sync(FULL, incl, o);
+                if (lane >= (uint32_t)o) incl += x;
             }
+            const uint32_t total = __shfl_sync(FULL, incl, 31);
+            for (uint32_t t0 = 0; t0 < total; t0 += 32) {
+                const uint32_t t = t0 + lane;
+                uint32_t ow = 0;   // the owner: the first lane whose inclusive count exceeds t
+#pragma unroll
+                for (uint32_t step = 16; step >= 1; step >>= 1)
+                    if (__shfl_sync(FULL, incl, ow + step - 1) <= t) ow += step;
+                const uint32_t io = __shfl_sync(FULL, incl, ow), co = __shfl_sync(FULL, cnt, ow);
+                const uint32_t mo = __shfl_sync(FULL, tmask, ow), mbo = __shfl_sync(FULL, mb, ow);
+                const uint32_t elo_o = __shfl_sync(FULL, elo, ow), ehi_o = __shfl_sync(FULL, ehi, ow);
+                const int d_o = __shfl_sync(FULL, d, ow);
+                const int64_t s0o = __shfl_sync(FULL, s0, ow), leno = __shfl_sync(FULL, len, ow);
+                const ItemGeom go{__shfl_sync(FULL, k, ow), __shfl_sync(FULL, g.seg, ow),
+                                  __shfl_sync(FULL, g.first, ow)};
+                if (t >= total) continue;
+                const uint32_t u = __fns(mo, 0, (int)(t - (io - co)) + 1);   // the owner's fix-up
+                const uint32_t e = (u < 4 ? elo_o >> (8 * u) : ehi_o >> (8 * (u - 4))) & 0xffu;
+                const uint32_t j = j0 + u;
+                const uint64_t rec = P.maps[mbo + j];
+                const uint32_t N = (uint32_t)P.desc[d_o].n_states;
+                int64_t b0, b1;
+                item_range(go, s0o, leno, j, &b0, &b1);
+                const uint32_t f = e < N ? fix_item(P, P.tmaps + P.desc[d_o].tmap_off, N, b0, b1, e, rec)
+                                         : 0xFFFFu;
+                if (f != ((uint32_t)(rec >> 8) & 0xffu)) atomicMin(&s_bad[wib][ow], (j << 8) | e);
+            }
+            __syncwarp();
+            const uint32_t bad = s_bad[wib][lane];
+            if (act && bad != 0xFFFFFFFFu) {   // the walk goes on from item bad >> 8
+                help = true;
+                jbad = bad >> 8;
+                st = bad & 0xffu;
+            }
+            s_bad[wib][lane] = 0xFFFFFFFFu;
+            __syncwarp();
+        }
+        if (k > 1 && !help) {
+            if (st < (uint32_t)P.desc[d].n_states) write_result(P, (uint32_t)i, st, P.desc[d].accept_off);
+            else atomicOr(P.err, kErrCapacity);   // records not written by this plan
         }
         // strings with a wrong guess: the warp re-walks that item and goes on checking
         for (uint32_t todo = __ballot_sync(FULL, help); todo; todo &= todo - 1) {
@@ -1557,11 +1598,11 @@ static int dfa_set_run_ex(trex_dfa_set *set, const uint8_t *data, const int64_t 
                                                   (int64_t)set->n_sms, (int64_t)kMaxPlanCtas});
     plan_count_kernel<<<plan_grid, kPlanThreads, 0, stream>>>(
         offsets, dfa_id, n, total_bytes, set->d_desc, set->n_dfas, seg_len, base_mis, multi_n,
-        cta_bins, cta_maps, q_bytes, n_items, err);
+        cta_bins, cta_maps, n_items, err);
     TREX_CHECK_LAUNCH();
     plan_scan_kernel<<<1, kPlanThreads, 0, stream>>>(cta_bins, bin_base, bin_end, cta_maps, plan_grid,
-                                                     set->n_dfas, q_base, q_count, n_items, L.max_items,
-                                                     err);
+                                                     set->n_dfas, q_base, q_count, q_bytes, n_items,
+                                                     L.max_items, err);
     TREX_CHECK_LAUNCH();
     plan_fill_kernel<<<plan_grid, kPlanThreads, 0, stream>>>(
         offsets, dfa_id, n, total_bytes, set->d_desc, set->n_dfas, seg_len, base_mis, multi_n,

@@ -864,7 +864,11 @@ __device__ void pn_epilogue(const PnParams &P, const PnShared &S, uint32_t tbase
                 float scl = 1.f;
                 {
                     const int col = c + lane;
-                    if (lane < 16 && col >= c_lo && col < c_hi) {
+                    if (lane < 16 && col >= c_lo && col < c_hi && bmode) {
+                        // Boolean forms: no scaling, the exponent sum stays 0
+                        const uint2 rcl = rec[d.row0 + col];
+                        if (owner && (rcl.x & kRecFinish)) finE[rcl.y & 1023u] = 0;
+                    } else if (lane < 16 && col >= c_lo && col < c_hi) {
                         const int row = d.row0 + col;
                         const uint2 rcl = rec[row];
                         const bool fresh = (rcl.y & kRecFresh) != 0;
@@ -877,7 +881,7 @@ __device__ void pn_epilogue(const PnParams &P, const PnShared &S, uint32_t tbase
                             m = fmaxf(x2.x, x2.y);
                         }
                         int f = pn_ceil_exp(m * R);
-                        f = bmode ? 0 : min(max(f, -125), 125);
+                        f = min(max(f, -125), 125);
                         scl = pn_pow2(-f);
                         if (owner) {
                             const int e = (fresh ? 0 : E[jl]) + f;
@@ -939,14 +943,17 @@ __device__ void pn_epilogue(const PnParams &P, const PnShared &S, uint32_t tbase
                                 : 0.f;
                 }
                 // column maxima over this warp's 32 states: the 8 threads with the same cp
+                // (they set the next step's scale; the Boolean forms do not scale)
+                if (!bmode) {
 #pragma unroll
-                for (int o = 4; o < 32; o <<= 1)
+                    for (int o = 4; o < 32; o <<= 1)
 #pragma unroll
-                    for (int i = 0; i < 4; ++i) m[i] = fmaxf(m[i], __shfl_xor_sync(0xffffffffu, m[i], o));
-                if (j == 0) {
+                        for (int i = 0; i < 4; ++i) m[i] = fmaxf(m[i], __shfl_xor_sync(0xffffffffu, m[i], o));
+                    if (j == 0) {
 #pragma unroll
-                    for (int i = 0; i < 4; ++i)
-                        if (valid[i] && !(rc[i].x & kRecFinish)) xn[(rc[i].x >> 4) * 2] = m[i];
+                        for (int i = 0; i < 4; ++i)
+                            if (valid[i] && !(rc[i].x & kRecFinish)) xn[(rc[i].x >> 4) * 2] = m[i];
+                    }
                 }
                 if (__any_sync(0xffffffffu, any_fin)) {   // last symbols: accept-weighted sums
                     float pz[4];
@@ -1145,10 +1152,21 @@ __global__ void __launch_bounds__(kPnPlainWarps * 32) pnfa_plain_kernel(PnPlainP
 }
 
 // CUDA-core form with 16-bit tables in shared memory (modes BF16_CC / FP16_CC):
-// the transition tables of all symbols (sigma x 8 KB) are copied into shared
-// memory once per CTA, so a step reads no global memory; the state stays in
-// FP32 with the plain kernel's exact power-of-two rescale. A warp per string,
-// lane l owns states l and l + 32. Its per-step latency is far below the
+// the low-latency chain. The transition tables of all symbols (sigma x 8 KB)
+// are copied into shared memory once per CTA, so a step reads no global
+// memory; the state stays in FP32. Four warps advance one string: thread
+// (o, h) = (gt / 2, gt % 2) of the group forms the dot product of row o of
+// T[c] with states 32h .. 32h + 31 (four independent FMA chains of eight),
+// the two halves meet by one shuffle and the new state goes to the other of
+// two state buffers, so a step costs one named barrier of the group. Rows are
+// stored with their 16-byte chunks permuted by (o & 3), so the eight lanes of
+// a quarter-warp read eight different chunks (no bank conflicts), and the two
+// state halves sit 144 bytes apart for the same reason. Every `resc` steps
+// the group finds max|s| (warp maxima through shared memory) and the next
+// step scales by the exact power of two 2^-f and adds f to the exponent sum,
+// as the plain kernel does every step (power-of-two scaling is exact, so only
+// the rounding of the products differs between the forms). CTA = four groups
+// = four strings in flight; the per-step latency is far below the
 // tensor-core kernel's (which advances many strings per step): the form for
 // few strings, long ones included (serving).
 template <bool FP16>
@@ -1157,96 +1175,131 @@ __device__ __forceinline__ float pn_h2f(uint32_t h) {
     else return __uint_as_float(h << 16);
 }
 
+constexpr int kChainThreads = 128;   // one string per group of four warps
+constexpr int kChainGroups = 4;      // strings per CTA
+struct ChainShared {
+    float s[2][72];        // the state, double-buffered; state i at i + (i >= 32 ? 4 : 0)
+    float wmax[2][4];      // warp maxima of a check step (by its parity)
+    float red[4];
+    unsigned long long idx;
+    uint32_t pad[2];
+};
+constexpr uint32_t kChainSharedBytes = kChainGroups * (uint32_t)sizeof(ChainShared);
+
+__device__ __forceinline__ void pn_group_bar(int g) {
+    asm volatile("bar.sync %0, %1;" :: "r"(g + 1), "r"(kChainThreads) : "memory");
+}
+__device__ __forceinline__ int pn_sidx(int i) { return i + (i >= 32 ? 4 : 0); }
+
 template <bool FP16>
-__global__ void __launch_bounds__(kPnPlainWarps * 32) pnfa_cc_kernel(PnPlainParams P, const uint16_t *T16) {
-    extern __shared__ __align__(16) uint8_t pn_cc_smem[];
-    float *sv_all = reinterpret_cast<float *>(pn_cc_smem);                    // [warps][64]
-    uint16_t *tbl = reinterpret_cast<uint16_t *>(pn_cc_smem + kPnPlainWarps * 64 * 4);
+__global__ void __launch_bounds__(kChainThreads * kChainGroups, 1)
+pnfa_chain_kernel(PnPlainParams P, const uint16_t *T16, int resc) {
+    extern __shared__ __align__(16) uint8_t pn_ch_smem[];
+    const uint32_t FULL = 0xffffffffu;
+    const int g = threadIdx.x / kChainThreads, gt = threadIdx.x % kChainThreads;
+    const int lane = threadIdx.x & 31, wg = gt >> 5;
+    const int o = gt >> 1, h = gt & 1, sw = o & 3;
+    uint4 *tbl = reinterpret_cast<uint4 *>(pn_ch_smem);   // [sigma][64 rows][8 chunks], chunk p at p ^ (row & 3)
+    ChainShared *cs = reinterpret_cast<ChainShared *>(pn_ch_smem + (size_t)P.sigma * 8192) + g;
     {
         const uint4 *src = reinterpret_cast<const uint4 *>(T16);
-        uint4 *dst = reinterpret_cast<uint4 *>(tbl);
-        const int words = P.sigma * 64 * 64 * 2 / 16;
-        for (int i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
+        const int chunks = P.sigma * 64 * 8;
+        for (int i = threadIdx.x; i < chunks; i += blockDim.x) {
+            const int row = i >> 3, p = i & 7;
+            tbl[(row << 3) | (p ^ (row & 3))] = src[i];
+        }
         __syncthreads();
     }
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    float *v = sv_all + w * 64;
+    const float acc_o = gt < 64 ? P.acc[gt] : 0.f;
+    const float start_o = gt < 64 ? P.start[gt] : 0.f;
     for (;;) {
-        unsigned long long idx = 0;
-        if (lane == 0) idx = atomicAdd(P.queue, 1ull);
-        idx = __shfl_sync(0xffffffffu, idx, 0);
+        if (gt == 0) cs->idx = atomicAdd(P.queue, 1ull);
+        pn_group_bar(g);
+        const unsigned long long idx = cs->idx;
         if (idx >= (unsigned long long)P.n) break;
         const int64_t p0 = P.offsets[idx], p1 = P.offsets[idx + 1];
         if (p0 < 0 || p1 < p0 || p1 > P.total_bytes) {
-            if (lane == 0) atomicOr(P.err, kPnErrOffsets);
+            if (gt == 0) atomicOr(P.err, kPnErrOffsets);
+            pn_group_bar(g);
             continue;
         }
-        float s0 = P.start[lane], s1 = P.start[lane + 32];
+        if (gt < 64) cs->s[0][pn_sidx(gt)] = start_o;
+        pn_group_bar(g);
+        int cur = 0;          // the buffer holding the state
         int64_t E = 0;
+        bool any = false;     // some symbol was applied
+        bool pend = false;    // the previous step was a check step
+        uint32_t par = 0;     // parity of the step
+        int chk = resc;       // steps to the next check step
         for (int64_t base = p0; base < p1; base += 32) {
             const int64_t pl = base + lane;
-            const uint32_t mybyte = pl < p1 ? P.data[pl] : 255u;
-            const int nb = (int)min((int64_t)32, p1 - base);
-            for (int k = 0; k < nb; ++k) {
-                const uint32_t c = __shfl_sync(0xffffffffu, mybyte, k);
-                if (c >= (uint32_t)P.sigma) continue;
-                v[lane] = s0;
-                v[lane + 32] = s1;
-                __syncwarp();
-                const uint4 *r0 = reinterpret_cast<const uint4 *>(tbl + ((size_t)c * 64 + lane) * 64);
-                const uint4 *r1 = reinterpret_cast<const uint4 *>(tbl + ((size_t)c * 64 + lane + 32) * 64);
-                const float4 *vv = reinterpret_cast<const float4 *>(v);
-                float a0 = 0.f, a1 = 0.f;
-#pragma unroll
-                for (int q = 0; q < 8; ++q) {   // 8 source states per 16 bytes of a row
-                    const float4 xa = vv[2 * q], xb = vv[2 * q + 1];
-                    const uint4 t0 = r0[q], t1 = r1[q];
-                    const uint32_t u0[4] = {t0.x, t0.y, t0.z, t0.w}, u1[4] = {t1.x, t1.y, t1.z, t1.w};
-                    const float x[8] = {xa.x, xa.y, xa.z, xa.w, xb.x, xb.y, xb.z, xb.w};
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        a0 = fmaf(pn_h2f<FP16>(u0[j] & 0xFFFFu), x[2 * j], a0);
-                        a0 = fmaf(pn_h2f<FP16>(u0[j] >> 16), x[2 * j + 1], a0);
-                        a1 = fmaf(pn_h2f<FP16>(u1[j] & 0xFFFFu), x[2 * j], a1);
-                        a1 = fmaf(pn_h2f<FP16>(u1[j] >> 16), x[2 * j + 1], a1);
+            const uint32_t byte = pl < p1 ? P.data[pl] : 255u;
+            uint32_t m = __ballot_sync(FULL, byte < (uint32_t)P.sigma);
+            while (m) {
+                const int src = __ffs(m) - 1;
+                m &= m - 1;
+                const uint32_t c = __shfl_sync(FULL, byte, src);
+                const uint4 *row = tbl + ((c * 64 + o) << 3);
+                float sc = 1.f;
+                if (pend) {   // the maxima of the previous step's outputs: exact power-of-two scale
+                    const float4 w4 = *reinterpret_cast<const float4 *>(cs->wmax[par ^ 1u]);
+                    const float mx = fmaxf(fmaxf(w4.x, w4.y), fmaxf(w4.z, w4.w));
+                    const uint32_t eb = (__float_as_uint(mx) >> 23) & 0xFFu;
+                    if (mx > 0.f && eb != 0) {
+                        const int f = min(max((int)eb - 126, -125), 125);
+                        sc = pn_pow2(-f);
+                        E += f;
                     }
+                    pend = false;
                 }
-                __syncwarp();
-                float m = fmaxf(fabsf(a0), fabsf(a1));
+                const float4 *sv = reinterpret_cast<const float4 *>(&cs->s[cur][h * 36]);
+                float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
 #pragma unroll
-                for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-                if (m > 0.f) {
-                    uint32_t bits = __float_as_uint(m);
-                    int pre = 0;
-                    if (((bits >> 23) & 0xFFu) == 0) {   // subnormal: lift by 2^64 first
-                        m *= 18446744073709551616.0f;
-                        bits = __float_as_uint(m);
-                        pre = 64;
-                    }
-                    const int e = (int)((bits >> 23) & 0xFFu) - 126 - pre;
-                    const int e1 = max(min(e, 126), -126);
-                    const float sc1 = pn_pow2(-e1);
-                    s0 = a0 * sc1;
-                    s1 = a1 * sc1;
-                    if (e != e1) {
-                        const float sc2 = pn_pow2(-(e - e1));
-                        s0 *= sc2;
-                        s1 *= sc2;
-                    }
-                    E += e;
-                } else {
-                    s0 = 0.f;
-                    s1 = 0.f;
+                for (int k = 0; k < 4; ++k) {
+                    const uint4 t = row[(4 * h + k) ^ sw];   // states 32h + 8k .. + 7 of row o
+                    const float4 x0 = sv[2 * k], x1 = sv[2 * k + 1];
+                    a0 = fmaf(pn_h2f<FP16>(t.x & 0xFFFFu), x0.x, a0);
+                    a1 = fmaf(pn_h2f<FP16>(t.x >> 16), x0.y, a1);
+                    a2 = fmaf(pn_h2f<FP16>(t.y & 0xFFFFu), x0.z, a2);
+                    a3 = fmaf(pn_h2f<FP16>(t.y >> 16), x0.w, a3);
+                    a0 = fmaf(pn_h2f<FP16>(t.z & 0xFFFFu), x1.x, a0);
+                    a1 = fmaf(pn_h2f<FP16>(t.z >> 16), x1.y, a1);
+                    a2 = fmaf(pn_h2f<FP16>(t.w & 0xFFFFu), x1.z, a2);
+                    a3 = fmaf(pn_h2f<FP16>(t.w >> 16), x1.w, a3);
                 }
+                float sum = (a0 + a1) + (a2 + a3);
+                sum += __shfl_xor_sync(FULL, sum, 1);
+                sum *= sc;
+                if (--chk == 0) {   // a check step: this group's max|s'|
+                    float mx = fabsf(sum);
+#pragma unroll
+                    for (int d = 2; d < 32; d <<= 1) mx = fmaxf(mx, __shfl_xor_sync(FULL, mx, d));
+                    if (lane == 0) cs->wmax[par][wg] = mx;
+                    pend = true;
+                    chk = resc;
+                }
+                if (h == 0) cs->s[cur ^ 1][pn_sidx(o)] = sum;
+                cur ^= 1;
+                par ^= 1u;
+                any = true;
+                pn_group_bar(g);
             }
         }
-        float d = s0 * P.acc[lane] + s1 * P.acc[lane + 32];
+        if (!any) {
+            if (gt == 0) pn_write_result(P.loglik, P.accept, P.accept_i32, (int64_t)idx, P.ll_empty);
+        } else {
+            float d = gt < 64 ? cs->s[cur][pn_sidx(gt)] * acc_o : 0.f;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
-        if (lane == 0) {
-            const double ll = d > 0.f ? log((double)d) + (double)E * 0.69314718055994530942 : -INFINITY;
-            pn_write_result(P.loglik, P.accept, P.accept_i32, (int64_t)idx, ll);
+            for (int k = 16; k > 0; k >>= 1) d += __shfl_xor_sync(FULL, d, k);
+            if (lane == 0) cs->red[wg] = d;
+            pn_group_bar(g);
+            if (gt == 0) {
+                const float dot = (cs->red[0] + cs->red[1]) + (cs->red[2] + cs->red[3]);
+                const double ll = dot > 0.f ? log((double)dot) + (double)E * 0.69314718055994530942 : -INFINITY;
+                pn_write_result(P.loglik, P.accept, P.accept_i32, (int64_t)idx, ll);
+            }
         }
+        pn_group_bar(g);   // the slot (idx, red) is free again
     }
 }
 
@@ -1264,6 +1317,10 @@ struct trex_pnfa {
     float *d_rsym[4] = {nullptr, nullptr, nullptr, nullptr};
     uint4 *d_simg[4] = {nullptr, nullptr, nullptr, nullptr};
     uint8_t *d_misc = nullptr;   // [0,8) queue, [8,12) error word
+    // steps between the rescale checks of the chain kernel per 16-bit table type: 4
+    // when the tables' growth bound allows (max |T s| / max |s| <= 16 a step, so five
+    // unchecked steps stay far inside FP32), else every step
+    int chain_resc[2] = {1, 1};
 };
 
 namespace trex {
@@ -1397,6 +1454,11 @@ int trex_pnfa_create(int n_states, int sigma, const float *T, const float *start
             w[(i & 7) >> 1] |= (uint32_t)v << (16 * (i & 1));
         }
         h->start_max16[k] = smax;
+        if (k < 2) {
+            float rmax = 0.f;
+            for (int c = 0; c < sigma; ++c) rmax = std::max(rmax, rs[k][c]);
+            h->chain_resc[k] = rmax <= 16.f ? 4 : 1;
+        }
     }
     {   // int8 Boolean tables: the same A rows as above with 0/1 bytes, four K values a word
         tp[3].assign((size_t)h->npairs * 128 * 16, 0u);
@@ -1444,10 +1506,10 @@ int trex_pnfa_create(int n_states, int sigma, const float *T, const float *start
         e = cudaFuncSetAttribute(pnfa_tc_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)kPnSmemCap);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(pnfa_cc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        e = cudaFuncSetAttribute(pnfa_chain_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)kPnSmemCap);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(pnfa_cc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        e = cudaFuncSetAttribute(pnfa_chain_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)kPnSmemCap);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(pnfa_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1498,18 +1560,22 @@ int trex_pnfa_run(trex_pnfa *h, int mode, const uint8_t *data, const int64_t *of
         Q.queue = queue;
         Q.err = err;
         if (mode != TREX_PNFA_FP32) {
-            const size_t smem = (size_t)kPnPlainWarps * 64 * 4 + (size_t)h->sigma * 64 * 64 * 2;
+            const size_t smem = (size_t)h->sigma * 64 * 64 * 2 + kChainSharedBytes;
             if (smem > kPnSmemCap) {
                 set_last_error_msg("trex_pnfa_run: the shared-memory CUDA-core form takes at most 28 symbols");
                 return TREX_ERR_SHAPE;
             }
-            // one CTA an SM (the tables fill its shared memory), 8 strings at a time each
-            const int64_t warps = std::min<int64_t>(n_strings, (int64_t)h->n_sms * kPnPlainWarps);
-            const int grid = (int)std::max<int64_t>(1, (warps + kPnPlainWarps - 1) / kPnPlainWarps);
+            // one CTA an SM (the tables fill its shared memory), four strings at a time each
+            const int grid = (int)std::max<int64_t>(
+                1, std::min<int64_t>((n_strings + kChainGroups - 1) / kChainGroups, (int64_t)h->n_sms));
             const bool fp16 = mode == TREX_PNFA_FP16_CC;
             profile_kernel_begin(st);
-            if (fp16) pnfa_cc_kernel<true><<<grid, kPnPlainWarps * 32, smem, st>>>(Q, h->d_T16[1]);
-            else pnfa_cc_kernel<false><<<grid, kPnPlainWarps * 32, smem, st>>>(Q, h->d_T16[0]);
+            if (fp16)
+                pnfa_chain_kernel<true><<<grid, kChainThreads * kChainGroups, smem, st>>>(Q, h->d_T16[1],
+                                                                                          h->chain_resc[1]);
+            else
+                pnfa_chain_kernel<false><<<grid, kChainThreads * kChainGroups, smem, st>>>(Q, h->d_T16[0],
+                                                                                           h->chain_resc[0]);
             profile_kernel_end(st);
             TREX_CHECK_LAUNCH();
             return TREX_OK;
