@@ -88,7 +88,7 @@ def parse_args(argv=None):
     ap.add_argument("--impl", choices=["trex", "reference"], default="trex")
     ap.add_argument("--workload", choices=["ragged", "plain", "scan", "nfa", "pnfa", "serve"],
                     default="ragged")
-    ap.add_argument("--serve-rates", type=str, default="2000,8000,32000,64000,128000",
+    ap.add_argument("--serve-rates", type=str, default="2000,8000,32000,128000,256000,512000",
                     help="offered request rates (requests/s) of the serve workload, swept upwards "
                          "until the served rate falls below 90%% of the offered one")
     ap.add_argument("--serve-seconds", type=float, default=2.0)
@@ -299,8 +299,9 @@ class DFAWorkload:
 
     @property
     def launches_per_step(self):
-        # scan: tile bases, empty strings, scan; ragged: count, scan, fill, walk, compose
-        return 3 if self.kind == "scan" else 5
+        # scan: tile bases, empty strings, scan; ragged: count, class prefix, queue scan, fill,
+        # walk, compose
+        return 3 if self.kind == "scan" else 6
 
     def config(self):
         return {"workload": self.workload, "n_strings": self.n, "total_bytes_per_gpu": self.total,
@@ -824,13 +825,15 @@ def serve_measure(args) -> dict:
     # the limiter at the last rate: the device (busy most of the span) or the host loop
     gpu_busy = last.get("gpu_busy_frac") or 0.0
     loop_busy = last.get("loop_busy_frac") or 0.0
+    lag_ms = last.get("client_max_lag_ms") or 0.0
+    shares = "request loop busy {:.0%}, device busy {:.0%} of the span, client behind the arrivals by up " \
+             "to {:.0f} ms".format(loop_busy, gpu_busy, lag_ms)
     if last is top:
         limiter = "not reached (served >= 90% of offered at the highest rate tried)"
-    elif gpu_busy >= 0.8:
-        limiter = "GPU (device busy {:.0%} of the span)".format(gpu_busy)
+    elif loop_busy >= gpu_busy or loop_busy >= 0.8:
+        limiter = "host: the Python request loop (" + shares + ")"
     else:
-        limiter = ("host: the Python request loop and client (loop busy {:.0%}, device busy {:.0%} of "
-                   "the span)".format(loop_busy, gpu_busy))
+        limiter = "GPU (" + shares + ")"
     keys = ("offered_req_s", "offered_gchar_s", "gchar_s", "p50_ms", "p99_ms", "requests", "batches",
             "by_kind", "client_max_lag_ms", "loop_busy_frac", "gpu_busy_frac")
     return {
@@ -1230,7 +1233,7 @@ def plain_per_pattern(args, torch, dev, wl):
     chars = int(wl.total)
     return {"workload": "the ragged batch (same strings and automata) as 16 per-automaton launches",
             "value": chars / (dev_ms * 1e-3) / 1e9, "unit": "Gchar/s", "ms_per_step": dev_ms,
-            "steps": steps, "launches_per_step": 16 * 5,
+            "steps": steps, "launches_per_step": 16 * 6,
             "e2e_reference_abi": {"value": chars / host_s / 1e9, "unit": "Gchar/s",
                                   "ms_per_step": host_s * 1e3,
                                   "dispatch_only_value": chars / (np.mean(disp) * 1e-3) / 1e9,

@@ -68,10 +68,13 @@ class TuneReport:
 
 class Autotuner:
     def __init__(self, cache_path: Optional[str] = None, warmup: int = 2, reps: int = 5,
-                 sample_bytes: int = 256 << 20, scan_bytes: int = 4 << 30):
+                 sample_bytes: int = 256 << 20, scan_bytes: int = 4 << 30, seg_bytes: int = 8 << 30):
         p = cache_path or os.environ.get("TREX_TUNE_CACHE")
         self.path = Path(p) if p else None
         self.warmup, self.reps, self.sample_bytes = warmup, reps, sample_bytes
+        # the work-item length is timed on the whole batch up to seg_bytes: the planning and
+        # chaining kernels are latency-bound, so a sample understates their share
+        self.seg_bytes = seg_bytes
         self.scan_bytes = scan_bytes
         self.cache: dict = {}
         if self.path is not None and self.path.exists():
@@ -190,9 +193,15 @@ class Autotuner:
             rep.seg_len = int(self.cache[key])
         else:
             all_cached = False
-            sub = self._sample(off, self.sample_bytes)
-            sdata, soff = self._gather(data, off, sub)
-            sids = torch.from_numpy(ids[sub].astype(np.int32)).to(dev)
+            if int(off[-1]) <= self.seg_bytes:
+                sdata = data
+                soff = offsets if hasattr(offsets, "cpu") else torch.from_numpy(off).to(dev)
+                sids = (dfa_id if hasattr(dfa_id, "cpu") else torch.from_numpy(ids.astype(np.int32)).to(dev)) \
+                    if dfa_id is not None else torch.zeros(len(off) - 1, dtype=torch.int32, device=dev)
+            else:
+                sub = self._sample(off, self.sample_bytes)
+                sdata, soff = self._gather(data, off, sub)
+                sids = torch.from_numpy(ids[sub].astype(np.int32)).to(dev)
             if not apply:
                 for d, k in enumerate(rep.kgram):
                     dfa_set.set_kgram(d, k)

@@ -52,16 +52,17 @@ struct WorkItem {
 };
 constexpr int64_t kMaxItemsPerString = 65535;
 constexpr int64_t kMaxWalkBytes = (int64_t)1 << 36;   // one item: a 32-bit count of windows
-// Warm-up bytes of an item after the first of its string: one window (a
-// multiple of 32 keeps aligned cuts aligned). Two chains of a random N-state
-// automaton merge with probability ~1/N per byte, so the warm-up chain has
-// reached the true entry state with probability 1 - (1 - 1/N)^32 (87% for
-// N = 16, 99% for N = 8). When it has not, the item's checkpoints (its chain's
-// state 1, 2, 4 and 8 windows into its own bytes) let compose_kernel walk from
-// the true entry state only until the two chains meet (about one window).
+// Warm-up bytes of an item after the first of its string: one window for
+// automata of at most 8 states, two above (multiples of 32 keep aligned cuts
+// aligned). Two chains of a random N-state automaton merge with probability
+// ~1/N per byte, so the warm-up chain has missed the true entry state with
+// probability (1 - 1/N)^W: 1.4% for N = 8 (W = 32), 0.4% for N = 12 and 1.6%
+// for N = 16 (W = 64). When it has, the item's checkpoints (its chain's state
+// 1, 2, 4 and 8 windows into its own bytes) let compose_kernel walk from the
+// true entry state only until the two chains meet (about one window).
 __host__ __device__ __forceinline__ int64_t warm_bytes(int n_states, int64_t seg) {
-    (void)n_states;
-    return 32 < seg ? 32 : seg;
+    const int64_t w = n_states <= 8 ? 32 : 64;
+    return w < seg ? w : seg;
 }
 
 // Error bits reported through the device error word.
@@ -79,8 +80,8 @@ constexpr int kLenClasses = 64;
 
 // ---- scratch layout -----------------------------------------------------------
 struct ScratchLayout {
-    size_t q_base, q_count, q_head, q_bytes, err, n_items, items, maps, str_map, cta_bins, bin_base,
-        bin_end, cta_maps, total;
+    size_t q_base, q_count, q_head, q_bytes, err, n_items, items, maps, split_list, cta_bins, bin_base,
+        bin_end, cta_maps, cta_splits, total;
     int64_t max_items;
 };
 
@@ -107,13 +108,16 @@ static ScratchLayout scratch_layout(int64_t n_strings, int64_t total_bytes, int3
     L.n_items = take(8);
     L.items = take((size_t)L.max_items * sizeof(WorkItem));
     L.maps = take((size_t)L.max_items * sizeof(uint64_t));
-    L.str_map = take((size_t)std::max<int64_t>(n_strings, 1) * 4);
+    // every string cut into several items: string, first map slot, items | automaton << 16 |
+    // (states - 1) << 24, offset of its accept table
+    L.split_list = take((size_t)std::max<int64_t>(n_strings, 1) * 16);
     // planning: items per (planning CTA, DFA x length class), then those CTAs' first
     // queue positions; each class's end; map slots per planning CTA, then its first slot
     L.cta_bins = take((size_t)kMaxPlanCtas * kMaxDfasPerSet * kLenClasses * 4);
     L.bin_base = take(kMaxDfasPerSet * kLenClasses * 4);
     L.bin_end = take(kMaxDfasPerSet * kLenClasses * 4);
     L.cta_maps = take((kMaxPlanCtas + 1) * 4);
+    L.cta_splits = take((kMaxPlanCtas + 1) * 4);
     L.total = o;
     return L;
 }
@@ -231,14 +235,15 @@ __device__ __forceinline__ uint32_t warp_rank(uint32_t *cnt, bool pred, int key)
 __global__ void __launch_bounds__(kPlanThreads)
 plan_count_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n, int64_t total_bytes,
                   const DfaDesc *desc, int n_dfas, int32_t seg_len, uint32_t base_mis, int64_t multi_n,
-                  uint32_t *cta_bins, uint32_t *cta_maps, unsigned long long *n_items, uint32_t *err) {
+                  uint32_t *cta_bins, uint32_t *cta_maps, uint32_t *cta_splits, unsigned long long *n_items,
+                  uint32_t *err) {
     __shared__ uint32_t cnt[kMaxDfasPerSet * kLenClasses];
     __shared__ unsigned long long items;
-    __shared__ uint32_t maps;
+    __shared__ uint32_t maps, splits;
     const uint32_t lane = threadIdx.x & 31u;
     const int n_bins = n_dfas * kLenClasses;
     for (int t = threadIdx.x; t < n_bins; t += blockDim.x) cnt[t] = 0;
-    if (threadIdx.x == 0) { items = 0; maps = 0; }
+    if (threadIdx.x == 0) { items = 0; maps = 0; splits = 0; }
     __syncthreads();
     for (int64_t tile = blockIdx.x; tile * kPlanThreads < n; tile += gridDim.x) {
         const int64_t i = tile * kPlanThreads + threadIdx.x;
@@ -259,13 +264,16 @@ plan_count_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n, int6
         const uint32_t ksum = __reduce_add_sync(0xffffffffu, k);
         const uint32_t msum = __reduce_add_sync(0xffffffffu, k > 1 ? k : 0u);
         if (lane == 0 && ksum) atomicAdd(&items, (unsigned long long)ksum);
+        const uint32_t ssum = __popc(__ballot_sync(0xffffffffu, k > 1));
         if (lane == 0 && msum) atomicAdd(&maps, msum);
+        if (lane == 0 && ssum) atomicAdd(&splits, ssum);
     }
     __syncthreads();
     uint32_t *row = cta_bins + (size_t)blockIdx.x * n_bins;
     for (int t = threadIdx.x; t < n_bins; t += blockDim.x) row[t] = cnt[t];
     if (threadIdx.x == 0) {
         cta_maps[blockIdx.x] = maps;
+        cta_splits[blockIdx.x] = splits;
         if (items) atomicAdd(n_items, items);
     }
 }
@@ -278,10 +286,44 @@ __device__ __forceinline__ unsigned long long class_bytes(int c) {
     return 3ull << (e - 1);
 }
 
-// One CTA of kPlanThreads threads. Turns the per-CTA counts of the G planning
-// CTAs into positions: over each class b, the exclusive prefix of the CTAs'
-// counts (written over cta_bins), so that class b of CTA c starts at
-// bin_base[b] + cta_bins[c][b]; classes follow each other by DFA and, inside a
+// Per class, the exclusive prefix of the G planning CTAs' counts, written over
+// cta_bins, and the class's total into bin_end. Eight threads share a class:
+// thread r of a class sums rows r * G / 8 .. (r + 1) * G / 8 (all loads in
+// flight), the eight partial sums are scanned by shuffles.
+constexpr int kPrefixParts = 8;
+constexpr int kPrefixRows = (kMaxPlanCtas + kPrefixParts - 1) / kPrefixParts;
+constexpr int kPrefixThreads = 256;
+__global__ void __launch_bounds__(kPrefixThreads)
+plan_prefix_kernel(uint32_t *cta_bins, uint32_t *bin_end, int G, int n_bins) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int b = t / kPrefixParts, r = t % kPrefixParts;
+    const bool on = b < n_bins;
+    const int c0 = r * G / kPrefixParts, c1 = (r + 1) * G / kPrefixParts;
+    uint32_t v[kPrefixRows], part = 0;
+#pragma unroll
+    for (int u = 0; u < kPrefixRows; ++u) {
+        v[u] = on && c0 + u < c1 ? cta_bins[(size_t)(c0 + u) * n_bins + b] : 0u;
+        part += v[u];
+    }
+    uint32_t incl = part;
+#pragma unroll
+    for (int o = 1; o < kPrefixParts; o <<= 1) {
+        const uint32_t x = __shfl_up_sync(0xffffffffu, incl, o, kPrefixParts);
+        if (r >= o) incl += x;
+    }
+    uint32_t run = incl - part;
+#pragma unroll
+    for (int u = 0; u < kPrefixRows; ++u)
+        if (on && c0 + u < c1) {
+            cta_bins[(size_t)(c0 + u) * n_bins + b] = run;
+            run += v[u];
+        }
+    if (on && r == kPrefixParts - 1) bin_end[b] = incl;
+}
+
+// One CTA of kPlanThreads threads. Turns the class totals into positions: class
+// b of CTA c starts at bin_base[b] + cta_bins[c][b] (cta_bins holds the prefix
+// over the CTAs after plan_prefix_kernel); classes follow each other by DFA and, inside a
 // DFA, by class (each DFA's queue is one range, longest items first). bin_end
 // gets each class's end and cta_maps each CTA's first map slot (cta_maps[G]:
 // the total). Offsets that overlap (each string in range, but their lengths
@@ -289,36 +331,25 @@ __device__ __forceinline__ unsigned long long class_bytes(int c) {
 // for: then the error bit is set and every queue is left empty, so neither the
 // fill kernel nor the ragged kernel writes an item.
 __global__ void __launch_bounds__(kPlanThreads)
-plan_scan_kernel(uint32_t *cta_bins, uint32_t *bin_base, uint32_t *bin_end, uint32_t *cta_maps, int G,
+plan_scan_kernel(uint32_t *cta_bins, uint32_t *bin_base, uint32_t *bin_end, uint32_t *cta_maps,
+                 uint32_t *cta_splits, int G,
                  int n_dfas, uint32_t *q_base, uint32_t *q_count, unsigned long long *q_bytes,
                  const unsigned long long *n_items, int64_t max_items, uint32_t *err) {
     constexpr int kPer = kMaxDfasPerSet * kLenClasses / kPlanThreads;   // classes a thread (pass 2)
-    constexpr int kRows = 16;                                           // CTAs' counts in flight
     __shared__ uint32_t s_tot[kMaxDfasPerSet * kLenClasses];
     __shared__ uint32_t s_warp[kPlanThreads / 32];
     const int n_bins = n_dfas * kLenClasses;
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     if (*n_items > (unsigned long long)max_items) {
-        if (threadIdx.x == 0) atomicOr(err, kErrCapacity);
+        if (threadIdx.x == 0) {
+            atomicOr(err, kErrCapacity);
+            cta_splits[G] = 0;
+        }
         if ((int)threadIdx.x < n_dfas) q_base[threadIdx.x] = q_count[threadIdx.x] = 0;
         return;
     }
-    // pass 1: per class, the exclusive prefix over the CTAs (kRows loads in flight)
-    for (int b = threadIdx.x; b < n_bins; b += kPlanThreads) {
-        uint32_t run = 0;
-        for (int c0 = 0; c0 < G; c0 += kRows) {
-            uint32_t v[kRows];
-#pragma unroll
-            for (int u = 0; u < kRows; ++u) v[u] = c0 + u < G ? cta_bins[(size_t)(c0 + u) * n_bins + b] : 0u;
-#pragma unroll
-            for (int u = 0; u < kRows; ++u)
-                if (c0 + u < G) {
-                    cta_bins[(size_t)(c0 + u) * n_bins + b] = run;
-                    run += v[u];
-                }
-        }
-        s_tot[b] = run;
-    }
+    // the class totals (plan_prefix_kernel left them in bin_end)
+    for (int b = threadIdx.x; b < n_bins; b += kPlanThreads) s_tot[b] = bin_end[b];
     __syncthreads();
     // pass 2: exclusive scan of the class totals in class order (thread t: classes kPer t ..)
     uint32_t tot[kPer], mine = 0;
@@ -370,6 +401,13 @@ plan_scan_kernel(uint32_t *cta_bins, uint32_t *bin_base, uint32_t *bin_end, uint
             run += v;
         }
         cta_maps[G] = run;
+        run = 0;
+        for (int c = 0; c < G; ++c) {
+            const uint32_t v = cta_splits[c];
+            cta_splits[c] = run;
+            run += v;
+        }
+        cta_splits[G] = run;
     }
 }
 
@@ -382,11 +420,11 @@ __global__ void __launch_bounds__(kPlanThreads)
 plan_fill_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n, int64_t total_bytes,
                  const DfaDesc *desc, int n_dfas, int32_t seg_len, uint32_t base_mis,
                  int64_t multi_n, const uint32_t *cta_bins, const uint32_t *bin_base,
-                 const uint32_t *bin_end, const uint32_t *cta_maps, WorkItem *items, int64_t max_items,
-                 uint32_t *str_map, uint32_t *err) {
+                 const uint32_t *bin_end, const uint32_t *cta_maps, const uint32_t *cta_splits, WorkItem *items,
+                 int64_t max_items, uint4 *split_list, uint32_t *err) {
     __shared__ uint32_t s_pos[kMaxDfasPerSet * kLenClasses];
     __shared__ uint32_t s_end[kMaxDfasPerSet * kLenClasses];
-    __shared__ uint32_t s_map, s_map_end;
+    __shared__ uint32_t s_map, s_map_end, s_split, s_split_end;
     const int n_bins = n_dfas * kLenClasses;
     const int G = gridDim.x, c = blockIdx.x;
     if (*(volatile uint32_t *)err & kErrCapacity) return;   // set by plan_scan_kernel: no items
@@ -397,6 +435,8 @@ plan_fill_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n, int64
     if (threadIdx.x == 0) {
         s_map = cta_maps[c];
         s_map_end = cta_maps[c + 1];
+        s_split = cta_splits[c];
+        s_split_end = cta_splits[c + 1];
     }
     __syncthreads();
     bool bad = false;
@@ -433,6 +473,14 @@ plan_fill_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n, int64
             wb = __shfl_sync(0xffffffffu, wb, 31);
             mb = wb + incl - want;
         }
+        uint32_t sp = 0;   // this string's place in the list of split strings
+        {
+            const uint32_t lane = threadIdx.x & 31u;
+            const uint32_t sb = __ballot_sync(0xffffffffu, d >= 0 && k > 1);
+            uint32_t base = 0;
+            if (lane == 0 && sb) base = atomicAdd(&s_split, (uint32_t)__popc(sb));
+            sp = __shfl_sync(0xffffffffu, base, 0) + (uint32_t)__popc(sb & ((1u << lane) - 1u));
+        }
         uint32_t warm = 0, start = 0;
         if (d >= 0) {
             warm = (uint32_t)warm_bytes(desc[d].n_states, g.seg);
@@ -441,60 +489,75 @@ plan_fill_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n, int64
             const bool in = (k <= 1 || (uint64_t)p_first < s_end[ic.first]) &&
                             (k <= 2 || (uint64_t)p_mid + (k - 2) <= s_end[ic.mid]) &&
                             p_last < s_end[ic.last] &&
-                            (k <= 1 || ((uint64_t)mb + k <= s_map_end && (int64_t)mb + k <= max_items));
+                            (k <= 1 || ((uint64_t)mb + k <= s_map_end && (int64_t)mb + k <= max_items &&
+                                        sp < s_split_end));
             if (!in) {
                 bad = true;
                 k = 0;
             }
-            if (k > 1) str_map[i] = mb;
+            if (k > 1)
+                split_list[sp] = make_uint4((uint32_t)i, mb,
+                                            k | ((uint32_t)d << 16) | ((uint32_t)(desc[d].n_states - 1) << 24),
+                                            (uint32_t)desc[d].accept_off);
             start = (uint32_t)desc[d].start;
         } else {
             k = 0;
         }
-        // The warp writes its strings' items together, 32 at a time (a string
-        // of many pieces would otherwise keep its lane busy while the others
-        // idle): item t of the warp belongs to the lane whose inclusive prefix
-        // sum of item counts first exceeds t.
+        // Items 0..3 of a string are written by its lane; the rest of long strings by the
+        // warp together, 32 at a time (a string of many pieces would otherwise keep its
+        // lane busy while the others idle): item t of the warp's rest belongs to the lane
+        // whose inclusive prefix sum of rest counts first exceeds t.
+        auto item_at = [&](const ItemGeom &go, int64_t so, int64_t lo_, uint32_t j, uint32_t pf, uint32_t pm,
+                           uint32_t pl, uint32_t mbo, uint32_t wo, uint32_t sto, uint32_t stro) {
+            const uint32_t pos = (j + 1 == go.k) ? pl : j == 0 ? pf : pm + (j - 1);
+            if ((int64_t)pos >= max_items) {
+                bad = true;
+                return;
+            }
+            int64_t b0, b1;
+            item_range(go, so, lo_, j, &b0, &b1);
+            items[pos] = (j == 0) ? WorkItem{b0, b1, stro, j | (go.k << 16), mbo, sto}
+                                  : WorkItem{b0 - wo, b1, stro, j | (go.k << 16), mbo, wo << 8};
+        };
+        constexpr uint32_t kOwn = 4;
+#pragma unroll
+        for (uint32_t j = 0; j < kOwn; ++j)
+            if (j < k) item_at(g, s0, len, j, p_first, p_mid, p_last, mb, warm, start, (uint32_t)i);
         {
             const uint32_t FULL = 0xffffffffu, lane = threadIdx.x & 31u;
-            uint32_t incl = k;
+            const uint32_t kx = k > kOwn ? k - kOwn : 0u;
+            if (__any_sync(FULL, kx != 0)) {
+                uint32_t incl = kx;
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t v = __shfl_up_sync(FULL, incl, o);
-                if (lane >= (uint32_t)o) incl += v;
-            }
-            const uint32_t total = __shfl_sync(FULL, incl, 31);
-            for (uint32_t t0 = 0; t0 < total; t0 += 32) {
-                const uint32_t t = t0 + lane;
-                uint32_t o = 0;   // lanes whose inclusive count is <= t
-#pragma unroll
-                for (uint32_t step = 16; step >= 1; step >>= 1)
-                    if (__shfl_sync(FULL, incl, o + step - 1) <= t) o += step;
-                const uint32_t ko = __shfl_sync(FULL, k, o), io = __shfl_sync(FULL, incl, o);
-                const int64_t so = __shfl_sync(FULL, s0, o), lo_ = __shfl_sync(FULL, len, o);
-                const ItemGeom go{ko, __shfl_sync(FULL, g.seg, o), __shfl_sync(FULL, g.first, o)};
-                const uint32_t pf = __shfl_sync(FULL, p_first, o), pm = __shfl_sync(FULL, p_mid, o);
-                const uint32_t pl = __shfl_sync(FULL, p_last, o), mbo = __shfl_sync(FULL, mb, o);
-                const uint32_t wo = __shfl_sync(FULL, warm, o), sto = __shfl_sync(FULL, start, o);
-                const uint32_t stro = __shfl_sync(FULL, (uint32_t)i, o);
-                if (t >= total) continue;
-                const uint32_t j = t - (io - ko);   // the item's index in its string
-                const uint32_t pos = (j + 1 == ko) ? pl : j == 0 ? pf : pm + (j - 1);
-                if ((int64_t)pos >= max_items) {
-                    bad = true;
-                    continue;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t v = __shfl_up_sync(FULL, incl, o);
+                    if (lane >= (uint32_t)o) incl += v;
                 }
-                int64_t b0, b1;
-                item_range(go, so, lo_, j, &b0, &b1);
-                items[pos] = (j == 0) ? WorkItem{b0, b1, stro, j | (ko << 16), mbo, sto}
-                                      : WorkItem{b0 - wo, b1, stro, j | (ko << 16), mbo, wo << 8};
+                const uint32_t total = __shfl_sync(FULL, incl, 31);
+                for (uint32_t t0 = 0; t0 < total; t0 += 32) {
+                    const uint32_t t = t0 + lane;
+                    uint32_t o = 0;   // lanes whose inclusive count is <= t
+#pragma unroll
+                    for (uint32_t step = 16; step >= 1; step >>= 1)
+                        if (__shfl_sync(FULL, incl, o + step - 1) <= t) o += step;
+                    const uint32_t ko = __shfl_sync(FULL, k, o), io = __shfl_sync(FULL, incl, o);
+                    const int64_t so = __shfl_sync(FULL, s0, o), lo_ = __shfl_sync(FULL, len, o);
+                    const ItemGeom go{ko, __shfl_sync(FULL, g.seg, o), __shfl_sync(FULL, g.first, o)};
+                    const uint32_t pf = __shfl_sync(FULL, p_first, o), pm = __shfl_sync(FULL, p_mid, o);
+                    const uint32_t pl = __shfl_sync(FULL, p_last, o), mbo = __shfl_sync(FULL, mb, o);
+                    const uint32_t wo = __shfl_sync(FULL, warm, o), sto = __shfl_sync(FULL, start, o);
+                    const uint32_t stro = __shfl_sync(FULL, (uint32_t)i, o);
+                    if (t >= total) continue;
+                    const uint32_t j = kOwn + t - (io - (ko - kOwn));   // the item's index in its string
+                    item_at(go, so, lo_, j, pf, pm, pl, mbo, wo, sto, stro);
+                }
             }
         }
     }
     __syncthreads();
     // every range of this CTA must have been filled exactly
     for (int t = threadIdx.x; t < n_bins; t += blockDim.x) bad |= s_pos[t] != s_end[t];
-    if (threadIdx.x == 0) bad |= s_map != s_map_end;
+    if (threadIdx.x == 0) bad |= s_map != s_map_end || s_split != s_split_end;
     if (bad) atomicOr(err, kErrCapacity);
 }
 
@@ -515,7 +578,9 @@ struct RaggedParams {
     const unsigned long long *q_bytes;
     uint32_t *err;
     uint64_t *maps;
-    const uint32_t *str_map;
+    const uint4 *split_list;     // every split string: string, first map slot, items | automaton << 16
+                                 // | (states - 1) << 24, offset of its accept table
+    const uint32_t *n_split;     // their number
     const int32_t *dfa_id;
     int64_t n;
     int64_t max_items;
@@ -1345,37 +1410,43 @@ __device__ __noinline__ uint32_t fix_item(const RaggedParams &P, const uint8_t *
 // lane of the warp. The first item whose chains never meet (automata that do
 // not synchronise, such as permutations) is walked again whole by the warp, and
 // the check goes on from there, 32 records at a time.
-__global__ void __launch_bounds__(kComposeThreads) compose_kernel(RaggedParams P) {
+__global__ void __launch_bounds__(kComposeThreads, 3) compose_kernel(RaggedParams P) {
     __shared__ __align__(16) uint8_t s_tbl[kComposeThreads / 32][256 * kSmallDfaStates];
-    __shared__ uint32_t s_bad[kComposeThreads / 32][32];   // per string of a warp: first failed fix-up
+    __shared__ uint32_t s_bad[kComposeThreads / 32][32];    // per string of a warp: first failed fix-up
+    __shared__ uint32_t s_last[kComposeThreads / 32][32];   // its final state from a fix-up of its last item
     if (*(volatile uint32_t *)P.err & kErrCapacity) return;   // the plan was refused
     const uint32_t FULL = 0xffffffffu;
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
     s_bad[wib][lane] = 0xFFFFFFFFu;
+    s_last[wib][lane] = 0u;
     __syncwarp();
     uint8_t *tbl = s_tbl[wib];
     int tbl_dfa = -1;
     const int64_t nwarps = (int64_t)gridDim.x * (kComposeThreads / 32);
-    for (int64_t base = ((int64_t)blockIdx.x * (kComposeThreads / 32) + wib) * 32; base < P.n;
+    const int64_t n_split = *P.n_split;   // only split strings need chaining
+    for (int64_t base = ((int64_t)blockIdx.x * (kComposeThreads / 32) + wib) * 32; base < n_split;
          base += nwarps * 32) {
-        const int64_t i = base + lane;
-        int64_t len = 0, s0 = 0;
-        const int d = i < P.n ? checked_dfa(P.offsets, P.dfa_id, i, P.n_dfas, P.total_bytes, P.err,
-                                            &len, &s0, P.multi_n)
-                              : -1;
-        uint32_t k = 0, mb = 0;
-        ItemGeom g{0, 0, 0};
-        if (d >= 0) {
-            g = item_geom(len, s0, P.desc[d].n_states, P.seg_len, P.base_mis);
-            k = g.k;
-            if (k > 1) {
-                mb = P.str_map[i];
-                if ((int64_t)mb + (int64_t)k > P.max_items) {   // offsets changed since the plan
-                    atomicOr(P.err, kErrCapacity);
-                    k = 0;
-                }
-            }
+        uint4 ent = make_uint4(0u, 0u, 0u, 0u);
+        if (base + lane < n_split) ent = P.split_list[base + lane];
+        const int64_t i = (int64_t)ent.x;
+        const int d = (int)((ent.z >> 16) & 0xffu);
+        const uint32_t N = (ent.z >> 24) + 1u, aoff = ent.w, mb = ent.y;
+        uint32_t k = base + lane < n_split ? ent.z & 0xffffu : 0u;
+        if (k > 1 && (int64_t)mb + (int64_t)k > P.max_items) {   // not written by this plan
+            atomicOr(P.err, kErrCapacity);
+            k = 0;
         }
+        // the string's geometry, only where a fix-up or a re-walk needs it
+        int64_t len = 0, s0 = 0;
+        ItemGeom g{0, 0, 0};
+        auto geometry = [&]() {
+            if (checked_dfa(P.offsets, P.dfa_id, i, P.n_dfas, P.total_bytes, P.err, &len, &s0, P.multi_n) == d)
+                g = item_geom(len, s0, (int)N, P.seg_len, P.base_mis);
+            if (g.k != k) {   // offsets changed since the plan
+                atomicOr(P.err, kErrCapacity);
+                g = ItemGeom{0, 0, 0};
+            }
+        };
         // Each lane chains its own string's records, as if every wrong guess were fixed by
         // meeting the recorded chain at a checkpoint (true unless the automaton does not
         // synchronise): the entry of item j is then the recorded end state of item j - 1.
@@ -1404,6 +1475,8 @@ __global__ void __launch_bounds__(kComposeThreads) compose_kernel(RaggedParams P
                     st = (uint32_t)(v[u] >> 8) & 0xffu;
                 }
             }
+            if (tmask && g.k == 0) geometry();
+            if (tmask && g.k == 0) tmask = 0;   // changed offsets: no fix-up (the error bit is set)
             const uint32_t cnt = __popc(tmask);
             uint32_t incl = cnt;
 #pragma unroll
@@ -1430,25 +1503,33 @@ __global__ void __launch_bounds__(kComposeThreads) compose_kernel(RaggedParams P
                 const uint32_t e = (u < 4 ? elo_o >> (8 * u) : ehi_o >> (8 * (u - 4))) & 0xffu;
                 const uint32_t j = j0 + u;
                 const uint64_t rec = P.maps[mbo + j];
-                const uint32_t N = (uint32_t)P.desc[d_o].n_states;
+                const uint32_t No = (uint32_t)P.desc[d_o].n_states;
                 int64_t b0, b1;
                 item_range(go, s0o, leno, j, &b0, &b1);
-                const uint32_t f = e < N ? fix_item(P, P.tmaps + P.desc[d_o].tmap_off, N, b0, b1, e, rec)
-                                         : 0xFFFFu;
-                if (f != ((uint32_t)(rec >> 8) & 0xffu)) atomicMin(&s_bad[wib][ow], (j << 8) | e);
+                const uint32_t f = e < No ? fix_item(P, P.tmaps + P.desc[d_o].tmap_off, No, b0, b1, e, rec)
+                                          : 0xFFFFu;
+                if (f != ((uint32_t)(rec >> 8) & 0xffu)) {
+                    // a last item walked to its end: that is the string's final state (a short
+                    // item can end before the chains meet); otherwise the string is walked again
+                    if (f != 0xFFFFu && j + 1 == go.k) s_last[wib][ow] = 0x100u | f;
+                    else atomicMin(&s_bad[wib][ow], (j << 8) | e);
+                }
             }
             __syncwarp();
-            const uint32_t bad = s_bad[wib][lane];
+            const uint32_t bad = s_bad[wib][lane], last = s_last[wib][lane];
             if (act && bad != 0xFFFFFFFFu) {   // the walk goes on from item bad >> 8
                 help = true;
                 jbad = bad >> 8;
                 st = bad & 0xffu;
+            } else if (act && last) {
+                st = last & 0xffu;
             }
             s_bad[wib][lane] = 0xFFFFFFFFu;
+            s_last[wib][lane] = 0u;
             __syncwarp();
         }
         if (k > 1 && !help) {
-            if (st < (uint32_t)P.desc[d].n_states) write_result(P, (uint32_t)i, st, P.desc[d].accept_off);
+            if (st < N) write_result(P, (uint32_t)i, st, aoff);
             else atomicOr(P.err, kErrCapacity);   // records not written by this plan
         }
         // strings with a wrong guess: the warp re-walks that item and goes on checking
@@ -1584,11 +1665,12 @@ static int dfa_set_run_ex(trex_dfa_set *set, const uint8_t *data, const int64_t 
     auto *n_items = reinterpret_cast<unsigned long long *>(sc + L.n_items);
     WorkItem *items = reinterpret_cast<WorkItem *>(sc + L.items);
     uint64_t *maps = reinterpret_cast<uint64_t *>(sc + L.maps);
-    uint32_t *str_map = reinterpret_cast<uint32_t *>(sc + L.str_map);
+    uint4 *split_list = reinterpret_cast<uint4 *>(sc + L.split_list);
     uint32_t *cta_bins = reinterpret_cast<uint32_t *>(sc + L.cta_bins);
     uint32_t *bin_base = reinterpret_cast<uint32_t *>(sc + L.bin_base);
     uint32_t *bin_end = reinterpret_cast<uint32_t *>(sc + L.bin_end);
     uint32_t *cta_maps = reinterpret_cast<uint32_t *>(sc + L.cta_maps);
+    uint32_t *cta_splits = reinterpret_cast<uint32_t *>(sc + L.cta_splits);
     const uint32_t base_mis = (uint32_t)((uintptr_t)data & 31u);
 
     // Queue bases, counts and heads, byte counts, the error word and the item
@@ -1598,15 +1680,22 @@ static int dfa_set_run_ex(trex_dfa_set *set, const uint8_t *data, const int64_t 
                                                   (int64_t)set->n_sms, (int64_t)kMaxPlanCtas});
     plan_count_kernel<<<plan_grid, kPlanThreads, 0, stream>>>(
         offsets, dfa_id, n, total_bytes, set->d_desc, set->n_dfas, seg_len, base_mis, multi_n,
-        cta_bins, cta_maps, n_items, err);
+        cta_bins, cta_maps, cta_splits, n_items, err);
     TREX_CHECK_LAUNCH();
-    plan_scan_kernel<<<1, kPlanThreads, 0, stream>>>(cta_bins, bin_base, bin_end, cta_maps, plan_grid,
+    {
+        const int n_bins = set->n_dfas * kLenClasses;
+        const int prefix_grid = (n_bins * kPrefixParts + kPrefixThreads - 1) / kPrefixThreads;
+        plan_prefix_kernel<<<prefix_grid, kPrefixThreads, 0, stream>>>(cta_bins, bin_end, plan_grid, n_bins);
+        TREX_CHECK_LAUNCH();
+    }
+    plan_scan_kernel<<<1, kPlanThreads, 0, stream>>>(cta_bins, bin_base, bin_end, cta_maps, cta_splits,
+                                                     plan_grid,
                                                      set->n_dfas, q_base, q_count, q_bytes, n_items,
                                                      L.max_items, err);
     TREX_CHECK_LAUNCH();
     plan_fill_kernel<<<plan_grid, kPlanThreads, 0, stream>>>(
         offsets, dfa_id, n, total_bytes, set->d_desc, set->n_dfas, seg_len, base_mis, multi_n,
-        cta_bins, bin_base, bin_end, cta_maps, items, L.max_items, str_map, err);
+        cta_bins, bin_base, bin_end, cta_maps, cta_splits, items, L.max_items, split_list, err);
     TREX_CHECK_LAUNCH();
 
     RaggedParams P;
@@ -1625,7 +1714,8 @@ static int dfa_set_run_ex(trex_dfa_set *set, const uint8_t *data, const int64_t 
     P.q_bytes = q_bytes;
     P.err = err;
     P.maps = maps;
-    P.str_map = str_map;
+    P.split_list = split_list;
+    P.n_split = cta_splits + plan_grid;
     P.dfa_id = dfa_id;
     P.n = n;
     P.max_items = L.max_items;
@@ -1645,8 +1735,9 @@ static int dfa_set_run_ex(trex_dfa_set *set, const uint8_t *data, const int64_t 
     dfa_ragged_kernel<<<ragged_grid, kRaggedThreads, set->smem_bytes, stream>>>(P);
     TREX_CHECK_LAUNCH();
     profile_kernel_end(stream);
+    // resident CTAs (three an SM) loop over the list of split strings
     compose_kernel<<<(int)std::min<int64_t>((n + kComposeThreads - 1) / kComposeThreads,
-                                            (int64_t)set->n_sms * 8),
+                                            (int64_t)set->n_sms * 3),
                      kComposeThreads, 0, stream>>>(P);
     TREX_CHECK_LAUNCH();
     if (err_word_out) *err_word_out = err;

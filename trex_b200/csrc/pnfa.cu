@@ -208,6 +208,8 @@ struct PnParams {
     int boolean;               // Boolean NFA: threshold every product to {0, 1}, no rescale
     int kcols;                 // 16-byte core-matrix columns of a B row: 8 (16-bit), 4 (int8)
     long long wait_cycles;     // limit of one hand-off wait
+    int resc;                  // steps between rescales (power-of-two scaling is exact, so only
+                               // the range matters: 4 for BF16 with growth <= 16 a step, else 1)
     double ll_empty;
     int sigma;
     double *loglik;
@@ -837,6 +839,8 @@ __device__ void pn_epilogue(const PnParams &P, const PnShared &S, uint32_t tbase
         const PnChunk *ch = S.chunks(t);
         const uint2 *rec = S.rec(t);
         const float2 *xm = S.xmax(t);
+        // a rescale step scales by the maxima that the step before it found
+        const bool scale_step = t % P.resc == 0, max_step = (t + 1) % P.resc == 0;
         float *xn = reinterpret_cast<float *>(S.xmax(t + 1)) + (q & 1);
         float *fin = reinterpret_cast<float *>(S.fin(t)) + (q & 1);
         int32_t *finE = S.finE(t);
@@ -868,6 +872,15 @@ __device__ void pn_epilogue(const PnParams &P, const PnShared &S, uint32_t tbase
                         // Boolean forms: no scaling, the exponent sum stays 0
                         const uint2 rcl = rec[d.row0 + col];
                         if (owner && (rcl.x & kRecFinish)) finE[rcl.y & 1023u] = 0;
+                    } else if (lane < 16 && col >= c_lo && col < c_hi && !scale_step) {
+                        // no rescale this step: a string that begins starts its exponent sum
+                        const uint2 rcl = rec[d.row0 + col];
+                        const int jl = (int)(rcl.y & 1023u);
+                        if (owner) {
+                            const int e = (rcl.y & kRecFresh) ? 0 : E[jl];
+                            if (rcl.y & kRecFresh) E[jl] = 0;
+                            if (rcl.x & kRecFinish) finE[jl] = e;
+                        }
                     } else if (lane < 16 && col >= c_lo && col < c_hi) {
                         const int row = d.row0 + col;
                         const uint2 rcl = rec[row];
@@ -943,8 +956,8 @@ __device__ void pn_epilogue(const PnParams &P, const PnShared &S, uint32_t tbase
                                 : 0.f;
                 }
                 // column maxima over this warp's 32 states: the 8 threads with the same cp
-                // (they set the next step's scale; the Boolean forms do not scale)
-                if (!bmode) {
+                // (they set the next rescale step's scale; the Boolean forms do not scale)
+                if (!bmode && max_step) {
 #pragma unroll
                     for (int o = 4; o < 32; o <<= 1)
 #pragma unroll
@@ -1321,6 +1334,7 @@ struct trex_pnfa {
     // when the tables' growth bound allows (max |T s| / max |s| <= 16 a step, so five
     // unchecked steps stay far inside FP32), else every step
     int chain_resc[2] = {1, 1};
+    int tc_resc = 1;   // the tensor-core kernel's rescale period for BF16 operands (same bound)
 };
 
 namespace trex {
@@ -1458,6 +1472,7 @@ int trex_pnfa_create(int n_states, int sigma, const float *T, const float *start
             float rmax = 0.f;
             for (int c = 0; c < sigma; ++c) rmax = std::max(rmax, rs[k][c]);
             h->chain_resc[k] = rmax <= 16.f ? 4 : 1;
+            if (k == 0) h->tc_resc = h->chain_resc[0];
         }
     }
     {   // int8 Boolean tables: the same A rows as above with 0/1 bytes, four K values a word
@@ -1610,6 +1625,7 @@ int trex_pnfa_run(trex_pnfa *h, int mode, const uint8_t *data, const int64_t *of
     P.boolean = k >= 2;
     P.kcols = k == 3 ? 4 : 8;
     P.wait_cycles = mbar_wait_cycles();
+    P.resc = k == 0 ? h->tc_resc : 1;
     P.sigma = h->sigma;
     P.loglik = loglik;
     P.accept = accept;

@@ -9,24 +9,21 @@
 // every string.
 //
 // Design (N <= 16; the per-lane replicated table of dfa_walk.cuh)
-//  * Strings are cut into tiles of tile_len bytes; a warp takes two chunks of
-//    32 consecutive tiles with one atomic, lane l tiles l and 32 + l.
+//  * Strings are cut into tiles of tile_len bytes; a warp takes 32
+//    consecutive tiles (a chunk) with one atomic.
 //  * Sync: every lane walks all 16 states of its tile together (16
 //    independent chains) until they coincide, at the same byte offset S for
 //    the whole warp. From there the tile's states no longer depend on its
 //    entry state: its map is constant. A tile that starts a string begins in
 //    the start state and needs no sync.
-//  * Body: each lane walks bytes [tile + S, tile end) of its two tiles as two
-//    interleaved chains (two table lookups in flight; one chain a thread is
-//    bound by the latency of its dependent lookups) and writes every state
-//    (16-byte stores of packed states).
+//  * Body: each lane walks bytes [tile + S, tile end) with one chain and
+//    writes every state (16-byte stores of packed states).
 //  * Entry states: inside the warp, the entry of tile i is the exit of tile
 //    i-1 (a shuffle scan over tile maps handles the general case). Across
 //    warps, chunk c publishes its composed map (AGGREGATE) as soon as its body
 //    is walked and its exit state (PREFIX) once its entry is known; chunk c
 //    looks back over c-1, c-2, ... composing aggregates until it meets a
-//    prefix (or a constant map). A warp publishes both its chunks' aggregates
-//    before it looks back, and its second chunk's entry is its first one's exit. Every poll is bounded; a wait that runs out
+//    prefix (or a constant map). Every poll is bounded; a wait that runs out
 //    sets the error word and the chunk gives up.
 //  * Head: with the entry state known, each lane walks bytes [tile,
 //    tile + S) again from it and writes those states.
@@ -47,11 +44,11 @@ enum : uint32_t { kStAgg = 1u, kStPrefix = 2u };
 enum : uint32_t { kScanErrOffsets = 1u, kScanErrTimeout = 4u, kScanErrCapacity = 8u };
 
 // Tile length: the requested one (>= 64), or by default the length that gives
-// every resident warp one pair of 32-tile chunks (1 KiB multiples, 1 KiB .. 64 KiB).
+// every resident warp one 32-tile chunk (1 KiB multiples, 1 KiB .. 64 KiB).
 static int32_t scan_tile_len(int32_t tile_len, int64_t total_bytes, int n_sms) {
     if (tile_len > 0) return tile_len < 64 ? 64 : tile_len;
     const int64_t warps = (int64_t)(n_sms > 0 ? n_sms : 148) * (kScanThreads / 32);
-    int64_t t = total_bytes / (warps * 64);
+    int64_t t = total_bytes / (warps * 32);
     t = ((t + 1023) / 1024) * 1024;
     return (int32_t)std::min<int64_t>(65536, std::max<int64_t>(1024, t));
 }
@@ -262,77 +259,6 @@ __device__ uint32_t walk_write(const W &w, const ScanParams &P, int64_t p, int64
     return e;
 }
 
-// Two chains over 16-byte vectors: the bytes of va and vb are applied to xa and
-// xb alternately (two table lookups in flight), returns both 16 decoded states.
-template <class W>
-__device__ __forceinline__ void walk16_states2(const W &w, uint32_t &xa, uint4 va, uint4 &oa, uint32_t &xb,
-                                               uint4 vb, uint4 &ob) {
-    const uint32_t ya[4] = {va.x, va.y, va.z, va.w}, yb[4] = {vb.x, vb.y, vb.z, vb.w};
-    uint32_t ra[4], rb[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const uint32_t a0 = w.template step<0>(xa, ya[k]), b0 = w.template step<0>(xb, yb[k]);
-        const uint32_t a1 = w.template step<1>(a0, ya[k]), b1 = w.template step<1>(b0, yb[k]);
-        const uint32_t a2 = w.template step<2>(a1, ya[k]), b2 = w.template step<2>(b1, yb[k]);
-        const uint32_t a3 = w.template step<3>(a2, ya[k]), b3 = w.template step<3>(b2, yb[k]);
-        xa = a3;
-        xb = b3;
-        ra[k] = dec4<W>(a0 | (a1 << 8) | (a2 << 16) | (a3 << 24));
-        rb[k] = dec4<W>(b0 | (b1 << 8) | (b2 << 16) | (b3 << 24));
-    }
-    oa = make_uint4(ra[0], ra[1], ra[2], ra[3]);
-    ob = make_uint4(rb[0], rb[1], rb[2], rb[3]);
-}
-
-// Walks bytes [pa, ea) from xa and [pb, eb) from xb and writes every state: each
-// start is first brought to a 32-byte boundary alone, then 32 bytes of each per
-// step as two interleaved chains (the next 32 bytes of each in flight), then the
-// rests alone.
-template <class W>
-__device__ void walk_write2(const W &w, const ScanParams &P, int64_t pa, int64_t ea, uint32_t &xa,
-                            int64_t pb, int64_t eb, uint32_t &xb) {
-    const int64_t ha = min(ea, pa + (int64_t)((32u - ((uint32_t)(uintptr_t)(P.data + pa) & 31u)) & 31u));
-    const int64_t hb = min(eb, pb + (int64_t)((32u - ((uint32_t)(uintptr_t)(P.data + pb) & 31u)) & 31u));
-    xa = walk_write(w, P, pa, ha, xa);
-    xb = walk_write(w, P, pb, hb, xb);
-    pa = ha;
-    pb = hb;
-    const int64_t n = min(ea - pa, eb - pb) & ~(int64_t)31;
-    const bool aligned = ((((uintptr_t)(P.data + pa)) | ((uintptr_t)(P.data + pb))) & 31u) == 0 &&
-                         ((((uintptr_t)(P.out + pa)) | ((uintptr_t)(P.out + pb))) & 15u) == 0;
-    if (aligned && n >= 32) {
-        uint4 a0, a1, b0, b1;
-        ld_stream32(P.data + pa, a0, a1);
-        ld_stream32(P.data + pb, b0, b1);
-        for (int64_t q = 0; q < n; q += 32) {
-            uint4 na0 = make_uint4(0, 0, 0, 0), na1 = na0, nb0 = na0, nb1 = na0;
-            if (q + 32 < n) {
-                ld_stream32(P.data + pa + q + 32, na0, na1);
-                ld_stream32(P.data + pb + q + 32, nb0, nb1);
-                if (((q + 32) & 255) == 0 && q + 512 < n) {
-                    prefetch_l2(P.data + pa + q + 288);
-                    prefetch_l2(P.data + pb + q + 288);
-                }
-            }
-            uint4 sa, sb;
-            walk16_states2(w, xa, a0, sa, xb, b0, sb);
-            st_stream16(P.out + pa + q, sa);
-            st_stream16(P.out + pb + q, sb);
-            walk16_states2(w, xa, a1, sa, xb, b1, sb);
-            st_stream16(P.out + pa + q + 16, sa);
-            st_stream16(P.out + pb + q + 16, sb);
-            a0 = na0;
-            a1 = na1;
-            b0 = nb0;
-            b1 = nb1;
-        }
-        pa += n;
-        pb += n;
-    }
-    xa = walk_write(w, P, pa, ea, xa);
-    xb = walk_write(w, P, pb, eb, xb);
-}
-
 // Tile geometry: string, first byte, end, whether it starts / ends the string.
 struct TileInfo {
     int64_t str, b0, b1;
@@ -358,22 +284,15 @@ __device__ __forceinline__ TileInfo locate_tile(const ScanParams &P, int64_t t) 
     return ti;
 }
 
-// A tile after its sync: the byte S (the same for the warp) from which its map
-// is constant (conv), the encoded state there; for a tile whose states never
-// coincided (not conv) its full map, walked with all 16 chains.
-struct TileSync {
-    int64_t S;
-    bool conv;
-    uint32_t e;
-    uint64_t map;
-};
-
-// Sync of one tile a lane: every lane walks all 16 states of its tile together
-// (16 independent chains) until they coincide, at the same byte S for the whole
-// warp. A tile that starts a string begins in the start state and needs none.
 template <class W>
-__device__ TileSync tile_sync(const ScanParams &P, const W &w, const TileInfo &ti, bool have) {
+__device__ void scan_chunk(const ScanParams &P, const W &w, int64_t chunk, int64_t n_tiles) {
     const uint32_t FULL = 0xffffffffu;
+    const uint32_t lane = threadIdx.x & 31u;
+    const int64_t t = chunk * 32 + lane;
+    const bool have = t < n_tiles;
+    TileInfo ti{0, 0, 0, true, false};
+    if (have) ti = locate_tile(P, t);
+    // ---- sync: 16 chains until they coincide (same S for the whole warp)
     uint32_t ch[16];
 #pragma unroll
     for (int j = 0; j < 16; ++j)
@@ -397,172 +316,105 @@ __device__ TileSync tile_sync(const ScanParams &P, const W &w, const TileInfo &t
         for (int j = 1; j < 16; ++j) conv &= (ch[j] == ch[0]);
     }
     if (S > len) S = len;
-    TileSync r{S, conv, ch[0], kMapIdentity};
-    if (have && !conv) {
-        // does not synchronise: carry all 16 chains over the tile
-        for (int64_t p = ti.b0 + S; p < ti.b1; ++p) {
-            const uint32_t c = __ldg(P.data + p);
-#pragma unroll
-            for (int j = 0; j < 16; ++j) ch[j] = w.template step<0>(ch[j], c);
-        }
-        uint64_t map = 0;
-#pragma unroll
-        for (int j = 0; j < 16; ++j) map |= (uint64_t)W::dec(ch[j]) << (4 * j);
-        r.map = ti.first ? map_const(map_at(map, (uint32_t)P.start)) : map;
-    }
-    return r;
-}
-
-// Entry state of chunk c (lane 0): composes the aggregates of chunks c-1, c-2,
-// ... until one has published its exit state (PREFIX) or the composition is a
-// constant map. Every poll is bounded; a wait that runs out sets the error word
-// and the chunk gives up (entry: the start state).
-__device__ uint32_t look_back(const ScanParams &P, int64_t chunk) {
-    uint64_t acc = kMapIdentity;   // maps of chunks (j, chunk) applied in order
-    for (int64_t j = chunk - 1; j >= 0; --j) {
-        uint32_t st = 0, polls = 0;
-        while (((st = ld_acquire_u32(P.chunk_status + j)) & 3u) == 0u) {
-            if (++polls >= P.poll_limit) break;
-            __nanosleep(64);
-        }
-        if ((st & 3u) == 0u) {
-            atomicOr(P.err, kScanErrTimeout);
-            break;
-        }
-        if (st & kStPrefix) return map_at(acc, (st >> 8) & 15u);
-        acc = map_then(ld_relaxed_u64(P.chunk_map + j), acc);
-        if (map_is_const(acc)) return (uint32_t)acc & 15u;
-    }
-    return (uint32_t)P.start;
-}
-
-// Head of a tile from its true entry state (or the whole tile when its states
-// never coincided), and its string's final state and accept flag.
-template <class W>
-__device__ __forceinline__ void tile_head(const ScanParams &P, const W &w, const TileInfo &ti,
-                                          const TileSync &ts, uint32_t e_body, uint32_t entry) {
-    uint32_t fin;
-    if (ts.conv) {
-        walk_write(w, P, ti.b0, ti.b0 + ts.S, w.enc(entry));
-        fin = W::dec(e_body);   // body exit (independent of the entry)
-    } else {
-        fin = W::dec(walk_write(w, P, ti.b0, ti.b1, w.enc(entry)));
-    }
-    if (ti.last) {
-        if (P.final_state) P.final_state[ti.str] = (uint8_t)fin;
-        if (P.accept) P.accept[ti.str] = P.accept_tbl[fin];
-    }
-}
-
-// Dynamic shared memory of the scan kernel: the table (kRepTableBytes16), then
-// each thread's sync records of its two tiles (16 bytes each), kept there across
-// the body walk so that the walk has the registers.
-struct SyncRec {
-    int32_t S;
-    uint32_t conv_e;   // bit 8: converged; bits 0-7: encoded state at S
-    uint64_t map;      // full map of a tile whose states never coincided
-};
-constexpr uint32_t kScanSyncOff = kRepTableBytes16;
-constexpr uint32_t kScanSmemBytes = kScanSyncOff + 2 * kScanThreads * (uint32_t)sizeof(SyncRec);
-__device__ __forceinline__ SyncRec *sync_rec(int which) {
-    return reinterpret_cast<SyncRec *>(g_dfa_tbl + kScanSyncOff) + which * kScanThreads + threadIdx.x;
-}
-
-// A pair of chunks (64 consecutive tiles) with one warp: lane l takes tiles l
-// (chunk 2p) and 32 + l (chunk 2p + 1). Both tiles are synced, then both bodies
-// are walked as two interleaved chains (two table lookups in flight); the
-// aggregates of both chunks are published before the look-back (so every
-// chunk's aggregate appears without waiting on anything: the look-back cannot
-// deadlock), the second chunk's entry is the first one's exit.
-template <class W>
-__device__ void scan_pair(const ScanParams &P, const W &w, int64_t pair, int64_t n_tiles) {
-    const uint32_t FULL = 0xffffffffu;
-    const uint32_t lane = threadIdx.x & 31u;
-    const int64_t ca = 2 * pair, cb = ca + 1;
-    const int64_t ta_i = ca * 32 + lane, tb_i = cb * 32 + lane;
-    const bool have_a = ta_i < n_tiles, have_b = tb_i < n_tiles;
-    const TileInfo none{0, 0, 0, true, false};
-#pragma unroll 1
-    for (int k = 0; k < 2; ++k) {   // sync of both tiles (every lane: the warp votes inside)
-        const bool have = k == 0 ? have_a : have_b;
-        const TileInfo ti = have ? locate_tile(P, k == 0 ? ta_i : tb_i) : none;
-        const TileSync r = tile_sync(P, w, ti, have);
-        *sync_rec(k) = SyncRec{(int32_t)r.S, (r.conv ? 0x100u : 0u) | (r.e & 0xffu), r.map};
-    }
-    // ---- bodies
-    const SyncRec ra = *sync_rec(0), rb = *sync_rec(1);
-    const bool body_a = have_a && (ra.conv_e & 0x100u), body_b = have_b && (rb.conv_e & 0x100u);
-    uint32_t ea = ra.conv_e & 0xffu, eb = rb.conv_e & 0xffu;
-    {
-        const TileInfo ta = have_a ? locate_tile(P, ta_i) : none;
-        const TileInfo tb = have_b ? locate_tile(P, tb_i) : none;
-        if (body_a && body_b) {
-            walk_write2(w, P, ta.b0 + ra.S, ta.b1, ea, tb.b0 + rb.S, tb.b1, eb);
+    // ---- body (converged) or full map (not converged)
+    uint64_t map = kMapIdentity;
+    uint32_t e = ch[0];
+    if (have) {
+        if (conv) {
+            e = walk_write(w, P, ti.b0 + S, ti.b1, e);
+            map = map_const(W::dec(e));
         } else {
-            if (body_a) ea = walk_write(w, P, ta.b0 + ra.S, ta.b1, ea);
-            if (body_b) eb = walk_write(w, P, tb.b0 + rb.S, tb.b1, eb);
+            // does not synchronise: carry all 16 chains over the tile
+            for (int64_t p = ti.b0 + S; p < ti.b1; ++p) {
+                const uint32_t c = __ldg(P.data + p);
+#pragma unroll
+                for (int j = 0; j < 16; ++j) ch[j] = w.template step<0>(ch[j], c);
+            }
+            map = 0;
+#pragma unroll
+            for (int j = 0; j < 16; ++j) map |= (uint64_t)W::dec(ch[j]) << (4 * j);
+            if (ti.first) map = map_const(map_at(map, (uint32_t)P.start));
         }
     }
-    const uint64_t map_a = body_a ? map_const(W::dec(ea)) : sync_rec(0)->map;
-    const uint64_t map_b = body_b ? map_const(W::dec(eb)) : sync_rec(1)->map;
-    // ---- chunk aggregates: compositions of the 32 tile maps, published at once
-    uint64_t inc_a = map_a, inc_b = map_b;   // inclusive scans: maps of lanes 0..lane in order
+    // ---- chunk aggregate: composition of the 32 tile maps, published at once
+    uint64_t incl = map;   // inclusive scan: maps of lanes 0..lane applied in order
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-        const uint64_t pa = __shfl_up_sync(FULL, inc_a, o), pb = __shfl_up_sync(FULL, inc_b, o);
-        if (lane >= (uint32_t)o) {
-            inc_a = map_then(pa, inc_a);
-            inc_b = map_then(pb, inc_b);
+        const uint64_t prev = __shfl_up_sync(FULL, incl, o);
+        if (lane >= (uint32_t)o) incl = map_then(prev, incl);
+    }
+    const uint64_t agg = __shfl_sync(FULL, incl, 31);
+    if (lane == 0) {
+        P.chunk_map[chunk] = agg;
+        __threadfence();
+        st_release_u32(P.chunk_status + chunk, kStAgg);
+    }
+    // ---- look-back for the chunk's entry state (lane 0)
+    uint32_t entry0 = (uint32_t)P.start;
+    if (lane == 0) {
+        uint64_t acc = kMapIdentity;   // maps of chunks (j, chunk) applied in order
+        bool found = false;
+        for (int64_t j = chunk - 1; j >= 0 && !found; --j) {
+            uint32_t st = 0;
+            uint32_t polls = 0;
+            while (((st = ld_acquire_u32(P.chunk_status + j)) & 3u) == 0u) {
+                if (++polls >= P.poll_limit) break;
+                __nanosleep(64);
+            }
+            if ((st & 3u) == 0u) {
+                atomicOr(P.err, kScanErrTimeout);
+                break;
+            }
+            if (st & kStPrefix) {
+                entry0 = map_at(acc, (st >> 8) & 15u);
+                found = true;
+            } else {
+                acc = map_then(ld_relaxed_u64(P.chunk_map + j), acc);
+                if (map_is_const(acc)) {
+                    entry0 = (uint32_t)acc & 15u;
+                    found = true;
+                }
+            }
         }
     }
-    const uint64_t agg_a = __shfl_sync(FULL, inc_a, 31), agg_b = __shfl_sync(FULL, inc_b, 31);
-    if (lane == 0) {
-        P.chunk_map[ca] = agg_a;
-        P.chunk_map[cb] = agg_b;
-        __threadfence();
-        st_release_u32(P.chunk_status + ca, kStAgg);
-        st_release_u32(P.chunk_status + cb, kStAgg);
-    }
-    // ---- look-back for the first chunk's entry state (lane 0); the second follows it
-    uint32_t entry_a = 0;
-    if (lane == 0) entry_a = look_back(P, ca);
-    entry_a = __shfl_sync(FULL, entry_a, 0);
-    const uint32_t entry_b = map_at(agg_a, entry_a);
-    if (lane == 0) {
-        st_release_u32(P.chunk_status + ca, kStPrefix | (entry_b << 8));
-        st_release_u32(P.chunk_status + cb, kStPrefix | (map_at(agg_b, entry_b) << 8));
-    }
-    // ---- heads from the true entry states: tile `lane` starts in (maps of lanes 0..lane-1)(entry)
-    const uint64_t exc_a = __shfl_up_sync(FULL, inc_a, 1), exc_b = __shfl_up_sync(FULL, inc_b, 1);
-    if (have_a) {
-        const TileInfo ta = locate_tile(P, ta_i);
-        const SyncRec r = *sync_rec(0);
-        const TileSync ts{r.S, (r.conv_e & 0x100u) != 0, r.conv_e & 0xffu, r.map};
-        tile_head(P, w, ta, ts, ea, ta.first ? (uint32_t)P.start : (lane == 0 ? entry_a : map_at(exc_a, entry_a)));
-    }
-    if (have_b) {
-        const TileInfo tb = locate_tile(P, tb_i);
-        const SyncRec r = *sync_rec(1);
-        const TileSync ts{r.S, (r.conv_e & 0x100u) != 0, r.conv_e & 0xffu, r.map};
-        tile_head(P, w, tb, ts, eb, tb.first ? (uint32_t)P.start : (lane == 0 ? entry_b : map_at(exc_b, entry_b)));
+    entry0 = __shfl_sync(FULL, entry0, 0);
+    // entry of tile `lane` = (maps of lanes 0..lane-1)(entry0)
+    const uint64_t excl = __shfl_up_sync(FULL, incl, 1);
+    const uint32_t entry = ti.first ? (uint32_t)P.start : (lane == 0 ? entry0 : map_at(excl, entry0));
+    // ---- publish the chunk's exit state
+    const uint32_t chunk_exit = map_at(agg, entry0);
+    if (lane == 0) st_release_u32(P.chunk_status + chunk, kStPrefix | (chunk_exit << 8));
+    // ---- head (or whole tile when the states never coincided) from the true entry
+    if (have) {
+        uint32_t fin;
+        if (conv) {
+            walk_write(w, P, ti.b0, ti.b0 + S, w.enc(entry));
+            fin = W::dec(e);   // body exit (independent of the entry)
+        } else {
+            fin = W::dec(walk_write(w, P, ti.b0, ti.b1, w.enc(entry)));
+        }
+        if (ti.last) {
+            if (P.final_state) P.final_state[ti.str] = (uint8_t)fin;
+            if (P.accept) P.accept[ti.str] = P.accept_tbl[fin];
+        }
     }
 }
 
 __global__ void __launch_bounds__(kScanThreads, 1) dfa_scan_kernel(ScanParams P) {
-    __shared__ unsigned long long s_pair[kScanThreads / 32];
+    __shared__ unsigned long long s_chunk[kScanThreads / 32];
     build_table(P.tmap, P.n_states);
     __syncthreads();
     const int64_t n_tiles = P.tile_base[P.n_strings];
-    const int64_t n_pairs = (n_tiles + 63) / 64;
+    const int64_t n_chunks = (n_tiles + 31) / 32;
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     while (true) {
-        if (lane == 0) s_pair[warp] = atomicAdd(P.head, 1ull);
+        if (lane == 0) s_chunk[warp] = atomicAdd(P.head, 1ull);
         __syncwarp();
-        const int64_t pair = (int64_t)s_pair[warp];
+        const int64_t chunk = (int64_t)s_chunk[warp];
         __syncwarp();
-        if (pair >= n_pairs) break;
-        if (P.n_states <= 8) scan_pair(P, Walker<8>{lane}, pair, n_tiles);
-        else scan_pair(P, Walker<16>{lane}, pair, n_tiles);
+        if (chunk >= n_chunks) break;
+        if (P.n_states <= 8) scan_chunk(P, Walker<8>{lane}, chunk, n_tiles);
+        else scan_chunk(P, Walker<16>{lane}, chunk, n_tiles);
     }
 }
 
@@ -636,11 +488,11 @@ int trex_dfa_scan_run(trex_dfa_set *set, int dfa_index, const uint8_t *data,
     static bool attr_set = false;
     if (!attr_set) {
         TREX_CUDA(cudaFuncSetAttribute(dfa_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       kScanSmemBytes));
+                                       kRepTableBytes16));
         attr_set = true;
     }
     profile_kernel_begin(stream);
-    dfa_scan_kernel<<<n_sms, kScanThreads, kScanSmemBytes, stream>>>(P);
+    dfa_scan_kernel<<<n_sms, kScanThreads, kRepTableBytes16, stream>>>(P);
     TREX_CHECK_LAUNCH();
     profile_kernel_end(stream);
     return TREX_OK;
