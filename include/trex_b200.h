@@ -207,7 +207,7 @@ int trex_dfa_batch_error(trex_dfa_set *set, void *scratch, int32_t *err_out);
  * scratch is a file-scope device array of 8 MiB (every GPU that loads the
  * library holds it until the process exits), so a batch whose
  * trex_dfa_batch_scratch_bytes is above 8 MiB is refused with
- * TREX_ERR_CAPACITY (about 70K strings of 2 KiB at the default segment length;
+ * TREX_ERR_CAPACITY (about 58K strings of 2 KiB at the default segment length;
  * the scratch grows with strings + total_bytes / seg_len work items). The
  * caller still passes inputs and outputs, and calls it with the set's device
  * current (else TREX_ERR_ARG). The first call on each device (and again after

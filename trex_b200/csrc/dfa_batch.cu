@@ -17,9 +17,11 @@
 //    the previous item, from state 0; for a synchronising DFA (random DFAs
 //    merge two chains with probability ~1/N per byte) the chain has then
 //    reached the true entry state. The item records that guess next to its
-//    end state; compose_kernel chains each string's records and re-walks, with
-//    a whole warp, any item whose guess was wrong. Results are exact for every
-//    DFA; only non-synchronising DFAs pay for re-walks.
+//    end state; three small kernels chain each string's records (a thread per
+//    string), walk each item whose guess was wrong from its true entry state
+//    until it meets the recorded chain at a checkpoint (a thread per item), and
+//    walk again, with a whole warp, the items whose chains never meet. Results
+//    are exact for every DFA; only non-synchronising DFAs pay for re-walks.
 //  * Main kernel: one persistent 1024-thread CTA per SM. The CTA expands the
 //    current DFA's byte map (or its K-gram tables) into a per-lane replicated
 //    shared-memory table (dfa_walk.cuh) so table lookups never conflict on
@@ -58,7 +60,7 @@ constexpr int64_t kMaxWalkBytes = (int64_t)1 << 36;   // one item: a 32-bit coun
 // ~1/N per byte, so the warm-up chain has missed the true entry state with
 // probability (1 - 1/N)^W: 1.4% for N = 8 (W = 32), 0.4% for N = 12 and 1.6%
 // for N = 16 (W = 64). When it has, the item's checkpoints (its chain's state
-// 1, 2, 4 and 8 windows into its own bytes) let compose_kernel walk from the
+// 1, 2, 4 and 8 windows into its own bytes) let compose_fix_kernel walk from the
 // true entry state only until the two chains meet (about one window).
 __host__ __device__ __forceinline__ int64_t warm_bytes(int n_states, int64_t seg) {
     const int64_t w = n_states <= 8 ? 32 : 64;
@@ -80,9 +82,9 @@ constexpr int kLenClasses = 64;
 
 // ---- scratch layout -----------------------------------------------------------
 struct ScratchLayout {
-    size_t q_base, q_count, q_head, q_bytes, err, n_items, items, maps, split_list, cta_bins, bin_base,
-        bin_end, cta_maps, cta_splits, total;
-    int64_t max_items;
+    size_t q_base, q_count, q_head, q_bytes, err, n_items, n_fix, n_rw, items, maps, split_list, fix_list,
+        rw_list, cta_bins, bin_base, bin_end, cta_maps, cta_splits, total;
+    int64_t max_items, fix_cap;
 };
 
 // Bytes per work item: at least 64, a multiple of 32 (item cuts fall on window
@@ -106,11 +108,19 @@ static ScratchLayout scratch_layout(int64_t n_strings, int64_t total_bytes, int3
     L.q_bytes = take(kMaxDfasPerSet * 8);
     L.err = take(4);
     L.n_items = take(8);
+    L.n_fix = take(4);
+    L.n_rw = take(4);
     L.items = take((size_t)L.max_items * sizeof(WorkItem));
     L.maps = take((size_t)L.max_items * sizeof(uint64_t));
     // every string cut into several items: string, first map slot, items | automaton << 16 |
     // (states - 1) << 24, offset of its accept table
     L.split_list = take((size_t)std::max<int64_t>(n_strings, 1) * 16);
+    // chaining the records: fix-up tasks (string, item << 8 | entry state), about 1% of the
+    // items of split strings for the random automata of the benchmarks; a string whose task
+    // finds the list full is walked again instead. Then the strings to walk again.
+    L.fix_cap = std::max<int64_t>(1024, L.max_items / 8);
+    L.fix_list = take((size_t)L.fix_cap * 8);
+    L.rw_list = take((size_t)std::max<int64_t>(n_strings, 1) * 4);
     // planning: items per (planning CTA, DFA x length class), then those CTAs' first
     // queue positions; each class's end; map slots per planning CTA, then its first slot
     L.cta_bins = take((size_t)kMaxPlanCtas * kMaxDfasPerSet * kLenClasses * 4);
@@ -205,6 +215,46 @@ __device__ __forceinline__ int checked_dfa(const int64_t *offsets, const int32_t
     return d;
 }
 
+// A string's offsets and automaton as loaded (the planning kernels load the
+// next tile's while they work on the current one); checked by checked_loaded.
+struct StringIn {
+    int64_t a, b;
+    int32_t d;
+    bool any;   // i < n
+};
+__device__ __forceinline__ StringIn load_string(const int64_t *offsets, const int32_t *dfa_id, int64_t i,
+                                                int64_t n, int64_t multi_n) {
+    StringIn r{0, 0, 0, false};
+    if (i < n) {
+        const int64_t ii = multi_n > 0 ? i % multi_n : i;
+        r.a = offsets[ii];
+        r.b = offsets[ii + 1];
+        r.d = multi_n > 0 ? (int)(i / multi_n) : dfa_id ? dfa_id[i] : 0;
+        r.any = true;
+    }
+    return r;
+}
+// checked_dfa on loaded values: -1 for no string or a malformed one (error bit raised).
+__device__ __forceinline__ int checked_loaded(const StringIn &s, int n_dfas, int64_t total_bytes,
+                                              uint32_t *err, int64_t *len_out, int64_t *start_out) {
+    if (!s.any) return -1;
+    if (s.a < 0 || s.b < s.a || s.b > total_bytes) {
+        atomicOr(err, kErrBadOffsets);
+        return -1;
+    }
+    if (s.d < 0 || s.d >= n_dfas) {
+        atomicOr(err, kErrBadDfaId);
+        return -1;
+    }
+    if (s.b - s.a > kMaxWalkBytes) {
+        atomicOr(err, kErrCapacity);
+        return -1;
+    }
+    *len_out = s.b - s.a;
+    *start_out = s.a;
+    return s.d;
+}
+
 // Warp-aggregated shared-memory counting: lanes with pred set add 1 to
 // cnt[key]; one atomic per distinct key of the warp (all lanes call it).
 __device__ __forceinline__ void warp_count(uint32_t *cnt, bool pred, int key) {
@@ -245,11 +295,13 @@ plan_count_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n, int6
     for (int t = threadIdx.x; t < n_bins; t += blockDim.x) cnt[t] = 0;
     if (threadIdx.x == 0) { items = 0; maps = 0; splits = 0; }
     __syncthreads();
+    StringIn cur = load_string(offsets, dfa_id, (int64_t)blockIdx.x * kPlanThreads + threadIdx.x, n, multi_n);
     for (int64_t tile = blockIdx.x; tile * kPlanThreads < n; tile += gridDim.x) {
-        const int64_t i = tile * kPlanThreads + threadIdx.x;
+        const StringIn nxt =
+            load_string(offsets, dfa_id, (tile + gridDim.x) * kPlanThreads + threadIdx.x, n, multi_n);
         int64_t len = 0, s0 = 0;
-        int d = i < n ? checked_dfa(offsets, dfa_id, i, n_dfas, total_bytes, err, &len, &s0, multi_n)
-                      : -1;
+        const int d = checked_loaded(cur, n_dfas, total_bytes, err, &len, &s0);
+        cur = nxt;
         uint32_t k = 0;
         ItemClasses ic{0, 0, 0};
         if (d >= 0) {
@@ -440,14 +492,17 @@ plan_fill_kernel(const int64_t *offsets, const int32_t *dfa_id, int64_t n, int64
     }
     __syncthreads();
     bool bad = false;
+    StringIn cur = load_string(offsets, dfa_id, (int64_t)blockIdx.x * kPlanThreads + threadIdx.x, n, multi_n);
     for (int64_t tile = blockIdx.x; tile * kPlanThreads < n; tile += gridDim.x) {
         const int64_t i = tile * kPlanThreads + threadIdx.x;
-        int d = -1;
+        const StringIn nxt =
+            load_string(offsets, dfa_id, (tile + gridDim.x) * kPlanThreads + threadIdx.x, n, multi_n);
         int64_t len = 0, s0 = 0;
+        const int d = checked_loaded(cur, n_dfas, total_bytes, err, &len, &s0);
+        cur = nxt;
         uint32_t k = 0, p_first = 0, p_mid = 0, p_last = 0, mb = 0;
         ItemClasses ic{0, 0, 0};
         ItemGeom g{0, 0, 0};
-        if (i < n) d = checked_dfa(offsets, dfa_id, i, n_dfas, total_bytes, err, &len, &s0, multi_n);
         if (d >= 0) {
             g = item_geom(len, s0, desc[d].n_states, seg_len, base_mis);
             k = g.k;
@@ -581,6 +636,11 @@ struct RaggedParams {
     const uint4 *split_list;     // every split string: string, first map slot, items | automaton << 16
                                  // | (states - 1) << 24, offset of its accept table
     const uint32_t *n_split;     // their number
+    uint2 *fix_list;             // fix-up tasks: split string, item << 8 | entry state
+    uint32_t fix_cap;
+    uint32_t *n_fix;
+    uint32_t *rw_list;           // split strings to walk again
+    uint32_t *n_rw;
     const int32_t *dfa_id;
     int64_t n;
     int64_t max_items;
@@ -599,7 +659,7 @@ __device__ __forceinline__ void write_result(const RaggedParams &P, uint32_t str
     if (P.accept_i32) P.accept_i32[str] = a ? 1 : 0;
 }
 
-// Record of one item of a split string, for compose_kernel, which chains the
+// Record of one item of a split string, for the compose kernels, which chain the
 // items of the string after the walk: bits 0-7 the guessed entry state (the
 // state after the warm-up; the start state for the first item), 8-15 the end
 // state, 16-47 the checkpoints (four states, see capture_cp).
@@ -1402,183 +1462,193 @@ __device__ __noinline__ uint32_t fix_item(const RaggedParams &P, const uint8_t *
     return 0xFFFFu;
 }
 
-// Strings cut into several items: chains the items' records in order, one lane
-// per string. Item j's record is right when its guessed entry equals the end
-// state of item j - 1 (item 0 starts from the start state); otherwise the item
-// is walked from the true entry state until it meets the recorded chain at a
-// checkpoint (fix_item: about one window for synchronising automata), by any
-// lane of the warp. The first item whose chains never meet (automata that do
-// not synchronise, such as permutations) is walked again whole by the warp, and
-// the check goes on from there, 32 records at a time.
-__global__ void __launch_bounds__(kComposeThreads, 3) compose_kernel(RaggedParams P) {
-    __shared__ __align__(16) uint8_t s_tbl[kComposeThreads / 32][256 * kSmallDfaStates];
-    __shared__ uint32_t s_bad[kComposeThreads / 32][32];    // per string of a warp: first failed fix-up
-    __shared__ uint32_t s_last[kComposeThreads / 32][32];   // its final state from a fix-up of its last item
+// Index in a device list, with one atomic per group of lanes that append together.
+__device__ __forceinline__ uint32_t append_slot(uint32_t *count) {
+    const uint32_t m = __activemask();
+    const uint32_t lane = threadIdx.x & 31u;
+    const int leader = __ffs(m) - 1;
+    uint32_t base = 0;
+    if ((int)lane == leader) base = atomicAdd(count, (uint32_t)__popc(m));
+    base = __shfl_sync(m, base, leader);
+    return base + (uint32_t)__popc(m & ((1u << lane) - 1u));
+}
+
+// Split string x must be walked again from item j with entry state e (word j << 8 | e): the
+// earliest such item wins. The word lives in the low half of item 0's record, which nothing
+// reads once the records are chained; the first mark puts the string on the re-walk list.
+__device__ __forceinline__ void mark_rewalk(const RaggedParams &P, uint32_t x, uint32_t mb, uint32_t word) {
+    if (atomicMin(reinterpret_cast<uint32_t *>(P.maps + mb), word) == 0xFFFFFFFFu)
+        P.rw_list[append_slot(P.n_rw)] = x;
+}
+
+// Strings cut into several items, step 1 of 3: chains each string's records.
+// Item j's record is right when its guessed entry equals the end state of item
+// j - 1 (item 0 starts from the start state). A record whose guess is wrong
+// becomes a fix-up task (string, item, entry state) and the chain goes on as if
+// the fix-up meets the recorded chain, so the entry of item j + 1 is item j's
+// recorded end state; the string's final state is written on that assumption and
+// corrected by the two kernels below where it fails. A warp takes 32 strings of
+// the list and checks one string at a time across its lanes: lane j holds record
+// j (one coalesced load per 32 records) and compares its guess with lane j - 1's
+// end state; the first 32 records of eight strings are loaded together.
+__global__ void __launch_bounds__(kComposeThreads) compose_chain_kernel(RaggedParams P) {
     if (*(volatile uint32_t *)P.err & kErrCapacity) return;   // the plan was refused
     const uint32_t FULL = 0xffffffffu;
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
-    s_bad[wib][lane] = 0xFFFFFFFFu;
-    s_last[wib][lane] = 0u;
-    __syncwarp();
-    uint8_t *tbl = s_tbl[wib];
-    int tbl_dfa = -1;
+    const int64_t n_split = *P.n_split;
     const int64_t nwarps = (int64_t)gridDim.x * (kComposeThreads / 32);
-    const int64_t n_split = *P.n_split;   // only split strings need chaining
     for (int64_t base = ((int64_t)blockIdx.x * (kComposeThreads / 32) + wib) * 32; base < n_split;
          base += nwarps * 32) {
-        uint4 ent = make_uint4(0u, 0u, 0u, 0u);
-        if (base + lane < n_split) ent = P.split_list[base + lane];
-        const int64_t i = (int64_t)ent.x;
-        const int d = (int)((ent.z >> 16) & 0xffu);
-        const uint32_t N = (ent.z >> 24) + 1u, aoff = ent.w, mb = ent.y;
-        uint32_t k = base + lane < n_split ? ent.z & 0xffffu : 0u;
-        if (k > 1 && (int64_t)mb + (int64_t)k > P.max_items) {   // not written by this plan
-            atomicOr(P.err, kErrCapacity);
-            k = 0;
-        }
-        // the string's geometry, only where a fix-up or a re-walk needs it
-        int64_t len = 0, s0 = 0;
-        ItemGeom g{0, 0, 0};
-        auto geometry = [&]() {
-            if (checked_dfa(P.offsets, P.dfa_id, i, P.n_dfas, P.total_bytes, P.err, &len, &s0, P.multi_n) == d)
-                g = item_geom(len, s0, (int)N, P.seg_len, P.base_mis);
-            if (g.k != k) {   // offsets changed since the plan
-                atomicOr(P.err, kErrCapacity);
-                g = ItemGeom{0, 0, 0};
+        const bool mine = base + lane < n_split;
+        const uint4 ent = mine ? P.split_list[base + lane] : make_uint4(0u, 0u, 0u, 0u);
+        uint32_t fin = 0xffu;   // lane s: the final state of string s of the warp
+#pragma unroll 1
+        for (int s0 = 0; s0 < 32; s0 += 8) {
+            uint64_t r[8];
+            uint32_t mbs[8], ks[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                mbs[u] = __shfl_sync(FULL, ent.y, s0 + u);
+                ks[u] = __shfl_sync(FULL, ent.z, s0 + u) & 0xffffu;
+                if (base + s0 + u >= n_split) ks[u] = 0;
+                if (ks[u] != 0 && (ks[u] < 2 || (int64_t)mbs[u] + (int64_t)ks[u] > P.max_items)) {
+                    if (lane == 0) atomicOr(P.err, kErrCapacity);   // not written by this plan
+                    ks[u] = 0;
+                }
+                r[u] = lane < ks[u] ? P.maps[mbs[u] + lane] : 0ull;
             }
-        };
-        // Each lane chains its own string's records, as if every wrong guess were fixed by
-        // meeting the recorded chain at a checkpoint (true unless the automaton does not
-        // synchronise): the entry of item j is then the recorded end state of item j - 1.
-        // The fix-ups of eight records of the warp's 32 strings are shared out over the
-        // lanes, one a lane at a time (a lane per string would run them one after another:
-        // SIMT serialises divergent calls). A fix-up that does not end in the recorded end
-        // state hands the string to the warp re-walk below from that item.
-        uint32_t st = 0, jbad = 0;
-        bool help = false;
-        if (k > 1) st = (uint32_t)(P.maps[mb] >> 8) & 0xffu;   // item 0 starts from the start state
-        for (uint32_t j0 = 1; __any_sync(FULL, k > 1 && j0 < k && !help); j0 += 8) {
-            const bool act = k > 1 && j0 < k && !help;
-            uint32_t tmask = 0, elo = 0, ehi = 0;   // records needing a fix-up, their entry states
-            if (act) {
-                uint64_t v[8];   // eight records loaded together (one load latency for most strings)
 #pragma unroll
-                for (int u = 0; u < 8; ++u) v[u] = j0 + u < k ? P.maps[mb + j0 + u] : 0ull;
-#pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    if (j0 + u >= k) continue;
-                    if (((uint32_t)v[u] & 0xffu) != st) {
-                        tmask |= 1u << u;
-                        if (u < 4) elo |= st << (8 * u);
-                        else ehi |= st << (8 * (u - 4));
+            for (int u = 0; u < 8; ++u) {
+                const uint32_t k = ks[u], mb = mbs[u];
+                if (k == 0) continue;   // warp-uniform
+                const uint32_t x = (uint32_t)(base + s0 + u);
+                if (lane == 0) *reinterpret_cast<uint32_t *>(P.maps + mb) = 0xFFFFFFFFu;   // no re-walk yet
+                __syncwarp();
+                uint64_t rec = r[u];
+                uint32_t carry = 0;
+                for (uint32_t j0 = 0; j0 < k; j0 += 32) {
+                    if (j0 > 0) rec = j0 + lane < k ? P.maps[mb + j0 + lane] : 0ull;
+                    const uint32_t end = (uint32_t)(rec >> 8) & 0xffu;
+                    uint32_t prev = __shfl_up_sync(FULL, end, 1);
+                    if (lane == 0) prev = carry;
+                    const uint32_t j = j0 + lane;
+                    if (j > 0 && j < k && ((uint32_t)rec & 0xffu) != prev) {
+                        const uint32_t word = (j << 8) | prev;
+                        const uint32_t t = append_slot(P.n_fix);
+                        if (t < P.fix_cap) P.fix_list[t] = make_uint2(x, word);
+                        else mark_rewalk(P, x, mb, word);   // the list is full: walk again from here
                     }
-                    st = (uint32_t)(v[u] >> 8) & 0xffu;
+                    carry = __shfl_sync(FULL, end, (int)min(31u, k - 1 - j0));
                 }
+                if (lane == (uint32_t)(s0 + u)) fin = carry;
             }
-            if (tmask && g.k == 0) geometry();
-            if (tmask && g.k == 0) tmask = 0;   // changed offsets: no fix-up (the error bit is set)
-            const uint32_t cnt = __popc(tmask);
-            uint32_t incl = cnt;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t x = __shfl_up_sync(FULL, incl, o);
-                if (lane >= (uint32_t)o) incl += x;
-            }
-            const uint32_t total = __shfl_sync(FULL, incl, 31);
-            for (uint32_t t0 = 0; t0 < total; t0 += 32) {
-                const uint32_t t = t0 + lane;
-                uint32_t ow = 0;   // the owner: the first lane whose inclusive count exceeds t
-#pragma unroll
-                for (uint32_t step = 16; step >= 1; step >>= 1)
-                    if (__shfl_sync(FULL, incl, ow + step - 1) <= t) ow += step;
-                const uint32_t io = __shfl_sync(FULL, incl, ow), co = __shfl_sync(FULL, cnt, ow);
-                const uint32_t mo = __shfl_sync(FULL, tmask, ow), mbo = __shfl_sync(FULL, mb, ow);
-                const uint32_t elo_o = __shfl_sync(FULL, elo, ow), ehi_o = __shfl_sync(FULL, ehi, ow);
-                const int d_o = __shfl_sync(FULL, d, ow);
-                const int64_t s0o = __shfl_sync(FULL, s0, ow), leno = __shfl_sync(FULL, len, ow);
-                const ItemGeom go{__shfl_sync(FULL, k, ow), __shfl_sync(FULL, g.seg, ow),
-                                  __shfl_sync(FULL, g.first, ow)};
-                if (t >= total) continue;
-                const uint32_t u = __fns(mo, 0, (int)(t - (io - co)) + 1);   // the owner's fix-up
-                const uint32_t e = (u < 4 ? elo_o >> (8 * u) : ehi_o >> (8 * (u - 4))) & 0xffu;
-                const uint32_t j = j0 + u;
-                const uint64_t rec = P.maps[mbo + j];
-                const uint32_t No = (uint32_t)P.desc[d_o].n_states;
-                int64_t b0, b1;
-                item_range(go, s0o, leno, j, &b0, &b1);
-                const uint32_t f = e < No ? fix_item(P, P.tmaps + P.desc[d_o].tmap_off, No, b0, b1, e, rec)
-                                          : 0xFFFFu;
-                if (f != ((uint32_t)(rec >> 8) & 0xffu)) {
-                    // a last item walked to its end: that is the string's final state (a short
-                    // item can end before the chains meet); otherwise the string is walked again
-                    if (f != 0xFFFFu && j + 1 == go.k) s_last[wib][ow] = 0x100u | f;
-                    else atomicMin(&s_bad[wib][ow], (j << 8) | e);
-                }
-            }
-            __syncwarp();
-            const uint32_t bad = s_bad[wib][lane], last = s_last[wib][lane];
-            if (act && bad != 0xFFFFFFFFu) {   // the walk goes on from item bad >> 8
-                help = true;
-                jbad = bad >> 8;
-                st = bad & 0xffu;
-            } else if (act && last) {
-                st = last & 0xffu;
-            }
-            s_bad[wib][lane] = 0xFFFFFFFFu;
-            s_last[wib][lane] = 0u;
-            __syncwarp();
         }
-        if (k > 1 && !help) {
-            if (st < N) write_result(P, (uint32_t)i, st, aoff);
+        if (mine && (ent.z & 0xffffu) >= 2) {
+            if (fin < (ent.z >> 24) + 1u) write_result(P, ent.x, fin, ent.w);
             else atomicOr(P.err, kErrCapacity);   // records not written by this plan
         }
-        // strings with a wrong guess: the warp re-walks that item and goes on checking
-        for (uint32_t todo = __ballot_sync(FULL, help); todo; todo &= todo - 1) {
-            const int src = __ffs(todo) - 1;
-            const int sd = __shfl_sync(FULL, d, src);
-            const uint32_t sk = __shfl_sync(FULL, k, src), smb = __shfl_sync(FULL, mb, src);
-            const uint32_t sj = __shfl_sync(FULL, jbad, src), s_entry = __shfl_sync(FULL, st, src);
-            const int64_t ss0 = __shfl_sync(FULL, s0, src), slen = __shfl_sync(FULL, len, src);
-            const ItemGeom sg{sk, __shfl_sync(FULL, g.seg, src), __shfl_sync(FULL, g.first, src)};
-            const DfaDesc D = P.desc[sd];
-            const uint32_t N = (uint32_t)D.n_states;
-            auto rewalk = [&](uint32_t jb, uint32_t s_in) {
-                if (tbl_dfa != sd) {   // this warp's copy of the automaton's byte map
-                    __syncwarp();
-                    const uint8_t *tm = P.tmaps + D.tmap_off;
-                    for (uint32_t t = lane; t < 256 * N; t += 32) tbl[t] = tm[t];
-                    __syncwarp();
-                    tbl_dfa = sd;
-                }
-                int64_t b0, b1;
-                item_range(sg, ss0, slen, jb, &b0, &b1);
-                return warp_rewalk(tbl, N, P.data, b0, b1, s_in);
-            };
-            uint32_t s = s_entry < N ? rewalk(sj, s_entry) : 0xffu;
-            for (uint32_t j0 = sj + 1; j0 < sk && s < N; j0 += 32) {
-                const uint32_t j = j0 + lane;
-                const bool in = j < sk;
-                const uint32_t v = in ? (uint32_t)P.maps[smb + j] : 0u;
-                uint32_t g = v & 0xffu, f = (v >> 8) & 0xffu;
-                for (;;) {
-                    uint32_t pf = __shfl_up_sync(FULL, f, 1);
-                    if (lane == 0) pf = s;
-                    const uint32_t bad = __ballot_sync(FULL, in && g != pf);
-                    if (!bad) break;
-                    const int b = __ffs(bad) - 1;
-                    const uint32_t s_in = __shfl_sync(FULL, pf, b);
-                    const uint32_t s_out = s_in < N ? rewalk(j0 + (uint32_t)b, s_in) : s_in;
-                    if (lane == (uint32_t)b) {
-                        g = s_in;
-                        f = s_out;
-                    }
-                }
-                s = __shfl_sync(FULL, f, (int)min(31u, sk - 1 - j0));
+    }
+}
+
+// Step 2 of 3, one thread per fix-up task: walks item j from its true entry state
+// until it meets the recorded chain at a checkpoint (fix_item: about one window for
+// synchronising automata). Met: the chained result stands. A last item walked to
+// its end: its end state is the string's final state. Otherwise (automata that do
+// not synchronise, such as permutations) the string is marked to be walked again
+// from item j.
+__global__ void __launch_bounds__(kComposeThreads) compose_fix_kernel(RaggedParams P) {
+    if (*(volatile uint32_t *)P.err & kErrCapacity) return;
+    const uint32_t n_fix = min(*(volatile uint32_t *)P.n_fix, P.fix_cap);
+    for (uint32_t t = blockIdx.x * kComposeThreads + threadIdx.x; t < n_fix; t += gridDim.x * kComposeThreads) {
+        const uint2 task = P.fix_list[t];
+        const uint32_t x = task.x, j = task.y >> 8, e = task.y & 0xffu;
+        const uint4 ent = P.split_list[x];
+        const uint32_t mb = ent.y, k = ent.z & 0xffffu, N = (ent.z >> 24) + 1u;
+        const int d = (int)((ent.z >> 16) & 0xffu);
+        int64_t len = 0, s0 = 0;
+        ItemGeom g{0, 0, 0};
+        if (checked_dfa(P.offsets, P.dfa_id, (int64_t)ent.x, P.n_dfas, P.total_bytes, P.err, &len, &s0,
+                        P.multi_n) == d)
+            g = item_geom(len, s0, (int)N, P.seg_len, P.base_mis);
+        if (g.k != k || j >= k) {   // offsets changed since the plan
+            atomicOr(P.err, kErrCapacity);
+            continue;
+        }
+        const uint64_t rec = P.maps[mb + j];
+        int64_t b0, b1;
+        item_range(g, s0, len, j, &b0, &b1);
+        const uint32_t f = e < N ? fix_item(P, P.tmaps + P.desc[d].tmap_off, N, b0, b1, e, rec) : 0xFFFFu;
+        if (f == ((uint32_t)(rec >> 8) & 0xffu)) continue;
+        if (f != 0xFFFFu && j + 1 == k) write_result(P, ent.x, f, ent.w);
+        else mark_rewalk(P, x, mb, task.y);
+    }
+}
+
+// Step 3 of 3, a warp per string on the re-walk list: walks the marked item again
+// whole from its entry state (each lane maps all N states over 1/32 of the item),
+// then checks the following records 32 at a time, walking again every item whose
+// guess differs from its predecessor's true end state. Exact for every DFA.
+__global__ void __launch_bounds__(kComposeThreads) compose_rewalk_kernel(RaggedParams P) {
+    __shared__ __align__(16) uint8_t s_tbl[kComposeThreads / 32][256 * kSmallDfaStates];
+    if (*(volatile uint32_t *)P.err & kErrCapacity) return;
+    const uint32_t FULL = 0xffffffffu;
+    const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+    uint8_t *tbl = s_tbl[wib];
+    int tbl_dfa = -1;
+    const uint32_t n_rw = *(volatile uint32_t *)P.n_rw;
+    for (uint32_t r = blockIdx.x * (kComposeThreads / 32) + wib; r < n_rw;
+         r += gridDim.x * (kComposeThreads / 32)) {
+        const uint32_t x = P.rw_list[r];
+        const uint4 ent = P.split_list[x];
+        const uint32_t mb = ent.y, k = ent.z & 0xffffu, N = (ent.z >> 24) + 1u;
+        const int d = (int)((ent.z >> 16) & 0xffu);
+        const uint32_t word = *reinterpret_cast<const volatile uint32_t *>(P.maps + mb);
+        const uint32_t jb = word >> 8, s_entry = word & 0xffu;
+        int64_t len = 0, s0 = 0;
+        ItemGeom g{0, 0, 0};
+        if (checked_dfa(P.offsets, P.dfa_id, (int64_t)ent.x, P.n_dfas, P.total_bytes, P.err, &len, &s0,
+                        P.multi_n) == d)
+            g = item_geom(len, s0, (int)N, P.seg_len, P.base_mis);
+        if (g.k != k || jb >= k) {   // offsets changed since the plan
+            if (lane == 0) atomicOr(P.err, kErrCapacity);
+            continue;
+        }
+        auto rewalk = [&](uint32_t jw, uint32_t s_in) {
+            if (tbl_dfa != d) {   // this warp's copy of the automaton's byte map
+                __syncwarp();
+                const uint8_t *tm = P.tmaps + P.desc[d].tmap_off;
+                for (uint32_t t = lane; t < 256 * N; t += 32) tbl[t] = tm[t];
+                __syncwarp();
+                tbl_dfa = d;
             }
-            if ((int)lane == src) {
-                if (s < N) write_result(P, (uint32_t)i, s, D.accept_off);
-                else atomicOr(P.err, kErrCapacity);   // records not written by this plan
+            int64_t b0, b1;
+            item_range(g, s0, len, jw, &b0, &b1);
+            return warp_rewalk(tbl, N, P.data, b0, b1, s_in);
+        };
+        uint32_t s = s_entry < N ? rewalk(jb, s_entry) : 0xffu;
+        for (uint32_t j0 = jb + 1; j0 < k && s < N; j0 += 32) {
+            const uint32_t j = j0 + lane;
+            const bool in = j < k;
+            const uint32_t v = in ? (uint32_t)P.maps[mb + j] : 0u;
+            uint32_t gs = v & 0xffu, f = (v >> 8) & 0xffu;
+            for (;;) {
+                uint32_t pf = __shfl_up_sync(FULL, f, 1);
+                if (lane == 0) pf = s;
+                const uint32_t bad = __ballot_sync(FULL, in && gs != pf);
+                if (!bad) break;
+                const int b = __ffs(bad) - 1;
+                const uint32_t s_in = __shfl_sync(FULL, pf, b);
+                const uint32_t s_out = s_in < N ? rewalk(j0 + (uint32_t)b, s_in) : s_in;
+                if (lane == (uint32_t)b) {
+                    gs = s_in;
+                    f = s_out;
+                }
             }
+            s = __shfl_sync(FULL, f, (int)min(31u, k - 1 - j0));
+        }
+        if (lane == 0) {
+            if (s < N) write_result(P, ent.x, s, ent.w);
+            else atomicOr(P.err, kErrCapacity);   // records not written by this plan
         }
     }
 }
@@ -1716,6 +1786,11 @@ static int dfa_set_run_ex(trex_dfa_set *set, const uint8_t *data, const int64_t 
     P.maps = maps;
     P.split_list = split_list;
     P.n_split = cta_splits + plan_grid;
+    P.fix_list = reinterpret_cast<uint2 *>(sc + L.fix_list);
+    P.fix_cap = (uint32_t)std::min<int64_t>(L.fix_cap, 0xffffffffLL);
+    P.n_fix = reinterpret_cast<uint32_t *>(sc + L.n_fix);
+    P.rw_list = reinterpret_cast<uint32_t *>(sc + L.rw_list);
+    P.n_rw = reinterpret_cast<uint32_t *>(sc + L.n_rw);
     P.dfa_id = dfa_id;
     P.n = n;
     P.max_items = L.max_items;
@@ -1735,10 +1810,15 @@ static int dfa_set_run_ex(trex_dfa_set *set, const uint8_t *data, const int64_t 
     dfa_ragged_kernel<<<ragged_grid, kRaggedThreads, set->smem_bytes, stream>>>(P);
     TREX_CHECK_LAUNCH();
     profile_kernel_end(stream);
-    // resident CTAs (three an SM) loop over the list of split strings
-    compose_kernel<<<(int)std::min<int64_t>((n + kComposeThreads - 1) / kComposeThreads,
-                                            (int64_t)set->n_sms * 3),
-                     kComposeThreads, 0, stream>>>(P);
+    // chaining split strings: a thread per string, then per fix-up task, then a warp per
+    // string to walk again (the last two read their counts on the device)
+    compose_chain_kernel<<<(int)std::min<int64_t>((n + kComposeThreads - 1) / kComposeThreads,
+                                                  (int64_t)set->n_sms * 4),
+                           kComposeThreads, 0, stream>>>(P);
+    TREX_CHECK_LAUNCH();
+    compose_fix_kernel<<<set->n_sms * 2, kComposeThreads, 0, stream>>>(P);
+    TREX_CHECK_LAUNCH();
+    compose_rewalk_kernel<<<set->n_sms * 2, kComposeThreads, 0, stream>>>(P);
     TREX_CHECK_LAUNCH();
     if (err_word_out) *err_word_out = err;
     return TREX_OK;
