@@ -82,7 +82,7 @@ constexpr int kLenClasses = 64;
 
 // ---- scratch layout -----------------------------------------------------------
 struct ScratchLayout {
-    size_t q_base, q_count, q_head, q_bytes, err, n_items, n_fix, n_rw, items, maps, split_list, fix_list,
+    size_t q_base, q_count, q_head, q_serve, q_bytes, err, n_items, n_fix, n_rw, items, maps, split_list, fix_list,
         rw_list, cta_bins, bin_base, bin_end, cta_maps, cta_splits, total;
     int64_t max_items, fix_cap;
 };
@@ -105,6 +105,7 @@ static ScratchLayout scratch_layout(int64_t n_strings, int64_t total_bytes, int3
     L.q_base = take(kMaxDfasPerSet * 4);
     L.q_count = take(kMaxDfasPerSet * 4);
     L.q_head = take(kMaxDfasPerSet * 4);
+    L.q_serve = take(kMaxDfasPerSet * 4);
     L.q_bytes = take(kMaxDfasPerSet * 8);
     L.err = take(4);
     L.n_items = take(8);
@@ -630,6 +631,7 @@ struct RaggedParams {
     const uint32_t *q_base;
     const uint32_t *q_count;
     uint32_t *q_head;
+    uint32_t *q_serve;           // CTAs walking each queue
     const unsigned long long *q_bytes;
     uint32_t *err;
     uint64_t *maps;
@@ -1347,6 +1349,7 @@ __global__ void __launch_bounds__(kRaggedThreads, 1) dfa_ragged_kernel(RaggedPar
                 for (int d = P.n_dfas - 1; d >= 0; --d)
                     if (P.q_count[d]) { home = d; break; }
         }
+        if (home >= 0) atomicAdd(&P.q_serve[home], 1u);
         s_dfa = home;
     }
     __syncthreads();
@@ -1377,16 +1380,39 @@ __global__ void __launch_bounds__(kRaggedThreads, 1) dfa_ragged_kernel(RaggedPar
             drain(P, ByteMode<Walker<0>>{Walker<0>{(uint32_t)D.n_states}}, D, d);
         }
         __syncthreads();
-        if (threadIdx.x == 0) {
+        // Next queue: the one whose remaining walk per CTA walking it is the largest, so
+        // that the queues end together (the launch ends with its last queue). Its
+        // remaining bytes are estimated as items left x the longest of them (the head:
+        // queues run longest first); warp 0 scores the queues in parallel.
+        if (threadIdx.x < 32) {
+            if (threadIdx.x == 0) atomicSub(&P.q_serve[d], 1u);
+            unsigned long long best_score = 0;
             int best = -1;
-            uint32_t best_rem = 0;
-            for (int e = 0; e < P.n_dfas; ++e) {
-                uint32_t h = *(volatile uint32_t *)&P.q_head[e];
-                uint32_t c = P.q_count[e];
-                uint32_t rem = h < c ? c - h : 0;
-                if (rem > best_rem) { best_rem = rem; best = e; }
+            for (int e = (int)lane; e < P.n_dfas; e += 32) {
+                const uint32_t h = *(volatile uint32_t *)&P.q_head[e], c = P.q_count[e];
+                if (h >= c) continue;
+                const WorkItem w = P.items[P.q_base[e] + h];
+                const unsigned long long len = w.end > w.p0 ? (unsigned long long)(w.end - w.p0) : 1ull;
+                const uint32_t serve = *(volatile uint32_t *)&P.q_serve[e];
+                const unsigned long long score = (unsigned long long)(c - h) * len / (serve + 1ull);
+                if (best < 0 || score > best_score) {
+                    best_score = score;
+                    best = e;
+                }
             }
-            s_dfa = best;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const unsigned long long os = __shfl_xor_sync(0xffffffffu, best_score, o);
+                const int ob = __shfl_xor_sync(0xffffffffu, best, o);
+                if (ob >= 0 && (best < 0 || os > best_score || (os == best_score && ob < best))) {
+                    best_score = os;
+                    best = ob;
+                }
+            }
+            if (threadIdx.x == 0) {
+                if (best >= 0) atomicAdd(&P.q_serve[best], 1u);
+                s_dfa = best;
+            }
         }
         __syncthreads();
     }
@@ -1781,6 +1807,7 @@ static int dfa_set_run_ex(trex_dfa_set *set, const uint8_t *data, const int64_t 
     P.q_base = q_base;
     P.q_count = q_count;
     P.q_head = q_head;
+    P.q_serve = reinterpret_cast<uint32_t *>(sc + L.q_serve);
     P.q_bytes = q_bytes;
     P.err = err;
     P.maps = maps;
