@@ -37,8 +37,10 @@ prefix_engine_* ABI with host buffers), cfg3a_scan, cfg3b_nfa (bit-parallel and
 tensor-core forms), cfg4_pnfa (with the one-string chain latency per
 position), dfa_n32_64 (the ragged batch shape, 250K strings, on 32- and
 64-state automata), kgram_sweep (K = 1, 2, 4 on 4 GB of ACGT strings, where
-gram tables apply), cfg5_served (a Poisson sweep up to saturation, with the
-limiter named). --no-extras skips them.
+gram tables apply), ref_shapes (the NFA kernels on the shape the reference
+publishes its NFA numbers for: sigma 2, 262144 x 2048, with those numbers
+beside them), cfg5_served (a Poisson sweep up to saturation, with the limiter
+named). --no-extras skips them.
 
 Multi-GPU: one process per GPU (torchrun); every rank runs its own seeded
 batch (weak scaling, no data-path collective); times are the max over ranks
@@ -77,7 +79,7 @@ from trex_b200.sharding import max_over_ranks, rank_seed  # noqa: E402
 METRIC = "Gchar/s vs HBM roofline, plain vs batched/served; served p50/p99 ms (1 B200)"
 SUB_ALPHABET = b"ACGT"
 EXTRAS = ("cfg1_plain", "plain_per_pattern", "cfg3a_scan", "cfg3b_nfa", "cfg4_pnfa", "dfa_n32_64",
-          "kgram_sweep", "cfg5_served")
+          "kgram_sweep", "ref_shapes", "cfg5_served")
 
 
 def parse_args(argv=None):
@@ -411,12 +413,13 @@ class NFAWorkload:
         self.args = args
         self.host_data = None
         rng = np.random.default_rng(args.seed)
-        self.T, self.start, self.acc = random_bool_nfa(rng, n_states=64, sigma=20, density=0.05)
+        self.sigma = getattr(args, "nfa_sigma", None) or 20
+        self.T, self.start, self.acc = random_bool_nfa(rng, n_states=64, sigma=self.sigma, density=0.05)
         self.n = args.strings or 262144
-        self.L = 4096
+        self.L = getattr(args, "nfa_len", None) or 4096
         self.off = np.arange(self.n + 1, dtype=np.int64) * self.L
-        self.workload = ("Boolean NFA: random 64-state NFA over 20 symbols (bytes 0..19), edge density "
-                         f"0.05, {self.n} strings x 4096 symbols")
+        self.workload = (f"Boolean NFA: random 64-state NFA over {self.sigma} symbols (bytes 0..{self.sigma - 1}), "
+                         f"edge density 0.05, {self.n} strings x {self.L} symbols")
 
     def setup(self, torch, dev, seed):
         from trex_b200.engine import NFA
@@ -425,7 +428,7 @@ class NFAWorkload:
         self.off = np.arange(self.n + 1, dtype=np.int64) * self.L
         g = torch.Generator(device=dev)
         g.manual_seed(seed + 2)
-        self.data = torch.randint(0, 20, (self.total,), dtype=torch.uint8, device=dev, generator=g)
+        self.data = torch.randint(0, self.sigma, (self.total,), dtype=torch.uint8, device=dev, generator=g)
         self.d_off = torch.from_numpy(self.off).to(dev)
         self.nfa = NFA(self.T, self.start, self.acc, unknown_rejects=True)
         self.fm = torch.empty(self.n, dtype=torch.int64, device=dev)
@@ -529,15 +532,16 @@ class PNFAWorkload:
         self.args = args
         self.mode = args.pnfa_mode
         rng = np.random.default_rng(args.seed)
-        self.T, self.start, self.acc = random_prob_nfa(rng, 64, 20)
+        self.sigma = getattr(args, "nfa_sigma", None) or 20
+        self.T, self.start, self.acc = random_prob_nfa(rng, 64, self.sigma)
         self.n = args.strings or 65536
-        self.L = 2048
+        self.L = getattr(args, "nfa_len", None) or 2048
         self.off = np.arange(self.n + 1, dtype=np.int64) * self.L
         self.kernel = "pnfa_plain_kernel" if self.mode == "fp32" else "pnfa_tc_kernel"
         self.dtype = {"bf16": "bf16", "fp16": "f16", "fp32": "f32"}[self.mode]
-        self.workload = ("probabilistic NFA: 64 states, 20 symbols (bytes 0..19), rows of T[c] "
+        self.workload = (f"probabilistic NFA: 64 states, {self.sigma} symbols (bytes 0..{self.sigma - 1}), rows of T[c] "
                          "Dirichlet(0.5) x 0.9 with ~30% kept, start e0, accept all states; "
-                         f"{self.n} strings x 2048 symbols; {self.mode} operands"
+                         f"{self.n} strings x {self.L} symbols; {self.mode} operands"
                          + ("" if self.mode == "fp32" else ", FP32 accumulation (tcgen05)"))
 
     def setup(self, torch, dev, seed):
@@ -546,7 +550,7 @@ class PNFAWorkload:
         self.total = self.n * self.L
         g = torch.Generator(device=dev)
         g.manual_seed(seed + 4)
-        self.data = torch.randint(0, 20, (self.total,), dtype=torch.uint8, device=dev, generator=g)
+        self.data = torch.randint(0, self.sigma, (self.total,), dtype=torch.uint8, device=dev, generator=g)
         self.d_off = torch.from_numpy(self.off).to(dev)
         self.pnfa = PNFA(self.T, self.start, self.acc)
         self.ll = torch.empty(self.n, dtype=torch.float64, device=dev)
@@ -657,18 +661,19 @@ class NFATcWorkload(PNFAWorkload):
         self.args = args
         self.mode = "bool8" if args.nfa_method == "tc8" else "bool"
         rng = np.random.default_rng(args.seed)
-        T, start, acc = random_bool_nfa(rng, n_states=64, sigma=20, density=0.05)
+        self.sigma = getattr(args, "nfa_sigma", None) or 20
+        T, start, acc = random_bool_nfa(rng, n_states=64, sigma=self.sigma, density=0.05)
         self.T, self.start, self.acc = (x.astype(np.float32) for x in (T, start, acc))
         self.n = args.strings or 262144
-        self.L = 4096
+        self.L = getattr(args, "nfa_len", None) or 4096
         self.off = np.arange(self.n + 1, dtype=np.int64) * self.L
         self.kernel = "pnfa_tc_kernel"
         self.dtype = "s8" if self.mode == "bool8" else "bf16"
         ops = ("0/1 int8 operands, int32 sums (tcgen05 kind::i8)" if self.mode == "bool8"
                else "0/1 BF16 operands, FP32 sums (tcgen05 kind::f16)")
-        self.workload = ("Boolean NFA: random 64-state NFA over 20 symbols (bytes 0..19), edge density "
-                         f"0.05, {self.n} strings x 4096 symbols; tensor cores, {ops} thresholded "
-                         "every step")
+        self.workload = (f"Boolean NFA: random 64-state NFA over {self.sigma} symbols (bytes "
+                         f"0..{self.sigma - 1}), edge density 0.05, {self.n} strings x {self.L} symbols; "
+                         f"tensor cores, {ops} thresholded every step")
 
     def config(self):
         return {"workload": self.workload, "n_strings": self.n, "total_bytes_per_gpu": self.total,
@@ -997,7 +1002,8 @@ def make_workload(args):
 def sub_args(args, **kw):
     """A copy of the command line for one sub-configuration (defaults for it)."""
     d = dict(vars(args))
-    d.update({"strings": None, "seg_len": 0, "kgram": None, "dfa_sizes": None})
+    d.update({"strings": None, "seg_len": 0, "kgram": None, "dfa_sizes": None, "nfa_sigma": None,
+              "nfa_len": None})
     d.update(kw)
     return argparse.Namespace(**d)
 
@@ -1337,6 +1343,8 @@ def run_extras(args, torch, dev, main_wl, names):
         except Exception as e:
             extras[name] = {"error": repr(e)[:400]}
         torch.cuda.empty_cache()
+    if "ref_shapes" in names:
+        extras["ref_shapes"] = ref_shapes(args, torch, dev)
     if "cfg4_pnfa" in names:
         try:
             extras["cfg4_pnfa_latency"] = pnfa_latency(args, torch, dev)
@@ -1353,6 +1361,35 @@ def run_extras(args, torch, dev, main_wl, names):
         except Exception as e:
             extras["cfg5_served"] = {"error": repr(e)[:400]}
     return extras
+
+
+def ref_shapes(args, torch, dev):
+    """The NFA kernels on the shape the reference publishes its NFA numbers for: 64 states,
+    sigma 2, 262144 strings x 2048 symbols (README.md:12-15, H200), each checked against the
+    oracle like the default configurations."""
+    R = 262144
+    kw = dict(nfa_sigma=2, nfa_len=2048, strings=R)
+    runs = [("nfa_bitpar", lambda: NFAWorkload(sub_args(args, workload="nfa", **kw)), 10,
+             {"value": 185.0, "kernel": "bit-parallel V4", "source": "README.md:12"}),
+            ("nfa_tensor_int8", lambda: NFATcWorkload(sub_args(args, workload="nfa", nfa_method="tc8", **kw)), 2,
+             {"value": 12.5, "kernel": "tensor-core V3 (FP16 WMMA, 0/1 operands)", "source": "README.md:14"}),
+            ("pnfa_fp16", lambda: PNFAWorkload(sub_args(args, workload="pnfa", pnfa_mode="fp16", **kw)), 3,
+             {"value": 10.9, "kernel": "probabilistic V5 (FP16 WMMA)", "source": "README.md:15"}),
+            ("pnfa_bf16", lambda: PNFAWorkload(sub_args(args, workload="pnfa", pnfa_mode="bf16", **kw)), 3,
+             {"value": 10.9, "kernel": "probabilistic V5 (FP16 WMMA)", "source": "README.md:15"})]
+    out = {}
+    for name, make, steps, pub in runs:
+        try:
+            wl = make()
+            m = measure(wl, wl.args, torch, dev, steps=steps, warmup=3, e2e_steps=0, roof_tag="ref_" + name)
+            m["reference_published"] = dict(pub, unit="Gchar/s", hardware="H200")
+            out[name] = m
+            wl.close()
+            del wl
+        except Exception as e:
+            out[name] = {"error": repr(e)[:400]}
+        torch.cuda.empty_cache()
+    return {"shape": f"64-state NFAs over 2 symbols, {R} strings x 2048 symbols", "by_kernel": out}
 
 
 def trex_arm(args, rank, world, local_rank):
@@ -1387,6 +1424,8 @@ def trex_arm(args, rank, world, local_rank):
             line["configs"] = run_extras(args, torch, dev, wl, names)
             for v in line["configs"].values():
                 failed |= isinstance(v, dict) and (failed_checks(v) or bool(v.get("mismatches_vs_batched")))
+            for v in line["configs"].get("ref_shapes", {}).get("by_kernel", {}).values():
+                failed |= isinstance(v, dict) and failed_checks(v)
         else:
             wl.close()
         print(json.dumps(line), flush=True)
