@@ -199,3 +199,65 @@ def test_bool_mode_small_nfa_both_outcomes(cuda, oracle, mode):
     assert err == 0
     assert 0 < ref.sum() < len(ref)
     assert np.array_equal(ac.astype(bool), ref.astype(bool))
+
+
+@pytest.mark.parametrize("sigma", [1, 2])
+@pytest.mark.parametrize("mode", ["bf16", "fp16"])
+def test_pnfa_lane_kernel_small_alphabet(cuda, oracle, sigma, mode):
+    # alphabets of at most two symbols run one string a TMEM lane (no sorting by symbol):
+    # ragged and empty strings, bytes >= sigma skipped, more strings than the launch has
+    # lanes (148 x 512), so lanes take several strings one after another
+    rng = np.random.default_rng(20 + sigma)
+    T, start, acc = random_prob_nfa(rng, 64, sigma)
+    n = 100_000
+    lens = rng.integers(0, 20, size=n)
+    lens[:6] = [0, 1, 2, 3, 64, 0]
+    off = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(lens, out=off[1:])
+    data = rng.integers(0, sigma + 2, size=int(off[-1]), dtype=np.uint8)
+    ll, ac, err = _run(cuda, T, start, acc, data, off, mode)
+    ref = oracle.pnfa_fp64(T, start, acc, data, off)
+    assert err == 0
+    _check(ll, ac, ref, mode, _symbols(data, off, sigma))
+
+
+@pytest.mark.parametrize("mode", ["bf16", "fp16"])
+def test_pnfa_lane_kernel_long_and_few(cuda, oracle, mode):
+    # the lane kernel on long strings (the reference's shape, 2048 symbols, sigma 2) and on a
+    # batch of three strings (one CTA, most lanes idle from the start)
+    rng = np.random.default_rng(31)
+    T, start, acc = random_prob_nfa(rng, 64, 2)
+    for n, L in ((1024, 2048), (3, 500)):
+        off = np.arange(n + 1, dtype=np.int64) * L
+        data = rng.integers(0, 2, size=n * L, dtype=np.uint8)
+        ll, ac, err = _run(cuda, T, start, acc, data, off, mode)
+        ref = oracle.pnfa_fp64(T, start, acc, data, off)
+        assert err == 0
+        _check(ll, ac, ref, mode, _symbols(data, off, 2), rtol=RTOL[mode] if L == 2048 else None)
+
+
+@pytest.mark.parametrize("sigma", [1, 2])
+@pytest.mark.parametrize("mode", ["bool", "bool8"])
+def test_bool_lane_kernel_small_alphabet(cuda, oracle, sigma, mode):
+    # Boolean NFA with one or two symbols on the lane kernel: bit-exact accept flags and
+    # log(number of active accepting states) against the bit-parallel oracle
+    from trex_b200.workloads import random_bool_nfa
+    rng = np.random.default_rng(40 + sigma)
+    T, start, acc = random_bool_nfa(rng, 64, sigma, density=0.05)
+    T = T.astype(np.float32)
+    n = 90_000
+    lens = rng.integers(0, 24, size=n)
+    lens[:4] = [0, 1, 2, 3]
+    off = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(lens, out=off[1:])
+    data = rng.integers(0, sigma + 1, size=int(off[-1]), dtype=np.uint8)   # byte sigma skipped
+    ll, ac, err = _run(cuda, T, start.astype(np.float32), acc.astype(np.float32), data, off, mode)
+    rfm, ref = oracle.nfa_bool(T != 0, start, acc, data, off, unknown_rejects=False)
+    assert err == 0
+    assert np.array_equal(ac.astype(bool), ref.astype(bool)), np.flatnonzero(ac.astype(bool) != ref.astype(bool))[:8]
+    accmask = np.uint64(sum(1 << int(i) for i in np.flatnonzero(acc)))
+    n_act = np.array([bin(int(m)).count("1") for m in (rfm & accmask)], dtype=np.float64)
+    want = np.where(n_act > 0, np.log(np.maximum(n_act, 1)), -np.inf)
+    assert np.array_equal(np.isfinite(ll), np.isfinite(want))
+    fin = np.isfinite(want)
+    assert np.allclose(ll[fin], want[fin], rtol=0, atol=1e-6)

@@ -1064,6 +1064,414 @@ __global__ void __launch_bounds__(kPnThreads, 1) pnfa_tc_kernel(PnParams P) {
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tbase), "r"(512));
 }
 
+// ---- strings on TMEM lanes (alphabets of at most two symbols) -------------------------------
+// Each of four tiles of 128 strings keeps one string on each TMEM lane: the string's state is
+// row m of the tile's A operand, K = 64 * sigma, with the 64 states in the K range of the
+// string's next symbol and zeros in the other range; B (shared memory) stacks the tables,
+// B[n][64 c + q] = T_c[n][q]. One MMA chain (M = 128, N = 64) then gives every string the
+// product with its own symbol, D[m][n] = (T_c s_m)[n], with no sorting of strings by symbol.
+// The epilogue is thread-local (thread = TMEM lane = string): it reads its 64 states, finds
+// their maximum and rescales by an exact power of two, rounds them to the operand type and
+// writes its next A row with tcgen05.st; at the string's end it forms the log-likelihood and
+// takes the next string from the queue. The MMA warp issues the tiles round robin, so the
+// epilogue of one tile overlaps the products of the others. Hand-offs per tile: `full`
+// (tcgen05.commit, one arrival) and `ready` (the four epilogue warps, after their A rows and a
+// liveness flag are written); every wait is bounded.
+constexpr int kLnTiles = 4;
+constexpr int kLnEpiWarps = 4 * kLnTiles;   // tile T: warps 4T .. 4T + 3 (lane quadrants 0-3)
+constexpr int kLnMmaWarp = kLnEpiWarps;
+constexpr int kLnThreads = 32 * (kLnEpiWarps + 1);
+constexpr int kLnMaxSigma = 2;
+constexpr uint32_t kLnTileCols = 128;       // TMEM columns of a tile: A at 0, D (64 columns) at 64
+constexpr uint32_t kLnLbo = 1024;           // B: bytes between 16-byte K columns (64 rows x 16 B)
+
+struct LnParams {
+    const uint8_t *data;
+    int64_t total_bytes;
+    const int64_t *offsets;
+    int64_t n;
+    const uint16_t *T16;   // [sigma][64][64] row-major in the operand type (probabilistic forms)
+    const float *T32;      // [sigma][64][64] (Boolean forms: a nonzero entry is an edge)
+    const float *start;    // [64]
+    const float *acc;      // [64] accept weights (Boolean forms: 0/1)
+    int sigma;
+    int resc;              // steps between rescales (1 for FP16 operands)
+    long long wait_cycles;
+    double ll_empty;
+    double *loglik;
+    uint8_t *accept;
+    int32_t *accept_i32;
+    unsigned long long *queue;
+    uint32_t *err;
+};
+
+// A string's symbols: aligned 8-byte words of the batch, the next word loaded while this one
+// is used; bytes >= sigma are skipped.
+struct LnSym {
+    uintptr_t p, e;        // next byte, end of the string (addresses)
+    uintptr_t cw;          // address of the word in `cur`
+    uint64_t cur, nxt;
+};
+__device__ __forceinline__ uint64_t ln_word(uintptr_t w, uintptr_t lo, uintptr_t hi) {
+    if (w >= lo && w + 8 <= hi) return __ldg(reinterpret_cast<const unsigned long long *>(w));
+    uint64_t v = 0;
+    for (int k = 0; k < 8; ++k)
+        if (w + k >= lo && w + k < hi) v |= (uint64_t)__ldg(reinterpret_cast<const uint8_t *>(w + k)) << (8 * k);
+    return v;
+}
+// next symbol < sigma of the string, or -1 at its end
+__device__ __forceinline__ int ln_next(LnSym &s, int sigma, uintptr_t lo, uintptr_t hi) {
+    while (s.p < s.e) {
+        const uintptr_t w = s.p & ~(uintptr_t)7;
+        if (w != s.cw) {
+            s.cur = (s.cw != 0 && w == s.cw + 8) ? s.nxt : ln_word(w, lo, hi);
+            s.cw = w;
+            s.nxt = ln_word(w + 8, lo, hi);
+        }
+        const int b = (int)((s.cur >> (8 * (s.p & 7))) & 0xffu);
+        ++s.p;
+        if (b < sigma) return b;
+    }
+    return -1;
+}
+// The next string from the queue (index and byte range); seq = -1 when the queue is empty.
+// Not inlined: a rare path, kept out of the epilogue's registers.
+struct LnRange {
+    int64_t seq, a, b;
+};
+__device__ __noinline__ LnRange ln_take(const LnParams &P) {
+    while (true) {
+        const unsigned long long idx = atomicAdd(P.queue, 1ull);
+        if (idx >= (unsigned long long)P.n) return LnRange{-1, 0, 0};
+        const int64_t a = P.offsets[idx], b = P.offsets[idx + 1];
+        if (a < 0 || b < a || b > P.total_bytes) {
+            atomicOr(P.err, kPnErrOffsets);
+            continue;
+        }
+        return LnRange{(int64_t)idx, a, b};
+    }
+}
+__device__ __noinline__ void ln_empty(const LnParams &P, int64_t seq) {
+    pn_write_result(P.loglik, P.accept, P.accept_i32, seq, P.ll_empty);
+}
+
+// A finished string: log-likelihood from the accept-weighted sum of its last state and its
+// exponent sum.
+__device__ __noinline__ void ln_finish(const LnParams &P, int64_t seq, float dot, int E) {
+    const double ll = dot > 0.f ? log((double)dot) + (double)E * 0.69314718055994530942 : -INFINITY;
+    pn_write_result(P.loglik, P.accept, P.accept_i32, seq, ll);
+}
+
+__device__ __forceinline__ void ln_tmem_st8(uint32_t taddr, const uint32_t (&r)[8]) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};"
+                 :: "r"(taddr), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]),
+                    "r"(r[7])
+                 : "memory");
+}
+
+__device__ __forceinline__ void ln_tmem_ld32(uint32_t taddr, uint32_t *r) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,"
+        "%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+          "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
+          "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]),
+          "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr) : "memory");
+}
+
+// KIND: 0 = BF16, 1 = FP16 operands (kind::f16, FP32 sums, rescaled by exact powers of two);
+// 2 = Boolean 0/1 int8 (kind::i8, int32 sums); 3 = Boolean 0/1 BF16. The Boolean forms
+// threshold every product to {0, 1} (exact).
+template <int KIND>
+__global__ void __launch_bounds__(kLnThreads, 1) pnfa_lane_kernel(LnParams P) {
+    constexpr bool I8 = KIND == 2, BOOL = KIND >= 2, FP16 = KIND == 1;
+    __shared__ __align__(1024) uint8_t s_b[64 * 64 * kLnMaxSigma * 2];
+    __shared__ __align__(8) uint64_t s_bar[2 * kLnTiles];   // full[T], then ready[T]
+    __shared__ uint32_t s_tmem, s_abort;
+    // liveness flags of a tile's four warps per ready phase parity (a warp can write the next
+    // phase's flag while another still reads this phase's)
+    __shared__ uint32_t s_alive[kLnTiles][2][4];
+    __shared__ float s_acc[64], s_start[64];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int sig = P.sigma;
+    const int K = 64 * sig;
+    // B: row n = destination state, K index 64 c + q (symbol c, source state q); 16-byte K
+    // columns kLnLbo bytes apart, rows 16 bytes apart inside 8-row core matrices
+    if constexpr (I8) {
+        for (int t = threadIdx.x; t < 64 * (K / 16); t += blockDim.x) {
+            const int n = t & 63, kc = t >> 6;
+            uint32_t w[4] = {0u, 0u, 0u, 0u};
+            for (int j = 0; j < 16; ++j) {
+                const int k = 16 * kc + j;
+                if (P.T32[((size_t)(k >> 6) * 64 + n) * 64 + (k & 63)] != 0.f) w[j >> 2] |= 1u << (8 * (j & 3));
+            }
+            *reinterpret_cast<uint4 *>(s_b + kc * kLnLbo + (n >> 3) * 128 + (n & 7) * 16) =
+                make_uint4(w[0], w[1], w[2], w[3]);
+        }
+    } else {
+        for (int t = threadIdx.x; t < 64 * (K / 8); t += blockDim.x) {
+            const int n = t & 63, kc = t >> 6;
+            uint32_t w[4];
+            for (int j = 0; j < 4; ++j) {
+                const int k = 8 * kc + 2 * j;   // k and k + 1 belong to the same symbol
+                const size_t o = ((size_t)(k >> 6) * 64 + n) * 64 + (k & 63);
+                uint32_t lo16, hi16;
+                if constexpr (BOOL) {
+                    lo16 = P.T32[o] != 0.f ? 0x3F80u : 0u;   // BF16 1.0
+                    hi16 = P.T32[o + 1] != 0.f ? 0x3F80u : 0u;
+                } else {
+                    lo16 = P.T16[o];
+                    hi16 = P.T16[o + 1];
+                }
+                w[j] = lo16 | (hi16 << 16);
+            }
+            *reinterpret_cast<uint4 *>(s_b + kc * kLnLbo + (n >> 3) * 128 + (n & 7) * 16) =
+                make_uint4(w[0], w[1], w[2], w[3]);
+        }
+    }
+    if (threadIdx.x < 64) {
+        s_acc[threadIdx.x] = P.acc[threadIdx.x];
+        s_start[threadIdx.x] = P.start[threadIdx.x];
+    }
+    if (threadIdx.x == 0) {
+        s_abort = 0u;
+        for (int T = 0; T < kLnTiles; ++T) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(pn_smem_u32(&s_bar[T])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;" :: "r"(pn_smem_u32(&s_bar[kLnTiles + T])));
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == kLnMmaWarp) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(pn_smem_u32(&s_tmem)), "r"(512));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    pn_fence_async_smem();   // B, written by these stores, is read by the tensor cores
+    pn_tc_before();
+    __syncthreads();
+    pn_tc_after();
+    const uint32_t tbase = *reinterpret_cast<volatile uint32_t *>(&s_tmem);
+    volatile uint32_t *abort_flag = &s_abort;
+    if (warp < kLnEpiWarps) {
+        const int T = warp >> 2, qd = warp & 3;
+        const uint32_t tA = tbase + ((uint32_t)(32 * qd) << 16) + (uint32_t)T * kLnTileCols;
+        const uint32_t tD = tA + 64u;
+        const uint32_t bar_full = pn_smem_u32(&s_bar[T]), bar_ready = pn_smem_u32(&s_bar[kLnTiles + T]);
+        const uintptr_t lo = reinterpret_cast<uintptr_t>(P.data), hi = lo + (uintptr_t)P.total_bytes;
+        LnSym sy{0, 0, 0, 0, 0};
+        int64_t seq = -1;
+        int c = 0, E = 0, since = 0;
+        // the next string with its first symbol in c (strings with no symbol get their result
+        // at once); false when the queue is empty
+        auto fetch = [&]() -> bool {
+            while (true) {
+                const LnRange r = ln_take(P);
+                if (r.seq < 0) return false;
+                sy.p = lo + (uintptr_t)r.a;
+                sy.e = lo + (uintptr_t)r.b;
+                sy.cw = 0;
+                c = ln_next(sy, sig, lo, hi);
+                if (c >= 0) {
+                    seq = r.seq;
+                    return true;
+                }
+                ln_empty(P, r.seq);
+            }
+        };
+        bool live = fetch();
+        // A row chunk j (states 32 j .. 32 j + 31) of this string: in the K range of symbol c, zeros
+        // in the other ranges (tcgen05.st is warp-wide; each thread supplies its own row)
+        auto store_chunk = [&](int j, const float (&v)[32]) {
+            if constexpr (I8) {
+                uint32_t r[8];
+#pragma unroll
+                for (int k = 0; k < 8; ++k)
+                    r[k] = (v[4 * k] != 0.f ? 1u : 0u) | (v[4 * k + 1] != 0.f ? 0x100u : 0u) |
+                           (v[4 * k + 2] != 0.f ? 0x10000u : 0u) | (v[4 * k + 3] != 0.f ? 0x1000000u : 0u);
+                for (int h = 0; h < sig; ++h) {
+                    uint32_t q[8];
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) q[k] = h == c ? r[k] : 0u;
+                    ln_tmem_st8(tA + 16u * (uint32_t)h + 8u * (uint32_t)j, q);
+                }
+            } else {
+                uint32_t r[16];
+#pragma unroll
+                for (int k = 0; k < 16; ++k) r[k] = pn_pack2<FP16>(v[2 * k], v[2 * k + 1]);
+                for (int h = 0; h < sig; ++h) {
+                    uint32_t q[16];
+#pragma unroll
+                    for (int k = 0; k < 16; ++k) q[k] = h == c ? r[k] : 0u;
+                    pn_tmem_st16(tA + 32u * (uint32_t)h + 16u * (uint32_t)j, q);
+                }
+            }
+        };
+        auto start_chunk = [&](int j, float (&v)[32]) {
+#pragma unroll
+            for (int i = 0; i < 32; ++i) {
+                const float s0 = s_start[32 * j + i];
+                v[i] = live ? (BOOL ? (s0 != 0.f ? 1.f : 0.f) : s0) : 0.f;
+            }
+        };
+        auto d_value = [&](uint32_t w) -> float {
+            if constexpr (I8) return w != 0u ? 1.f : 0.f;
+            else if constexpr (BOOL) return __uint_as_float(w) > 0.f ? 1.f : 0.f;
+            else return __uint_as_float(w);
+        };
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            float v[32];
+            start_chunk(j, v);
+            store_chunk(j, v);
+        }
+        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+        pn_tc_before();
+        const uint32_t FULL = 0xffffffffu;
+        for (uint32_t ph = 0;; ph ^= 1u) {
+            const uint32_t any_live = __any_sync(FULL, live) ? 1u : 0u;
+            if (lane == 0) {
+                *reinterpret_cast<volatile uint32_t *>(&s_alive[T][ph][qd]) = any_live;
+                pn_mbar_arrive(bar_ready);
+            }
+            __syncwarp();
+            // all four warps of the tile have arrived: their flags decide whether it goes on
+            if (!pn_wait(bar_ready, ph, abort_flag, P.err, P.wait_cycles)) break;
+            const volatile uint32_t *fl = s_alive[T][ph];
+            if ((fl[0] | fl[1] | fl[2] | fl[3]) == 0u) break;
+            if (!pn_wait(bar_full, ph, abort_flag, P.err, P.wait_cycles)) break;
+            pn_tc_after();
+            // D row = this string's state after its symbol; what comes next
+            const int nc = live ? ln_next(sy, sig, lo, hi) : -1;
+            const bool ending = live && nc < 0;
+            bool resc_now = false;
+            if (live && !ending) {
+                c = nc;
+                if (!BOOL && ++since >= P.resc) {
+                    since = 0;
+                    resc_now = true;
+                }
+            }
+            bool from_d = live && !ending;
+            float sc = 1.f;
+            if (__any_sync(FULL, ending || resc_now)) {   // pass 1: the row's maximum, accept sum
+                float m = 0.f, dot = 0.f;
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    uint32_t d[32];
+                    ln_tmem_ld32(tD + 32u * (uint32_t)j, d);
+                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                    for (int i = 0; i < 32; ++i) {
+                        const float v = d_value(d[i]);
+                        m = fmaxf(m, fabsf(v));
+                        dot = fmaf(s_acc[32 * j + i], v, dot);
+                    }
+                }
+                if (ending) {   // the string's log-likelihood, then the next string
+                    ln_finish(P, seq, dot, E);
+                    live = fetch();
+                    E = 0;
+                    since = 0;
+                } else if (resc_now) {   // exact power-of-two rescale
+                    int f = pn_ceil_exp(m);
+                    f = min(max(f, -125), 125);
+                    sc = pn_pow2(-f);
+                    E += f;
+                }
+            }
+            if (!live) c = 0;
+            // pass 2: the next A row, 32 states at a time
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                uint32_t d[32];
+                ln_tmem_ld32(tD + 32u * (uint32_t)j, d);
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                float v[32];
+                if (from_d) {
+#pragma unroll
+                    for (int i = 0; i < 32; ++i) v[i] = d_value(d[i]) * sc;
+                } else {
+                    start_chunk(j, v);
+                }
+                store_chunk(j, v);
+            }
+            asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+            pn_tc_before();
+        }
+    } else {
+        // MMA issuer: the tiles round robin, one K chain (4 sigma K16 or 2 sigma K32 steps) each
+        const uint32_t fmt = KIND == 1 ? 0u : 1u;
+        const uint32_t idesc = I8 ? ((2u << 4) | ((64u >> 3) << 17) | ((128u >> 4) << 24))
+                                  : ((1u << 4) | (fmt << 7) | (fmt << 10) | ((64u >> 3) << 17) |
+                                     ((128u >> 4) << 24));
+        const uint32_t sb = pn_smem_u32(s_b);
+        const int nk = I8 ? 2 * sig : 4 * sig;
+        uint32_t done = 0u, phs = 0u, pend = 0u;
+        bool aborted = false;
+        while (done != (1u << kLnTiles) - 1u && !aborted) {
+            for (int T = 0; T < kLnTiles; ++T) {
+                if ((done >> T) & 1u) continue;
+                if (!pn_wait(pn_smem_u32(&s_bar[kLnTiles + T]), (phs >> T) & 1u, abort_flag, P.err, P.wait_cycles)) {
+                    aborted = true;
+                    break;
+                }
+                pn_tc_after();
+                const volatile uint32_t *fl = s_alive[T][(phs >> T) & 1u];
+                phs ^= 1u << T;
+                pend &= ~(1u << T);   // the epilogue has read the previous product
+                if ((fl[0] | fl[1] | fl[2] | fl[3]) == 0u) {
+                    done |= 1u << T;
+                    continue;
+                }
+                if (lane == 0) {
+                    const uint32_t tA = tbase + (uint32_t)T * kLnTileCols, tD = tA + 64u;
+                    for (int kk = 0; kk < nk; ++kk) {
+                        const uint32_t saddr = sb + (uint32_t)kk * 2u * kLnLbo;
+                        const uint64_t desc = (uint64_t)(((saddr >> 4) & 0x3FFFu) | ((kLnLbo >> 4) << 16)) |
+                                              ((uint64_t)((128u >> 4) | (1u << 14)) << 32);
+                        const uint32_t ta = tA + 8u * (uint32_t)kk;
+                        const uint32_t acc = kk > 0;
+                        if constexpr (I8)
+                            asm volatile(
+                                "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                                "tcgen05.mma.cta_group::1.kind::i8 [%0], [%1], %2, %3, p;\n\t}"
+                                :: "r"(tD), "r"(ta), "l"(desc), "r"(idesc), "r"(acc) : "memory");
+                        else
+                            asm volatile(
+                                "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                                "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}"
+                                :: "r"(tD), "r"(ta), "l"(desc), "r"(idesc), "r"(acc) : "memory");
+                    }
+                    asm volatile(
+                        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                        :: "r"(pn_smem_u32(&s_bar[T])) : "memory");
+                }
+                __syncwarp();
+                pend |= 1u << T;
+            }
+        }
+        // a product committed but not read must be complete before the TMEM is freed
+        for (int T = 0; T < kLnTiles; ++T) {
+            if (!((pend >> T) & 1u)) continue;
+            if (lane == 0) {
+                const uint32_t par = ((phs >> T) & 1u) ^ 1u;   // the phase of the last commit
+                const long long t0 = clock64();
+                while (!pn_mbar_test(pn_smem_u32(&s_bar[T]), par)) {
+                    if (clock64() - t0 > kPnDrainCycles) { atomicOr(P.err, kPnErrTimeout); break; }
+                }
+            }
+            __syncwarp();
+        }
+    }
+    pn_tc_before();
+    __syncthreads();
+    pn_tc_after();
+    if (warp == kLnMmaWarp)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tbase), "r"(512));
+}
+
 // ---- plain FP32 form -------------------------------------------------------------------------
 struct PnPlainParams {
     const uint8_t *data;
@@ -1599,6 +2007,38 @@ int trex_pnfa_run(trex_pnfa *h, int mode, const uint8_t *data, const int64_t *of
         const int grid = (int)std::max<int64_t>(1, (warps + kPnPlainWarps - 1) / kPnPlainWarps);
         profile_kernel_begin(st);
         pnfa_plain_kernel<<<grid, kPnPlainWarps * 32, 0, st>>>(Q);
+        profile_kernel_end(st);
+        TREX_CHECK_LAUNCH();
+        return TREX_OK;
+    }
+    if (h->sigma <= kLnMaxSigma) {   // strings on TMEM lanes, no sorting by symbol
+        const int k = mode == TREX_PNFA_FP16 ? 1 : mode == TREX_PNFA_BOOL8 ? 2 : mode == TREX_PNFA_BOOL ? 3 : 0;
+        LnParams Q;
+        Q.data = data;
+        Q.total_bytes = total_bytes;
+        Q.offsets = offsets;
+        Q.n = n_strings;
+        Q.T16 = h->d_T16[k == 1 ? 1 : 0];
+        Q.T32 = h->d_T32;
+        Q.start = h->d_start32;
+        Q.acc = k >= 2 ? h->d_acc_bool : h->d_acc;
+        Q.sigma = h->sigma;
+        Q.resc = k == 0 ? h->tc_resc : 1;
+        Q.wait_cycles = mbar_wait_cycles();
+        Q.ll_empty = k >= 2 ? h->ll_empty_bool : h->ll_empty;
+        Q.loglik = loglik;
+        Q.accept = accept;
+        Q.accept_i32 = accept_i32;
+        Q.queue = queue;
+        Q.err = err;
+        // one CTA an SM (it owns the 512 TMEM columns), 512 strings in flight each
+        const int grid = (int)std::max<int64_t>(
+            1, std::min<int64_t>((n_strings + kLnTiles * 128 - 1) / (kLnTiles * 128), (int64_t)h->n_sms));
+        profile_kernel_begin(st);
+        if (k == 1) pnfa_lane_kernel<1><<<grid, kLnThreads, 0, st>>>(Q);
+        else if (k == 2) pnfa_lane_kernel<2><<<grid, kLnThreads, 0, st>>>(Q);
+        else if (k == 3) pnfa_lane_kernel<3><<<grid, kLnThreads, 0, st>>>(Q);
+        else pnfa_lane_kernel<0><<<grid, kLnThreads, 0, st>>>(Q);
         profile_kernel_end(st);
         TREX_CHECK_LAUNCH();
         return TREX_OK;
