@@ -201,12 +201,13 @@ def test_bool_mode_small_nfa_both_outcomes(cuda, oracle, mode):
     assert np.array_equal(ac.astype(bool), ref.astype(bool))
 
 
-@pytest.mark.parametrize("sigma", [1, 2])
+@pytest.mark.parametrize("sigma", [1, 2, 3, 4])
 @pytest.mark.parametrize("mode", ["bf16", "fp16"])
 def test_pnfa_lane_kernel_small_alphabet(cuda, oracle, sigma, mode):
-    # alphabets of at most two symbols run one string a TMEM lane (no sorting by symbol):
+    # alphabets of at most four symbols run one string a TMEM lane (no sorting by symbol):
     # ragged and empty strings, bytes >= sigma skipped, more strings than the launch has
-    # lanes (148 x 512), so lanes take several strings one after another
+    # lanes (148 x 512 for two symbols; fewer tiles for three and four), so lanes take
+    # several strings one after another
     rng = np.random.default_rng(20 + sigma)
     T, start, acc = random_prob_nfa(rng, 64, sigma)
     n = 100_000
@@ -236,10 +237,10 @@ def test_pnfa_lane_kernel_long_and_few(cuda, oracle, mode):
         _check(ll, ac, ref, mode, _symbols(data, off, 2), rtol=RTOL[mode] if L == 2048 else None)
 
 
-@pytest.mark.parametrize("sigma", [1, 2])
+@pytest.mark.parametrize("sigma", [1, 2, 3, 4])
 @pytest.mark.parametrize("mode", ["bool", "bool8"])
 def test_bool_lane_kernel_small_alphabet(cuda, oracle, sigma, mode):
-    # Boolean NFA with one or two symbols on the lane kernel: bit-exact accept flags and
+    # Boolean NFA with one to four symbols on the lane kernel: bit-exact accept flags and
     # log(number of active accepting states) against the bit-parallel oracle
     from trex_b200.workloads import random_bool_nfa
     rng = np.random.default_rng(40 + sigma)

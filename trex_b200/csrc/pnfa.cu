@@ -1080,9 +1080,9 @@ __global__ void __launch_bounds__(kPnThreads, 1) pnfa_tc_kernel(PnParams P) {
 constexpr int kLnTiles = 4;
 constexpr int kLnEpiWarps = 4 * kLnTiles;   // tile T: warps 4T .. 4T + 3 (lane quadrants 0-3)
 constexpr int kLnMmaWarp = kLnEpiWarps;
-constexpr int kLnThreads = 32 * (kLnEpiWarps + 1);
-constexpr int kLnMaxSigma = 2;
-constexpr uint32_t kLnTileCols = 128;       // TMEM columns of a tile: A at 0, D (64 columns) at 64
+constexpr int kLnMmaWarps = 2;         // issuers: warp kLnMmaWarp + i takes tiles i, i + 2
+constexpr int kLnThreads = 32 * (kLnEpiWarps + kLnMmaWarps);
+constexpr int kLnMaxSigma = 4;
 constexpr uint32_t kLnLbo = 1024;           // B: bytes between 16-byte K columns (64 rows x 16 B)
 
 struct LnParams {
@@ -1095,6 +1095,9 @@ struct LnParams {
     const float *start;    // [64]
     const float *acc;      // [64] accept weights (Boolean forms: 0/1)
     int sigma;
+    int tiles;             // tiles in flight: as many of kLnTiles as fit in the 512 TMEM columns
+    uint32_t a_cols;       // TMEM columns of a tile's A (32 sigma, int8: 16 sigma); D follows
+    uint32_t tile_cols;    // a_cols + 64, rounded up to 32
     int resc;              // steps between rescales (1 for FP16 operands)
     long long wait_cycles;
     double ll_empty;
@@ -1194,6 +1197,7 @@ __global__ void __launch_bounds__(kLnThreads, 1) pnfa_lane_kernel(LnParams P) {
     // phase's flag while another still reads this phase's)
     __shared__ uint32_t s_alive[kLnTiles][2][4];
     __shared__ float s_acc[64], s_start[64];
+    __shared__ uint32_t s_start8[16];   // int8 Boolean form: the start set, four states a word
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int sig = P.sigma;
     const int K = 64 * sig;
@@ -1235,6 +1239,11 @@ __global__ void __launch_bounds__(kLnThreads, 1) pnfa_lane_kernel(LnParams P) {
         s_acc[threadIdx.x] = P.acc[threadIdx.x];
         s_start[threadIdx.x] = P.start[threadIdx.x];
     }
+    if (threadIdx.x < 16) {
+        uint32_t w = 0u;
+        for (int b = 0; b < 4; ++b) w |= (P.start[4 * threadIdx.x + b] != 0.f ? 1u : 0u) << (8 * b);
+        s_start8[threadIdx.x] = w;
+    }
     if (threadIdx.x == 0) {
         s_abort = 0u;
         for (int T = 0; T < kLnTiles; ++T) {
@@ -1254,10 +1263,10 @@ __global__ void __launch_bounds__(kLnThreads, 1) pnfa_lane_kernel(LnParams P) {
     pn_tc_after();
     const uint32_t tbase = *reinterpret_cast<volatile uint32_t *>(&s_tmem);
     volatile uint32_t *abort_flag = &s_abort;
-    if (warp < kLnEpiWarps) {
+    if (warp < kLnEpiWarps && (warp >> 2) < P.tiles) {   // fewer tiles for larger alphabets
         const int T = warp >> 2, qd = warp & 3;
-        const uint32_t tA = tbase + ((uint32_t)(32 * qd) << 16) + (uint32_t)T * kLnTileCols;
-        const uint32_t tD = tA + 64u;
+        const uint32_t tA = tbase + ((uint32_t)(32 * qd) << 16) + (uint32_t)T * P.tile_cols;
+        const uint32_t tD = tA + P.a_cols;
         const uint32_t bar_full = pn_smem_u32(&s_bar[T]), bar_ready = pn_smem_u32(&s_bar[kLnTiles + T]);
         const uintptr_t lo = reinterpret_cast<uintptr_t>(P.data), hi = lo + (uintptr_t)P.total_bytes;
         LnSym sy{0, 0, 0, 0, 0};
@@ -1388,6 +1397,22 @@ __global__ void __launch_bounds__(kLnThreads, 1) pnfa_lane_kernel(LnParams P) {
                 uint32_t d[32];
                 ln_tmem_ld32(tD + 32u * (uint32_t)j, d);
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                if constexpr (I8) {   // 0/1 bytes straight from the int32 path counts
+                    uint32_t r[8];
+#pragma unroll
+                    for (int k = 0; k < 8; ++k)
+                        r[k] = from_d ? ((d[4 * k] != 0u ? 1u : 0u) | (d[4 * k + 1] != 0u ? 0x100u : 0u) |
+                                         (d[4 * k + 2] != 0u ? 0x10000u : 0u) |
+                                         (d[4 * k + 3] != 0u ? 0x1000000u : 0u))
+                                      : (live ? s_start8[8 * j + k] : 0u);
+                    for (int h = 0; h < sig; ++h) {
+                        uint32_t q[8];
+#pragma unroll
+                        for (int k = 0; k < 8; ++k) q[k] = h == c ? r[k] : 0u;
+                        ln_tmem_st8(tA + 16u * (uint32_t)h + 8u * (uint32_t)j, q);
+                    }
+                    continue;
+                }
                 float v[32];
                 if (from_d) {
 #pragma unroll
@@ -1400,18 +1425,24 @@ __global__ void __launch_bounds__(kLnThreads, 1) pnfa_lane_kernel(LnParams P) {
             asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
             pn_tc_before();
         }
-    } else {
-        // MMA issuer: the tiles round robin, one K chain (4 sigma K16 or 2 sigma K32 steps) each
+    } else if (warp >= kLnEpiWarps) {
+        // MMA issuers: each its tiles round robin, one K chain (4 sigma K16 or 2 sigma K32 steps)
+        // each (two issuing threads: one alone spends ~135 cycles an instruction)
         const uint32_t fmt = KIND == 1 ? 0u : 1u;
         const uint32_t idesc = I8 ? ((2u << 4) | ((64u >> 3) << 17) | ((128u >> 4) << 24))
                                   : ((1u << 4) | (fmt << 7) | (fmt << 10) | ((64u >> 3) << 17) |
                                      ((128u >> 4) << 24));
         const uint32_t sb = pn_smem_u32(s_b);
+        const uint64_t desc0 = (uint64_t)(((sb >> 4) & 0x3FFFu) | ((kLnLbo >> 4) << 16)) |
+                               ((uint64_t)((128u >> 4) | (1u << 14)) << 32);
         const int nk = I8 ? 2 * sig : 4 * sig;
+        const int mw = warp - kLnMmaWarp;
         uint32_t done = 0u, phs = 0u, pend = 0u;
+        for (int T = 0; T < kLnTiles; ++T)
+            if (T % kLnMmaWarps != mw || T >= P.tiles) done |= 1u << T;
         bool aborted = false;
         while (done != (1u << kLnTiles) - 1u && !aborted) {
-            for (int T = 0; T < kLnTiles; ++T) {
+            for (int T = mw; T < kLnTiles; T += kLnMmaWarps) {
                 if ((done >> T) & 1u) continue;
                 if (!pn_wait(pn_smem_u32(&s_bar[kLnTiles + T]), (phs >> T) & 1u, abort_flag, P.err, P.wait_cycles)) {
                     aborted = true;
@@ -1426,11 +1457,11 @@ __global__ void __launch_bounds__(kLnThreads, 1) pnfa_lane_kernel(LnParams P) {
                     continue;
                 }
                 if (lane == 0) {
-                    const uint32_t tA = tbase + (uint32_t)T * kLnTileCols, tD = tA + 64u;
+                    // K step kk: B 2 kLnLbo bytes further (+128 in the descriptor's start field,
+                    // which stays below 2^14 for shared addresses), A 8 TMEM columns further
+                    const uint32_t tA = tbase + (uint32_t)T * P.tile_cols, tD = tA + P.a_cols;
                     for (int kk = 0; kk < nk; ++kk) {
-                        const uint32_t saddr = sb + (uint32_t)kk * 2u * kLnLbo;
-                        const uint64_t desc = (uint64_t)(((saddr >> 4) & 0x3FFFu) | ((kLnLbo >> 4) << 16)) |
-                                              ((uint64_t)((128u >> 4) | (1u << 14)) << 32);
+                        const uint64_t desc = desc0 + (uint64_t)(128u * (uint32_t)kk);
                         const uint32_t ta = tA + 8u * (uint32_t)kk;
                         const uint32_t acc = kk > 0;
                         if constexpr (I8)
@@ -2011,7 +2042,7 @@ int trex_pnfa_run(trex_pnfa *h, int mode, const uint8_t *data, const int64_t *of
         TREX_CHECK_LAUNCH();
         return TREX_OK;
     }
-    if (h->sigma <= kLnMaxSigma) {   // strings on TMEM lanes, no sorting by symbol
+    if (h->sigma <= kLnMaxSigma) {   // strings on TMEM lanes, no sorting by symbol (sigma <= 4)
         const int k = mode == TREX_PNFA_FP16 ? 1 : mode == TREX_PNFA_BOOL8 ? 2 : mode == TREX_PNFA_BOOL ? 3 : 0;
         LnParams Q;
         Q.data = data;
@@ -2023,6 +2054,9 @@ int trex_pnfa_run(trex_pnfa *h, int mode, const uint8_t *data, const int64_t *of
         Q.start = h->d_start32;
         Q.acc = k >= 2 ? h->d_acc_bool : h->d_acc;
         Q.sigma = h->sigma;
+        Q.a_cols = (uint32_t)(k == 2 ? 16 : 32) * (uint32_t)h->sigma;
+        Q.tile_cols = (Q.a_cols + 64u + 31u) & ~31u;
+        Q.tiles = (int)std::min<uint32_t>((uint32_t)kLnTiles, 512u / Q.tile_cols);
         Q.resc = k == 0 ? h->tc_resc : 1;
         Q.wait_cycles = mbar_wait_cycles();
         Q.ll_empty = k >= 2 ? h->ll_empty_bool : h->ll_empty;
@@ -2031,9 +2065,10 @@ int trex_pnfa_run(trex_pnfa *h, int mode, const uint8_t *data, const int64_t *of
         Q.accept_i32 = accept_i32;
         Q.queue = queue;
         Q.err = err;
-        // one CTA an SM (it owns the 512 TMEM columns), 512 strings in flight each
+        // one CTA an SM (it owns the 512 TMEM columns), 128 strings in flight a tile
+        const int64_t per_cta = (int64_t)Q.tiles * 128;
         const int grid = (int)std::max<int64_t>(
-            1, std::min<int64_t>((n_strings + kLnTiles * 128 - 1) / (kLnTiles * 128), (int64_t)h->n_sms));
+            1, std::min<int64_t>((n_strings + per_cta - 1) / per_cta, (int64_t)h->n_sms));
         profile_kernel_begin(st);
         if (k == 1) pnfa_lane_kernel<1><<<grid, kLnThreads, 0, st>>>(Q);
         else if (k == 2) pnfa_lane_kernel<2><<<grid, kLnThreads, 0, st>>>(Q);
