@@ -312,8 +312,12 @@ void trex_pnfa_destroy(trex_pnfa *pnfa);
  * TREX_PNFA_BOOL8: the same Boolean NFA with 0/1 int8 operands and int32
  * sums (tcgen05 kind::i8: K = 32 an instruction, so half the MMA
  * instructions of TREX_PNFA_BOOL), thresholded to {0, 1} every step (exact).
+ * The four tensor-core modes run with sigma <= 4 on a kernel that keeps one
+ * string on each TMEM lane (the symbol folded into K: no sorting of strings by
+ * symbol; 2-4x the throughput), above it on the kernel that groups strings by
+ * symbol pair each step; results are the same within each mode's rounding.
  * TREX_PNFA_BF16_CC / TREX_PNFA_FP16_CC: CUDA cores with the 16-bit tables in
- * shared memory and an FP32 state, a warp per string: the low-latency form
+ * shared memory and an FP32 state, four warps per string: the low-latency form
  * for few (possibly long) strings, sigma <= 28. DEVICE buffers;
  * loglik[n] (-inf when the likelihood is 0), accept[n], accept_i32[n]
  * (dot > 0.5) may each be NULL. One run at a time per handle. */
