@@ -103,6 +103,10 @@ def parse_args(argv=None):
     ap.add_argument("--nfa-method", choices=["bitpar", "tc", "tc8"], default="bitpar",
                     help="nfa workload: bit-parallel kernel, or the Boolean NFA on the tensor cores "
                          "with 0/1 BF16 (tc) or int8 (tc8) operands")
+    ap.add_argument("--nfa-sigma", type=int, default=None,
+                    help="nfa / pnfa workloads: alphabet size (default 20)")
+    ap.add_argument("--nfa-len", type=int, default=None,
+                    help="nfa / pnfa workloads: symbols a string (default 4096 / 2048)")
     ap.add_argument("--strings", type=int, default=None, help="override the number of strings")
     ap.add_argument("--seg-len", type=int, default=0, help="bytes per work item / scan tile (0 = default)")
     ap.add_argument("--kgram", type=int, default=None,
