@@ -541,7 +541,9 @@ class PNFAWorkload:
         self.n = args.strings or 65536
         self.L = getattr(args, "nfa_len", None) or 2048
         self.off = np.arange(self.n + 1, dtype=np.int64) * self.L
-        self.kernel = "pnfa_plain_kernel" if self.mode == "fp32" else "pnfa_tc_kernel"
+        # alphabets of at most four symbols run one string a TMEM lane
+        self.kernel = ("pnfa_plain_kernel" if self.mode == "fp32" else
+                       "pnfa_lane_kernel" if self.sigma <= 4 else "pnfa_tc_kernel")
         self.dtype = {"bf16": "bf16", "fp16": "f16", "fp32": "f32"}[self.mode]
         self.workload = (f"probabilistic NFA: 64 states, {self.sigma} symbols (bytes 0..{self.sigma - 1}), rows of T[c] "
                          "Dirichlet(0.5) x 0.9 with ~30% kept, start e0, accept all states; "
@@ -671,7 +673,7 @@ class NFATcWorkload(PNFAWorkload):
         self.n = args.strings or 262144
         self.L = getattr(args, "nfa_len", None) or 4096
         self.off = np.arange(self.n + 1, dtype=np.int64) * self.L
-        self.kernel = "pnfa_tc_kernel"
+        self.kernel = "pnfa_lane_kernel" if self.sigma <= 4 else "pnfa_tc_kernel"
         self.dtype = "s8" if self.mode == "bool8" else "bf16"
         ops = ("0/1 int8 operands, int32 sums (tcgen05 kind::i8)" if self.mode == "bool8"
                else "0/1 BF16 operands, FP32 sums (tcgen05 kind::f16)")

@@ -278,6 +278,29 @@ __device__ __forceinline__ bool pn_wait(uint32_t addr, uint32_t parity, volatile
     return ok != 0;
 }
 
+// pn_wait with the suspending test: a thread whose phase is not complete may be parked by the
+// hardware instead of spinning, which leaves the issue slots to the warps with work (the lane
+// kernel, whose warps wait a large share of each step)
+__device__ __forceinline__ bool pn_wait_park(uint32_t addr, uint32_t parity, volatile uint32_t *abort_flag,
+                                             uint32_t *err, long long limit) {
+    int ok = 1;
+    if ((threadIdx.x & 31) == 0) {
+        const long long t0 = clock64();
+        while (!pn_mbar_test(addr, parity)) {
+            if (*abort_flag) { ok = 0; break; }
+            if (clock64() - t0 > limit) {
+                atomicOr(err, kPnErrTimeout);
+                *abort_flag = 1u;
+                ok = 0;
+                break;
+            }
+        }
+    }
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    __syncwarp();
+    return ok != 0;
+}
+
 __device__ __forceinline__ void pn_write_result(double *loglik, uint8_t *accept, int32_t *accept_i32,
                                                 int64_t seq, double ll) {
     if (loglik) loglik[seq] = ll;
@@ -1346,10 +1369,10 @@ __global__ void __launch_bounds__(kLnThreads, 1) pnfa_lane_kernel(LnParams P) {
             }
             __syncwarp();
             // all four warps of the tile have arrived: their flags decide whether it goes on
-            if (!pn_wait(bar_ready, ph, abort_flag, P.err, P.wait_cycles)) break;
+            if (!pn_wait_park(bar_ready, ph, abort_flag, P.err, P.wait_cycles)) break;
             const volatile uint32_t *fl = s_alive[T][ph];
             if ((fl[0] | fl[1] | fl[2] | fl[3]) == 0u) break;
-            if (!pn_wait(bar_full, ph, abort_flag, P.err, P.wait_cycles)) break;
+            if (!pn_wait_park(bar_full, ph, abort_flag, P.err, P.wait_cycles)) break;
             pn_tc_after();
             // D row = this string's state after its symbol; what comes next
             const int nc = live ? ln_next(sy, sig, lo, hi) : -1;
@@ -1444,7 +1467,7 @@ __global__ void __launch_bounds__(kLnThreads, 1) pnfa_lane_kernel(LnParams P) {
         while (done != (1u << kLnTiles) - 1u && !aborted) {
             for (int T = mw; T < kLnTiles; T += kLnMmaWarps) {
                 if ((done >> T) & 1u) continue;
-                if (!pn_wait(pn_smem_u32(&s_bar[kLnTiles + T]), (phs >> T) & 1u, abort_flag, P.err, P.wait_cycles)) {
+                if (!pn_wait_park(pn_smem_u32(&s_bar[kLnTiles + T]), (phs >> T) & 1u, abort_flag, P.err, P.wait_cycles)) {
                     aborted = true;
                     break;
                 }
