@@ -26,7 +26,7 @@ def _run_set(torch, dfas, data, off, ids=None, seg_len=0):
     return fs.cpu().numpy(), ac.cpu().numpy(), err
 
 
-@pytest.mark.parametrize("n_states", [1, 2, 5, 8, 9, 12, 16, 17, 100, 255])
+@pytest.mark.parametrize("n_states", [1, 2, 5, 8, 9, 12, 16, 17, 24, 32, 48, 64, 65, 100, 255])
 def test_random_dfa_matches_oracle(cuda, oracle, n_states):
     rng = np.random.default_rng(100 + n_states)
     d = random_dfa(n_states, np.arange(256), rng)
@@ -63,6 +63,46 @@ def test_segment_maps_compose_exactly(cuda, oracle, seg_len):
     assert err == 0
     assert np.array_equal(fs, rfs)
     assert np.array_equal(ac, rac)
+
+
+@pytest.mark.parametrize("n_states", [32, 64])
+@pytest.mark.parametrize("seg_len", [64, 1000])
+def test_split_strings_large_automata(cuda, oracle, n_states, seg_len):
+    # Automata of 17 to 64 states have their strings cut too (warm-up 4 N bytes); a
+    # permutation automaton of as many states never synchronises, so its fix-ups never meet
+    # and the string is walked again from that item (one lane through the global byte map).
+    rng = np.random.default_rng(n_states + seg_len)
+    from trex_b200.workloads import ByteDFA
+    perm = np.stack([rng.permutation(n_states) for _ in range(256)]).astype(np.uint8)
+    acc = np.zeros(n_states, np.uint8)
+    acc[[1, n_states - 2]] = 1
+    dfas = [random_dfa(n_states, np.arange(256), rng),
+            ByteDFA(n_states, np.ascontiguousarray(perm.reshape(-1)), acc, start=3)]
+    lens = rng.integers(0, 30000, size=80)
+    lens[:4] = [0, 1, 31, 33]
+    off = np.zeros(len(lens) + 1, dtype=np.int64)
+    np.cumsum(lens, out=off[1:])
+    data = rng.integers(0, 256, size=int(off[-1]), dtype=np.uint8)
+    ids = (np.arange(len(lens)) % 2).astype(np.int32)
+    fs, ac, err = _run_set(cuda, dfas, data, off, ids, seg_len=seg_len)
+    rfs, rac = oracle.dfa_walk([d.tmap for d in dfas], [d.n_states for d in dfas],
+                               [d.start for d in dfas], [d.accept for d in dfas], data, off, ids)
+    assert err == 0
+    assert np.array_equal(fs, rfs)
+    assert np.array_equal(ac, rac)
+
+
+def test_ragged_batch_mixed_sizes_to_64(cuda, oracle):
+    rng = np.random.default_rng(64)
+    sizes = (8, 12, 16, 24, 32, 48, 64, 64)
+    dfas = [random_dfa(n, np.arange(256), rng) for n in sizes]
+    data, off, ids, _ = ragged_batch(12000, rng, median=1024, hi=30000)
+    ids = (ids % len(sizes)).astype(np.int32)
+    fs, ac, err = _run_set(cuda, dfas, data, off, ids, seg_len=512)
+    rfs, rac = oracle.dfa_walk([d.tmap for d in dfas], [d.n_states for d in dfas],
+                               [0] * len(sizes), [d.accept for d in dfas], data, off, ids)
+    assert err == 0
+    assert np.array_equal(fs, rfs) and np.array_equal(ac, rac)
 
 
 @pytest.mark.parametrize("n_states", [8, 12, 100])

@@ -54,16 +54,20 @@ struct WorkItem {
 };
 constexpr int64_t kMaxItemsPerString = 65535;
 constexpr int64_t kMaxWalkBytes = (int64_t)1 << 36;   // one item: a 32-bit count of windows
-// Warm-up bytes of an item after the first of its string: one window for
-// automata of at most 8 states, two above (multiples of 32 keep aligned cuts
-// aligned). Two chains of a random N-state automaton merge with probability
-// ~1/N per byte, so the warm-up chain has missed the true entry state with
-// probability (1 - 1/N)^W: 1.4% for N = 8 (W = 32), 0.4% for N = 12 and 1.6%
-// for N = 16 (W = 64). When it has, the item's checkpoints (its chain's state
-// 1, 2, 4 and 8 windows into its own bytes) let compose_fix_kernel walk from the
-// true entry state only until the two chains meet (about one window).
+// Warm-up bytes of an item after the first of its string: 4 N rounded up to
+// whole 32-byte windows (multiples of 32 keep aligned cuts aligned), at most
+// seven windows (the record keeps the warm-up length in 8 bits). Two chains of
+// a random N-state automaton merge with probability ~1/N per byte, so the
+// warm-up chain has missed the true entry state with probability
+// (1 - 1/N)^W: 1.4% for N = 8 (W = 32), 0.4% for N = 12 and 1.6% for N = 16
+// (W = 64), 1.8% for N = 32 (W = 128), 2.9% for N = 64 (W = 224). When it has,
+// the item's checkpoints (its chain's state 1, 2, 4 and 8 windows into its own
+// bytes) let compose_fix_kernel walk from the true entry state only until the
+// two chains meet (about N bytes).
+constexpr int kSplitDfaStates = 64;   // strings of larger automata are not cut
 __host__ __device__ __forceinline__ int64_t warm_bytes(int n_states, int64_t seg) {
-    const int64_t w = n_states <= 8 ? 32 : 64;
+    int64_t w = ((4 * (int64_t)n_states + 31) / 32) * 32;
+    w = w < 32 ? 32 : w > 224 ? 224 : w;
     return w < seg ? w : seg;
 }
 
@@ -140,15 +144,15 @@ static ScratchLayout scratch_layout(int64_t n_strings, int64_t total_bytes, int3
 // address, the others seg bytes (a multiple of 32), the last the rest; so an
 // item after the first starts its warm-up, its own bytes and (but the last) its
 // end on window boundaries. seg grows for strings that would need more than
-// kMaxItemsPerString items; strings of automata with more than 16 states are
-// never cut.
+// kMaxItemsPerString items; strings of automata with more than kSplitDfaStates
+// states are never cut.
 struct ItemGeom {
     uint32_t k;
     int64_t seg, first;
 };
 __device__ __forceinline__ ItemGeom item_geom(int64_t len, int64_t s0, int n_states, int32_t seg_len,
                                               uint32_t base_mis) {
-    if (len <= 0 || n_states > kSmallDfaStates) return ItemGeom{1, len, len};
+    if (len <= 0 || n_states > kSplitDfaStates) return ItemGeom{1, len, len};
     int64_t seg = seg_len;
     if ((len + seg - 1) / seg > kMaxItemsPerString)
         seg = (((len + kMaxItemsPerString - 1) / kMaxItemsPerString) + 31) & ~(int64_t)31;
@@ -1376,6 +1380,10 @@ __global__ void __launch_bounds__(kRaggedThreads, 1) dfa_ragged_kernel(RaggedPar
             drain(P, ByteMode<Walker<8>>{Walker<8>{lane}}, D, d);
         } else if (D.n_states <= 16) {
             drain(P, ByteMode<Walker<16>>{Walker<16>{lane}}, D, d);
+        } else if (D.n_states <= 32) {
+            drain(P, ByteMode<Walker<32>>{Walker<32>{lane}}, D, d);
+        } else if (D.n_states <= 64) {
+            drain(P, ByteMode<Walker<64>>{Walker<64>{lane}}, D, d);
         } else {
             drain(P, ByteMode<Walker<0>>{Walker<0>{(uint32_t)D.n_states}}, D, d);
         }
@@ -1454,10 +1462,13 @@ constexpr int kComposeThreads = 256;
 __device__ __forceinline__ uint32_t lane_walk(const RaggedParams &P, const uint8_t *__restrict__ tm,
                                               uint32_t N, int64_t p, int64_t q, uint32_t s) {
     const uint8_t *lo = P.data + p, *hi = P.data + q;
-    for (const uint8_t *w = reinterpret_cast<const uint8_t *>((uintptr_t)lo & ~(uintptr_t)31); w < hi;
-         w += 32) {
-        uint4 a, b;
-        load_window(w, lo, hi, a, b);
+    const uint8_t *w = reinterpret_cast<const uint8_t *>((uintptr_t)lo & ~(uintptr_t)31);
+    uint4 na = make_uint4(0u, 0u, 0u, 0u), nb = na;
+    if (w < hi) load_window(w, lo, hi, na, nb);
+    for (; w < hi; w += 32) {
+        // the next window is loaded while this one is walked
+        const uint4 a = na, b = nb;
+        if (w + 32 < hi) load_window(w + 32, lo, hi, na, nb);
         const uint32_t x[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
 #pragma unroll
         for (int j = 0; j < 32; ++j)
@@ -1472,8 +1483,9 @@ __device__ __forceinline__ uint32_t lane_walk(const RaggedParams &P, const uint8
 // bytes); from there the two chains are one, so the item ends in the recorded
 // end state. Returns the item's end state, or 0xFFFF when the chains had not
 // met by the last checkpoint (the caller then walks the item whole).
-__device__ __noinline__ uint32_t fix_item(const RaggedParams &P, const uint8_t *__restrict__ tm, uint32_t N,
-                                          int64_t b0, int64_t b1, uint32_t s_in, uint64_t rec) {
+__device__ __forceinline__ uint32_t fix_item_body(const RaggedParams &P, const uint8_t *__restrict__ tm,
+                                                  uint32_t N, int64_t b0, int64_t b1, uint32_t s_in,
+                                                  uint64_t rec) {
     // the item's own bytes start on a window boundary (aligned cuts, whole-window warm-up)
     const int64_t a0 = b0 - (int64_t)((P.base_mis + (uint32_t)b0) & 31u);
     int64_t p = b0;
@@ -1486,6 +1498,12 @@ __device__ __noinline__ uint32_t fix_item(const RaggedParams &P, const uint8_t *
         p = q;
     }
     return 0xFFFFu;
+}
+// Not inlined into the fix-up kernel's loop (keeps its registers); the re-walk
+// path inlines the body instead.
+__device__ __noinline__ uint32_t fix_item(const RaggedParams &P, const uint8_t *__restrict__ tm, uint32_t N,
+                                          int64_t b0, int64_t b1, uint32_t s_in, uint64_t rec) {
+    return fix_item_body(P, tm, N, b0, b1, s_in, rec);
 }
 
 // Index in a device list, with one atomic per group of lanes that append together.
@@ -1610,6 +1628,33 @@ __global__ void __launch_bounds__(kComposeThreads) compose_fix_kernel(RaggedPara
     }
 }
 
+// The re-walk of a split string of an automaton of more than 16 states, by one
+// lane through the byte map in global memory: item jb (its fix-up never met the
+// recorded chain) is walked whole from s_entry; each later item takes its
+// recorded end state when its guess is the true entry, else a fix-up, and is
+// walked whole only when that does not meet either, so a lane walks about one
+// item, not the rest of the string.
+__device__ __noinline__ void rewalk_lane(const RaggedParams &P, const ItemGeom &g, int64_t s0, int64_t len,
+                                         int d, uint32_t N, uint32_t mb, uint32_t k, uint32_t jb,
+                                         uint32_t s_entry, uint32_t str, uint32_t aoff) {
+    const uint8_t *tm = P.tmaps + P.desc[d].tmap_off;
+    uint32_t s = s_entry;
+    for (uint32_t j = jb; j < k && s < N; ++j) {
+        int64_t b0, b1;
+        item_range(g, s0, len, j, &b0, &b1);
+        uint32_t f = 0xFFFFu;
+        bool known = false;
+        if (j > jb) {
+            const uint64_t rec = P.maps[mb + j];
+            known = ((uint32_t)rec & 0xffu) == s;
+            f = known ? ((uint32_t)(rec >> 8) & 0xffu) : fix_item_body(P, tm, N, b0, b1, s, rec);
+        }
+        s = (known || f != 0xFFFFu) ? f : lane_walk(P, tm, N, b0, b1, s);
+    }
+    if (s < N) write_result(P, str, s, aoff);
+    else atomicOr(P.err, kErrCapacity);   // records not written by this plan
+}
+
 // Step 3 of 3, a warp per string on the re-walk list: walks the marked item again
 // whole from its entry state (each lane maps all N states over 1/32 of the item),
 // then checks the following records 32 at a time, walking again every item whose
@@ -1637,6 +1682,11 @@ __global__ void __launch_bounds__(kComposeThreads) compose_rewalk_kernel(RaggedP
             g = item_geom(len, s0, (int)N, P.seg_len, P.base_mis);
         if (g.k != k || jb >= k) {   // offsets changed since the plan
             if (lane == 0) atomicOr(P.err, kErrCapacity);
+            continue;
+        }
+        if (N > (uint32_t)kSmallDfaStates) {   // the warp re-walk maps at most 16 states
+            if (lane == 0) rewalk_lane(P, g, s0, len, d, N, mb, k, jb, s_entry, ent.x, ent.w);
+            __syncwarp();
             continue;
         }
         auto rewalk = [&](uint32_t jw, uint32_t s_in) {

@@ -11,7 +11,15 @@
 //   N <= 16  byte address = c<<9 | (s>>2)<<7 | lane<<2 | (s&3)       128 KiB
 //            stored byte  = (s'&3) | (s'>>2)<<6: a step is PRMT, LOP3, IADD3,
 //            LDS.U8 (t = e | c<<8; addr = t + (t & 0xFFC0) + lane*4).
-//   N <= 256 plain tmap[c*N + s] (bank conflicts; strings are never split).
+//   N <= 32  byte address = c<<9 | (s>>2)<<6 | (lane&15)<<2 | (s&3)  128 KiB
+//            (16 replicas: lanes l and l + 16 share one, so at most two-way
+//            bank conflicts); stored byte = (s'&3) | (s'>>2)<<5: a step is
+//            PRMT, LOP3, IADD3, LDS.U8 (addr = t + (t & 0xFFE0) + (lane&15)*4).
+//   N <= 64  byte address = c<<9 | (s>>2)<<5 | (lane&7)<<2 | (s&3)   128 KiB
+//            (8 replicas, a replica for lanes l, l + 8, l + 16, l + 24);
+//            stored byte = (s'&3) | (s'>>2)<<4: the same four-instruction
+//            step with mask 0xFFF0.
+//   N <= 256 plain tmap[c*N + s] (bank conflicts).
 #pragma once
 
 #include "trex_internal.cuh"
@@ -73,6 +81,30 @@ template <> struct Walker<16> {
     }
 };
 
+template <> struct Walker<32> {
+    static constexpr int kChains = 32;
+    uint32_t lane;
+    __device__ uint32_t enc(uint32_t s) const { return (s & 3u) | ((s >> 2) << 5); }
+    __device__ static uint32_t dec(uint32_t e) { return (e & 3u) | ((e >> 5) << 2); }
+    template <int I>
+    __device__ __forceinline__ uint32_t step(uint32_t e, uint32_t x) const {
+        uint32_t t = __byte_perm(e, x, 0x1100 | ((4 + I) << 4));
+        return tbl_u8(((lane & 15u) << 2) + t + (t & 0xFFE0u));
+    }
+};
+
+template <> struct Walker<64> {
+    static constexpr int kChains = 64;
+    uint32_t lane;
+    __device__ uint32_t enc(uint32_t s) const { return (s & 3u) | ((s >> 2) << 4); }
+    __device__ static uint32_t dec(uint32_t e) { return (e & 3u) | ((e >> 4) << 2); }
+    template <int I>
+    __device__ __forceinline__ uint32_t step(uint32_t e, uint32_t x) const {
+        uint32_t t = __byte_perm(e, x, 0x1100 | ((4 + I) << 4));
+        return tbl_u8(((lane & 7u) << 2) + t + (t & 0xFFF0u));
+    }
+};
+
 template <> struct Walker<0> {
     static constexpr int kChains = 0;
     uint32_t n;
@@ -87,7 +119,7 @@ template <> struct Walker<0> {
 
 // Shared-memory bytes a DFA of n states needs.
 __host__ __device__ inline int table_bytes_for(int n) {
-    return n <= 8 ? 256 * 256 : n <= 16 ? 256 * 512 : 256 * n;
+    return n <= 8 ? 256 * 256 : n <= 64 ? 256 * 512 : 256 * n;
 }
 
 // Fills ncols columns of a replicated table (N <= 16) at byte `off` of shared
@@ -144,6 +176,30 @@ __device__ inline void build_table(const uint8_t *__restrict__ src, int N) {
                 uint32_t s = q * 4 + b;
                 uint32_t t = s < (uint32_t)N ? src[c * N + s] : s;
                 word |= ((t & 3u) | ((t >> 2) << 6)) << (8 * b);
+            }
+            w32[w] = word;
+        }
+    } else if (N <= 32) {
+        // word address c<<7 | (s>>2)<<4 | replica: four states s = 4 q .. 4 q + 3 a word
+        for (int w = threadIdx.x; w < 256 * 512 / 4; w += blockDim.x) {
+            uint32_t c = w >> 7, q = (w >> 4) & 7u, word = 0;
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                uint32_t s = q * 4 + b;
+                uint32_t t = s < (uint32_t)N ? src[c * N + s] : s;
+                word |= ((t & 3u) | ((t >> 2) << 5)) << (8 * b);
+            }
+            w32[w] = word;
+        }
+    } else if (N <= 64) {
+        // word address c<<7 | (s>>2)<<3 | replica: four states s = 4 q .. 4 q + 3 a word
+        for (int w = threadIdx.x; w < 256 * 512 / 4; w += blockDim.x) {
+            uint32_t c = w >> 7, q = (w >> 3) & 15u, word = 0;
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                uint32_t s = q * 4 + b;
+                uint32_t t = s < (uint32_t)N ? src[c * N + s] : s;
+                word |= ((t & 3u) | ((t >> 2) << 4)) << (8 * b);
             }
             w32[w] = word;
         }
