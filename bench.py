@@ -94,6 +94,11 @@ def parse_args(argv=None):
                     help="offered request rates (requests/s) of the serve workload, swept upwards "
                          "until the served rate falls below 90%% of the offered one")
     ap.add_argument("--serve-seconds", type=float, default=2.0)
+    ap.add_argument("--serve-bulk-rates", type=str, default="256000,1000000,2000000,4000000,8000000,16000000",
+                    help="offered request rates of the bulk-submission sweep of the serve workload")
+    ap.add_argument("--serve-bulk-seconds", type=float, default=1.0)
+    ap.add_argument("--serve-bulk-tick-ms", type=float, default=1.0,
+                    help="period of the bulk client: it submits what arrived since its last tick")
     ap.add_argument("--serve-no-graphs", action="store_true",
                     help="launch the DFA batches directly instead of replaying CUDA graphs")
     ap.add_argument("--serve-plain", type=int, default=2000,
@@ -768,6 +773,76 @@ def poisson_run(srv, pool, rate: float, duration: float, seed: int):
     return st
 
 
+def bulk_pool(pool):
+    """The request pool as arrays per kind (the pool's order within each kind):
+    kinds of the pool in order, and per kind (engines, data, offsets)."""
+    kinds = np.array([("dfa", "nfa", "pnfa").index(p[0]) for p in pool], dtype=np.int64)
+    per = {}
+    for ki, kind in enumerate(("dfa", "nfa", "pnfa")):
+        sel = [p for p in pool if p[0] == kind]
+        off = np.zeros(len(sel) + 1, dtype=np.int64)
+        off[1:] = np.cumsum([len(p[2]) for p in sel])
+        data = np.frombuffer(b"".join(p[2] for p in sel), dtype=np.uint8)
+        per[kind] = (np.array([p[1] for p in sel], dtype=np.int32), data, off)
+    return kinds, per
+
+
+def poisson_bulk_run(srv, bpool, rate: float, duration: float, seed: int, tick: float = 1e-3):
+    """Open-loop Poisson load through the bulk form: the same arrival process and
+    request sequence as poisson_run, but the client wakes every `tick` seconds
+    and submits the requests that arrived since as one array submission per kind
+    (Server.submit_arrays; latency from each request's own arrival time, so the
+    wait for the tick counts)."""
+    kinds, per = bpool
+    P = len(kinds)
+    prefix = {ki: np.concatenate(([0], np.cumsum(kinds == ki))) for ki in range(3)}
+
+    def n_before(ki, k):   # requests of kind ki among the first k of the cyclic sequence
+        return (k // P) * int(prefix[ki][-1]) + int(prefix[ki][k % P])
+
+    rng = np.random.default_rng(seed + 17)
+    n = max(1, int(rate * duration))
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n))
+    arrivals = arrivals[arrivals <= duration]
+    srv.reset_stats()
+    subs = []
+    lag = 0.0
+    t0 = time.perf_counter()
+    k = 0
+    while k < len(arrivals):
+        now = time.perf_counter() - t0
+        j = int(np.searchsorted(arrivals, now, side="right"))
+        if j > k:
+            lag = max(lag, now - arrivals[k])
+            km = kinds[np.arange(k, j) % P]
+            for ki, kind in enumerate(("dfa", "nfa", "pnfa")):
+                eng, data, off = per[kind]
+                m = len(eng)
+                a, b = n_before(ki, k), n_before(ki, j)
+                if b == a:
+                    continue
+                t = t0 + arrivals[k:j][km == ki]
+                done = 0
+                while a < b:   # split where the kind's cyclic sequence wraps
+                    lo = a % m
+                    hi = min(m, lo + (b - a))
+                    subs.append(srv.submit_arrays(kind, eng[lo:hi], data, off[lo:hi + 1],
+                                                  t_arrival=t[done:done + hi - lo]))
+                    done += hi - lo
+                    a += hi - lo
+            k = j
+        if k < len(arrivals):
+            wake = max(now + tick, arrivals[k])
+            time.sleep(max(0.0, wake - (time.perf_counter() - t0)))
+    srv.wait(subs, timeout=600)
+    st = srv.stats()
+    st["offered_req_s"] = rate
+    st["offered_gchar_s"] = rate * float(sum(int(per[kd][2][-1]) for kd in per)) / P / 1e9
+    st["client_max_lag_ms"] = lag * 1e3
+    st["submissions"] = len(subs)
+    return st
+
+
 def plain_run(engines, pool, n_req: int):
     """Baseline: each request alone (host-to-device copy, one launch, device-to-
     host copy, synchronise), one after another."""
@@ -811,17 +886,15 @@ def serve_measure(args) -> dict:
                  use_graphs=not args.serve_no_graphs)
     # warm-up (graphs captured per size bucket, first launches)
     poisson_run(srv, pool, 20000, 0.5, args.seed)
-    rates = [float(r) for r in args.serve_rates.split(",")]
     clocks = ClockSampler(gpu_index_for(0))
     clocks.start()
-    runs = []
-    for k, r in enumerate(rates):
-        util = UtilSampler(gpu_index_for(0))
-        util.start()
-        runs.append(poisson_run(srv, pool, r, args.serve_seconds, args.seed + k))
-        runs[-1]["gpu_busy_frac"] = util.stop()
-        if runs[-1]["gchar_s"] < 0.9 * runs[-1]["offered_gchar_s"]:
-            break
+    runs = _serve_sweep(lambda r, k: poisson_run(srv, pool, r, args.serve_seconds, args.seed + k),
+                        [float(r) for r in args.serve_rates.split(",")])
+    bpool = bulk_pool(pool)
+    poisson_bulk_run(srv, bpool, 200000, 0.3, args.seed)   # warm-up of the bulk path
+    bulk_runs = _serve_sweep(lambda r, k: poisson_bulk_run(srv, bpool, r, args.serve_bulk_seconds,
+                                                           args.seed + k, args.serve_bulk_tick_ms * 1e-3),
+                             [float(r) for r in args.serve_bulk_rates.split(",")])
     clock_info = clocks.stop()
     srv.close()
     engines = (DFASet(dfas), [NFA(*x, unknown_rejects=True) for x in nfas], [PNFA(*x) for x in pnfas])
@@ -830,21 +903,8 @@ def serve_measure(args) -> dict:
     engines[0].close()
     for m in engines[1] + engines[2]:
         m.close()
-    sustained = [r for r in runs if r["gchar_s"] >= 0.9 * r["offered_gchar_s"]]
-    top = max(sustained, key=lambda r: r["offered_req_s"]) if sustained else runs[0]
-    last = runs[-1]
-    # the limiter at the last rate: the device (busy most of the span) or the host loop
-    gpu_busy = last.get("gpu_busy_frac") or 0.0
-    loop_busy = last.get("loop_busy_frac") or 0.0
-    lag_ms = last.get("client_max_lag_ms") or 0.0
-    shares = "request loop busy {:.0%}, device busy {:.0%} of the span, client behind the arrivals by up " \
-             "to {:.0f} ms".format(loop_busy, gpu_busy, lag_ms)
-    if last is top:
-        limiter = "not reached (served >= 90% of offered at the highest rate tried)"
-    elif loop_busy >= gpu_busy or loop_busy >= 0.8:
-        limiter = "host: the Python request loop (" + shares + ")"
-    else:
-        limiter = "GPU (" + shares + ")"
+    top, limiter = _serve_limiter(runs, "the Python request loop")
+    btop, blimiter = _serve_limiter(bulk_runs, "the request loop")
     keys = ("offered_req_s", "offered_gchar_s", "gchar_s", "p50_ms", "p99_ms", "requests", "batches",
             "by_kind", "client_max_lag_ms", "loop_busy_frac", "gpu_busy_frac")
     return {
@@ -859,8 +919,50 @@ def serve_measure(args) -> dict:
         "sustained_req_s": top["offered_req_s"], "p50_ms_at_sustained": top["p50_ms"],
         "p99_ms_at_sustained": top["p99_ms"], "limiter": limiter,
         "sweep": [{k: r.get(k) for k in keys} for r in runs],
+        "bulk": {
+            "form": "Server.submit_arrays: every tick_ms the client submits the requests that "
+                    "arrived since its last tick as one array submission per kind (latency from each "
+                    "request's arrival); same arrival process, request sequence and server",
+            "tick_ms": args.serve_bulk_tick_ms,
+            "value": btop["gchar_s"], "unit": "Gchar/s",
+            "sustained_req_s": btop["offered_req_s"], "p50_ms_at_sustained": btop["p50_ms"],
+            "p99_ms_at_sustained": btop["p99_ms"], "limiter": blimiter,
+            "sweep": [{k: r.get(k) for k in keys + ("submissions",)} for r in bulk_runs],
+        },
         "plain_per_request": plain, "clocks": clock_info,
     }
+
+
+def _serve_sweep(run, rates):
+    """run(rate, k) for each offered rate, upwards, until the served rate falls
+    below 90% of the offered one; each run carries the device's busy share."""
+    runs = []
+    for k, r in enumerate(rates):
+        util = UtilSampler(gpu_index_for(0))
+        util.start()
+        runs.append(run(r, k))
+        runs[-1]["gpu_busy_frac"] = util.stop()
+        if runs[-1]["gchar_s"] < 0.9 * runs[-1]["offered_gchar_s"]:
+            break
+    return runs
+
+
+def _serve_limiter(runs, loop_name):
+    """The highest sustained run, and what limited the next rate: the device (busy
+    most of the span) or the host (the request loop busy, the client behind)."""
+    sustained = [r for r in runs if r["gchar_s"] >= 0.9 * r["offered_gchar_s"]]
+    top = max(sustained, key=lambda r: r["offered_req_s"]) if sustained else runs[0]
+    last = runs[-1]
+    gpu_busy = last.get("gpu_busy_frac") or 0.0
+    loop_busy = last.get("loop_busy_frac") or 0.0
+    lag_ms = last.get("client_max_lag_ms") or 0.0
+    shares = "request loop busy {:.0%}, device busy {:.0%} of the span, client behind the arrivals by up " \
+             "to {:.0f} ms".format(loop_busy, gpu_busy, lag_ms)
+    if sustained and last is top:
+        return top, "not reached (served >= 90% of offered at the highest rate tried)"
+    if loop_busy >= gpu_busy or loop_busy >= 0.8:
+        return top, "host: " + loop_name + " (" + shares + ")"
+    return top, "GPU (" + shares + ")"
 
 
 def serve_arm(args):

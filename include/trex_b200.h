@@ -277,6 +277,18 @@ int trex_nfa_run(trex_nfa *nfa, const uint8_t *data, const int64_t *offsets, int
                  void *stream);
 /* Error word of the last run (bit 0: malformed offsets). Synchronises. */
 int trex_nfa_error(trex_nfa *nfa, int32_t *err_out);
+/* Many automata in one call (a serving batch): strings group_first[g] ..
+ * group_first[g+1] - 1 of offsets run on nfas[g], for n_groups <= 64 groups;
+ * group_first (HOST, n_groups + 1 entries, nondecreasing from 0) gives the
+ * groups. The groups run side by side: one launch per table layout, each CTA
+ * loading its own group's tables. DEVICE buffers as in trex_nfa_run, indexed
+ * by the string's position in offsets; scratch holds 8 * (n_groups + 1)
+ * bytes (work counters, then the error word at byte 8 * n_groups: bit 0
+ * malformed offsets), zeroed by the call. Asynchronous on stream. */
+int trex_nfa_run_multi(trex_nfa *const *nfas, int n_groups, const int64_t *group_first,
+                       const uint8_t *data, const int64_t *offsets, int64_t total_bytes,
+                       uint64_t *final_mask, uint8_t *accept, int32_t *accept_i32, void *scratch,
+                       void *stream);
 
 /* ---- probabilistic NFA (<= 64 states): s' = T[c] s ----------------------
  * Replaces the reference's nfa_prob_v5_tc_kernel / nfa_prob_v6_cuda_kernel
@@ -327,6 +339,25 @@ int trex_pnfa_run(trex_pnfa *pnfa, int mode, const uint8_t *data, const int64_t 
 /* Error word of the last run: bit 0 malformed offsets (those strings get no
  * result), bit 2 an internal wait ran out. Synchronises. */
 int trex_pnfa_error(trex_pnfa *pnfa, int32_t *err_out);
+/* Sizes every later launch of this handle for at most max_sms SMs (one CTA an
+ * SM for the tensor-core and shared-memory forms, 64 warps an SM for FP32);
+ * 0 restores all SMs. The kernels take strings from a work queue, so results
+ * do not change, only how much of the GPU a run may hold: a server uses it to
+ * leave SMs to other work beside long probabilistic chains. */
+int trex_pnfa_set_sm_limit(trex_pnfa *pnfa, int max_sms);
+
+/* ---- serving: strings from a staging buffer to their batch places ---------
+ * No reference counterpart (the reference serves one static batch per call,
+ * cuda/monoid_batch.cu:498-588). String i of the staging buffer,
+ * src[src_offsets[i] .. src_offsets[i+1]), is copied to dst[dst_begin[i] ..].
+ * DEVICE buffers: src (src_bytes), src_offsets[n+1] (nondecreasing, from 0,
+ * src_offsets[n] <= src_bytes), dst (dst_bytes), dst_begin[n], err (one
+ * int32 the call ORs into). A byte outside its string's source range or the
+ * destination is not written and sets bit 0 of *err. Asynchronous on stream;
+ * destination ranges that overlap leave those bytes unspecified. */
+int trex_scatter_strings(const uint8_t *src, int64_t src_bytes, const int64_t *src_offsets,
+                         int64_t n_strings, uint8_t *dst, int64_t dst_bytes,
+                         const int64_t *dst_begin, int32_t *err, void *stream);
 
 #ifdef __cplusplus
 }

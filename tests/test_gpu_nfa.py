@@ -102,3 +102,53 @@ def test_nfa_bridge_regexes(cuda):
         strs = ["".join(rng.choice(alpha, size=rng.integers(0, 30))) for _ in range(300)] + [""]
         assert eng.simulate_batch(strs) == [simulate_nfa(nm, s) for s in strs], pat
         eng.destroy()
+
+
+def test_nfa_run_multi_matches_oracle(cuda, oracle):
+    """trex_nfa_run_multi over automata of four table layouts (sigma 2, 20, 100 in
+    shared memory, 255 in global memory), an empty group and a group of one string:
+    every string's mask and accept flag equals its automaton's oracle result; a
+    string that ends past the data is flagged in the error word and the rest still
+    run."""
+    torch = cuda
+    from trex_b200.engine import NFA, nfa_run_multi
+    rng = np.random.default_rng(77)
+    sigmas = [20, 2, 100, 255, 20, 2, 20]
+    counts = [300, 50, 80, 40, 0, 1, 700]
+    autos = [random_bool_nfa(rng, n_states=64, sigma=s, density=0.05) for s in sigmas]
+    nfas = [NFA(*a, unknown_rejects=True) for a in autos]
+    lens = [rng.integers(0, 900, size=c) for c in counts]
+    datas = [[rng.integers(0, min(256, s + 2), size=int(L), dtype=np.uint8) for L in ls]
+             for s, ls in zip(sigmas, lens)]
+    flat = [x for ds in datas for x in ds]
+    off = np.zeros(len(flat) + 1, dtype=np.int64)
+    off[1:] = np.cumsum([len(x) for x in flat])
+    data = np.concatenate(flat)
+    gf = np.concatenate(([0], np.cumsum(counts)))
+    d = torch.from_numpy(data).cuda()
+    for bad in (False, True):
+        o = off.copy()
+        if bad:   # the last string ends past the data
+            o[-1] += 5
+        n = len(flat)
+        fm = torch.zeros(n, dtype=torch.int64, device="cuda")
+        ac = torch.full((n,), 7, dtype=torch.uint8, device="cuda")
+        scr = torch.zeros(8 * (len(nfas) + 1), dtype=torch.uint8, device="cuda")
+        nfa_run_multi(nfas, gf, d, torch.from_numpy(o).cuda(), final_mask=fm, accept=ac, scratch=scr)
+        fm = fm.cpu().numpy().view(np.uint64)
+        ac = ac.cpu().numpy()
+        err = int(scr[8 * len(nfas):8 * len(nfas) + 4].view(torch.int32).item())
+        assert bool(err & 1) == bad
+        for g, (a, ds) in enumerate(zip(autos, datas)):
+            if not ds:
+                continue
+            so = np.zeros(len(ds) + 1, dtype=np.int64)
+            so[1:] = np.cumsum([len(x) for x in ds])
+            rfm, rac = oracle.nfa_bool(*a, np.concatenate(ds), so, unknown_rejects=True)
+            sel = np.arange(gf[g], gf[g + 1])
+            if bad and g == len(autos) - 1:
+                assert ac[n - 1] == 7   # the malformed string gets no result
+                sel, rfm, rac = sel[:-1], rfm[:-1], rac[:-1]
+            assert np.array_equal(fm[sel], rfm) and np.array_equal(ac[sel], rac)
+    for m in nfas:
+        m.close()

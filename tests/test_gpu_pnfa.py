@@ -262,3 +262,30 @@ def test_bool_lane_kernel_small_alphabet(cuda, oracle, sigma, mode):
     assert np.array_equal(np.isfinite(ll), np.isfinite(want))
     fin = np.isfinite(want)
     assert np.allclose(ll[fin], want[fin], rtol=0, atol=1e-6)
+
+
+@pytest.mark.parametrize("sigma,mode", [(20, "bf16"), (20, "bf16cc"), (20, "fp32"), (20, "bool8"),
+                                        (2, "bf16"), (2, "bool")])
+def test_sm_limit_keeps_results(cuda, sigma, mode):
+    """A handle sized for one or a few SMs (serving beside other work) gives the
+    same results as one sized for the whole GPU: the kernels take strings from a
+    work queue, so only the number of CTAs changes."""
+    torch = cuda
+    from trex_b200.engine import PNFA
+    rng = np.random.default_rng(41)
+    T, start, acc = random_prob_nfa(rng, 64, sigma)
+    n = 700
+    lens = rng.integers(0, 600, size=n)
+    off = np.zeros(n + 1, dtype=np.int64)
+    off[1:] = np.cumsum(lens)
+    data = rng.integers(0, sigma, size=int(off[-1]), dtype=np.uint8)
+    d, o = torch.from_numpy(data).cuda(), torch.from_numpy(off).cuda()
+    m = PNFA(T, start, acc)
+    ll0, ac0 = (x.cpu().numpy() for x in m.run(d, o, mode))
+    for lim in (1, 3):
+        m.set_sm_limit(lim)
+        ll, ac = (x.cpu().numpy() for x in m.run(d, o, mode))
+        assert m.error_word() == 0
+        assert np.array_equal(ll, ll0) and np.array_equal(ac, ac0)
+    m.set_sm_limit(0)
+    m.close()

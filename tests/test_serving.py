@@ -8,7 +8,7 @@ import time
 import numpy as np
 import pytest
 
-from trex_b200.serving import Request, pack_batch, take_batch
+from trex_b200.serving import Bulk, Request, plan_batch, take_batch
 from trex_b200.workloads import random_bool_nfa, random_dfa, random_prob_nfa
 
 
@@ -26,15 +26,108 @@ def test_take_batch_respects_capacities():
     assert take_batch(collections.deque(), 4, 100) == []
 
 
-def test_pack_batch_orders_and_offsets():
+def _bulk(rid, kind, engines, lens, seed=0):
+    rng = np.random.default_rng(seed)
+    off = np.zeros(len(lens) + 1, dtype=np.int64)
+    off[1:] = np.cumsum(lens)
+    data = rng.integers(0, 256, size=int(off[-1]), dtype=np.uint8)
+    n = len(lens)
+    z = np.zeros(n)
+    return Bulk(rid, kind, np.asarray(engines, dtype=np.int32), data, off, z, z.copy(), z.copy(), z.copy())
+
+
+def _emulate(plan):
+    """The batch bytes a plan gives the kernels: host copies, then the device scatter."""
+    out = np.zeros(plan.total, dtype=np.uint8)
+    for off, src in plan.copies:
+        a = np.frombuffer(src, dtype=np.uint8) if isinstance(src, (bytes, bytearray)) else src
+        out[off:off + len(a)] = a
+    stage = np.zeros(plan.stage_bytes, dtype=np.uint8)
+    for off, a in plan.stage:
+        stage[off:off + len(a)] = a
+    for i in range(len(plan.stage_dst)):
+        a, b = int(plan.stage_off[i]), int(plan.stage_off[i + 1])
+        out[int(plan.stage_dst[i]):int(plan.stage_dst[i]) + b - a] = stage[a:b]
+    return out
+
+
+def _strings(plan, out):
+    """(kind, engine, bytes) of every output slot: DFA slots, then the others."""
+    res = {}
+    for k in range(plan.nd):
+        res[("dfa", k)] = (int(plan.ids[k]), out[plan.doff[k]:plan.doff[k + 1]].tobytes())
+    for kind, eng, first, cnt in plan.groups:
+        for k in range(first, first + cnt):
+            res[("rest", k)] = (kind, eng, out[plan.roff[k]:plan.roff[k + 1]].tobytes())
+    return res
+
+
+def test_plan_batch_orders_and_offsets():
     batch = [_req(0, "nfa", 1, 3), _req(1, "dfa", 2, 4), _req(2, "pnfa", 0, 2), _req(3, "nfa", 0, 0),
              _req(4, "dfa", 0, 5), _req(5, "nfa", 1, 1)]
-    order, blob, doff, ids, roff, groups = pack_batch(batch)
-    assert [r.rid for r in order] == [1, 4, 3, 0, 5, 2]
-    assert list(doff) == [0, 4, 9] and list(ids) == [2, 0]
-    assert list(roff) == [9, 9, 12, 13, 15]
-    assert groups == [("nfa", 0, 0, 1), ("nfa", 1, 1, 2), ("pnfa", 0, 3, 1)]
-    assert blob == b"".join(r.data for r in order)
+    plan = plan_batch(batch)
+    assert list(plan.doff) == [0, 4, 9] and list(plan.ids) == [2, 0]
+    assert list(plan.roff) == [9, 9, 12, 13, 15]
+    assert plan.groups == [("nfa", 0, 0, 1), ("nfa", 1, 1, 2), ("pnfa", 0, 3, 1)]
+    assert [(r.rid, j) for r, j in plan.reqs] == [(1, 0), (4, 1), (0, 1), (2, 3), (3, 0), (5, 2)]
+    assert len(plan.stage_dst) == 0 and plan.parts == []
+    out = _emulate(plan)
+    assert out.tobytes() == b"".join(r.data for r in (batch[1], batch[4], batch[3], batch[0], batch[5],
+                                                      batch[2]))
+
+
+def test_take_batch_splits_bulk_submissions():
+    b = _bulk(10, "nfa", [0] * 6, [10, 20, 30, 0, 40, 5])
+    q = collections.deque([_req(0, "dfa", 0, 15), b, _req(1, "dfa", 0, 5)])
+    t = take_batch(q, max_requests=10, max_bytes=80)
+    assert t[0].rid == 0 and t[1] == (b, 0, 4)          # 15 + 10 + 20 + 30 + 0 = 75; 40 more would not fit
+    assert b.next == 4 and q[0] is b
+    t = take_batch(q, max_requests=1, max_bytes=1000)
+    assert t == [(b, 4, 5)] and b.next == 5               # the request cap
+    t = take_batch(q, max_requests=10, max_bytes=1000)
+    assert t[0] == (b, 5, 6) and t[1].rid == 1 and not q  # the rest of b, then the next request
+    big = _bulk(20, "dfa", [0, 0], [50, 50])
+    q = collections.deque([_req(2, "dfa", 0, 60), big])
+    assert [e.rid for e in take_batch(q, 10, 100)] == [2] and q[0] is big and big.next == 0
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_plan_batch_with_bulk_places_every_string(seed):
+    rng = np.random.default_rng(seed)
+    batch = []
+    for i in range(12):
+        if rng.random() < 0.5:
+            kind = ("dfa", "nfa", "pnfa")[int(rng.integers(0, 3))]
+            batch.append(_req(i, kind, int(rng.integers(0, 3)), int(rng.integers(0, 40))))
+        else:
+            kind = ("dfa", "nfa", "pnfa")[int(rng.integers(0, 3))]
+            n = int(rng.integers(1, 30))
+            bk = _bulk(100 + i, kind, rng.integers(0, 3, size=n), rng.integers(0, 50, size=n), seed=i)
+            lo = int(rng.integers(0, n))
+            batch.append((bk, lo, int(rng.integers(lo + 1, n + 1))))
+    plan = plan_batch(batch)
+    out = _emulate(plan)
+    slots = _strings(plan, out)
+    # every request and every bulk string sits in its output slot, on its automaton
+    seen = set()
+    for r, j in plan.reqs:
+        key = ("dfa", j) if r.kind == "dfa" else ("rest", j)
+        got = slots[key]
+        assert got == ((r.engine, r.data) if r.kind == "dfa" else (r.kind, r.engine, r.data))
+        seen.add(key)
+    for bk, lo, hi, js in plan.parts:
+        for i, j in zip(range(lo, hi), js.tolist()):
+            data = bk.data[bk.offsets[i]:bk.offsets[i + 1]].tobytes()
+            key = ("dfa", j) if bk.kind == "dfa" else ("rest", j)
+            got = slots[key]
+            e = int(bk.engines[i])
+            assert got == ((e, data) if bk.kind == "dfa" else (bk.kind, e, data))
+            seen.add(key)
+    assert len(seen) == len(slots) == plan.nd + plan.nr
+    # groups tile the non-DFA part in (kind, engine) order
+    assert sum(c for *_, c in plan.groups) == plan.nr
+    keys = [(("dfa", "nfa", "pnfa").index(k), e) for k, e, _, _ in plan.groups]
+    assert keys == sorted(keys) and len(set(keys)) == len(keys)
 
 
 @pytest.mark.gpu
@@ -124,3 +217,126 @@ def test_server_from_file(cuda, oracle, tmp_path):
         else:
             _, ac = oracle.nfa_bool(*nfas[0], d, off, unknown_rejects=True)
             assert r[0] == bool(ac[0])
+
+
+@pytest.mark.gpu
+def test_scatter_strings_places_and_checks(cuda):
+    """trex_scatter_strings against a host copy. With bad entries (a place past
+    the destination, a place before it, a source size that ends inside the last
+    string) those bytes are not written, the error word is set, the other
+    strings still land, and nothing past dst_bytes changes."""
+    torch = cuda
+    from trex_b200 import _lib
+    L = _lib.load()
+    rng = np.random.default_rng(5)
+    for n, hi, bad in ((1, 5000, False), (300, 3000, False), (4000, 200, False), (300, 3000, True),
+                       (4000, 200, True)):
+        lens = rng.integers(0, hi, size=n)
+        lens[rng.random(n) < 0.1] = 0
+        lens[:2] = np.maximum(lens[:2], 1)
+        lens[-1] = max(lens[-1], 1)
+        soff = np.zeros(n + 1, dtype=np.int64)
+        soff[1:] = np.cumsum(lens)
+        total = int(soff[-1])
+        src = rng.integers(0, 256, size=total, dtype=np.uint8)
+        perm = rng.permutation(n)
+        doff = np.zeros(n + 1, dtype=np.int64)
+        doff[1:] = np.cumsum(lens[perm])
+        dst_begin = np.empty(n, dtype=np.int64)
+        dst_begin[perm] = doff[:-1]
+        slot = dst_begin.copy()
+        src_bytes = total
+        if bad:
+            dst_begin[0] = total + 8              # wholly past the destination
+            dst_begin[1] = -(int(lens[1]) + 3)    # wholly before it
+            src_bytes = total - 1                 # the source ends inside the last string
+        d_src = torch.from_numpy(src).cuda()
+        d_soff = torch.from_numpy(soff).cuda()
+        d_dst = torch.full((total + 64,), 7, dtype=torch.uint8, device="cuda")
+        d_db = torch.from_numpy(dst_begin).cuda()
+        d_err = torch.zeros(1, dtype=torch.int32, device="cuda")
+        _lib.check(L.trex_scatter_strings(d_src.data_ptr(), src_bytes, d_soff.data_ptr(), n,
+                                          d_dst.data_ptr(), total, d_db.data_ptr(), d_err.data_ptr(),
+                                          torch.cuda.current_stream().cuda_stream), "scatter")
+        got = d_dst.cpu().numpy()
+        assert (got[total:] == 7).all()
+        assert bool(int(d_err.item()) & 1) == bad
+        for i in range(n):
+            a = int(slot[i])
+            if bad and i < 2:
+                assert (got[a:a + lens[i]] == 7).all()
+            elif bad and i == n - 1:
+                assert (got[a:a + lens[i] - 1] == src[soff[i]:soff[i + 1] - 1]).all()
+            else:
+                assert (got[a:a + lens[i]] == src[soff[i]:soff[i + 1]]).all()
+
+
+@pytest.mark.gpu
+def test_bulk_submissions_match_batched_runs(cuda, oracle):
+    """Bulk submissions (arrays in, arrays out) of all three kinds, mixed with
+    single requests and split over several batches, give each request the result
+    of the engines run directly on the same strings, and the oracle's."""
+    torch = cuda
+    from trex_b200.engine import NFA, PNFA, DFASet
+    from trex_b200.serving import Server
+    rng = np.random.default_rng(9)
+    dfas = [random_dfa(n, np.arange(256), rng) for n in (16, 8, 12, 16)]
+    nfas = [random_bool_nfa(rng, 64, 20, 0.05) for _ in range(3)]
+    pnfas = [random_prob_nfa(rng, 64, 20) for _ in range(2)]
+    srv = Server(dfas, nfas, pnfas, hbm_budget=16 << 20, max_batch_requests=256)
+    n_eng = {"dfa": 4, "nfa": 3, "pnfa": 2}
+    subs = []
+    singles = []
+    for rep in range(3):
+        for kind in ("dfa", "nfa", "pnfa"):
+            n = int(rng.integers(200, 900))
+            lens = rng.integers(0, 4000, size=n)
+            lens[rng.random(n) < 0.05] = 0
+            off = np.zeros(n + 1, dtype=np.int64)
+            off[1:] = np.cumsum(lens)
+            hi = 256 if kind == "dfa" else 22
+            data = rng.integers(0, hi, size=int(off[-1]), dtype=np.uint8)
+            eng = rng.integers(0, n_eng[kind], size=n)
+            subs.append((kind, eng, data, off, srv.submit_arrays(kind, eng, data, off)))
+            for _ in range(20):
+                d = rng.integers(0, hi, size=int(rng.integers(0, 3000)), dtype=np.uint8).tobytes()
+                singles.append(srv.submit(kind, int(rng.integers(0, n_eng[kind])), d))
+    res = srv.wait([b for *_, b in subs] + singles, timeout=300)
+    st = srv.stats()
+    assert st["requests"] == sum(len(s[1]) for s in subs) + len(singles)
+    assert st["batches"] > len(subs)   # the 16 MiB budget splits the submissions
+    srv.close()
+    dset = DFASet(dfas)
+    nfa_h = [NFA(*x, unknown_rejects=True) for x in nfas]
+    pnfa_h = [PNFA(*x) for x in pnfas]
+    for (kind, eng, data, off, b), (r0, r1) in zip(subs, res):
+        assert b.done and b.error is None and (b.t_done > 0).all()
+        dd = torch.from_numpy(data if data.size else np.zeros(1, np.uint8)).cuda()
+        if kind == "dfa":
+            fs, ac, _ = dset.run(dd, torch.from_numpy(off).cuda(),
+                                 torch.from_numpy(eng.astype(np.int32)).cuda())
+            assert (r0 == ac.cpu().numpy().astype(bool)).all() and (r1 == fs.cpu().numpy()).all()
+            fs_o, ac_o = oracle.dfa_walk([x.tmap for x in dfas], [x.n_states for x in dfas],
+                                         [x.start for x in dfas], [x.accept for x in dfas], data, off,
+                                         eng.astype(np.int32))
+            assert (r1 == fs_o).all() and (r0 == ac_o.astype(bool)).all()
+            continue
+        for e in range(n_eng[kind]):
+            idx = np.flatnonzero(eng == e)
+            sub = np.concatenate([data[off[i]:off[i + 1]] for i in idx] + [np.zeros(0, np.uint8)])
+            so = np.zeros(len(idx) + 1, dtype=np.int64)
+            so[1:] = np.cumsum(off[idx + 1] - off[idx])
+            ds = torch.from_numpy(sub if sub.size else np.zeros(1, np.uint8)).cuda()
+            if kind == "nfa":
+                fm, ac = nfa_h[e].run(ds, torch.from_numpy(so).cuda())
+                assert (r0[idx] == ac.cpu().numpy().astype(bool)).all()
+                assert (r1[idx] == fm.cpu().numpy().view(np.uint64)).all()
+                fm_o, ac_o = oracle.nfa_bool(*nfas[e], sub, so, unknown_rejects=True)
+                assert (r1[idx] == np.asarray(fm_o).astype(np.uint64)).all()
+            else:
+                ll, ac = pnfa_h[e].run(ds, torch.from_numpy(so).cuda(), "bf16")
+                assert (r0[idx] == ll.cpu().numpy()).all()
+                assert (r1[idx] == ac.cpu().numpy().astype(bool)).all()
+    dset.close()
+    for m in nfa_h + pnfa_h:
+        m.close()

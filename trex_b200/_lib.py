@@ -65,12 +65,17 @@ SIGNATURES = {
     "trex_nfa_run": (ctypes.c_int, [c_vp, c_vp, c_vp, ctypes.c_int64, ctypes.c_int64, c_vp, c_vp,
                                     c_vp, c_vp]),
     "trex_nfa_error": (ctypes.c_int, [c_vp, c_i32p]),
+    "trex_nfa_run_multi": (ctypes.c_int, [ctypes.POINTER(c_vp), ctypes.c_int, c_i64p, c_vp, c_vp,
+                                          ctypes.c_int64, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "trex_pnfa_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, c_f32p, c_f32p, c_f32p,
                                         ctypes.POINTER(c_vp)]),
     "trex_pnfa_destroy": (None, [c_vp]),
     "trex_pnfa_run": (ctypes.c_int, [c_vp, ctypes.c_int, c_vp, c_vp, ctypes.c_int64, ctypes.c_int64,
                                      c_vp, c_vp, c_vp, c_vp]),
     "trex_pnfa_error": (ctypes.c_int, [c_vp, c_i32p]),
+    "trex_pnfa_set_sm_limit": (ctypes.c_int, [c_vp, ctypes.c_int]),
+    "trex_scatter_strings": (ctypes.c_int, [c_vp, ctypes.c_int64, c_vp, ctypes.c_int64, c_vp,
+                                            ctypes.c_int64, c_vp, c_vp, c_vp]),
     # handle API
     "trex_dfa_set_create": (ctypes.c_int, [ctypes.c_int, c_i32p, c_i32p, c_u8p, c_u8p,
                                            ctypes.POINTER(c_vp)]),

@@ -70,6 +70,48 @@ __device__ __forceinline__ uint64_t nfa_step(const uint64_t *tbl, uint64_t s, ui
     return acc;
 }
 
+// Threads take strings first .. first + n - 1 from the counter *head and walk them
+// in 16-byte windows; results go to index i of the output arrays.
+template <int B>
+__device__ __forceinline__ void nfa_walk_queue(const uint64_t *tbl, int sigma, uint64_t start_mask,
+                                               uint64_t accept_mask, const uint8_t *d, int64_t total_bytes,
+                                               const int64_t *offsets, int64_t first, int64_t n,
+                                               unsigned long long *head, uint32_t *err, uint64_t *final_mask,
+                                               uint8_t *accept, int32_t *accept_i32) {
+    while (true) {
+        const unsigned long long k = atomicAdd(head, 1ull);
+        if (k >= (unsigned long long)n) break;
+        const int64_t i = first + (int64_t)k;
+        const int64_t a = offsets[i], b = offsets[i + 1];
+        if (a < 0 || b < a || b > total_bytes) {
+            atomicOr(err, 1u);
+            continue;
+        }
+        uint64_t s = start_mask;
+        int64_t p = a;
+        while (p < b && (((uintptr_t)(d + p)) & 15u)) s = nfa_step<B>(tbl, s, __ldg(d + p++), sigma);
+        if (b - p >= 16) {
+            uint4 v = ld_stream16(d + p);
+            while (true) {
+                const bool more = b - p >= 32;
+                uint4 nv = make_uint4(0, 0, 0, 0);
+                if (more) nv = ld_stream16(d + p + 16);
+                const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                for (int k2 = 0; k2 < 16; ++k2) s = nfa_step<B>(tbl, s, (w[k2 >> 2] >> (8 * (k2 & 3))) & 0xffu, sigma);
+                p += 16;
+                if (!more) break;
+                v = nv;
+            }
+        }
+        while (p < b) s = nfa_step<B>(tbl, s, __ldg(d + p++), sigma);
+        const bool ok = (s & accept_mask) != 0;
+        if (final_mask) final_mask[i] = s;
+        if (accept) accept[i] = ok ? 1 : 0;
+        if (accept_i32) accept_i32[i] = ok ? 1 : 0;
+    }
+}
+
 template <int B, bool SMEM>
 __global__ void __launch_bounds__(kNfaThreads, 1) nfa_bitpar_kernel(NfaParams P) {
     extern __shared__ __align__(16) uint64_t s_tbl[];
@@ -80,38 +122,48 @@ __global__ void __launch_bounds__(kNfaThreads, 1) nfa_bitpar_kernel(NfaParams P)
         __syncthreads();
         tbl = s_tbl;
     }
-    while (true) {
-        const unsigned long long i = atomicAdd(P.head, 1ull);
-        if (i >= (unsigned long long)P.n) break;
-        const int64_t a = P.offsets[i], b = P.offsets[i + 1];
-        if (a < 0 || b < a || b > P.total_bytes) {
-            atomicOr(P.err, 1u);
-            continue;
-        }
-        uint64_t s = P.start_mask;
-        int64_t p = a;
-        const uint8_t *d = P.data;
-        while (p < b && (((uintptr_t)(d + p)) & 15u)) s = nfa_step<B>(tbl, s, __ldg(d + p++), P.sigma);
-        if (b - p >= 16) {
-            uint4 v = ld_stream16(d + p);
-            while (true) {
-                const bool more = b - p >= 32;
-                uint4 nv = make_uint4(0, 0, 0, 0);
-                if (more) nv = ld_stream16(d + p + 16);
-                const uint32_t w[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-                for (int k = 0; k < 16; ++k) s = nfa_step<B>(tbl, s, (w[k >> 2] >> (8 * (k & 3))) & 0xffu, P.sigma);
-                p += 16;
-                if (!more) break;
-                v = nv;
-            }
-        }
-        while (p < b) s = nfa_step<B>(tbl, s, __ldg(d + p++), P.sigma);
-        const bool ok = (s & P.accept_mask) != 0;
-        if (P.final_mask) P.final_mask[i] = s;
-        if (P.accept) P.accept[i] = ok ? 1 : 0;
-        if (P.accept_i32) P.accept_i32[i] = ok ? 1 : 0;
+    nfa_walk_queue<B>(tbl, P.sigma, P.start_mask, P.accept_mask, P.data, P.total_bytes, P.offsets, 0, P.n,
+                      P.head, P.err, P.final_mask, P.accept, P.accept_i32);
+}
+
+// Many automata in one launch (a serving batch: strings grouped by automaton). Group g
+// owns CTAs cta_first[g] .. cta_first[g+1] - 1 and strings first[g] .. first[g] +
+// count[g] - 1; each CTA loads its group's tables and its threads take the group's
+// strings, so the groups run side by side instead of one launch after another.
+constexpr int kNfaMultiMax = 64;
+struct NfaMultiParams {
+    const uint8_t *data;
+    int64_t total_bytes;
+    const int64_t *offsets;
+    uint64_t *final_mask;
+    uint8_t *accept;
+    int32_t *accept_i32;
+    unsigned long long *heads;   // one counter a group
+    uint32_t *err;
+    int n_groups;
+    const uint64_t *tables[kNfaMultiMax];
+    uint64_t start_mask[kNfaMultiMax], accept_mask[kNfaMultiMax];
+    int64_t first[kNfaMultiMax], count[kNfaMultiMax];
+    int32_t cta_first[kNfaMultiMax + 1];
+    int32_t sigma[kNfaMultiMax];
+};
+
+template <int B, bool SMEM>
+__global__ void __launch_bounds__(kNfaThreads, 1) nfa_bitpar_multi_kernel(const __grid_constant__ NfaMultiParams P) {
+    extern __shared__ __align__(16) uint64_t s_tbl[];
+    int g = 0;
+    while (g + 1 < P.n_groups && (int)blockIdx.x >= P.cta_first[g + 1]) ++g;
+    const int sigma = P.sigma[g];
+    const uint64_t *tbl = P.tables[g];
+    if (SMEM) {
+        const int words = (sigma + 1) * nfa_table_entries(B);
+        for (int i = threadIdx.x; i < words; i += blockDim.x) s_tbl[i] = tbl[i];
+        __syncthreads();
+        tbl = s_tbl;
     }
+    nfa_walk_queue<B>(tbl, sigma, P.start_mask[g], P.accept_mask[g], P.data, P.total_bytes, P.offsets,
+                      P.first[g], P.count[g], P.heads + g, P.err, P.final_mask, P.accept,
+                      P.accept_i32);
 }
 
 }  // namespace trex
@@ -208,6 +260,86 @@ int nfa_run(trex_nfa *nfa, const uint8_t *data, const int64_t *offsets, int64_t 
     return TREX_OK;
 }
 
+template <int B, bool SMEM>
+static cudaError_t nfa_multi_launch(const NfaMultiParams &P, int grid, size_t smem, cudaStream_t st) {
+    if (SMEM) {
+        const cudaError_t e = cudaFuncSetAttribute(nfa_bitpar_multi_kernel<B, SMEM>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    nfa_bitpar_multi_kernel<B, SMEM><<<grid, kNfaThreads, SMEM ? smem : 0, st>>>(P);
+    return cudaGetLastError();
+}
+
+int nfa_run_multi(trex_nfa *const *nfas, int n_groups, const int64_t *group_first, const uint8_t *data,
+                  const int64_t *offsets, int64_t total_bytes, uint64_t *final_mask, uint8_t *accept,
+                  int32_t *accept_i32, void *scratch, cudaStream_t st) {
+    if (n_groups < 1 || n_groups > kNfaMultiMax || !nfas || !group_first || !scratch) return TREX_ERR_ARG;
+    if (group_first[0] != 0) return TREX_ERR_ARG;
+    for (int g = 0; g < n_groups; ++g)
+        if (!nfas[g] || group_first[g + 1] < group_first[g]) return TREX_ERR_ARG;
+    const int64_t n = group_first[n_groups];
+    if (total_bytes < 0 || (n > 0 && !offsets) || (total_bytes > 0 && !data)) return TREX_ERR_ARG;
+    TREX_CUDA(cudaMemsetAsync(scratch, 0, 8 * (size_t)(n_groups + 1), st));
+    if (n == 0) return TREX_OK;
+    unsigned long long *heads = static_cast<unsigned long long *>(scratch);
+    uint32_t *err = reinterpret_cast<uint32_t *>(heads + n_groups);
+    // one launch per table layout (bits a lookup; tables in shared or global memory)
+    bool taken[kNfaMultiMax] = {};
+    int used_heads = 0;
+    for (int g0 = 0; g0 < n_groups; ++g0) {
+        if (taken[g0]) continue;
+        const int B = nfas[g0]->B;
+        const bool sm = nfas[g0]->smem;
+        NfaMultiParams P{};
+        P.data = data;
+        P.total_bytes = total_bytes;
+        P.offsets = offsets;
+        P.final_mask = final_mask;
+        P.accept = accept;
+        P.accept_i32 = accept_i32;
+        P.heads = heads + used_heads;
+        P.err = err;
+        int k = 0, ctas = 0;
+        size_t smem = 0;
+        for (int g = g0; g < n_groups; ++g) {
+            const trex_nfa *h = nfas[g];
+            if (taken[g] || h->B != B || h->smem != sm) continue;
+            taken[g] = true;
+            const int64_t cnt = group_first[g + 1] - group_first[g];
+            if (cnt == 0) continue;
+            P.tables[k] = h->d_tables;
+            P.start_mask[k] = h->start_mask;
+            P.accept_mask[k] = h->accept_mask;
+            P.sigma[k] = h->sigma;
+            P.first[k] = group_first[g];
+            P.count[k] = cnt;
+            P.cta_first[k] = ctas;
+            // a thread a string, as in a single-automaton run
+            ctas += (int)std::max<int64_t>(1, std::min<int64_t>(h->n_sms, (cnt + 31) / 32));
+            smem = std::max(smem, h->table_words * 8);
+            ++k;
+        }
+        if (k == 0) continue;
+        P.n_groups = k;
+        P.cta_first[k] = ctas;
+        used_heads += k;
+        cudaError_t e;
+        switch (B) {
+            case 8: e = sm ? nfa_multi_launch<8, true>(P, ctas, smem, st) : nfa_multi_launch<8, false>(P, ctas, 0, st); break;
+            case 7: e = nfa_multi_launch<7, true>(P, ctas, smem, st); break;
+            case 6: e = nfa_multi_launch<6, true>(P, ctas, smem, st); break;
+            case 5: e = nfa_multi_launch<5, true>(P, ctas, smem, st); break;
+            default: e = nfa_multi_launch<4, true>(P, ctas, smem, st); break;
+        }
+        if (e != cudaSuccess) {
+            set_last_error("trex_nfa_run_multi", e);
+            return TREX_ERR_CUDA;
+        }
+    }
+    return TREX_OK;
+}
+
 }  // namespace trex
 
 extern "C" {
@@ -282,6 +414,14 @@ int trex_nfa_run(trex_nfa *nfa, const uint8_t *data, const int64_t *offsets, int
                  void *stream) {
     return trex::nfa_run(nfa, data, offsets, n_strings, total_bytes, final_mask, accept, accept_i32,
                          static_cast<cudaStream_t>(stream), nullptr);
+}
+
+int trex_nfa_run_multi(trex_nfa *const *nfas, int n_groups, const int64_t *group_first,
+                       const uint8_t *data, const int64_t *offsets, int64_t total_bytes,
+                       uint64_t *final_mask, uint8_t *accept, int32_t *accept_i32, void *scratch,
+                       void *stream) {
+    return trex::nfa_run_multi(nfas, n_groups, group_first, data, offsets, total_bytes, final_mask, accept,
+                               accept_i32, scratch, static_cast<cudaStream_t>(stream));
 }
 
 int trex_nfa_error(trex_nfa *nfa, int32_t *err_out) {

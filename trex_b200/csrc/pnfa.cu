@@ -1797,6 +1797,7 @@ struct trex_pnfa {
     // unchecked steps stay far inside FP32), else every step
     int chain_resc[2] = {1, 1};
     int tc_resc = 1;   // the tensor-core kernel's rescale period for BF16 operands (same bound)
+    int sm_limit = 0;  // launches size their grids for at most this many SMs (0: all)
 };
 
 namespace trex {
@@ -1829,12 +1830,16 @@ static void pn_free(trex_pnfa *h) {
     cudaFree(h->d_misc);
 }
 
+static int64_t pn_sms(const trex_pnfa *h) {
+    return h->sm_limit > 0 ? std::min(h->sm_limit, h->n_sms) : h->n_sms;
+}
+
 static int pn_choose(const trex_pnfa *h, int64_t n, int *grid, int *p_sub) {
     int pmax = 0;
     for (int p = 32; p <= kPnMaxPSub; p += 32)
         if (pn_layout(p, h->sigma).total <= kPnSmemCap) pmax = p;
     if (pmax == 0) return TREX_ERR_SHAPE;
-    const int64_t sms = h->n_sms;
+    const int64_t sms = pn_sms(h);
     if (n <= sms * 64) {
         *grid = (int)std::max<int64_t>(1, (n + 63) / 64);
         *p_sub = 64;
@@ -2044,7 +2049,7 @@ int trex_pnfa_run(trex_pnfa *h, int mode, const uint8_t *data, const int64_t *of
             }
             // one CTA an SM (the tables fill its shared memory), four strings at a time each
             const int grid = (int)std::max<int64_t>(
-                1, std::min<int64_t>((n_strings + kChainGroups - 1) / kChainGroups, (int64_t)h->n_sms));
+                1, std::min<int64_t>((n_strings + kChainGroups - 1) / kChainGroups, pn_sms(h)));
             const bool fp16 = mode == TREX_PNFA_FP16_CC;
             profile_kernel_begin(st);
             if (fp16)
@@ -2057,7 +2062,7 @@ int trex_pnfa_run(trex_pnfa *h, int mode, const uint8_t *data, const int64_t *of
             TREX_CHECK_LAUNCH();
             return TREX_OK;
         }
-        const int64_t warps = std::min<int64_t>(n_strings, (int64_t)h->n_sms * 64);
+        const int64_t warps = std::min<int64_t>(n_strings, pn_sms(h) * 64);
         const int grid = (int)std::max<int64_t>(1, (warps + kPnPlainWarps - 1) / kPnPlainWarps);
         profile_kernel_begin(st);
         pnfa_plain_kernel<<<grid, kPnPlainWarps * 32, 0, st>>>(Q);
@@ -2091,7 +2096,7 @@ int trex_pnfa_run(trex_pnfa *h, int mode, const uint8_t *data, const int64_t *of
         // one CTA an SM (it owns the 512 TMEM columns), 128 strings in flight a tile
         const int64_t per_cta = (int64_t)Q.tiles * 128;
         const int grid = (int)std::max<int64_t>(
-            1, std::min<int64_t>((n_strings + per_cta - 1) / per_cta, (int64_t)h->n_sms));
+            1, std::min<int64_t>((n_strings + per_cta - 1) / per_cta, pn_sms(h)));
         profile_kernel_begin(st);
         if (k == 1) pnfa_lane_kernel<1><<<grid, kLnThreads, 0, st>>>(Q);
         else if (k == 2) pnfa_lane_kernel<2><<<grid, kLnThreads, 0, st>>>(Q);
@@ -2139,6 +2144,12 @@ int trex_pnfa_run(trex_pnfa *h, int mode, const uint8_t *data, const int64_t *of
     else pnfa_tc_kernel<0><<<grid, kPnThreads, smem, st>>>(P);
     profile_kernel_end(st);
     TREX_CHECK_LAUNCH();
+    return TREX_OK;
+}
+
+int trex_pnfa_set_sm_limit(trex_pnfa *pnfa, int max_sms) {
+    if (!pnfa || max_sms < 0) return TREX_ERR_ARG;
+    pnfa->sm_limit = max_sms;
     return TREX_OK;
 }
 

@@ -279,6 +279,25 @@ class NFA:
         return v.value
 
 
+def nfa_run_multi(nfas: Sequence["NFA"], group_first, data, offsets, *, final_mask, accept, scratch,
+                  stream=None) -> None:
+    """One call over strings grouped by automaton: strings group_first[g] ..
+    group_first[g+1] - 1 of offsets run on nfas[g] (at most 64 groups), side by
+    side. final_mask (int64) / accept (uint8) are indexed by the string's
+    position; scratch is a device buffer of at least 8 * (len(nfas) + 1) bytes
+    whose last word is the error word (bit 0: malformed offsets)."""
+    lib = _lib.load()
+    g = len(nfas)
+    gf = np.ascontiguousarray(group_first, dtype=np.int64)
+    if gf.size != g + 1:
+        raise ValueError("group_first needs len(nfas) + 1 entries")
+    hs = (ctypes.c_void_p * max(g, 1))(*[m._h.value for m in nfas])
+    rc = lib.trex_nfa_run_multi(hs, g, _lib.ptr(gf, ctypes.c_int64), _dptr(data), _dptr(offsets),
+                                data.numel(), _dptr(final_mask), _dptr(accept), None, _dptr(scratch),
+                                _stream_handle(stream))
+    _lib.check(rc, "trex_nfa_run_multi")
+
+
 PNFA_MODES = {"bf16": 0, "fp16": 1, "fp32": 2, "bool": 3, "bf16cc": 4, "fp16cc": 5, "bool8": 6}
 
 
@@ -297,7 +316,7 @@ class PNFA:
     "bool8": the same Boolean NFA with 0/1 int8 operands and int32 sums (tcgen05
     kind::i8, K = 32 an instruction: half the MMA instructions of "bool").
     "bf16cc" / "fp16cc": CUDA cores with the 16-bit tables in shared memory and an
-    FP32 state, a warp per string: the low-latency form for few strings.
+    FP32 state, four warps per string: the low-latency form for few strings.
     """
 
     def __init__(self, T, start_vec, accept_vec):
@@ -343,6 +362,10 @@ class PNFA:
                                     _stream_handle(stream))
         _lib.check(rc, "trex_pnfa_run")
         return loglik[:n], accept[:n]
+
+    def set_sm_limit(self, max_sms: int) -> None:
+        """Size later runs for at most max_sms SMs (0: all); results do not change."""
+        _lib.check(self.lib.trex_pnfa_set_sm_limit(self._h, int(max_sms)), "trex_pnfa_set_sm_limit")
 
     def error_word(self) -> int:
         v = ctypes.c_int32(0)
