@@ -53,7 +53,7 @@ import numpy as np
 from . import _lib
 
 KINDS = ("dfa", "nfa", "pnfa")
-kAuxStreams = 4   # extra streams of a fast-lane slot
+kAuxStreams = 8   # most extra streams of a slot (the probabilistic lane's groups run side by side)
 
 
 @dataclass(slots=True)
@@ -178,8 +178,10 @@ class BatchPlan:
     stage_bytes: int
     stage_off: np.ndarray   # int64 [ns + 1]
     stage_dst: np.ndarray   # int64 [ns]
-    reqs: list              # (Request, index into its kind's outputs)
-    parts: list             # (Bulk, lo, hi, indices into its kind's outputs)
+    reqs: list              # (Request, index into its kind's outputs), DFA ones first
+    parts: list             # (Bulk, lo, hi, indices into its kind's outputs), DFA ones first
+    n_dfa_reqs: int = 0
+    n_dfa_parts: int = 0
     dfa_out: bool = False   # the DFA results were handed out (before the rest)
 
     @property
@@ -211,11 +213,10 @@ def plan_batch(batch: Sequence) -> BatchPlan:
     np.cumsum(dlen, out=doff[1:])
     copies, out_reqs, out_parts = [], [], []
     pos = 0
-    if dreq:
-        blob = b"".join(r.data for r in dreq)
-        copies.append((0, blob))
-        pos = len(blob)
-        out_reqs += [(r, i) for i, r in enumerate(dreq)]
+    for i, r in enumerate(dreq):   # one copy each, straight into the batch buffer (no join)
+        copies.append((pos, r.data))
+        pos += len(r.data)
+    out_reqs += [(r, i) for i, r in enumerate(dreq)]
     k = len(dreq)
     for b, lo, hi in dparts:
         a0, a1 = int(b.offsets[lo]), int(b.offsets[hi])
@@ -252,12 +253,8 @@ def plan_batch(batch: Sequence) -> BatchPlan:
         for f, e in zip(firsts.tolist(), ends.tolist()):
             groups.append((KINDS[int(sk[f] >> 32)], int(sk[f] & 0xFFFFFFFF), f, e - f))
     if rreq:
-        if not rparts:   # the requests alone: their bytes in batch order, one copy
-            blob = b"".join(rreq[i].data for i in order.tolist())
-            copies.append((dfa_bytes, blob))
-        else:
-            copies += [(int(start[i]), r.data) for i, r in enumerate(rreq)]
-        out_reqs += [(r, int(inv[i])) for i, r in enumerate(rreq)]
+        copies += [(p, r.data) for p, r in zip(start[:len(rreq)].tolist(), rreq)]
+        out_reqs += [(r, j) for j, r in zip(inv[:len(rreq)].tolist(), rreq)]
     stage, soff, sdst = [], [], []
     spos = 0
     k = len(rreq)
@@ -273,7 +270,8 @@ def plan_batch(batch: Sequence) -> BatchPlan:
     stage_dst = np.concatenate(sdst) if sdst else np.zeros(0, dtype=i64)
     total = int(roff[-1])
     return BatchPlan(total, dfa_bytes, doff, np.concatenate(dids).astype(np.int32, copy=False), roff,
-                     groups, copies, bool(rreq), stage, spos, stage_off, stage_dst, out_reqs, out_parts)
+                     groups, copies, bool(rreq), stage, spos, stage_off, stage_dst, out_reqs, out_parts,
+                     len(dreq), len(dparts))
 
 
 def _bucket(x: int, lo: int) -> int:
@@ -286,7 +284,8 @@ def _bucket(x: int, lo: int) -> int:
 class _Slot:
     """Device and pinned host buffers of one in-flight batch."""
 
-    def __init__(self, torch, dev, lane: str, max_requests: int, max_bytes: int, dfa_scratch: int):
+    def __init__(self, torch, dev, lane: str, max_requests: int, max_bytes: int, dfa_scratch: int,
+                 n_aux: int = 1):
         self.lane = lane
         # the fast lane's streams take priority: when an SM frees, the block scheduler
         # starts their CTAs before the probabilistic lane's
@@ -327,12 +326,13 @@ class _Slot:
         self.h_err = torch.zeros(1, dtype=torch.int32, **pin)
         self.h_nerr = torch.zeros(1, dtype=torch.int32, **pin)
         self.h_data_np = self.h_data.numpy()
+        self.h_data_mv = memoryview(self.h_data_np)
         self.h_stage_np = self.h_stage.numpy()
         self.event = torch.cuda.Event()
-        # the automaton groups of a batch run side by side on these streams (each group's
-        # kernel is sized by its strings, so a few strings take one SM)
-        self.aux = [torch.cuda.Stream(device=dev, priority=prio) for _ in range(kAuxStreams)]
-        self.aux_ev = [torch.cuda.Event() for _ in range(kAuxStreams)]
+        # the non-DFA part of a batch runs on the first of these streams, beside the DFA
+        # part; the probabilistic groups of a batch run side by side on all of them
+        self.aux = [torch.cuda.Stream(device=dev, priority=prio) for _ in range(n_aux)]
+        self.aux_ev = [torch.cuda.Event() for _ in range(n_aux)]
         self.ready = torch.cuda.Event()
         self.rest_done = torch.cuda.Event()   # the non-DFA part's results are on the host
         self.dfa_done = torch.cuda.Event()    # the DFA part's results are on the host
@@ -346,7 +346,7 @@ class Server:
     def __init__(self, dfas=(), nfas=(), pnfas=(), *, hbm_budget: int = 1 << 30,
                  max_batch_requests: int = 1 << 14, pnfa_mode: str = "bf16", use_graphs: bool = True,
                  device: int = 0, pnfa_auto_threshold: int = 2048, precapture: bool = True,
-                 gc_freeze: bool = True, nfa_streams: int = kAuxStreams, pnfa_sms: int = 48):
+                 gc_freeze: bool = True, pnfa_streams: int = kAuxStreams, pnfa_sms: int = 96):
         import torch
         from .engine import NFA, PNFA, DFASet
         self.torch = torch
@@ -359,12 +359,12 @@ class Server:
         self.pnfas = [PNFA(T, s, a) for (T, s, a) in pnfas]
         # A probabilistic chain holds its SM for the whole string (milliseconds for long
         # ones), and the ragged DFA kernel needs whole SMs: the probabilistic lane's
-        # launches (up to nfa_streams at a time) together stay within pnfa_sms SMs, so the
+        # launches (up to pnfa_streams at a time) together stay within pnfa_sms SMs, so the
         # fast lane always finds free ones (0: no limit)
         self.pnfa_sms = pnfa_sms
         if pnfa_sms > 0:
             for m in self.pnfas:
-                m.set_sm_limit(max(1, pnfa_sms // max(1, min(kAuxStreams, nfa_streams))))
+                m.set_sm_limit(max(1, pnfa_sms // max(1, min(kAuxStreams, pnfa_streams))))
         # "auto": the CUDA-core kernel with BF16 tables in shared memory for groups of fewer
         # than pnfa_auto_threshold strings (its per-step latency is far lower than the
         # tensor-core kernel's), BF16 tcgen05 above
@@ -372,12 +372,13 @@ class Server:
             raise ValueError("pnfa_mode must be bf16, fp16, fp32, bf16cc, fp16cc or auto")
         self.pnfa_mode = pnfa_mode
         self.pnfa_auto_threshold = pnfa_auto_threshold
-        # The automaton groups of a batch run side by side on up to this many streams.
-        # The process keeps 4 x (1 + kAuxStreams) + 2 streams: CUDA maps streams onto
-        # CUDA_DEVICE_MAX_CONNECTIONS hardware queues (8 by default), and two streams on
-        # one queue serialise, so a serving process should raise it (to 32) before CUDA
-        # starts; otherwise a fast-lane kernel can wait behind a long probabilistic one.
-        self.nfa_streams = max(1, min(kAuxStreams, nfa_streams))
+        # The probabilistic groups of a batch run side by side on up to this many streams.
+        # The process keeps 2 x (1 + 1) + 2 x (1 + pnfa_streams) + 2 streams: CUDA maps
+        # streams onto CUDA_DEVICE_MAX_CONNECTIONS hardware queues (8 by default), and two
+        # streams on one queue serialise, so a serving process should raise it (to 32)
+        # before CUDA starts; otherwise a fast-lane kernel can wait behind a long
+        # probabilistic one.
+        self.pnfa_streams = max(1, min(kAuxStreams, pnfa_streams))
         self.use_graphs = use_graphs and self.dfa_set is not None
         # admission: the budget is split 3:1 between the two lanes, each with two slots;
         # a slot holds its bytes twice (the batch and the staging of bulk submissions);
@@ -399,7 +400,8 @@ class Server:
         self.max_pnfa_bytes, _ = slot_bytes(hbm_budget // 8, lambda b: 0)
         self.slots = [_Slot(torch, self.dev, "fast", max_batch_requests, self.max_bytes, scratch)
                       for _ in range(2)]
-        self.slots += [_Slot(torch, self.dev, "pnfa", max_batch_requests, self.max_pnfa_bytes, 0)
+        self.slots += [_Slot(torch, self.dev, "pnfa", max_batch_requests, self.max_pnfa_bytes, 0,
+                             n_aux=self.pnfa_streams)
                        for _ in range(2)]
         if self.dfa_set is not None:   # first run outside any graph capture (one-time setup)
             s0 = self.slots[0]
@@ -691,10 +693,12 @@ class Server:
         t_busy = time.perf_counter()
         plan = plan_batch(batch)
         nd, nr, total = plan.nd, plan.nr, plan.total
-        h = s.h_data_np
+        h, hv = s.h_data_np, s.h_data_mv
         for off, src in plan.copies:
-            a = np.frombuffer(src, dtype=np.uint8) if isinstance(src, (bytes, bytearray)) else src
-            h[off:off + len(a)] = a
+            if isinstance(src, bytes):
+                hv[off:off + len(src)] = src
+            else:
+                h[off:off + len(src)] = src
         s.h_doff[:nd + 1].copy_(torch.from_numpy(plan.doff))
         if nd:
             s.h_ids[:nd].copy_(torch.from_numpy(plan.ids))
@@ -743,7 +747,7 @@ class Server:
             # probabilistic NFA groups: one launch per automaton, side by side on the aux streams
             used = set()
             for gi, (kind, eng, first, cnt) in enumerate(g for g in plan.groups if g[0] == "pnfa"):
-                k = gi % self.nfa_streams
+                k = gi % self.pnfa_streams
                 ps = s.aux[k]
                 if k not in used:
                     if k:
@@ -780,8 +784,8 @@ class Server:
         t_busy = time.perf_counter()
         plan = s.batch
         nd, nr = plan.nd, plan.nr
-        reqs = [(r, j) for r, j in plan.reqs if (r.kind == "dfa") == dfa]
-        parts = [p for p in plan.parts if (p[0].kind == "dfa") == dfa]
+        reqs = plan.reqs[:plan.n_dfa_reqs] if dfa else plan.reqs[plan.n_dfa_reqs:]
+        parts = plan.parts[:plan.n_dfa_parts] if dfa else plan.parts[plan.n_dfa_parts:]
         err = None
         if dfa:
             fs = s.h_fs[:nd].numpy() if nd else None
@@ -795,15 +799,18 @@ class Server:
             if any(g[0] == "nfa" for g in plan.groups) and int(s.h_nerr[0]) != 0:
                 err = f"malformed NFA offsets (error word {int(s.h_nerr[0])})"
         now = time.perf_counter()
-        for r, j in reqs:
-            if r.kind == "dfa":
-                r.result = (bool(ac[j]), int(fs[j]))
-            elif r.kind == "nfa":
-                r.result = (bool(ac2[j]), int(mask[j]))
+        if reqs:   # plain Python values for the single requests (list indexing is cheap)
+            if dfa:
+                acl, fsl = ac.tolist(), fs.tolist()
+                for r, j in reqs:
+                    r.result = (acl[j] != 0, fsl[j])
             else:
-                r.result = (float(ll[j]), bool(ac2[j]))
+                acl, ml, lll = ac2.tolist(), mask.tolist(), ll.tolist()
+                for r, j in reqs:
+                    r.result = (acl[j] != 0, ml[j]) if r.kind == "nfa" else (lll[j], acl[j] != 0)
             if err:
-                r.error = err
+                for r, _ in reqs:
+                    r.error = err
         for b, lo, hi, j in parts:
             if b.kind == "dfa":
                 b.out0[lo:hi] = ac[j] != 0
