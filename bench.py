@@ -79,7 +79,7 @@ from trex_b200.sharding import max_over_ranks, rank_seed  # noqa: E402
 METRIC = "Gchar/s vs HBM roofline, plain vs batched/served; served p50/p99 ms (1 B200)"
 SUB_ALPHABET = b"ACGT"
 EXTRAS = ("cfg1_plain", "plain_per_pattern", "cfg3a_scan", "cfg3b_nfa", "cfg4_pnfa", "dfa_n32_64",
-          "kgram_sweep", "ref_shapes", "cfg5_served")
+          "kgram_sweep", "ref_shapes", "frontend", "cfg5_served")
 
 
 def parse_args(argv=None):
@@ -1463,12 +1463,70 @@ def run_extras(args, torch, dev, main_wl, names):
             extras["kgram_sweep"] = kgram_sweep(args, torch, dev)
         except Exception as e:
             extras["kgram_sweep"] = {"error": repr(e)[:400]}
+    if "frontend" in names:
+        try:
+            extras["frontend"] = frontend_measure(args)
+        except Exception as e:
+            extras["frontend"] = {"error": repr(e)[:400]}
     if "cfg5_served" in names:
         try:
             extras["cfg5_served"] = serve_measure(args)
         except Exception as e:
             extras["cfg5_served"] = {"error": repr(e)[:400]}
     return extras
+
+
+FRONTEND_PATTERNS = ("[a-z]+@[a-z]+\\.[a-z]+", "(if|else|while|for|return)", "((ab|cd)(ef|gh))+",
+                     "\\d+\\.\\d*", "(a|b)*abb")
+
+
+def frontend_measure(args) -> dict:
+    """The regex front end through the drop-in OptimizedEngine (README form,
+    config "auto"): engine setup per pattern (regex -> minimal DFA -> byte table ->
+    resident set on the device), the host preparation of a list of Python strings
+    (one byte buffer plus offsets: the character -> index map is folded into the
+    byte table, so no per-character mapping runs), and match_batch end to end,
+    per million characters; results checked against the CPU engine (config
+    "baseline") on every string."""
+    from trex_b200._batching import pack_strings
+    from trex_b200.optimized_engine import OptimizedEngine
+    rng = np.random.default_rng(args.seed + 29)
+    alphabet = np.frombuffer(b"abcdefghijklmnopqrstuvwxyz0123456789.@ ", dtype=np.uint8)
+    n, L = 1000, 1000   # 1 Mchar a batch
+    strings = [alphabet[rng.integers(0, len(alphabet), size=int(x))].tobytes().decode("latin-1")
+               for x in rng.integers(L // 2, 3 * L // 2, size=n)]
+    mchar = sum(len(x) for x in strings) / 1e6
+    prep = []
+    for _ in range(5):
+        t0 = time.perf_counter()
+        pack_strings(strings, offset_dtype=np.int64)
+        prep.append((time.perf_counter() - t0) * 1e3)
+    out = {"workload": "5 regexes; 1000 Python str of 500-1500 characters (1 Mchar) a batch",
+           "host_prep_ms_per_mchar": float(np.median(prep)) / mchar,
+           "reference_host_prep_ms_per_mchar": 88.0,
+           "patterns": []}
+    mism = 0
+    for p in FRONTEND_PATTERNS:
+        t0 = time.perf_counter()
+        eng = OptimizedEngine(p, config="auto")
+        setup_ms = (time.perf_counter() - t0) * 1e3
+        eng.match_batch(strings)   # warm
+        ts = []
+        for _ in range(5):
+            t0 = time.perf_counter()
+            res = eng.match_batch(strings)
+            ts.append((time.perf_counter() - t0) * 1e3)
+        cpu = OptimizedEngine(p, config="baseline")
+        want = cpu.match_batch(strings)
+        mism += sum(a != b for a, b in zip(res, want))
+        info = eng.config_info
+        out["patterns"].append({"pattern": p, "backend": info.get("scan_backend"),
+                                "dfa_states": info.get("dfa_states"),
+                                "setup_ms": setup_ms, "match_ms_per_mchar": float(np.median(ts)) / mchar,
+                                "accepted": int(sum(res))})
+        eng.close()
+    out["mismatches_vs_cpu_engine"] = int(mism)
+    return out
 
 
 def ref_shapes(args, torch, dev):
