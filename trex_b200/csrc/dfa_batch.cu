@@ -1497,7 +1497,9 @@ __device__ __forceinline__ uint32_t fix_item_body(const RaggedParams &P, const u
         if (s == ((uint32_t)(rec >> (16 + 8 * k)) & 0xffu)) return (uint32_t)(rec >> 8) & 0xffu;
         p = q;
     }
-    return 0xFFFFu;
+    // no meeting at a checkpoint (slowly merging or non-synchronising automata): walk on to
+    // the item's end, whose state is then known either way
+    return lane_walk(P, tm, N, p, b1, s);
 }
 // Not inlined into the fix-up kernel's loop (keeps its registers); the re-walk
 // path inlines the body instead.
@@ -1596,10 +1598,11 @@ __global__ void __launch_bounds__(kComposeThreads) compose_chain_kernel(RaggedPa
 
 // Step 2 of 3, one thread per fix-up task: walks item j from its true entry state
 // until it meets the recorded chain at a checkpoint (fix_item: about one window for
-// synchronising automata). Met: the chained result stands. A last item walked to
-// its end: its end state is the string's final state. Otherwise (automata that do
-// not synchronise, such as permutations) the string is marked to be walked again
-// from item j.
+// synchronising automata), else to the item's end. Met, or the same end state: the
+// chained result stands. A last item: its end state is the string's final state.
+// Otherwise (the chains never met: automata that do not synchronise, such as
+// permutations) the next item's entry is now known and the string is marked to be
+// walked again from there.
 __global__ void __launch_bounds__(kComposeThreads) compose_fix_kernel(RaggedParams P) {
     if (*(volatile uint32_t *)P.err & kErrCapacity) return;
     const uint32_t n_fix = min(*(volatile uint32_t *)P.n_fix, P.fix_cap);
@@ -1623,8 +1626,9 @@ __global__ void __launch_bounds__(kComposeThreads) compose_fix_kernel(RaggedPara
         item_range(g, s0, len, j, &b0, &b1);
         const uint32_t f = e < N ? fix_item(P, P.tmaps + P.desc[d].tmap_off, N, b0, b1, e, rec) : 0xFFFFu;
         if (f == ((uint32_t)(rec >> 8) & 0xffu)) continue;
-        if (f != 0xFFFFu && j + 1 == k) write_result(P, ent.x, f, ent.w);
-        else mark_rewalk(P, x, mb, task.y);
+        if (f >= N) mark_rewalk(P, x, mb, task.y);
+        else if (j + 1 == k) write_result(P, ent.x, f, ent.w);
+        else mark_rewalk(P, x, mb, ((j + 1) << 8) | f);
     }
 }
 
