@@ -340,3 +340,44 @@ def test_bulk_submissions_match_batched_runs(cuda, oracle):
     dset.close()
     for m in nfa_h + pnfa_h:
         m.close()
+
+
+@pytest.mark.gpu
+def test_submit_arrays_arguments(cuda, oracle):
+    """The bulk form's checks and edge cases: an empty submission is done at once;
+    engine ids out of range, offsets that run backwards or past the data, and a
+    request larger than a slot are refused at submit; bytes data and a scalar
+    engine id are accepted and give the oracle's results."""
+    from trex_b200.serving import Server
+    rng = np.random.default_rng(12)
+    dfas = [random_dfa(16, np.arange(256), rng) for _ in range(2)]
+    nfas = [random_bool_nfa(rng, 64, 20, 0.05)]
+    srv = Server(dfas, nfas, [], hbm_budget=8 << 20, max_batch_requests=64)
+    try:
+        b = srv.submit_arrays("dfa", [], b"", [0])
+        assert b.done and b.n == 0
+        (r0, r1), = srv.wait([b])
+        assert len(r0) == 0 and len(r1) == 0
+        data = rng.integers(0, 256, size=1000, dtype=np.uint8)
+        with pytest.raises(ValueError):
+            srv.submit_arrays("dfa", [0, 2], data, [0, 10, 20])          # no DFA 2
+        with pytest.raises(ValueError):
+            srv.submit_arrays("dfa", 0, data, [0, 30, 20])               # backwards
+        with pytest.raises(ValueError):
+            srv.submit_arrays("dfa", 0, data, [0, 10, 2000])             # past the data
+        with pytest.raises(ValueError):
+            srv.submit_arrays("pnfa", 0, data, [0, 10])                  # no probabilistic NFA
+        with pytest.raises(ValueError):
+            srv.submit_arrays("dfa", 0, np.zeros(srv.max_bytes + 1, np.uint8), [0, srv.max_bytes + 1])
+        off = np.array([0, 0, 17, 300, 1000], dtype=np.int64)
+        b = srv.submit_arrays("dfa", 1, data.tobytes(), off)             # bytes, one id for all
+        c = srv.submit_arrays("nfa", 0, (data % 22).astype(np.uint8), off)
+        (ac, fs), (ac2, fm) = srv.wait([b, c])
+        fs_o, ac_o = oracle.dfa_walk([dfas[1].tmap], [dfas[1].n_states], [dfas[1].start], [dfas[1].accept],
+                                     data, off)
+        assert np.array_equal(fs, fs_o) and np.array_equal(ac, ac_o.astype(bool))
+        fm_o, ac2_o = oracle.nfa_bool(*nfas[0], (data % 22).astype(np.uint8), off, unknown_rejects=True)
+        assert np.array_equal(fm, np.asarray(fm_o).astype(np.uint64)) and np.array_equal(ac2, ac2_o.astype(bool))
+        assert (b.latency_ms > 0).all() and (c.latency_ms > 0).all()
+    finally:
+        srv.close()
