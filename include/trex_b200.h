@@ -168,8 +168,9 @@ int64_t trex_dfa_batch_scratch_bytes(int64_t n_strings, int64_t total_bytes, int
  * pointers: data[total_bytes], offsets[n+1] (int64, non-decreasing),
  * dfa_id[n] (NULL = automaton 0), outputs (each may be NULL):
  * final_state[n], accept[n] (uint8 0/1), accept_i32[n] (int 0/1).
- * scratch: at least trex_dfa_batch_scratch_bytes bytes, or NULL to use a
- * buffer owned by the set. seg_len: characters per work item (0 = default;
+ * scratch: at least trex_dfa_batch_scratch_bytes bytes, 16-byte aligned (as
+ * cudaMalloc returns; else TREX_ERR_ARG), or NULL to use a buffer owned by the
+ * set. seg_len: characters per work item (0 = default;
  * longer strings are split and their segment maps composed). stream: a
  * cudaStream_t (NULL = legacy default stream). */
 int trex_dfa_batch_run(trex_dfa_set *set, const uint8_t *data, const int64_t *offsets,

@@ -44,7 +44,8 @@
 
 namespace trex {
 
-struct WorkItem {
+// 16-byte aligned: a record is stored and loaded as two 128-bit accesses
+struct alignas(16) WorkItem {
     int64_t p0;          // first byte walked (warm-up bytes included)
     int64_t end;         // one past the last byte of the item
     uint32_t str;
@@ -1804,8 +1805,8 @@ static int dfa_set_run_ex(trex_dfa_set *set, const uint8_t *data, const int64_t 
             set->own_scratch_bytes = L.total;
         }
         sc = static_cast<uint8_t *>(set->own_scratch);
-    } else if ((size_t)scratch_bytes < L.total) {
-        return TREX_ERR_ARG;
+    } else if ((size_t)scratch_bytes < L.total || ((uintptr_t)scratch & 15u) != 0) {
+        return TREX_ERR_ARG;   // too small, or not 16-byte aligned (records are 128-bit accesses)
     }
     uint32_t *q_count = reinterpret_cast<uint32_t *>(sc + L.q_count);
     uint32_t *q_base = reinterpret_cast<uint32_t *>(sc + L.q_base);
