@@ -1535,9 +1535,11 @@ __device__ __forceinline__ void mark_rewalk(const RaggedParams &P, uint32_t x, u
 // the fix-up meets the recorded chain, so the entry of item j + 1 is item j's
 // recorded end state; the string's final state is written on that assumption and
 // corrected by the two kernels below where it fails. A warp takes 32 strings of
-// the list and checks one string at a time across its lanes: lane j holds record
-// j (one coalesced load per 32 records) and compares its guess with lane j - 1's
-// end state; the first 32 records of eight strings are loaded together.
+// the list and lays their items out back to back (a prefix sum of the item
+// counts): a pass gives each lane one item, so most passes chain a dozen strings
+// at once (split strings have a few items each). Lane l compares its guess with
+// lane l - 1's end state (the previous item of the same string, or, for lane 0,
+// the last item of the previous pass).
 __global__ void __launch_bounds__(kComposeThreads) compose_chain_kernel(RaggedParams P) {
     if (*(volatile uint32_t *)P.err & kErrCapacity) return;   // the plan was refused
     const uint32_t FULL = 0xffffffffu;
@@ -1548,51 +1550,59 @@ __global__ void __launch_bounds__(kComposeThreads) compose_chain_kernel(RaggedPa
          base += nwarps * 32) {
         const bool mine = base + lane < n_split;
         const uint4 ent = mine ? P.split_list[base + lane] : make_uint4(0u, 0u, 0u, 0u);
-        uint32_t fin = 0xffu;   // lane s: the final state of string s of the warp
-#pragma unroll 1
-        for (int s0 = 0; s0 < 32; s0 += 8) {
-            uint64_t r[8];
-            uint32_t mbs[8], ks[8];
-#pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                mbs[u] = __shfl_sync(FULL, ent.y, s0 + u);
-                ks[u] = __shfl_sync(FULL, ent.z, s0 + u) & 0xffffu;
-                if (base + s0 + u >= n_split) ks[u] = 0;
-                if (ks[u] != 0 && (ks[u] < 2 || (int64_t)mbs[u] + (int64_t)ks[u] > P.max_items)) {
-                    if (lane == 0) atomicOr(P.err, kErrCapacity);   // not written by this plan
-                    ks[u] = 0;
-                }
-                r[u] = lane < ks[u] ? P.maps[mbs[u] + lane] : 0ull;
-            }
-#pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                const uint32_t k = ks[u], mb = mbs[u];
-                if (k == 0) continue;   // warp-uniform
-                const uint32_t x = (uint32_t)(base + s0 + u);
-                if (lane == 0) *reinterpret_cast<uint32_t *>(P.maps + mb) = 0xFFFFFFFFu;   // no re-walk yet
-                __syncwarp();
-                uint64_t rec = r[u];
-                uint32_t carry = 0;
-                for (uint32_t j0 = 0; j0 < k; j0 += 32) {
-                    if (j0 > 0) rec = j0 + lane < k ? P.maps[mb + j0 + lane] : 0ull;
-                    const uint32_t end = (uint32_t)(rec >> 8) & 0xffu;
-                    uint32_t prev = __shfl_up_sync(FULL, end, 1);
-                    if (lane == 0) prev = carry;
-                    const uint32_t j = j0 + lane;
-                    if (j > 0 && j < k && ((uint32_t)rec & 0xffu) != prev) {
-                        const uint32_t word = (j << 8) | prev;
-                        const uint32_t t = append_slot(P.n_fix);
-                        if (t < P.fix_cap) P.fix_list[t] = make_uint2(x, word);
-                        else mark_rewalk(P, x, mb, word);   // the list is full: walk again from here
-                    }
-                    carry = __shfl_sync(FULL, end, (int)min(31u, k - 1 - j0));
-                }
-                if (lane == (uint32_t)(s0 + u)) fin = carry;
-            }
+        uint32_t k = mine ? ent.z & 0xffffu : 0u;
+        if (k != 0 && (k < 2 || (int64_t)ent.y + (int64_t)k > P.max_items)) {
+            atomicOr(P.err, kErrCapacity);   // not written by this plan
+            k = 0;
         }
-        if (mine && (ent.z & 0xffffu) >= 2) {
-            if (fin < (ent.z >> 24) + 1u) write_result(P, ent.x, fin, ent.w);
-            else atomicOr(P.err, kErrCapacity);   // records not written by this plan
+        // inclusive prefix of the item counts: string s owns items [incl_s - k_s, incl_s)
+        uint32_t incl = k;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(FULL, incl, o);
+            if (lane >= (uint32_t)o) incl += v;
+        }
+        const uint32_t total = __shfl_sync(FULL, incl, 31);
+        uint32_t carry = 0;   // end state of the previous pass's last item
+        for (uint32_t t0 = 0; t0 < total; t0 += 32) {
+            const uint32_t t = t0 + lane;
+            // string of item t: the first s with incl_s > t (binary search over the lanes)
+            uint32_t lo = 0;
+#pragma unroll
+            for (uint32_t step = 16; step > 0; step >>= 1) {
+                const uint32_t v = __shfl_sync(FULL, incl, (int)(lo + step - 1));
+                if (v <= t) lo += step;
+            }
+            const uint32_t sidx = min(lo, 31u);
+            const uint32_t s_incl = __shfl_sync(FULL, incl, (int)sidx);
+            const uint32_t s_k = __shfl_sync(FULL, k, (int)sidx);
+            const uint32_t s_mb = __shfl_sync(FULL, ent.y, (int)sidx);
+            const uint32_t s_z = __shfl_sync(FULL, ent.z, (int)sidx);
+            const uint32_t s_str = __shfl_sync(FULL, ent.x, (int)sidx);
+            const uint32_t s_acc = __shfl_sync(FULL, ent.w, (int)sidx);
+            const bool live = t < total;
+            const uint32_t j = t - (s_incl - s_k);
+            const uint64_t rec = live ? P.maps[s_mb + j] : 0ull;
+            const uint32_t end = (uint32_t)(rec >> 8) & 0xffu;
+            uint32_t prev = __shfl_up_sync(FULL, end, 1);
+            if (lane == 0) prev = carry;
+            carry = __shfl_sync(FULL, end, 31);
+            // no re-walk yet: the low word of item 0's record (read above) becomes the mark,
+            // before any lane of the warp may lower it
+            if (live && j == 0) *reinterpret_cast<uint32_t *>(P.maps + s_mb) = 0xFFFFFFFFu;
+            __syncwarp();
+            if (!live) continue;
+            const uint32_t x = (uint32_t)(base + sidx);
+            if (j != 0 && ((uint32_t)rec & 0xffu) != prev) {
+                const uint32_t word = (j << 8) | prev;
+                const uint32_t f = append_slot(P.n_fix);
+                if (f < P.fix_cap) P.fix_list[f] = make_uint2(x, word);
+                else mark_rewalk(P, x, s_mb, word);   // the list is full: walk again from here
+            }
+            if (j + 1 == s_k) {
+                if (end < (s_z >> 24) + 1u) write_result(P, s_str, end, s_acc);
+                else atomicOr(P.err, kErrCapacity);   // records not written by this plan
+            }
         }
     }
 }
