@@ -82,6 +82,9 @@ enum : uint32_t {
 constexpr int kRaggedThreads = 1024;
 constexpr int kPlanThreads = 1024;
 constexpr int kMaxPlanCtas = 148;   // planning CTAs (one per SM on a B200)
+// byte maps of a set up to this size are copied into the fix-up kernel's shared memory
+// (two CTAs an SM); larger sets read them from global memory
+constexpr int64_t kFixSmemBytes = 96 * 1024;
 constexpr int kDefaultSegLen = 2048;
 constexpr int kLenClasses = 64;
 
@@ -645,6 +648,7 @@ struct RaggedParams {
     const uint32_t *n_split;     // their number
     uint2 *fix_list;             // fix-up tasks: split string, item << 8 | entry state
     uint32_t fix_cap;
+    uint32_t fix_tm_bytes;   // byte maps copied to shared memory by the fix-up kernel (0: read globally)
     uint32_t *n_fix;
     uint32_t *rw_list;           // split strings to walk again
     uint32_t *n_rw;
@@ -1460,6 +1464,9 @@ constexpr int kComposeThreads = 256;
 
 // Walks bytes [p, q) of the batch from state s through a byte map in global
 // memory (L1-cached): one lane, aligned 32-byte windows.
+// SHARED_TM: tm points into shared memory (a generic load; the read-only global load
+// below is for global memory only).
+template <bool SHARED_TM = false>
 __device__ __forceinline__ uint32_t lane_walk(const RaggedParams &P, const uint8_t *__restrict__ tm,
                                               uint32_t N, int64_t p, int64_t q, uint32_t s) {
     const uint8_t *lo = P.data + p, *hi = P.data + q;
@@ -1473,7 +1480,10 @@ __device__ __forceinline__ uint32_t lane_walk(const RaggedParams &P, const uint8
         const uint32_t x[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
 #pragma unroll
         for (int j = 0; j < 32; ++j)
-            if (w + j >= lo && w + j < hi) s = __ldg(tm + ((x[j >> 2] >> (8 * (j & 3))) & 0xffu) * N + s);
+            if (w + j >= lo && w + j < hi) {
+                const uint8_t *a = tm + ((x[j >> 2] >> (8 * (j & 3))) & 0xffu) * N + s;
+                s = SHARED_TM ? *a : __ldg(a);
+            }
     }
     return s;
 }
@@ -1484,6 +1494,7 @@ __device__ __forceinline__ uint32_t lane_walk(const RaggedParams &P, const uint8
 // bytes); from there the two chains are one, so the item ends in the recorded
 // end state. Returns the item's end state, or 0xFFFF when the chains had not
 // met by the last checkpoint (the caller then walks the item whole).
+template <bool SHARED_TM = false>
 __device__ __forceinline__ uint32_t fix_item_body(const RaggedParams &P, const uint8_t *__restrict__ tm,
                                                   uint32_t N, int64_t b0, int64_t b1, uint32_t s_in,
                                                   uint64_t rec) {
@@ -1493,20 +1504,21 @@ __device__ __forceinline__ uint32_t fix_item_body(const RaggedParams &P, const u
     uint32_t s = s_in;
     for (int k = 0; k < 4; ++k) {
         const int64_t q = min(a0 + ((int64_t)32 << k), b1);
-        s = lane_walk(P, tm, N, p, q, s);
+        s = lane_walk<SHARED_TM>(P, tm, N, p, q, s);
         if (q == b1) return s;
         if (s == ((uint32_t)(rec >> (16 + 8 * k)) & 0xffu)) return (uint32_t)(rec >> 8) & 0xffu;
         p = q;
     }
     // no meeting at a checkpoint (slowly merging or non-synchronising automata): walk on to
     // the item's end, whose state is then known either way
-    return lane_walk(P, tm, N, p, b1, s);
+    return lane_walk<SHARED_TM>(P, tm, N, p, b1, s);
 }
 // Not inlined into the fix-up kernel's loop (keeps its registers); the re-walk
 // path inlines the body instead.
+template <bool SHARED_TM>
 __device__ __noinline__ uint32_t fix_item(const RaggedParams &P, const uint8_t *__restrict__ tm, uint32_t N,
                                           int64_t b0, int64_t b1, uint32_t s_in, uint64_t rec) {
-    return fix_item_body(P, tm, N, b0, b1, s_in, rec);
+    return fix_item_body<SHARED_TM>(P, tm, N, b0, b1, s_in, rec);
 }
 
 // Index in a device list, with one atomic per group of lanes that append together.
@@ -1615,8 +1627,19 @@ __global__ void __launch_bounds__(kComposeThreads) compose_chain_kernel(RaggedPa
 // permutations) the next item's entry is now known and the string is marked to be
 // walked again from there.
 __global__ void __launch_bounds__(kComposeThreads) compose_fix_kernel(RaggedParams P) {
+    extern __shared__ __align__(16) uint8_t s_fix_tm[];
     if (*(volatile uint32_t *)P.err & kErrCapacity) return;
     const uint32_t n_fix = min(*(volatile uint32_t *)P.n_fix, P.fix_cap);
+    if (blockIdx.x * kComposeThreads >= n_fix) return;   // no task for this CTA
+    // small sets: every byte map in shared memory, so a fix-up's dependent lookups do not
+    // wait on L1 / L2 (the slowest tasks walk up to a few hundred bytes)
+    const bool shared_tm = P.fix_tm_bytes != 0;
+    if (shared_tm) {
+        const uint4 *src = reinterpret_cast<const uint4 *>(P.tmaps);
+        uint4 *dst = reinterpret_cast<uint4 *>(s_fix_tm);
+        for (uint32_t i = threadIdx.x; i < P.fix_tm_bytes / 16u; i += kComposeThreads) dst[i] = src[i];
+        __syncthreads();
+    }
     for (uint32_t t = blockIdx.x * kComposeThreads + threadIdx.x; t < n_fix; t += gridDim.x * kComposeThreads) {
         const uint2 task = P.fix_list[t];
         const uint32_t x = task.x, j = task.y >> 8, e = task.y & 0xffu;
@@ -1635,7 +1658,9 @@ __global__ void __launch_bounds__(kComposeThreads) compose_fix_kernel(RaggedPara
         const uint64_t rec = P.maps[mb + j];
         int64_t b0, b1;
         item_range(g, s0, len, j, &b0, &b1);
-        const uint32_t f = e < N ? fix_item(P, P.tmaps + P.desc[d].tmap_off, N, b0, b1, e, rec) : 0xFFFFu;
+        const uint32_t f = e >= N ? 0xFFFFu
+                           : shared_tm ? fix_item<true>(P, s_fix_tm + P.desc[d].tmap_off, N, b0, b1, e, rec)
+                                       : fix_item<false>(P, P.tmaps + P.desc[d].tmap_off, N, b0, b1, e, rec);
         if (f == ((uint32_t)(rec >> 8) & 0xffu)) continue;
         if (f >= N) mark_rewalk(P, x, mb, task.y);
         else if (j + 1 == k) write_result(P, ent.x, f, ent.w);
@@ -1753,6 +1778,7 @@ struct trex_dfa_set {
     std::vector<int64_t> tmap_off, accept_off;
     std::vector<uint8_t> h_accepts;      // host copy for empty-batch answers
     std::vector<uint8_t> h_tmaps;        // host copy: K-gram eligibility
+    int64_t tmap_bytes = 0;              // all byte maps (bytes)
     std::vector<trex::DfaDesc> h_desc;
     uint8_t *d_tmaps = nullptr;
     uint8_t *d_accepts = nullptr;
@@ -1880,6 +1906,7 @@ static int dfa_set_run_ex(trex_dfa_set *set, const uint8_t *data, const int64_t 
     P.n_split = cta_splits + plan_grid;
     P.fix_list = reinterpret_cast<uint2 *>(sc + L.fix_list);
     P.fix_cap = (uint32_t)std::min<int64_t>(L.fix_cap, 0xffffffffLL);
+    P.fix_tm_bytes = set->tmap_bytes <= kFixSmemBytes ? (uint32_t)set->tmap_bytes : 0u;
     P.n_fix = reinterpret_cast<uint32_t *>(sc + L.n_fix);
     P.rw_list = reinterpret_cast<uint32_t *>(sc + L.rw_list);
     P.n_rw = reinterpret_cast<uint32_t *>(sc + L.n_rw);
@@ -1908,7 +1935,7 @@ static int dfa_set_run_ex(trex_dfa_set *set, const uint8_t *data, const int64_t 
                                                   (int64_t)set->n_sms * 4),
                            kComposeThreads, 0, stream>>>(P);
     TREX_CHECK_LAUNCH();
-    compose_fix_kernel<<<set->n_sms * 2, kComposeThreads, 0, stream>>>(P);
+    compose_fix_kernel<<<set->n_sms * 2, kComposeThreads, P.fix_tm_bytes, stream>>>(P);
     TREX_CHECK_LAUNCH();
     compose_rewalk_kernel<<<set->n_sms * 2, kComposeThreads, 0, stream>>>(P);
     TREX_CHECK_LAUNCH();
@@ -1966,6 +1993,7 @@ int trex_dfa_set_create(int n_dfas, const int32_t *n_states, const int32_t *star
     }
     set->h_accepts.assign(accepts, accepts + asum);
     set->h_tmaps.assign(tmaps, tmaps + tsum);
+    set->tmap_bytes = tsum;
     set->h_desc = desc;
     set->n_sms = trex::sm_count();
     if (set->n_sms <= 0 || cudaGetDevice(&set->device) != cudaSuccess) {
@@ -2001,6 +2029,9 @@ int trex_dfa_set_create(int n_dfas, const int32_t *n_states, const int32_t *star
     if ((e = cudaFuncSetAttribute(trex::dfa_ragged_kernel,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   trex::kRaggedSmemBytes)) != cudaSuccess)
+        return fail(e, "cudaFuncSetAttribute");
+    if ((e = cudaFuncSetAttribute(trex::compose_fix_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)trex::kFixSmemBytes)) != cudaSuccess)
         return fail(e, "cudaFuncSetAttribute");
     *out = set;
     return TREX_OK;
