@@ -103,3 +103,23 @@ def test_kgram_mixed_set_default_segments(cuda, oracle):
     rfs, rac = oracle.dfa_walk([x.tmap for x in dfas], [x.n_states for x in dfas],
                                [x.start for x in dfas], [x.accept for x in dfas], data, off, ids)
     assert np.array_equal(fs0, rfs) and np.array_equal(fs, rfs) and np.array_equal(ac, rac)
+
+
+@pytest.mark.parametrize("k", [1, 2])
+def test_split_string_rewalk_marks_repeat(cuda, oracle, k):
+    """A 5-state automaton with a sink over two letters, cut into 256-byte items:
+    many items guess their entry wrong, some fix-ups never meet the chain, and the
+    fix-up list overflows, so one item can be marked for a re-walk twice, with the
+    chain's assumed entry and with a walked one. The walked entry must win whatever
+    the order of the marks; the order changes from run to run, so the case runs
+    several times."""
+    rng = np.random.default_rng(5 * 100 + 2 + 7)
+    d = _with_sink(random_dfa(4, AB, rng))
+    data, off = _batch(rng, AB)
+    ids = np.zeros(len(off) - 1, np.int32)
+    rfs, rac = oracle.dfa_walk([d.tmap], [d.n_states], [d.start], [d.accept], data, off)
+    for _ in range(6):
+        fs, ac, err, _ = _run(cuda, [d], data, off, ids, [k], seg_len=256)
+        assert err == 0
+        assert np.array_equal(fs, rfs), np.flatnonzero(fs != rfs)[:8]
+        assert np.array_equal(ac, rac)

@@ -158,12 +158,18 @@ __device__ __forceinline__ ItemGeom item_geom(int64_t len, int64_t s0, int n_sta
                                               uint32_t base_mis) {
     if (len <= 0 || n_states > kSplitDfaStates) return ItemGeom{1, len, len};
     int64_t seg = seg_len;
-    if ((len + seg - 1) / seg > kMaxItemsPerString)
+    // more than kMaxItemsPerString pieces (ceil(len / seg) > K exactly when len > K seg):
+    // longer pieces
+    if (len > kMaxItemsPerString * seg)
         seg = (((len + kMaxItemsPerString - 1) / kMaxItemsPerString) + 31) & ~(int64_t)31;
     const int64_t pad = (int64_t)((32u - ((base_mis + (uint32_t)s0) & 31u)) & 31u);
     const int64_t first = seg + pad;
     if (len <= first) return ItemGeom{1, seg, len};
-    return ItemGeom{(uint32_t)(1 + (len - first + seg - 1) / seg), seg, first};
+    // a 64-bit division is a long software routine on the GPU: 32 bits when they suffice
+    // (seg < 2^31 always)
+    const int64_t rest = len - first + seg - 1;
+    const int64_t q = rest < ((int64_t)1 << 32) ? (int64_t)((uint32_t)rest / (uint32_t)seg) : rest / seg;
+    return ItemGeom{(uint32_t)(1 + q), seg, first};
 }
 // Bytes [b0, b1) of item j of a string (s0, len).
 __device__ __forceinline__ void item_range(const ItemGeom &g, int64_t s0, int64_t len, uint32_t j,
@@ -1532,9 +1538,17 @@ __device__ __forceinline__ uint32_t append_slot(uint32_t *count) {
     return base + (uint32_t)__popc(m & ((1u << lane) - 1u));
 }
 
-// Split string x must be walked again from item j with entry state e (word j << 8 | e): the
-// earliest such item wins. The word lives in the low half of item 0's record, which nothing
-// reads once the records are chained; the first mark puts the string on the re-walk list.
+// Split string x must be walked again from item j with entry state e: word j << 9 | a << 8 |
+// e, where a = 1 when e is only the chain's assumption (item j - 1's recorded end) and a = 0
+// when e was walked (a fix-up of item j - 1 that never met the chain walked on to its end).
+// The smallest word wins: the earliest item, and for one item a walked entry over an
+// assumed one (two marks can name the same item with different entries: the assumed one
+// is then wrong, since item j - 1's fix-up found another end). The word lives in the low
+// half of item 0's record, which nothing reads once the records are chained; the first
+// mark puts the string on the re-walk list.
+__device__ __forceinline__ uint32_t rewalk_word(uint32_t j, uint32_t e, bool assumed) {
+    return (j << 9) | (assumed ? 256u : 0u) | e;
+}
 __device__ __forceinline__ void mark_rewalk(const RaggedParams &P, uint32_t x, uint32_t mb, uint32_t word) {
     if (atomicMin(reinterpret_cast<uint32_t *>(P.maps + mb), word) == 0xFFFFFFFFu)
         P.rw_list[append_slot(P.n_rw)] = x;
@@ -1606,10 +1620,9 @@ __global__ void __launch_bounds__(kComposeThreads) compose_chain_kernel(RaggedPa
             if (!live) continue;
             const uint32_t x = (uint32_t)(base + sidx);
             if (j != 0 && ((uint32_t)rec & 0xffu) != prev) {
-                const uint32_t word = (j << 8) | prev;
                 const uint32_t f = append_slot(P.n_fix);
-                if (f < P.fix_cap) P.fix_list[f] = make_uint2(x, word);
-                else mark_rewalk(P, x, s_mb, word);   // the list is full: walk again from here
+                if (f < P.fix_cap) P.fix_list[f] = make_uint2(x, (j << 8) | prev);
+                else mark_rewalk(P, x, s_mb, rewalk_word(j, prev, true));   // the list is full: walk again from here
             }
             if (j + 1 == s_k) {
                 if (end < (s_z >> 24) + 1u) write_result(P, s_str, end, s_acc);
@@ -1662,9 +1675,9 @@ __global__ void __launch_bounds__(kComposeThreads) compose_fix_kernel(RaggedPara
                            : shared_tm ? fix_item<true>(P, s_fix_tm + P.desc[d].tmap_off, N, b0, b1, e, rec)
                                        : fix_item<false>(P, P.tmaps + P.desc[d].tmap_off, N, b0, b1, e, rec);
         if (f == ((uint32_t)(rec >> 8) & 0xffu)) continue;
-        if (f >= N) mark_rewalk(P, x, mb, task.y);
+        if (f >= N) mark_rewalk(P, x, mb, rewalk_word(j, e, true));
         else if (j + 1 == k) write_result(P, ent.x, f, ent.w);
-        else mark_rewalk(P, x, mb, ((j + 1) << 8) | f);
+        else mark_rewalk(P, x, mb, rewalk_word(j + 1, f, false));
     }
 }
 
@@ -1714,7 +1727,7 @@ __global__ void __launch_bounds__(kComposeThreads) compose_rewalk_kernel(RaggedP
         const uint32_t mb = ent.y, k = ent.z & 0xffffu, N = (ent.z >> 24) + 1u;
         const int d = (int)((ent.z >> 16) & 0xffu);
         const uint32_t word = *reinterpret_cast<const volatile uint32_t *>(P.maps + mb);
-        const uint32_t jb = word >> 8, s_entry = word & 0xffu;
+        const uint32_t jb = word >> 9, s_entry = word & 0xffu;
         int64_t len = 0, s0 = 0;
         ItemGeom g{0, 0, 0};
         if (checked_dfa(P.offsets, P.dfa_id, (int64_t)ent.x, P.n_dfas, P.total_bytes, P.err, &len, &s0,
