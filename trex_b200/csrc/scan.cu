@@ -223,6 +223,8 @@ __device__ uint32_t walk_write(const W &w, const ScanParams &P, int64_t p, int64
     }
     // 64-byte blocks, the next block in flight, the L2 one 256-byte block ahead
     if (end - p >= 64) {
+        // data + p is 32-byte aligned here; so is out + p when out and data share it
+        const bool out32 = (((uintptr_t)(out + p)) & 31u) == 0;
         uint4 a0, a1, a2, a3;
         ld_stream32(data + p, a0, a1);
         ld_stream32(data + p + 32, a2, a3);
@@ -235,10 +237,19 @@ __device__ uint32_t walk_write(const W &w, const ScanParams &P, int64_t p, int64
                 if ((((uintptr_t)(data + p)) & 255u) == 0 && end - p >= 512)
                     prefetch_l2(data + p + 256);
             }
-            emit(p, walk16_states(w, e, a0));
-            emit(p + 16, walk16_states(w, e, a1));
-            emit(p + 32, walk16_states(w, e, a2));
-            emit(p + 48, walk16_states(w, e, a3));
+            if (out32) {   // two 16-state words a store: half the store instructions
+                const uint4 s0 = walk16_states(w, e, a0);
+                const uint4 s1 = walk16_states(w, e, a1);
+                st_stream32(out + p, s0, s1);
+                const uint4 s2 = walk16_states(w, e, a2);
+                const uint4 s3 = walk16_states(w, e, a3);
+                st_stream32(out + p + 32, s2, s3);
+            } else {
+                emit(p, walk16_states(w, e, a0));
+                emit(p + 16, walk16_states(w, e, a1));
+                emit(p + 32, walk16_states(w, e, a2));
+                emit(p + 48, walk16_states(w, e, a3));
+            }
             p += 64;
             if (!more) break;
             a0 = b0;
